@@ -1,0 +1,324 @@
+"""Benchmark: ms per 6-case homogenization solve to relthres 1e-5 at 256^3 on B200.
+
+One step = the forward pass a design iteration needs: load the physical density
+(rho^3 of a seeded trig-basis design, volume 0.3, E = 10, nu = 0.3), build the
+Galerkin hierarchy and the coarsest inverse, solve the six unit-strain cases from
+a zero start to relthres 1e-5, and reduce the 6x6 homogenized tensor C.
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl reference]
+
+N > 1 runs under torchrun as independent replicas (one design per rank, no
+collective on the data path): value = total solves / max-over-ranks time.
+--impl reference times the FP64 CPU restatement of the same V-cycle (the oracle)
+on the host cores, a bounded sample per step (see cpu_sample()).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "ms per 6-case solve to relthres 1e-5 at 256^3"
+
+
+def metric_name(args):
+    if args.reso == 256 and args.tol == 1e-5:
+        return METRIC
+    return "ms per 6-case solve to relthres %g at %d^3" % (args.tol, args.reso)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=5)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="h3d", choices=["h3d", "reference"])
+    p.add_argument("--reso", type=int, default=256)
+    p.add_argument("--tol", type=float, default=1e-5)
+    p.add_argument("--vol", type=float, default=0.3)
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--pin-mode", type=int, default=0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self._stop = threading.Event()
+        self._t = None
+
+    def start(self):
+        def run():
+            while not self._stop.is_set():
+                try:
+                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                                         timeout=5).stdout.strip()
+                    if out:
+                        self.rows.append([c.strip() for c in out.split(",")])
+                except Exception:
+                    pass
+                self._stop.wait(0.2)
+        self._t = threading.Thread(target=run, daemon=True)
+        self._t.start()
+
+    def stop(self):
+        self._stop.set()
+        if self._t:
+            self._t.join(timeout=10)
+        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def dist_init(n):
+    if n <= 1 or "RANK" not in os.environ:
+        return 0, 1, None
+    import torch
+    import torch.distributed as dist
+    from datetime import timedelta
+    rank = int(os.environ["RANK"])
+    world = int(os.environ["WORLD_SIZE"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=timedelta(seconds=600), device_id=torch.device("cuda", local))
+    return rank, world, dist
+
+
+def max_over_ranks(dist, value):
+    if dist is None:
+        return value
+    import torch
+    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def launches_per_step(nl, vcycles):
+    """kernel launches of this library in one step (counted from the code paths)"""
+    per_cycle = 8 * 2 + (nl - 2) * 8 * 2 + (nl - 1) + (nl - 1) + (nl - 1) + 1 + 1
+    setup = 1 + 1 + 1 + (nl - 2) + 1 + 1          # density, L1, pin patch, deeper, assemble, inverse
+    solve = 1 + 3 + 2 + vcycles * per_cycle + 2    # rhs, mean removal, f norms, cycles, C
+    return setup + solve
+
+
+def make_density(args, rank):
+    import numpy as np
+    from homo3d_b200.density import synthetic_density
+    rho = synthetic_density(args.reso, seed=args.seed + rank, vol=args.vol)
+    return (rho.ravel() ** 3).astype(np.float32)
+
+
+def gpu_arm(args):
+    import numpy as np
+    import torch
+
+    import homo3d_b200 as H
+
+    rank, world, dist = dist_init(args.gpus)
+    dev = torch.cuda.current_device()
+    rho_h = make_density(args, rank)
+    hd = H.Homogenization(args.reso, pin_mode=args.pin_mode)
+    stream = torch.cuda.ExternalStream(hd.stream)
+    rho_d = torch.tensor(rho_h, device="cuda")
+    rho_pin = torch.from_numpy(rho_h).pin_memory()
+    rho_e2e = torch.empty_like(rho_d)
+
+    def step():
+        hd.update(rho_d)
+        hd.reset_solutions()
+        C = hd.elasticMatrix(args.tol)
+        return C
+
+    def step_e2e():
+        with torch.cuda.stream(stream):
+            rho_e2e.copy_(rho_pin, non_blocking=True)
+        hd.update(rho_e2e)
+        hd.reset_solutions()
+        return hd.elasticMatrix(args.tol)
+
+    for _ in range(args.warmup):
+        step()
+    st = hd.last_stats
+    if st["status"] != H.H3D_OK:
+        raise RuntimeError("solve did not converge: %r" % (st,))
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    cycles = []
+    for _ in range(args.steps):
+        C = step()
+        cycles.append(hd.last_stats["vcycles"])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    if dist is not None:
+        dist.barrier()
+    clk = clocks.stop()
+    t_ms = ev0.elapsed_time(ev1)
+    t_max = max_over_ranks(dist, t_ms)
+    ms_per_solve = t_max / (args.steps * world)
+
+    # end to end through the public API with host buffers
+    torch.cuda.synchronize()
+    e0 = time.perf_counter()
+    for _ in range(args.steps):
+        Ce = step_e2e()
+    torch.cuda.synchronize()
+    e2e_ms = (time.perf_counter() - e0) * 1e3
+    e2e_ms = max_over_ranks(dist, e2e_ms) / (args.steps * world)
+
+    # setup alone, and the dominant kernel (fine-level Gauss-Seidel sweep) by itself
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record(stream)
+    for _ in range(args.steps):
+        hd.update(rho_d)
+    s1.record(stream)
+    torch.cuda.synchronize()
+    setup_ms = s0.elapsed_time(s1) / args.steps
+    nsweep = 10
+    hd.grid.gs_relaxation(1.0, 2)
+    g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    g0.record(stream)
+    hd.grid.gs_relaxation(1.0, nsweep)
+    g1.record(stream)
+    torch.cuda.synchronize()
+    sweep_ms = g0.elapsed_time(g1) / nsweep
+    n3 = args.reso ** 3
+    alg_bytes_sweep = 220.0 * n3          # 3L(2 s_u + s_f) + s_rho per vertex, L = 6, FP32
+    flops_sweep = 2.0 * (576 + 234 * 6) * n3
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {"hbm_gbs": 6650.0}
+    achieved = alg_bytes_sweep / (sweep_ms * 1e-3) / 1e9
+    vc = int(round(sum(cycles) / len(cycles)))
+
+    result = None
+    if rank == 0:
+        result = {
+            "metric": metric_name(args), "value": round(ms_per_solve, 3), "unit": "ms", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_max / args.steps, 3),
+            "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded trig-basis density, reflect6, vol %.2f, rho^3 (SIMP p=3)" % args.vol,
+            "config": {"workload": "6-case periodic homogenization solve, %d^3, E=10 nu=0.3, relthres %g, "
+                                   "zero start, plain FP32 MG with FP16 coarse stencils" % (args.reso, args.tol),
+                       "reso": args.reso, "load_cases": 6, "relthres": args.tol, "levels": hd.nlevels,
+                       "pin_mode": args.pin_mode, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "inputs larger than L2 (fields %.1f GB)" % (3 * 18 * 4 * n3 / 1e9)},
+            "vcycles": vc, "vcycles_per_s": round(vc / (ms_per_solve * world) * 1e3, 2),
+            "setup_ms": round(setup_ms, 3),
+            "C00": float(C[0, 0]), "C_e2e_match": bool(np.abs(Ce - C).max() <= 1e-6 * np.abs(C).max()),
+            "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(rho_h.nbytes),
+                    "d2h_bytes_per_step": 36 * 8},
+            "gpu_launches": launches_per_step(hd.nlevels, vc) * args.steps,
+            "roofline": {"kernel": "k_fine_gs (8 colour launches = one sweep)", "bound": "hbm",
+                         "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
+                         "frac": round(achieved / peaks.get("hbm_gbs"), 4), "traffic": None,
+                         "sweep_ms": round(sweep_ms, 4), "fp32_tflops": round(flops_sweep / sweep_ms / 1e9, 2),
+                         "peak_source": "measured" if "when" in peaks else "fallback"},
+            "clocks": clk,
+        }
+    hd.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    return result
+
+
+def cpu_sample(args, vcycles=None, cycles_timed=1):
+    """FP64 CPU restatement of the same solve, bounded: hierarchy setup and
+    `cycles_timed` V-cycles at reso/2 (6 cases), scaled by 8 to reso^3 (all the
+    work is proportional to the vertex count), times the V-cycle count (the GPU's
+    when given, else the oracle's own count at 64^3)."""
+    import numpy as np
+    from oracle import oracle as O
+    from homo3d_b200.density import synthetic_density
+
+    threads = os.cpu_count()
+    n = max(args.reso // 2, 16)
+    scale = (args.reso / n) ** 3
+    if vcycles is None:
+        m0 = O.MG((64, 64, 64))
+        m0.set_density(synthetic_density(64, seed=args.seed, vol=args.vol).ravel() ** 3)
+        m0.update_stencils()
+        m0.rhs()
+        vcycles, _ = m0.solve(args.tol, 200)
+        del m0
+    m = O.MG((n, n, n))
+    m.set_density(synthetic_density(n, seed=args.seed, vol=args.vol).ravel() ** 3)
+    t0 = time.perf_counter()
+    m.update_stencils()
+    m.rhs()
+    setup_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    for _ in range(cycles_timed):
+        m.vcycle(1.0)
+    cyc_s = (time.perf_counter() - t0) / cycles_timed
+    t0 = time.perf_counter()
+    m.elastic_matrix()
+    c_s = time.perf_counter() - t0
+    ms = (setup_s + vcycles * cyc_s + c_s) * scale * 1e3
+    return {"value": round(ms, 1), "unit": "ms", "cores": threads, "kind": "port",
+            "sample": "FP64 oracle, setup + %d V-cycle(s) + C at %d^3 scaled x%d to %d^3, x %d V-cycles"
+                      % (cycles_timed, n, int(scale), args.reso, vcycles),
+            "vcycles": int(vcycles), "ms_per_vcycle": round(cyc_s * scale * 1e3, 1),
+            "setup_ms": round(setup_s * scale * 1e3, 1)}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return None
+    os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+    samples = []
+    cb = None
+    for i in range(min(args.warmup, 1) + args.steps):
+        cb = cpu_sample(args, vcycles=cb["vcycles"] if cb else None)
+        if i >= min(args.warmup, 1):
+            samples.append(cb["value"])
+    value = statistics.median(samples)
+    cb["value"] = value
+    return {"metric": metric_name(args), "value": value, "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "impl": "reference",
+            "data": "synthetic: seeded trig-basis density, reflect6, vol %.2f, rho^3 (SIMP p=3)" % args.vol,
+            "config": {"workload": "6-case periodic homogenization solve, %d^3, E=10 nu=0.3, relthres %g, "
+                                   "zero start, plain FP32 MG with FP16 coarse stencils" % (args.reso, args.tol),
+                       "reso": args.reso, "load_cases": 6, "relthres": args.tol},
+            "cpu_baseline": cb,
+            "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        out = reference_arm(args)
+    else:
+        out = gpu_arm(args)
+        if out is not None and not args.no_cpu_baseline and out["n_gpus"] == 1:
+            out["cpu_baseline"] = cpu_sample(args, vcycles=out["vcycles"])
+    if out is not None:
+        print(json.dumps(out), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,344 @@
+"""homo3d_b200 -- B200-native periodic-homogenization solver (Python side).
+
+A thin ctypes binding of ``libh3d.so`` (the C ABI declared in include/h3d.h) that
+keeps the call surface of lavenklau/homo3d's hot path:
+
+  Homogenization  (homogenization/homogenization.h:17-61): update, elasticMatrix,
+                  Sensitivity
+  MG              (homogenization/MG.h:14-45): v_cycle, solveEquation,
+                  updateStencils, reset_displacement
+  Grid            (homogenization/grid.h:104-418): gs_relaxation, update_residual,
+                  restrict_residual, prolongate_correction, solveHostEquation,
+                  enforce_unit_macro_strain, field access
+  OCOptimizer     (optimization/OCOptimizer.h:16-19): update, filterSens
+  symmetrize      (AutoDiff/TensorExpression.h:425-445)
+
+Device buffers are passed as CUDA torch tensors (or raw integer device
+pointers).  All solver work runs in the CUDA library; importing this package on a
+machine without the built library raises ImportError.
+"""
+import ctypes
+import os
+
+import numpy as np
+
+__all__ = ["Homogenization", "MG", "Grid", "OCOptimizer", "H3DError", "symmetrize", "lib", "LIB_PATH",
+           "reference_resolution"]
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libh3d.so")
+
+H3D_OK, H3D_ERR_ARG, H3D_ERR_CUDA, H3D_ERR_NOMEM, H3D_NOT_CONVERGED, H3D_DIVERGED, H3D_ERR_STATE, \
+    H3D_ERR_SINGULAR = range(8)
+FIELD_U, FIELD_F, FIELD_R, FIELD_STENCIL, FIELD_CHI = range(5)
+COARSE_EXACT, COARSE_PROJECT = 0, 1
+PIN_IDENTITY, PIN_GALERKIN = 0, 1
+SYMMETRY = {"reflect3": 0, "reflect6": 1, "rotate3": 2}
+
+_STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "not converged",
+           5: "diverged", 6: "call order", 7: "singular coarsest matrix"}
+
+
+class H3DError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__("h3d error %d (%s): %s" % (code, _STATUS.get(code, "?"), msg))
+        self.code = code
+
+
+class Config(ctypes.Structure):
+    _fields_ = [("reso", ctypes.c_int * 3), ("youngs_modulus", ctypes.c_double),
+                ("poisson_ratio", ctypes.c_double), ("coarse_mode", ctypes.c_int), ("pin_mode", ctypes.c_int),
+                ("device", ctypes.c_int)]
+
+
+class SolveStats(ctypes.Structure):
+    _fields_ = [("vcycles", ctypes.c_int), ("status", ctypes.c_int), ("rel_res", ctypes.c_double * 6),
+                ("solve_ms", ctypes.c_double)]
+
+    def as_dict(self):
+        return {"vcycles": self.vcycles, "status": self.status, "rel_res": list(self.rel_res),
+                "solve_ms": self.solve_ms}
+
+
+_lib = None
+_vp, _ip, _dp, _fp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), \
+    ctypes.POINTER(ctypes.c_float)
+
+_SIGS = {
+    "h3d_create": [ctypes.POINTER(Config), ctypes.POINTER(ctypes.c_void_p)],
+    "h3d_destroy": [_vp],
+    "h3d_sync": [_vp],
+    "h3d_num_levels": [_vp],
+    "h3d_level_dims": [_vp, ctypes.c_int, _ip, _ip],
+    "h3d_element_matrix": [_vp, _dp],
+    "h3d_update_density": [_vp, _vp, ctypes.c_int],
+    "h3d_update_stencils": [_vp],
+    "h3d_restrict_stencil": [_vp, ctypes.c_int],
+    "h3d_factor_coarsest": [_vp],
+    "h3d_enforce_unit_macro_strain": [_vp],
+    "h3d_gs_relaxation": [_vp, ctypes.c_int, ctypes.c_float, ctypes.c_int],
+    "h3d_update_residual": [_vp, ctypes.c_int],
+    "h3d_restrict_residual": [_vp, ctypes.c_int],
+    "h3d_prolongate_correction": [_vp, ctypes.c_int],
+    "h3d_coarse_solve": [_vp],
+    "h3d_reset_displacement": [_vp, ctypes.c_int],
+    "h3d_field_norms": [_vp, ctypes.c_int, _dp],
+    "h3d_v_cycle": [_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int],
+    "h3d_solve": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(SolveStats)],
+    "h3d_elastic_matrix": [_vp, ctypes.c_double, _dp, ctypes.POINTER(SolveStats)],
+    "h3d_sensitivity": [_vp, _fp, _vp, ctypes.c_int],
+    "h3d_reset_solutions": [_vp],
+    "h3d_oc_update": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                      ctypes.c_float],
+    "h3d_oc_filter": [_vp, _vp, _vp, _ip, ctypes.c_int, ctypes.c_float, ctypes.c_int],
+    "h3d_symmetrize": [_vp, _vp, _ip, ctypes.c_int],
+    "h3d_get_field": [_vp, ctypes.c_int, ctypes.c_int, _fp],
+    "h3d_set_field": [_vp, ctypes.c_int, ctypes.c_int, _fp],
+}
+
+
+def lib():
+    """The loaded libh3d.so; raises ImportError when it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError("libh3d.so is not built (run __graft_entry__.build() or homo3d_b200/build.py)")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, args in _SIGS.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = ctypes.c_int
+        L.h3d_last_error.argtypes = [_vp]
+        L.h3d_last_error.restype = ctypes.c_char_p
+        L.h3d_stream.argtypes = [_vp]
+        L.h3d_stream.restype = ctypes.c_void_p
+        _lib = L
+    return _lib
+
+
+def _ptr(x):
+    if x is None:
+        return None
+    if isinstance(x, int):
+        return ctypes.c_void_p(x)
+    if hasattr(x, "data_ptr"):
+        if not x.is_cuda:
+            raise ValueError("expected a CUDA tensor")
+        if not x.is_contiguous():
+            raise ValueError("expected a contiguous tensor")
+        return ctypes.c_void_p(x.data_ptr())
+    raise TypeError("expected a CUDA tensor or a device pointer")
+
+
+def _i3(v):
+    return (ctypes.c_int * 3)(*[int(a) for a in v])
+
+
+def reference_resolution(reso):
+    """The resolution the reference rounds a requested size to (grid.cpp:21-66)."""
+    import math
+    out = []
+    for r in reso:
+        l2 = math.log2(r)
+        lcl = max(math.floor(l2) - 2, 0)
+        out.append(int(math.ceil(2 ** (l2 - lcl)) * 2 ** lcl))
+    return tuple(out)
+
+
+class _Handle:
+    def __init__(self, reso, E=10.0, nu=0.3, coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY, device=0):
+        L = lib()
+        if isinstance(reso, int):
+            reso = (reso, reso, reso)
+        cfg = Config((ctypes.c_int * 3)(*reso), float(E), float(nu), int(coarse_mode), int(pin_mode), int(device))
+        h = ctypes.c_void_p()
+        code = L.h3d_create(ctypes.byref(cfg), ctypes.byref(h))
+        if code != H3D_OK:
+            raise H3DError(code, "h3d_create failed for resolution %r" % (tuple(reso),))
+        self._h = h
+        self.nlevels = L.h3d_num_levels(h)
+        self.dims, self.ratios = [], []
+        for l in range(self.nlevels):
+            d, r = (ctypes.c_int * 3)(), (ctypes.c_int * 3)()
+            L.h3d_level_dims(h, l, d, r)
+            self.dims.append(tuple(d))
+            self.ratios.append(tuple(r))
+
+    def check(self, code):
+        if code != H3D_OK:
+            raise H3DError(code, lib().h3d_last_error(self._h).decode())
+        return code
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().h3d_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sync(self):
+        self.check(lib().h3d_sync(self._h))
+
+    @property
+    def stream(self):
+        return lib().h3d_stream(self._h)
+
+    def nv(self, level=0):
+        d = self.dims[level]
+        return d[0] * d[1] * d[2]
+
+
+class Grid:
+    """One multigrid level of a handle (grid.h:104-418); all six cases at once."""
+
+    def __init__(self, handle, level):
+        self._hd, self.level = handle, level
+        self.cellReso = handle.dims[level]
+        self.upCoarse = handle.ratios[level]
+        self.is_root = level == 0
+
+    def _c(self, code):
+        return self._hd.check(code)
+
+    def gs_relaxation(self, w_SOR=1.0, times=1):
+        self._c(lib().h3d_gs_relaxation(self._hd._h, self.level, w_SOR, times))
+
+    def update_residual(self):
+        self._c(lib().h3d_update_residual(self._hd._h, self.level))
+
+    def restrict_residual(self):
+        self._c(lib().h3d_restrict_residual(self._hd._h, self.level))
+
+    def prolongate_correction(self):
+        self._c(lib().h3d_prolongate_correction(self._hd._h, self.level))
+
+    def solveHostEquation(self):
+        self._c(lib().h3d_coarse_solve(self._hd._h))
+
+    def enforce_unit_macro_strain(self, istrain=None):
+        """Right-hand sides of all six unit strains (istrain is accepted for parity)."""
+        self._c(lib().h3d_enforce_unit_macro_strain(self._hd._h))
+
+    def reset_displacement(self):
+        self._c(lib().h3d_reset_displacement(self._hd._h, self.level))
+
+    def restrict_stencil(self):
+        self._c(lib().h3d_restrict_stencil(self._hd._h, self.level))
+
+    def assembleHostMatrix(self):
+        self._c(lib().h3d_factor_coarsest(self._hd._h))
+
+    def get(self, field):
+        """Host copy of a field: [6, nv, 3] float32 (stencil: [nv, 27, 9])."""
+        nv = self._hd.nv(self.level)
+        out = np.empty((nv, 27, 9) if field == FIELD_STENCIL else (6, nv, 3), dtype=np.float32)
+        self._c(lib().h3d_get_field(self._hd._h, self.level, field, out.ctypes.data_as(_fp)))
+        return out
+
+    def set(self, field, values):
+        a = np.ascontiguousarray(values, dtype=np.float32)
+        nv = self._hd.nv(self.level)
+        if a.size != nv * (243 if field == FIELD_STENCIL else 18):
+            raise ValueError("wrong field size")
+        self._c(lib().h3d_set_field(self._hd._h, self.level, field, a.ctypes.data_as(_fp)))
+
+
+class MG:
+    """Multigrid driver over a handle's levels (MG.h:14-45)."""
+
+    def __init__(self, handle):
+        self._hd = handle
+        self.grids = [Grid(handle, l) for l in range(handle.nlevels)]
+
+    def v_cycle(self, w_SOR=1.0, pre=1, post=1):
+        self._hd.check(lib().h3d_v_cycle(self._hd._h, w_SOR, pre, post))
+
+    def solveEquation(self, tol=1e-2, with_guess=True, case_mask=63):
+        st = SolveStats()
+        code = lib().h3d_solve(self._hd._h, case_mask, tol, int(with_guess), ctypes.byref(st))
+        if code not in (H3D_OK, H3D_NOT_CONVERGED):
+            self._hd.check(code)
+        return st.as_dict()
+
+    def updateStencils(self):
+        self._hd.check(lib().h3d_update_stencils(self._hd._h))
+
+    def reset_displacement(self):
+        self._hd.check(lib().h3d_reset_displacement(self._hd._h, -1))
+
+    def getRootGrid(self):
+        return self.grids[0]
+
+
+class Homogenization(_Handle):
+    """Homogenized elastic tensor of a periodic unit cell (homogenization.h:17-61)."""
+
+    def __init__(self, reso, E=10.0, nu=0.3, coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY, device=0):
+        super().__init__(reso, E, nu, coarse_mode, pin_mode, device)
+        self.mg = MG(self)
+        self.grid = self.mg.grids[0]
+        self.last_stats = None
+
+    def getGrid(self):
+        return self.grid
+
+    def element_matrix(self):
+        ke = np.zeros(576)
+        self.check(lib().h3d_element_matrix(self._h, ke.ctypes.data_as(_dp)))
+        return ke.reshape(24, 24)
+
+    def update(self, rho_phys, pitchT=-1):
+        """rho_phys: CUDA tensor of the physical (penalised) density, lexicographic."""
+        self.check(lib().h3d_update_density(self._h, _ptr(rho_phys), int(pitchT)))
+
+    def elasticMatrix(self, tol=1e-2):
+        C = np.zeros(36)
+        st = SolveStats()
+        code = lib().h3d_elastic_matrix(self._h, float(tol), C.ctypes.data_as(_dp), ctypes.byref(st))
+        self.last_stats = st.as_dict()
+        if code not in (H3D_OK, H3D_NOT_CONVERGED):
+            self.check(code)
+        return C.reshape(6, 6)
+
+    def Sensitivity(self, dC, sens, pitchT=-1):
+        d = np.ascontiguousarray(dC, dtype=np.float32).reshape(36)
+        self.check(lib().h3d_sensitivity(self._h, d.ctypes.data_as(_fp), _ptr(sens), int(pitchT)))
+
+    def reset_solutions(self):
+        self.check(lib().h3d_reset_solutions(self._h))
+
+    def field_norms(self, field):
+        out = np.zeros(6)
+        self.check(lib().h3d_field_norms(self._h, field, out.ctypes.data_as(_dp)))
+        return out
+
+
+class OCOptimizer:
+    """Optimality-criteria update and sensitivity filter (OCOptimizer.h:16-19)."""
+
+    def __init__(self, ne, min_density=1e-3, stepLimit=0.02, dampExponent=0.5, handle=None):
+        self.ne, self.minRho, self.step_limit, self.damp = int(ne), min_density, stepLimit, dampExponent
+        self._hd = handle
+
+    def _handle(self):
+        if self._hd is None:
+            raise ValueError("OCOptimizer needs the Homogenization handle whose stream it runs on")
+        return self._hd
+
+    def update(self, sens, rho, volratio):
+        hd = self._handle()
+        hd.check(lib().h3d_oc_update(hd._h, _ptr(sens), _ptr(rho), self.ne, volratio, self.minRho,
+                                     self.step_limit, self.damp))
+
+    def filterSens(self, sens, rho, pitchT, reso, radius=2.0, periodic=False):
+        hd = self._handle()
+        hd.check(lib().h3d_oc_filter(hd._h, _ptr(sens), _ptr(rho), _i3(reso), int(pitchT), radius, int(periodic)))
+
+
+def symmetrize(handle, field, reso, sym="reflect6"):
+    """Orbit-average a lexicographic CUDA field in place (TensorExpression.h:425-445)."""
+    handle.check(lib().h3d_symmetrize(handle._h, _ptr(field), _i3(reso), SYMMETRY[sym]))

@@ -1,0 +1,751 @@
+// h3d_api.cu -- host runtime and C ABI of libh3d.
+//
+// One handle = one periodic unit cell: its multigrid hierarchy, per-level
+// fields, coarse stencils, the coarsest-grid inverse, the stored solutions of
+// the six unit-strain cases, a CUDA stream, and a captured CUDA graph of one
+// V-cycle (all levels, then the level-0 residual norms and their copy to pinned
+// host memory).  The solve loop replays that graph and reads six doubles per
+// cycle; nothing else crosses to the host.
+//
+// Reference call surface mirrored (homo3d): Homogenization::{build, update,
+// elasticMatrix, Sensitivity} (homogenization.h:17-61), MG::{build, v_cycle,
+// solveEquation, updateStencils} (MG.h:14-45), Grid::{gs_relaxation,
+// update_residual, restrict_residual, prolongate_correction, solveHostEquation,
+// enforce_unit_macro_strain} (grid.h:104-418), OCOptimizer::{update, filterSens}
+// (OCOptimizer.h:16-19), Tensor::symmetrize (TensorExpression.h:425-445).
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "../../include/h3d.h"
+#include "h3d_internal.cuh"
+
+using namespace h3d;
+
+namespace {
+
+constexpr int MAXLV = 16;
+
+// element matrix for material matrix D by 2x2x2 Gauss quadrature on the unit
+// cube, symmetrised (templateMatrix.cpp:95-165)
+void ke_quadrature(const double D[6][6], double ke[576]) {
+    const double p = std::sqrt(1.0 / 3.0);
+    std::memset(ke, 0, sizeof(double) * 576);
+    for (int g = 0; g < 8; g++) {
+        const double gp[3] = {((2 * (g % 2) - 1) * p + 1) / 2, ((2 * (g / 2 % 2) - 1) * p + 1) / 2,
+                              ((2 * (g / 4) - 1) * p + 1) / 2};
+        double dn[8][3];
+        for (int k = 0; k < 8; k++) {
+            const int id[3] = {k % 2, k / 2 % 2, k / 4};
+            double r[3];
+            for (int a = 0; a < 3; a++) r[a] = id[a] ? gp[a] : 1 - gp[a];
+            for (int a = 0; a < 3; a++) dn[k][a] = (id[a] ? 1.0 : -1.0) * r[(a + 1) % 3] * r[(a + 2) % 3];
+        }
+        double B[6][24] = {};
+        for (int k = 0; k < 8; k++) {
+            for (int a = 0; a < 3; a++) B[a][3 * k + a] = dn[k][a];
+            B[3][3 * k + 1] = dn[k][2]; B[3][3 * k + 2] = dn[k][1];
+            B[4][3 * k + 0] = dn[k][2]; B[4][3 * k + 2] = dn[k][0];
+            B[5][3 * k + 0] = dn[k][1]; B[5][3 * k + 1] = dn[k][0];
+        }
+        for (int i = 0; i < 24; i++)
+            for (int j = 0; j < 24; j++) {
+                double s = 0;
+                for (int a = 0; a < 6; a++)
+                    for (int b = 0; b < 6; b++) s += B[a][i] * D[a][b] * B[b][j];
+                ke[i * 24 + j] += s;
+            }
+    }
+    for (int i = 0; i < 576; i++) ke[i] *= 0.125;
+    for (int i = 0; i < 24; i++)
+        for (int j = 0; j < i; j++) {
+            const double s = 0.5 * (ke[i * 24 + j] + ke[j * 24 + i]);
+            ke[i * 24 + j] = ke[j * 24 + i] = s;
+        }
+}
+
+void element_matrix(double E, double nu, double ke[576]) {
+    double D[6][6] = {};
+    const double s = E / ((1 + nu) * (1 - 2 * nu));
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) D[i][j] = s * (i == j ? 1 - nu : nu);
+    for (int i = 3; i < 6; i++) D[i][i] = s * (1 - 2 * nu) / 2;
+    ke_quadrature(D, ke);
+}
+
+double macro_disp_h(int a, int c, int m) {
+    const int p[3] = {a & 1, (a >> 1) & 1, a >> 2};
+    switch (c) {
+    case 0: return m == 0 ? p[0] : 0;
+    case 1: return m == 1 ? p[1] : 0;
+    case 2: return m == 2 ? p[2] : 0;
+    case 3: return m == 1 ? p[2] / 2.0 : m == 2 ? p[1] / 2.0 : 0;
+    case 4: return m == 0 ? p[2] / 2.0 : m == 2 ? p[0] / 2.0 : 0;
+    default: return m == 0 ? p[1] / 2.0 : m == 1 ? p[0] / 2.0 : 0;
+    }
+}
+
+// resolution correction and coarsening ratios (grid.cpp:21-151)
+int build_hierarchy(const int reso[3], int dims[MAXLV][3], int ratios[MAXLV][3]) {
+    int avail[3], n[3];
+    for (int a = 0; a < 3; a++) {
+        if (reso[a] < 2 || reso[a] > 1024) return -1;
+        const double l2 = std::log2((double)reso[a]);
+        const double lcl = std::fmax(std::floor(l2) - 2, 0.);
+        avail[a] = (int)std::ceil(std::pow(2, l2 - lcl));
+        n[a] = (int)(avail[a] * std::pow(2, lcl));
+    }
+    for (int a = 0; a < 3; a++) { dims[0][a] = n[a]; ratios[0][a] = 0; }
+    int nl = 1;
+    while (nl < MAXLV) {
+        int r[3], any = 0, all = 1;
+        for (int a = 0; a < 3; a++) {
+            const int c = dims[nl - 1][a];
+            if (c <= avail[a]) { r[a] = 0; all = 0; }
+            else if (c >= 256) { r[a] = 2; while (c / r[a] >= 256) r[a] *= 2; any = 1; }
+            else { r[a] = 2; any = 1; }
+        }
+        if (!any) break;
+        if (!all) return -2;
+        for (int a = 0; a < 3; a++) { ratios[nl][a] = r[a]; dims[nl][a] = dims[nl - 1][a] / r[a]; }
+        nl++;
+    }
+    return nl;
+}
+
+Planes make_planes(const int n[3]) {
+    Planes P;
+    for (int a = 0; a < 3; a++) P.n[a] = n[a];
+    long long b = 0;
+    for (int k = 0; k < 8; k++) {
+        for (int a = 0; a < 3; a++) {
+            const int par = ((k >> a) & 1) ^ 1;  // coordinate parity of colour k on axis a
+            P.pn[k][a] = (n[a] - par + 1) / 2;
+        }
+        P.base[k] = b;
+        b += (long long)P.pn[k][0] * P.pn[k][1] * P.pn[k][2];
+    }
+    P.nv = b;
+    P.even = (n[0] % 2 == 0 && n[1] % 2 == 0 && n[2] % 2 == 0);
+    return P;
+}
+
+}  // namespace
+
+struct h3d_handle {
+    h3d_config cfg;
+    int device = 0;
+    int nl = 0;
+    Level lv[MAXLV];
+    double ked[576];
+    KeMat ke;
+    RhsTab rhs;
+    std::vector<float> qhost;
+    int nsub = 0;
+    float *rho = nullptr;       // physical density on level 0
+    float *chi = nullptr;       // stored solutions [18][nv0]
+    float *q = nullptr;         // level-1 Galerkin sub-element matrices
+    double *d_ked = nullptr;
+    double *aug = nullptr;      // coarsest [K | K^-1]
+    int ndof = 0;
+    int *d_flag = nullptr;
+    double *partial = nullptr;  // reduction scratch
+    size_t partial_n = 0;
+    double *d_small = nullptr;  // 64 doubles: norms, C entries
+    double *h_small = nullptr;  // pinned mirror
+    float *tmp = nullptr;       // conversion / filter scratch
+    size_t tmp_n = 0;
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t vgraph = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool have_density = false, have_stencils = false;
+    std::string err;
+};
+
+namespace {
+
+int fail(h3d_handle *h, int code, const std::string &msg) {
+    if (h) h->err = msg;
+    return code;
+}
+
+#define CK(call)                                                                                    \
+    do {                                                                                            \
+        cudaError_t e_ = (call);                                                                    \
+        if (e_ != cudaSuccess)                                                                      \
+            return fail(h, e_ == cudaErrorMemoryAllocation ? H3D_ERR_NOMEM : H3D_ERR_CUDA,          \
+                        std::string(#call) + ": " + cudaGetErrorString(e_));                        \
+    } while (0)
+
+#define CKL()                                                                                       \
+    do {                                                                                            \
+        cudaError_t e_ = cudaGetLastError();                                                        \
+        if (e_ != cudaSuccess) return fail(h, H3D_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e_)); \
+    } while (0)
+
+int ensure_tmp(h3d_handle *h, size_t nfloat) {
+    if (h->tmp_n >= nfloat) return H3D_OK;
+    if (h->tmp) cudaFree(h->tmp);
+    h->tmp = nullptr;
+    h->tmp_n = 0;
+    CK(cudaMalloc(&h->tmp, nfloat * sizeof(float)));
+    h->tmp_n = nfloat;
+    return H3D_OK;
+}
+
+// Q_s = P_s^T Ke P_s for every fine sub-element s of a coarse element (ratio r)
+void build_q(const double ke[576], const int r[3], std::vector<float> &q, int &nsub) {
+    nsub = r[0] * r[1] * r[2];
+    q.assign((size_t)nsub * 576, 0.f);
+    for (int s = 0; s < nsub; s++) {
+        const int so[3] = {s % r[0], s / r[0] % r[1], s / (r[0] * r[1])};
+        double P[8][8];
+        for (int a = 0; a < 8; a++)
+            for (int b = 0; b < 8; b++) {
+                const int fo[3] = {so[0] + (a & 1), so[1] + ((a >> 1) & 1), so[2] + (a >> 2)};
+                const int co[3] = {(b & 1) * r[0], ((b >> 1) & 1) * r[1], (b >> 2) * r[2]};
+                double w = 1;
+                for (int t = 0; t < 3; t++) {
+                    const int o = std::abs(fo[t] - co[t]);
+                    w *= o >= r[t] ? 0.0 : (double)(r[t] - o) / r[t];
+                }
+                P[a][b] = w;
+            }
+        for (int A = 0; A < 8; A++)
+            for (int B = 0; B < 8; B++)
+                for (int i = 0; i < 3; i++)
+                    for (int j = 0; j < 3; j++) {
+                        double v = 0;
+                        for (int a = 0; a < 8; a++) {
+                            if (P[a][A] == 0) continue;
+                            for (int b = 0; b < 8; b++) v += P[a][A] * P[b][B] * ke[(3 * a + i) * 24 + 3 * b + j];
+                        }
+                        q[(size_t)s * 576 + (3 * A + i) * 24 + 3 * B + j] = (float)v;
+                    }
+    }
+}
+
+int destroy_graph(h3d_handle *h) {
+    if (h->vgraph) { cudaGraphExecDestroy(h->vgraph); h->vgraph = nullptr; }
+    return H3D_OK;
+}
+
+// the V-cycle of MG::v_cycle (MG.cpp:46-70) on the handle's stream; the level-0
+// residual of the down leg also yields the per-case norms
+int enqueue_vcycle(h3d_handle *h, float w) {
+    cudaStream_t s = h->stream;
+    const int nblk_r = (int)(((h->lv[0].P.nv / 8) + 127) / 128) * 8;
+    for (int l = 0; l < h->nl; l++) {
+        if (l > 0) {
+            if (l - 1 == 0) launch_fine_residual(h->lv[0], h->rho, h->ke, h->partial, nblk_r, s);
+            else launch_coarse_residual(h->lv[l - 1], s);
+            launch_restrict(h->lv[l - 1], h->lv[l], s);
+            cudaMemsetAsync(h->lv[l].u, 0, sizeof(float) * NF * h->lv[l].P.nv, s);
+        }
+        if (l == h->nl - 1) launch_coarse_apply(h->lv[l], h->aug, h->cfg.coarse_mode == H3D_COARSE_PROJECT, s);
+        else if (l == 0) launch_fine_gs(h->lv[0], h->rho, h->ke, w, s);
+        else launch_coarse_gs(h->lv[l], w, s);
+    }
+    for (int l = h->nl - 2; l >= 0; l--) {
+        launch_prolong(h->lv[l], h->lv[l + 1], l == 0, s);
+        if (l == 0) launch_fine_gs(h->lv[0], h->rho, h->ke, w, s);
+        else launch_coarse_gs(h->lv[l], w, s);
+    }
+    launch_norm_finish(h->partial, nblk_r, h->d_small, s);
+    cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, s);
+    return H3D_OK;
+}
+
+int build_graph(h3d_handle *h) {
+    if (h->vgraph) return H3D_OK;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
+    enqueue_vcycle(h, 1.f);
+    CK(cudaStreamEndCapture(h->stream, &g));
+    cudaError_t e = cudaGraphInstantiate(&h->vgraph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) { h->vgraph = nullptr; return fail(h, H3D_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e)); }
+    return H3D_OK;
+}
+
+int weighted_norms(h3d_handle *h, const Planes &P, const float *v, double out[6]) {
+    const int nb = norm_blocks(P);
+    launch_weighted_norm(P, v, h->partial, nb, h->stream);
+    launch_norm_finish(h->partial, nb, h->d_small, h->stream);
+    CKL();
+    CK(cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    for (int c = 0; c < NCASE; c++) out[c] = std::sqrt(h->h_small[c]);
+    return H3D_OK;
+}
+
+int check_level(h3d_handle *h, int level, bool coarse_only = false) {
+    if (!h) return H3D_ERR_ARG;
+    if (level < 0 || level >= h->nl || (coarse_only && level == 0))
+        return fail(h, H3D_ERR_ARG, "level out of range");
+    return H3D_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+static int create_impl(h3d_handle *h, const h3d_config *cfg) {
+    int dims[MAXLV][3], rat[MAXLV][3];
+    const int nl = build_hierarchy(cfg->reso, dims, rat);
+    if (nl < 2) return fail(h, H3D_ERR_ARG, "resolution gives fewer than two grid levels");
+    if (!(cfg->youngs_modulus > 0) || !(cfg->poisson_ratio > -1.0 && cfg->poisson_ratio < 0.5))
+        return fail(h, H3D_ERR_ARG, "invalid material");
+    if (cfg->coarse_mode != H3D_COARSE_EXACT && cfg->coarse_mode != H3D_COARSE_PROJECT)
+        return fail(h, H3D_ERR_ARG, "invalid coarse_mode");
+    if (cfg->pin_mode != H3D_PIN_IDENTITY && cfg->pin_mode != H3D_PIN_GALERKIN)
+        return fail(h, H3D_ERR_ARG, "invalid pin_mode");
+    h->cfg = *cfg;
+    h->device = cfg->device;
+    h->nl = nl;
+    CK(cudaSetDevice(h->device));
+    for (int l = 0; l < nl; l++) {
+        Level &L = h->lv[l];
+        L.P = make_planes(dims[l]);
+        for (int a = 0; a < 3; a++) L.ratio[a] = rat[l][a];
+        if (l < nl - 1 && !L.P.even) return fail(h, H3D_ERR_ARG, "every smoothed level needs even dimensions");
+        const size_t bytes = sizeof(float) * NF * (size_t)L.P.nv;
+        CK(cudaMalloc(&L.u, bytes));
+        CK(cudaMalloc(&L.f, bytes));
+        CK(cudaMalloc(&L.r, bytes));
+        CK(cudaMemset(L.u, 0, bytes));
+        CK(cudaMemset(L.f, 0, bytes));
+        CK(cudaMemset(L.r, 0, bytes));
+        if (l > 0) {
+            CK(cudaMalloc(&L.st, sizeof(uint4) * NCHUNK * (size_t)L.P.nv));
+            CK(cudaMemset(L.st, 0, sizeof(uint4) * NCHUNK * (size_t)L.P.nv));
+        }
+    }
+    const long long nv0 = h->lv[0].P.nv;
+    CK(cudaMalloc(&h->rho, sizeof(float) * nv0));
+    CK(cudaMalloc(&h->chi, sizeof(float) * NF * nv0));
+    CK(cudaMemset(h->chi, 0, sizeof(float) * NF * nv0));
+    // element matrix and derived tables
+    element_matrix(cfg->youngs_modulus, cfg->poisson_ratio, h->ked);
+    for (int i = 0; i < 576; i++) h->ke.k[i] = (float)h->ked[i];
+    for (int c = 0; c < NCASE; c++)
+        for (int a = 0; a < 24; a++) {
+            double s = 0;
+            for (int b = 0; b < 8; b++)
+                for (int m = 0; m < 3; m++) s += h->ked[a * 24 + 3 * b + m] * macro_disp_h(b, c, m);
+            h->rhs.g[c][a] = (float)s;
+        }
+    build_q(h->ked, h->lv[1].ratio, h->qhost, h->nsub);
+    CK(cudaMalloc(&h->q, sizeof(float) * h->qhost.size()));
+    CK(cudaMemcpy(h->q, h->qhost.data(), sizeof(float) * h->qhost.size(), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&h->d_ked, sizeof(double) * 576));
+    CK(cudaMemcpy(h->d_ked, h->ked, sizeof(double) * 576, cudaMemcpyHostToDevice));
+    const Level &C = h->lv[nl - 1];
+    h->ndof = (int)(3 * C.P.nv);
+    CK(cudaMalloc(&h->aug, sizeof(double) * (size_t)h->ndof * 2 * h->ndof));
+    CK(cudaMalloc(&h->d_flag, sizeof(int)));
+    // reduction scratch: residual partials, norms, C partials, means, OC
+    size_t pn = (size_t)((((nv0 / 8) + 127) / 128) * 8) * NCASE;
+    pn = std::max(pn, (size_t)4096 * 21);
+    pn = std::max(pn, (size_t)2048 * NF + NF);
+    pn = std::max(pn, (size_t)4 + 1184);
+    h->partial_n = pn;
+    CK(cudaMalloc(&h->partial, sizeof(double) * pn));
+    CK(cudaMalloc(&h->d_small, sizeof(double) * 64));
+    CK(cudaMallocHost(&h->h_small, sizeof(double) * 64));
+    CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    CK(cudaEventCreate(&h->ev0));
+    CK(cudaEventCreate(&h->ev1));
+    return H3D_OK;
+}
+
+int h3d_create(const h3d_config *cfg, h3d_handle **out) {
+    if (!cfg || !out) return H3D_ERR_ARG;
+    *out = nullptr;
+    h3d_handle *h = new (std::nothrow) h3d_handle();
+    if (!h) return H3D_ERR_NOMEM;
+    const int e = create_impl(h, cfg);
+    if (e != H3D_OK) {
+        h3d_destroy(h);
+        return e;
+    }
+    *out = h;
+    return H3D_OK;
+}
+
+int h3d_destroy(h3d_handle *h) {
+    if (!h) return H3D_ERR_ARG;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    destroy_graph(h);
+    for (int l = 0; l < h->nl; l++) {
+        cudaFree(h->lv[l].u); cudaFree(h->lv[l].f); cudaFree(h->lv[l].r); cudaFree(h->lv[l].st);
+    }
+    cudaFree(h->rho); cudaFree(h->chi); cudaFree(h->q); cudaFree(h->d_ked); cudaFree(h->aug);
+    cudaFree(h->d_flag); cudaFree(h->partial); cudaFree(h->d_small); cudaFree(h->tmp);
+    if (h->h_small) cudaFreeHost(h->h_small);
+    if (h->ev0) cudaEventDestroy(h->ev0);
+    if (h->ev1) cudaEventDestroy(h->ev1);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return H3D_OK;
+}
+
+const char *h3d_last_error(const h3d_handle *h) { return h ? h->err.c_str() : "null handle"; }
+
+int h3d_sync(h3d_handle *h) {
+    if (!h) return H3D_ERR_ARG;
+    CK(cudaStreamSynchronize(h->stream));
+    return H3D_OK;
+}
+
+void *h3d_stream(h3d_handle *h) { return h ? (void *)h->stream : nullptr; }
+
+int h3d_num_levels(const h3d_handle *h) { return h ? h->nl : -1; }
+
+int h3d_level_dims(const h3d_handle *h, int level, int dims[3], int ratio[3]) {
+    if (!h || level < 0 || level >= h->nl) return H3D_ERR_ARG;
+    for (int a = 0; a < 3; a++) {
+        if (dims) dims[a] = h->lv[level].P.n[a];
+        if (ratio) ratio[a] = h->lv[level].ratio[a];
+    }
+    return H3D_OK;
+}
+
+int h3d_element_matrix(const h3d_handle *h, double ke[576]) {
+    if (!h || !ke) return H3D_ERR_ARG;
+    std::memcpy(ke, h->ked, sizeof(double) * 576);
+    return H3D_OK;
+}
+
+int h3d_update_density(h3d_handle *h, const float *rho_dev, int pitchT) {
+    if (!h || !rho_dev) return H3D_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    const int *n = h->lv[0].P.n;
+    if (pitchT < 0) pitchT = n[0];
+    if (pitchT < n[0]) return fail(h, H3D_ERR_ARG, "pitchT smaller than the x resolution");
+    launch_density_in(n, rho_dev, pitchT, h->rho, h->stream);
+    CKL();
+    h->have_density = true;
+    return h3d_update_stencils(h);
+}
+
+int h3d_restrict_stencil(h3d_handle *h, int coarse_level) {
+    if (int e = check_level(h, coarse_level, true)) return e;
+    CK(cudaSetDevice(h->device));
+    if (coarse_level == 1) {
+        if (!h->have_density) return fail(h, H3D_ERR_STATE, "no density");
+        launch_galerkin_l1(h->lv[0], h->lv[1], h->rho, h->q, h->nsub, h->stream);
+        launch_dirichlet_patch(h->lv[0], h->lv[1], h->rho, h->d_ked, h->cfg.pin_mode == H3D_PIN_IDENTITY,
+                               h->stream);
+    } else {
+        launch_galerkin(h->lv[coarse_level - 1], h->lv[coarse_level], h->stream);
+    }
+    CKL();
+    h->have_stencils = false;
+    return H3D_OK;
+}
+
+int h3d_factor_coarsest(h3d_handle *h) {
+    if (!h) return H3D_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    cudaStream_t s = h->stream;
+    launch_coarse_assemble(h->lv[h->nl - 1], h->aug, s);
+    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), s));
+    launch_gauss_jordan(h->aug, h->ndof, h->d_flag, s);
+    CKL();
+    int flag = 0;
+    CK(cudaMemcpyAsync(&h->h_small[63], h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    std::memcpy(&flag, &h->h_small[63], sizeof(int));
+    if (flag) return fail(h, H3D_ERR_SINGULAR, "coarsest-grid matrix is singular");
+    h->have_stencils = true;
+    return H3D_OK;
+}
+
+int h3d_update_stencils(h3d_handle *h) {
+    if (!h) return H3D_ERR_ARG;
+    if (!h->have_density) return fail(h, H3D_ERR_STATE, "no density");
+    for (int l = 1; l < h->nl; l++)
+        if (int e = h3d_restrict_stencil(h, l)) return e;
+    return h3d_factor_coarsest(h);
+}
+
+int h3d_enforce_unit_macro_strain(h3d_handle *h) {
+    if (!h) return H3D_ERR_ARG;
+    if (!h->have_density) return fail(h, H3D_ERR_STATE, "no density");
+    launch_rhs(h->lv[0], h->rho, h->rhs, h->stream);
+    CKL();
+    return H3D_OK;
+}
+
+int h3d_gs_relaxation(h3d_handle *h, int level, float w, int times) {
+    if (int e = check_level(h, level)) return e;
+    if (level == h->nl - 1) return fail(h, H3D_ERR_ARG, "the coarsest level is solved directly");
+    if (level == 0 && !h->have_density) return fail(h, H3D_ERR_STATE, "no density");
+    if (level > 0 && !h->have_stencils) return fail(h, H3D_ERR_STATE, "no stencils");
+    for (int t = 0; t < times; t++) {
+        if (level == 0) launch_fine_gs(h->lv[0], h->rho, h->ke, w, h->stream);
+        else launch_coarse_gs(h->lv[level], w, h->stream);
+    }
+    CKL();
+    return H3D_OK;
+}
+
+int h3d_update_residual(h3d_handle *h, int level) {
+    if (int e = check_level(h, level)) return e;
+    if (level == 0) {
+        if (!h->have_density) return fail(h, H3D_ERR_STATE, "no density");
+        launch_fine_residual(h->lv[0], h->rho, h->ke, nullptr, 0, h->stream);
+    } else {
+        if (!h->have_stencils) return fail(h, H3D_ERR_STATE, "no stencils");
+        launch_coarse_residual(h->lv[level], h->stream);
+    }
+    CKL();
+    return H3D_OK;
+}
+
+int h3d_restrict_residual(h3d_handle *h, int coarse_level) {
+    if (int e = check_level(h, coarse_level, true)) return e;
+    launch_restrict(h->lv[coarse_level - 1], h->lv[coarse_level], h->stream);
+    CKL();
+    return H3D_OK;
+}
+
+int h3d_prolongate_correction(h3d_handle *h, int fine_level) {
+    if (int e = check_level(h, fine_level)) return e;
+    if (fine_level == h->nl - 1) return fail(h, H3D_ERR_ARG, "no coarser level");
+    launch_prolong(h->lv[fine_level], h->lv[fine_level + 1], fine_level == 0, h->stream);
+    CKL();
+    return H3D_OK;
+}
+
+int h3d_coarse_solve(h3d_handle *h) {
+    if (!h) return H3D_ERR_ARG;
+    if (!h->have_stencils) return fail(h, H3D_ERR_STATE, "no stencils");
+    launch_coarse_apply(h->lv[h->nl - 1], h->aug, h->cfg.coarse_mode == H3D_COARSE_PROJECT, h->stream);
+    CKL();
+    return H3D_OK;
+}
+
+int h3d_reset_displacement(h3d_handle *h, int level) {
+    if (!h) return H3D_ERR_ARG;
+    for (int l = 0; l < h->nl; l++)
+        if (level < 0 || level == l)
+            CK(cudaMemsetAsync(h->lv[l].u, 0, sizeof(float) * NF * h->lv[l].P.nv, h->stream));
+    return H3D_OK;
+}
+
+int h3d_field_norms(h3d_handle *h, int field, double out[6]) {
+    if (!h || !out) return H3D_ERR_ARG;
+    const Level &L = h->lv[0];
+    const float *v = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r
+                   : field == H3D_FIELD_CHI ? h->chi : nullptr;
+    if (!v) return fail(h, H3D_ERR_ARG, "field has no norm");
+    return weighted_norms(h, L.P, v, out);
+}
+
+int h3d_v_cycle(h3d_handle *h, float w, int pre, int post) {
+    if (!h) return H3D_ERR_ARG;
+    if (!h->have_stencils) return fail(h, H3D_ERR_STATE, "no stencils");
+    if (pre != 1 || post != 1) return fail(h, H3D_ERR_ARG, "only V(1,1) is supported");
+    CK(cudaSetDevice(h->device));
+    if (w == 1.f) {
+        if (int e = build_graph(h)) return e;
+        CK(cudaGraphLaunch(h->vgraph, h->stream));
+    } else {
+        enqueue_vcycle(h, w);
+        CKL();
+    }
+    return H3D_OK;
+}
+
+int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solve_stats *stats) {
+    if (!h) return H3D_ERR_ARG;
+    if (!h->have_stencils) return fail(h, H3D_ERR_STATE, "no stencils");
+    if (case_mask <= 0 || case_mask > 63) return fail(h, H3D_ERR_ARG, "case_mask must select load cases");
+    CK(cudaSetDevice(h->device));
+    if (!with_guess) CK(cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * NF * h->lv[0].P.nv, h->stream));
+    if (int e = build_graph(h)) return e;
+    double fn[6], rel[6] = {1, 1, 1, 1, 1, 1};
+    if (int e = weighted_norms(h, h->lv[0].P, h->lv[0].f, fn)) return e;
+    int it = 0, status = H3D_OK, explode_left = 2;
+    CK(cudaEventRecord(h->ev0, h->stream));
+    const int maxit = 200;
+    for (;;) {
+        if (it > 0) {
+            bool done = true;
+            for (int c = 0; c < NCASE; c++)
+                if ((case_mask >> c) & 1)
+                    if (!(rel[c] <= tol)) done = false;
+            if (done) break;
+        }
+        if (it >= maxit) { status = H3D_NOT_CONVERGED; break; }
+        CK(cudaGraphLaunch(h->vgraph, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        it++;
+        bool bad = false;
+        for (int c = 0; c < NCASE; c++) {
+            rel[c] = std::sqrt(h->h_small[c]) / (fn[c] + 1e-10);
+            if (((case_mask >> c) & 1) && (!(rel[c] <= 10.0))) bad = true;
+        }
+        if (bad) {  // MG.cpp:140-182: restart from zero once, then give up
+            if (--explode_left <= 0) { status = H3D_DIVERGED; break; }
+            CK(cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * NF * h->lv[0].P.nv, h->stream));
+        }
+    }
+    CK(cudaEventRecord(h->ev1, h->stream));
+    CK(cudaEventSynchronize(h->ev1));
+    if (stats) {
+        stats->vcycles = it;
+        stats->status = status;
+        for (int c = 0; c < NCASE; c++) stats->rel_res[c] = rel[c];
+        float ms = 0;
+        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+        stats->solve_ms = ms;
+    }
+    if (status != H3D_OK) return fail(h, status, status == H3D_DIVERGED ? "multigrid diverged" : "not converged");
+    return H3D_OK;
+}
+
+int h3d_reset_solutions(h3d_handle *h) {
+    if (!h) return H3D_ERR_ARG;
+    CK(cudaMemsetAsync(h->chi, 0, sizeof(float) * NF * h->lv[0].P.nv, h->stream));
+    return H3D_OK;
+}
+
+int h3d_elastic_matrix(h3d_handle *h, double tol, double C[36], h3d_solve_stats *stats) {
+    if (!h || !C) return H3D_ERR_ARG;
+    if (!h->have_stencils) return fail(h, H3D_ERR_STATE, "no stencils");
+    CK(cudaSetDevice(h->device));
+    Level &L = h->lv[0];
+    cudaStream_t s = h->stream;
+    const size_t bytes = sizeof(float) * NF * L.P.nv;
+    launch_rhs(L, h->rho, h->rhs, s);
+    CK(cudaMemcpyAsync(L.u, h->chi, bytes, cudaMemcpyDeviceToDevice, s));
+    const int nb = norm_blocks(L.P);
+    launch_mean_partial(L.P, L.u, h->partial, nb, s);
+    launch_remove_mean(L.P, L.u, h->partial, nb, s);
+    CKL();
+    h3d_solve_stats st;
+    int e = h3d_solve(h, 63, tol, 1, &st);
+    if (stats) *stats = st;
+    if (e != H3D_OK && e != H3D_NOT_CONVERGED) return e;
+    CK(cudaMemcpyAsync(h->chi, L.u, bytes, cudaMemcpyDeviceToDevice, s));
+    const int eb = elastic_blocks(L.P);
+    launch_elastic_partials(L.P, h->chi, h->rho, h->ke, h->partial, eb, s);
+    launch_elastic_finish(h->partial, eb, h->d_small, s);
+    CKL();
+    CK(cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * 21, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    const double vol = (double)L.P.nv;
+    int t = 0;
+    for (int i = 0; i < 6; i++)
+        for (int j = i; j < 6; j++) {
+            C[i * 6 + j] = C[j * 6 + i] = h->h_small[t] / vol;
+            t++;
+        }
+    return e;
+}
+
+int h3d_sensitivity(h3d_handle *h, const float dC[36], float *sens_dev, int pitchT) {
+    if (!h || !dC || !sens_dev) return H3D_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    const Planes &P = h->lv[0].P;
+    if (pitchT < 0) pitchT = P.n[0];
+    if (pitchT < P.n[0]) return fail(h, H3D_ERR_ARG, "pitchT smaller than the x resolution");
+    CK(cudaMemsetAsync(sens_dev, 0, sizeof(float) * (size_t)pitchT * P.n[1] * P.n[2], h->stream));
+    launch_sensitivity(P, h->chi, h->ke, dC, sens_dev, pitchT, h->stream);
+    CKL();
+    return H3D_OK;
+}
+
+int h3d_oc_update(h3d_handle *h, const float *sens_dev, float *rho_dev, int64_t n, float volratio, float min_rho,
+                  float step_limit, float damp) {
+    if (!h || !sens_dev || !rho_dev || n <= 0) return H3D_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    if (int e = ensure_tmp(h, (size_t)n)) return e;
+    launch_oc(sens_dev, rho_dev, h->tmp, n, volratio, min_rho, step_limit, damp, h->partial, h->stream);
+    CKL();
+    return H3D_OK;
+}
+
+int h3d_oc_filter(h3d_handle *h, float *sens_dev, const float *rho_dev, const int reso[3], int pitchT, float radius,
+                  int periodic) {
+    if (!h || !sens_dev || !rho_dev || !reso) return H3D_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    if (pitchT < 0) pitchT = reso[0];
+    const size_t n = (size_t)pitchT * reso[1] * reso[2];
+    if (int e = ensure_tmp(h, n)) return e;
+    CK(cudaMemsetAsync(h->tmp, 0, sizeof(float) * n, h->stream));
+    launch_filter(reso, pitchT, sens_dev, rho_dev, h->tmp, radius, periodic, h->stream);
+    CKL();
+    CK(cudaMemcpyAsync(sens_dev, h->tmp, sizeof(float) * n, cudaMemcpyDeviceToDevice, h->stream));
+    return H3D_OK;
+}
+
+int h3d_symmetrize(h3d_handle *h, float *field_dev, const int reso[3], int sym) {
+    if (!h || !field_dev || !reso || sym < 0 || sym > 2) return H3D_ERR_ARG;
+    if (sym > 0 && (reso[0] != reso[1] || reso[1] != reso[2]))
+        return fail(h, H3D_ERR_ARG, "reflect6 and rotate3 need a cubic grid");
+    CK(cudaSetDevice(h->device));
+    launch_symmetrize(reso, field_dev, sym, h->stream);
+    CKL();
+    return H3D_OK;
+}
+
+int h3d_get_field(h3d_handle *h, int level, int field, float *host) {
+    if (int e = check_level(h, level)) return e;
+    if (!host) return H3D_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    const Level &L = h->lv[level];
+    if (field == H3D_FIELD_STENCIL) {
+        if (level == 0) return fail(h, H3D_ERR_ARG, "level 0 has no stored stencil");
+        if (int e = ensure_tmp(h, (size_t)243 * L.P.nv)) return e;
+        launch_stencil_to_lex(L.P, L.st, h->tmp, h->stream);
+        CKL();
+        CK(cudaMemcpyAsync(host, h->tmp, sizeof(float) * 243 * L.P.nv, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        return H3D_OK;
+    }
+    const float *src = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r
+                     : (field == H3D_FIELD_CHI && level == 0) ? h->chi : nullptr;
+    if (!src) return fail(h, H3D_ERR_ARG, "unknown field");
+    if (int e = ensure_tmp(h, (size_t)NF * L.P.nv)) return e;
+    launch_field_to_lex(L.P, src, h->tmp, h->stream);
+    CKL();
+    CK(cudaMemcpyAsync(host, h->tmp, sizeof(float) * NF * L.P.nv, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    return H3D_OK;
+}
+
+int h3d_set_field(h3d_handle *h, int level, int field, const float *host) {
+    if (int e = check_level(h, level)) return e;
+    if (!host) return H3D_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    Level &L = h->lv[level];
+    if (field == H3D_FIELD_STENCIL) {
+        if (level == 0) return fail(h, H3D_ERR_ARG, "level 0 has no stored stencil");
+        if (int e = ensure_tmp(h, (size_t)243 * L.P.nv)) return e;
+        CK(cudaMemcpyAsync(h->tmp, host, sizeof(float) * 243 * L.P.nv, cudaMemcpyHostToDevice, h->stream));
+        launch_stencil_from_lex(L.P, h->tmp, L.st, h->stream);
+        CKL();
+        CK(cudaStreamSynchronize(h->stream));
+        return H3D_OK;
+    }
+    float *dst = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r
+               : (field == H3D_FIELD_CHI && level == 0) ? h->chi : nullptr;
+    if (!dst) return fail(h, H3D_ERR_ARG, "unknown field");
+    if (int e = ensure_tmp(h, (size_t)NF * L.P.nv)) return e;
+    CK(cudaMemcpyAsync(h->tmp, host, sizeof(float) * NF * L.P.nv, cudaMemcpyHostToDevice, h->stream));
+    launch_field_from_lex(L.P, h->tmp, dst, h->stream);
+    CKL();
+    CK(cudaStreamSynchronize(h->stream));
+    return H3D_OK;
+}
+
+}  // extern "C"

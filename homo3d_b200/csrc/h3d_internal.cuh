@@ -1,0 +1,153 @@
+// h3d_internal.cuh -- shared device layout and kernel launch declarations.
+//
+// Layout in HBM (every level):
+//   A vertex field holds the six load cases and three components as 18 planes
+//   of nv floats: value(case c, comp m, vertex v) = field[(3c + m) * nv + v].
+//   Vertices are ordered by Gauss-Seidel colour, then lexicographically inside
+//   the colour: a vertex (x,y,z) has colour k = ((x+1)&1) | ((y+1)&1)<<1 |
+//   ((z+1)&1)<<2 (the reference's padded-position parity, grid.cu:143-200) and
+//   index base[k] + (x>>1) + pn[k][0]*((y>>1) + pn[k][1]*(z>>1)).  A colour
+//   sweep therefore reads and writes contiguous runs, and the 26 neighbours of a
+//   vertex sit in the other colour planes at unit-stride offsets.
+//   Coarse stencils: 243 FP16 entries per vertex (27 neighbours x 3x3) packed
+//   eight to a uint4 chunk, chunk-major: st[q * nv + v], q = 0..30.
+//   Density: float, lexicographic cells (the fine level only).
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_fp16.h>
+#include <stdint.h>
+
+namespace h3d {
+
+constexpr int NCASE = 6;
+constexpr int NF = 18;          // floats per vertex (6 cases x 3 components)
+constexpr int NCHUNK = 31;      // uint4 chunks per stencil (243 halves -> 248)
+constexpr float RHO_PENAL_MIN = 1e-9f;  // grid.h:425
+
+struct Planes {
+    int n[3];        // vertices (= cells) per axis
+    int pn[8][3];    // plane dims of each colour
+    long long base[8];
+    long long nv;
+    int even;        // all axes even: pn uniform, base[k] = k * nv / 8
+};
+
+__host__ __device__ inline int color_of(int x, int y, int z) {
+    return ((x + 1) & 1) | (((y + 1) & 1) << 1) | (((z + 1) & 1) << 2);
+}
+
+__host__ __device__ inline long long vidx(const Planes &P, int x, int y, int z) {
+    int k = color_of(x, y, z);
+    return P.base[k] + (x >> 1) + (long long)P.pn[k][0] * ((y >> 1) + (long long)P.pn[k][1] * (z >> 1));
+}
+
+// inverse of vidx for the vertex with plane offset p in colour k
+__host__ __device__ inline void vpos(const Planes &P, int k, long long p, int &x, int &y, int &z) {
+    int i = (int)(p % P.pn[k][0]);
+    long long t = p / P.pn[k][0];
+    int j = (int)(t % P.pn[k][1]);
+    int l = (int)(t / P.pn[k][1]);
+    x = 2 * i + ((k & 1) ^ 1);
+    y = 2 * j + (((k >> 1) & 1) ^ 1);
+    z = 2 * l + (((k >> 2) & 1) ^ 1);
+}
+
+__host__ __device__ inline int wrap(int a, int n) { return a < 0 ? a + n : (a >= n ? a - n : a); }
+
+#ifdef __CUDACC__
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// block-reduce N per-thread values into partial[blk*N + i] in a fixed order;
+// every thread of the block must call it
+template <int N>
+__device__ __forceinline__ void block_reduce(const double *s, double *partial, long long blk) {
+    __shared__ double sm[N][32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int c = 0; c < N; ++c) {
+        double v = warp_sum(s[c]);
+        if (lane == 0) sm[c][wid] = v;
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int c = 0; c < N; ++c) {
+            double v = lane < nw ? sm[c][lane] : 0.0;
+            v = warp_sum(v);
+            if (lane == 0) partial[blk * N + c] = v;
+        }
+    }
+}
+
+// multiplicity of a unique vertex in the reference's padded periodic storage
+// (positions 0, 1 and n-1 are stored twice per axis, grid.cpp:155-198)
+__device__ __forceinline__ int axis_mult(int x, int n) { return (x == 0 || x == 1 || x == n - 1) ? 2 : 1; }
+
+__device__ __forceinline__ int color_of_index(const Planes &P, long long v) {
+    int k = 0;
+#pragma unroll
+    for (int q = 1; q < 8; ++q) k += (v >= P.base[q]) ? 1 : 0;
+    return k;
+}
+#endif
+
+struct KeMat { float k[576]; };        // element matrix, row-major, FP32
+struct RhsTab { float g[NCASE][24]; }; // Ke * chi0_c for the six unit strains
+
+struct Level {
+    Planes P;
+    int ratio[3];          // coarsening ratio from the finer level (0 on level 0)
+    float *u = nullptr, *f = nullptr, *r = nullptr;
+    uint4 *st = nullptr;   // coarse levels
+};
+
+// ---- launch wrappers (kernels in the .cu files) --------------------------
+// fine level (k_fine.cu)
+void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, cudaStream_t s);
+void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, double *norm_partial,
+                          int nblk_norm, cudaStream_t s);
+void launch_rhs(const Level &L, const float *rho, const RhsTab &g, cudaStream_t s);
+// coarse levels and transfers (k_coarse.cu)
+void launch_coarse_gs(const Level &L, float w, cudaStream_t s);
+void launch_coarse_residual(const Level &L, cudaStream_t s);
+void launch_restrict(const Level &F, const Level &C, cudaStream_t s);
+void launch_prolong(const Level &F, const Level &C, int is_root, cudaStream_t s);
+void launch_weighted_norm(const Planes &P, const float *v, double *partial, int nblk, cudaStream_t s);
+int norm_blocks(const Planes &P);
+void launch_norm_finish(const double *partial, int nblk, double *out6, cudaStream_t s);
+void launch_mean_partial(const Planes &P, const float *v, double *partial, int nblk, cudaStream_t s);
+void launch_remove_mean(const Planes &P, float *v, const double *partial, int nblk, cudaStream_t s);
+// Galerkin and coarsest solve (k_galerkin.cu)
+void launch_galerkin_l1(const Level &F, const Level &C, const float *rho, const float *q, int nsub,
+                        cudaStream_t s);
+void launch_dirichlet_patch(const Level &F, const Level &C, const float *rho, const double *ked, int pin_identity,
+                            cudaStream_t s);
+void launch_galerkin(const Level &F, const Level &C, cudaStream_t s);
+void launch_coarse_assemble(const Level &C, double *aug, cudaStream_t s);
+void launch_gauss_jordan(double *aug, int n, int *flag, cudaStream_t s);
+void launch_coarse_apply(const Level &C, const double *aug, int project, cudaStream_t s);
+// homogenized tensor, sensitivities (k_homog.cu)
+void launch_elastic_partials(const Planes &P, const float *chi, const float *rho, const KeMat &ke,
+                             double *partial, int nblk, cudaStream_t s);
+int elastic_blocks(const Planes &P);
+void launch_elastic_finish(const double *partial, int nblk, double *out21, cudaStream_t s);
+void launch_sensitivity(const Planes &P, const float *chi, const KeMat &ke, const float *dc36, float *sens,
+                        int pitch, cudaStream_t s);
+// design (k_design.cu)
+void launch_density_in(const int n[3], const float *src, int pitch, float *dst, cudaStream_t s);
+void launch_oc(const float *sens, float *rho, float *rho_new, long long n, float vol, float minrho, float step,
+               float damp, double *scratch, cudaStream_t s);
+void launch_filter(const int n[3], int pitch, const float *sens, const float *rho, float *out, float radius,
+                   int periodic, cudaStream_t s);
+void launch_symmetrize(const int n[3], float *v, int sym, cudaStream_t s);
+// field conversion (k_coarse.cu)
+void launch_field_to_lex(const Planes &P, const float *src, float *dst_lex, cudaStream_t s);
+void launch_field_from_lex(const Planes &P, const float *src_lex, float *dst, cudaStream_t s);
+void launch_stencil_to_lex(const Planes &P, const uint4 *st, float *dst_lex, cudaStream_t s);
+void launch_stencil_from_lex(const Planes &P, const float *src_lex, uint4 *st, cudaStream_t s);
+
+}  // namespace h3d

@@ -1,0 +1,382 @@
+// k_coarse.cu -- coarse-level stencil sweeps and residuals, grid transfers,
+// norms and layout conversions.
+//
+// Reference behaviour restated (homo3d grid.cu):
+//   gs_relaxation_kernel (grid.cu:556-689): 27-point stencil of FP16 3x3 blocks,
+//     FP32 accumulation, 3x3 block Gauss-Seidel on the components; no pin on
+//     coarse levels (the pinned origin enters through the Galerkin stencils).
+//   update_residual_kernel_1 (grid.cu:1465-1564): r = f - A u.
+//   restrict_residual_kernel_1 (grid.cu:917-994): f_c(X) = sum_{|o|<r}
+//     prod(r-|o|)/r^3 r_f(rX + o), periodic.
+//   prolongate_correction_kernel_1 (grid.cu:1120-1190, homoCommon.cuh:350-385):
+//     trilinear u_f += P u_c, the pinned fine origin is left unchanged.
+//   v3_norm (grid.cu:1954-1966): norms over the padded periodic storage, i.e.
+//     with the per-axis multiplicities of positions 0, 1 and n-1.
+#include "h3d_internal.cuh"
+
+namespace h3d {
+
+struct CoarseArgs {
+    float *u;
+    const float *__restrict__ f;
+    float *r;
+    const uint4 *__restrict__ st;
+    int n[3];
+    int h[3];
+    long long nv;
+    long long P;
+    float w;
+};
+
+__device__ __forceinline__ void axis_nbrs_c(int i, int p, int h, int &im, int &ip) {
+    if (p) { im = i; ip = (i + 1 == h) ? 0 : i + 1; }
+    else { im = (i == 0) ? h - 1 : i - 1; ip = i; }
+}
+
+__device__ __forceinline__ void unpack8(const uint4 &c, float o[8]) {
+    const __half2 *h = reinterpret_cast<const __half2 *>(&c);
+#pragma unroll
+    for (int t = 0; t < 4; ++t) {
+        const float2 v = __half22float2(h[t]);
+        o[2 * t] = v.x;
+        o[2 * t + 1] = v.y;
+    }
+}
+
+// the 9 entries of neighbour block d of vertex me
+template <int D>
+__device__ __forceinline__ void load_block(const CoarseArgs &a, long long me, float s[9]) {
+    constexpr int e0 = 9 * D, q0 = e0 / 8, q1 = (e0 + 8) / 8;
+    float v[16];
+    unpack8(a.st[q0 * a.nv + me], v);
+    if (q1 != q0) unpack8(a.st[q1 * a.nv + me], v + 8);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s[k] = v[e0 + k - 8 * q0];
+}
+
+template <int K, bool SELF>
+__device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, int i, int j, int l, float acc[NF]) {
+    constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
+    int ii[3], jj[3], ll[3];
+    axis_nbrs_c(i, px, a.h[0], ii[0], ii[2]);
+    axis_nbrs_c(j, py, a.h[1], jj[0], jj[2]);
+    axis_nbrs_c(l, pz, a.h[2], ll[0], ll[2]);
+    ii[1] = i; jj[1] = j; ll[1] = l;
+#pragma unroll
+    for (int q = 0; q < NF; ++q) acc[q] = 0.f;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        if (d == 13 && !SELF) continue;
+        const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
+        float s[9];
+        switch (d) {  // compile-time block index for the chunk arithmetic
+#define H3D_LB(D) case D: load_block<D>(a, me, s); break;
+            H3D_LB(0) H3D_LB(1) H3D_LB(2) H3D_LB(3) H3D_LB(4) H3D_LB(5) H3D_LB(6) H3D_LB(7) H3D_LB(8)
+            H3D_LB(9) H3D_LB(10) H3D_LB(11) H3D_LB(12) H3D_LB(13) H3D_LB(14) H3D_LB(15) H3D_LB(16)
+            H3D_LB(17) H3D_LB(18) H3D_LB(19) H3D_LB(20) H3D_LB(21) H3D_LB(22) H3D_LB(23) H3D_LB(24)
+            H3D_LB(25) H3D_LB(26)
+#undef H3D_LB
+        }
+        const int Kn = K ^ ((dx & 1) | ((dy & 1) << 1) | ((dz & 1) << 2));
+        const long long nid =
+            (long long)Kn * a.P + ii[dx + 1] + (long long)a.h[0] * (jj[dy + 1] + (long long)a.h[1] * ll[dz + 1]);
+        const float *up = a.u + nid;
+#pragma unroll
+        for (int c = 0; c < NCASE; ++c) {
+            const float u0 = up[(3 * c) * a.nv], u1 = up[(3 * c + 1) * a.nv], u2 = up[(3 * c + 2) * a.nv];
+            acc[3 * c + 0] = fmaf(s[0], u0, fmaf(s[1], u1, fmaf(s[2], u2, acc[3 * c + 0])));
+            acc[3 * c + 1] = fmaf(s[3], u0, fmaf(s[4], u1, fmaf(s[5], u2, acc[3 * c + 1])));
+            acc[3 * c + 2] = fmaf(s[6], u0, fmaf(s[7], u1, fmaf(s[8], u2, acc[3 * c + 2])));
+        }
+    }
+}
+
+template <int K>
+__global__ void __launch_bounds__(128) k_coarse_gs(CoarseArgs a) {
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= a.P) return;
+    const long long me = (long long)K * a.P + p;
+    const int i = (int)(p % a.h[0]);
+    const long long t = p / a.h[0];
+    const int j = (int)(t % a.h[1]), l = (int)(t / a.h[1]);
+    float acc[NF], ks[9];
+    coarse_apply<K, false>(a, me, i, j, l, acc);
+    load_block<13>(a, me, ks);
+    const float w = a.w;
+#pragma unroll
+    for (int c = 0; c < NCASE; ++c) {
+        float *u = a.u + me + (3 * c) * a.nv;
+        const float *f = a.f + me + (3 * c) * a.nv;
+        float u0 = u[0], u1 = u[a.nv], u2 = u[2 * a.nv];
+        u0 = w * (f[0] - acc[3 * c] - ks[1] * u1 - ks[2] * u2) / ks[0] + (1.f - w) * u0;
+        u1 = w * (f[a.nv] - acc[3 * c + 1] - ks[3] * u0 - ks[5] * u2) / ks[4] + (1.f - w) * u1;
+        u2 = w * (f[2 * a.nv] - acc[3 * c + 2] - ks[6] * u0 - ks[7] * u1) / ks[8] + (1.f - w) * u2;
+        u[0] = u0;
+        u[a.nv] = u1;
+        u[2 * a.nv] = u2;
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long p) {
+    const long long me = (long long)K * a.P + p;
+    const int i = (int)(p % a.h[0]);
+    const long long t = p / a.h[0];
+    const int j = (int)(t % a.h[1]), l = (int)(t / a.h[1]);
+    float acc[NF];
+    coarse_apply<K, true>(a, me, i, j, l, acc);
+#pragma unroll
+    for (int q = 0; q < NF; ++q) a.r[q * a.nv + me] = a.f[q * a.nv + me] - acc[q];
+}
+
+__global__ void __launch_bounds__(128) k_coarse_residual(CoarseArgs a) {
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= a.P) return;
+    switch (blockIdx.y) {
+    case 0: coarse_res_vertex<0>(a, p); break;
+    case 1: coarse_res_vertex<1>(a, p); break;
+    case 2: coarse_res_vertex<2>(a, p); break;
+    case 3: coarse_res_vertex<3>(a, p); break;
+    case 4: coarse_res_vertex<4>(a, p); break;
+    case 5: coarse_res_vertex<5>(a, p); break;
+    case 6: coarse_res_vertex<6>(a, p); break;
+    default: coarse_res_vertex<7>(a, p); break;
+    }
+}
+
+static CoarseArgs make_cargs(const Level &L) {
+    CoarseArgs a;
+    a.u = L.u;
+    a.f = L.f;
+    a.r = L.r;
+    a.st = L.st;
+    for (int d = 0; d < 3; ++d) { a.n[d] = L.P.n[d]; a.h[d] = L.P.n[d] / 2; }
+    a.nv = L.P.nv;
+    a.P = L.P.nv / 8;
+    a.w = 1.f;
+    return a;
+}
+
+void launch_coarse_gs(const Level &L, float w, cudaStream_t s) {
+    CoarseArgs a = make_cargs(L);
+    a.w = w;
+    const int bs = 128;
+    const unsigned nb = (unsigned)((a.P + bs - 1) / bs);
+    k_coarse_gs<0><<<nb, bs, 0, s>>>(a);
+    k_coarse_gs<1><<<nb, bs, 0, s>>>(a);
+    k_coarse_gs<2><<<nb, bs, 0, s>>>(a);
+    k_coarse_gs<3><<<nb, bs, 0, s>>>(a);
+    k_coarse_gs<4><<<nb, bs, 0, s>>>(a);
+    k_coarse_gs<5><<<nb, bs, 0, s>>>(a);
+    k_coarse_gs<6><<<nb, bs, 0, s>>>(a);
+    k_coarse_gs<7><<<nb, bs, 0, s>>>(a);
+}
+
+void launch_coarse_residual(const Level &L, cudaStream_t s) {
+    CoarseArgs a = make_cargs(L);
+    const int bs = 128;
+    const unsigned nb = (unsigned)((a.P + bs - 1) / bs);
+    k_coarse_residual<<<dim3(nb, 8), bs, 0, s>>>(a);
+}
+
+// ---- transfers ---------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_restrict(Planes F, Planes C, int r0, int r1, int r2,
+                                                  const float *__restrict__ rf, float *fc) {
+    const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (v >= C.nv) return;
+    const int k = color_of_index(C, v);
+    int x, y, z;
+    vpos(C, k, v - C.base[k], x, y, z);
+    const float pr = (float)(r0 * r1 * r2);
+    float acc[NF];
+#pragma unroll
+    for (int q = 0; q < NF; ++q) acc[q] = 0.f;
+    for (int ox = -r0 + 1; ox < r0; ox++) {
+        const int fx = wrap(r0 * x + ox, F.n[0]);
+        for (int oy = -r1 + 1; oy < r1; oy++) {
+            const int fy = wrap(r1 * y + oy, F.n[1]);
+            for (int oz = -r2 + 1; oz < r2; oz++) {
+                const int fz = wrap(r2 * z + oz, F.n[2]);
+                const float w = (float)((r0 - abs(ox)) * (r1 - abs(oy)) * (r2 - abs(oz))) / pr;
+                const long long fi = vidx(F, fx, fy, fz);
+#pragma unroll
+                for (int q = 0; q < NF; ++q) acc[q] = fmaf(__ldg(&rf[q * F.nv + fi]), w, acc[q]);
+            }
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NF; ++q) fc[q * C.nv + v] = acc[q];
+}
+
+__global__ void __launch_bounds__(256) k_prolong(Planes F, Planes C, int r0, int r1, int r2, int is_root,
+                                                 const float *__restrict__ uc, float *uf) {
+    const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (v >= F.nv) return;
+    const int k = color_of_index(F, v);
+    int x, y, z;
+    vpos(F, k, v - F.base[k], x, y, z);
+    if (is_root && x == 0 && y == 0 && z == 0) return;
+    const int rx = x % r0, ry = y % r1, rz = z % r2;
+    const int bx = x / r0, by = y / r1, bz = z / r2;
+    const float wc = (float)(r0 * r1 * r2);
+    float acc[NF];
+#pragma unroll
+    for (int q = 0; q < NF; ++q) acc[q] = 0.f;
+#pragma unroll
+    for (int id = 0; id < 8; ++id) {
+        const int ox = id & 1, oy = (id >> 1) & 1, oz = id >> 2;
+        const float w = (float)((r0 - abs(ox * r0 - rx)) * (r1 - abs(oy * r1 - ry)) * (r2 - abs(oz * r2 - rz))) / wc;
+        if (w == 0.f) continue;
+        const long long ci = vidx(C, wrap(bx + ox, C.n[0]), wrap(by + oy, C.n[1]), wrap(bz + oz, C.n[2]));
+#pragma unroll
+        for (int q = 0; q < NF; ++q) acc[q] = fmaf(__ldg(&uc[q * C.nv + ci]), w, acc[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < NF; ++q) uf[q * F.nv + v] += acc[q];
+}
+
+void launch_restrict(const Level &F, const Level &C, cudaStream_t s) {
+    const int bs = 256;
+    k_restrict<<<(unsigned)((C.P.nv + bs - 1) / bs), bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.r,
+                                                                  C.f);
+}
+
+void launch_prolong(const Level &F, const Level &C, int is_root, cudaStream_t s) {
+    const int bs = 256;
+    k_prolong<<<(unsigned)((F.P.nv + bs - 1) / bs), bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2],
+                                                                  is_root, C.u, F.u);
+}
+
+// ---- norms and means ---------------------------------------------------------
+constexpr int NORM_BS = 256;
+
+int norm_blocks(const Planes &P) {
+    long long nb = (P.nv + NORM_BS - 1) / NORM_BS;
+    return (int)(nb < 2048 ? nb : 2048);
+}
+
+__global__ void __launch_bounds__(NORM_BS) k_weighted_norm(Planes P, const float *__restrict__ v, double *partial) {
+    double s[NCASE] = {0, 0, 0, 0, 0, 0};
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < P.nv; i += (long long)gridDim.x * blockDim.x) {
+        const int k = color_of_index(P, i);
+        int x, y, z;
+        vpos(P, k, i - P.base[k], x, y, z);
+        const double m = (double)(axis_mult(x, P.n[0]) * axis_mult(y, P.n[1]) * axis_mult(z, P.n[2]));
+#pragma unroll
+        for (int c = 0; c < NCASE; ++c) {
+            double a = 0;
+#pragma unroll
+            for (int q = 0; q < 3; ++q) {
+                const double t = v[(3 * c + q) * P.nv + i];
+                a += t * t;
+            }
+            s[c] += m * a;
+        }
+    }
+    block_reduce<NCASE>(s, partial, blockIdx.x);
+}
+
+void launch_weighted_norm(const Planes &P, const float *v, double *partial, int nblk, cudaStream_t s) {
+    k_weighted_norm<<<nblk, NORM_BS, 0, s>>>(P, v, partial);
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_finish(const double *__restrict__ partial, int nblk, double *out) {
+    double s[N];
+#pragma unroll
+    for (int c = 0; c < N; ++c) s[c] = 0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+#pragma unroll
+        for (int c = 0; c < N; ++c) s[c] += partial[(long long)b * N + c];
+    block_reduce<N>(s, out, 0);
+}
+
+void launch_norm_finish(const double *partial, int nblk, double *out6, cudaStream_t s) {
+    k_finish<NCASE><<<1, 256, 0, s>>>(partial, nblk, out6);
+}
+
+__global__ void __launch_bounds__(NORM_BS) k_sum18(Planes P, const float *__restrict__ v, double *partial) {
+    double s[NF];
+#pragma unroll
+    for (int q = 0; q < NF; ++q) s[q] = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < P.nv; i += (long long)gridDim.x * blockDim.x)
+#pragma unroll
+        for (int q = 0; q < NF; ++q) s[q] += v[q * P.nv + i];
+    block_reduce<NF>(s, partial, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(256) k_sub_mean(Planes P, float *v, const double *__restrict__ sum18) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= P.nv) return;
+    const double inv = 1.0 / (double)P.nv;
+#pragma unroll
+    for (int q = 0; q < NF; ++q) v[q * P.nv + i] -= (float)(sum18[q] * inv);
+}
+
+void launch_mean_partial(const Planes &P, const float *v, double *partial, int nblk, cudaStream_t s) {
+    k_sum18<<<nblk, NORM_BS, 0, s>>>(P, v, partial);
+}
+
+// partial holds nblk rows of 18 sums; the total goes to partial[nblk*18 ..]
+void launch_remove_mean(const Planes &P, float *v, const double *partial, int nblk, cudaStream_t s) {
+    double *tot = const_cast<double *>(partial) + (long long)nblk * NF;
+    k_finish<NF><<<1, 256, 0, s>>>(partial, nblk, tot);
+    k_sub_mean<<<(unsigned)((P.nv + 255) / 256), 256, 0, s>>>(P, v, tot);
+}
+
+// ---- layout conversion: lexicographic [6][nv][3] <-> colour planes [18][nv] ----
+__global__ void k_field_lex(Planes P, const float *__restrict__ src, float *dst, int to_lex) {
+    const long long lex = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (lex >= P.nv) return;
+    const int x = (int)(lex % P.n[0]);
+    const long long t = lex / P.n[0];
+    const int y = (int)(t % P.n[1]), z = (int)(t / P.n[1]);
+    const long long v = vidx(P, x, y, z);
+#pragma unroll
+    for (int c = 0; c < NCASE; ++c)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const long long li = ((long long)c * P.nv + lex) * 3 + m, pi = (3 * c + m) * P.nv + v;
+            if (to_lex) dst[li] = src[pi];
+            else dst[pi] = src[li];
+        }
+}
+
+void launch_field_to_lex(const Planes &P, const float *src, float *dst_lex, cudaStream_t s) {
+    k_field_lex<<<(unsigned)((P.nv + 255) / 256), 256, 0, s>>>(P, src, dst_lex, 1);
+}
+void launch_field_from_lex(const Planes &P, const float *src_lex, float *dst, cudaStream_t s) {
+    k_field_lex<<<(unsigned)((P.nv + 255) / 256), 256, 0, s>>>(P, src_lex, dst, 0);
+}
+
+__global__ void k_stencil_lex(Planes P, const uint4 *st, float *lexf, const float *lexin, uint4 *stout) {
+    const long long lex = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (lex >= P.nv) return;
+    const int x = (int)(lex % P.n[0]);
+    const long long t = lex / P.n[0];
+    const int y = (int)(t % P.n[1]), z = (int)(t / P.n[1]);
+    const long long v = vidx(P, x, y, z);
+    for (int q = 0; q < NCHUNK; ++q) {
+        if (lexf) {
+            uint4 c = st[q * P.nv + v];
+            const __half *h = reinterpret_cast<const __half *>(&c);
+            for (int e = 0; e < 8; ++e)
+                if (8 * q + e < 243) lexf[lex * 243 + 8 * q + e] = __half2float(h[e]);
+        } else {
+            uint4 c;
+            __half *h = reinterpret_cast<__half *>(&c);
+            for (int e = 0; e < 8; ++e)
+                h[e] = (8 * q + e < 243) ? __float2half_rn(lexin[lex * 243 + 8 * q + e]) : __float2half_rn(0.f);
+            stout[q * P.nv + v] = c;
+        }
+    }
+}
+
+void launch_stencil_to_lex(const Planes &P, const uint4 *st, float *dst_lex, cudaStream_t s) {
+    k_stencil_lex<<<(unsigned)((P.nv + 127) / 128), 128, 0, s>>>(P, st, dst_lex, nullptr, nullptr);
+}
+void launch_stencil_from_lex(const Planes &P, const float *src_lex, uint4 *st, cudaStream_t s) {
+    k_stencil_lex<<<(unsigned)((P.nv + 127) / 128), 128, 0, s>>>(P, nullptr, nullptr, src_lex, st);
+}
+
+}  // namespace h3d

@@ -1,0 +1,259 @@
+// k_design.cu -- density input, OC update, sensitivity filter, symmetrisation.
+//
+// Reference behaviour restated (homo3d):
+//   update_rho_kernel (grid.cu:4025-4064): pitched lexicographic density in.
+//   OCOptimizer::update (OCOptimizer.cu:12-67): rho_new = clamp(rho *
+//     max(-s/g, 0.01)^damp, rho +- step, [rho_min, 1]), 20 bisection steps on g
+//     over [0, max|s|] until |vol - target| <= 1e-4.  Here the bisection state
+//     lives on the device, so the update needs no host round trip per step.
+//   OCOptimizer::filterSens (OCOptimizer.cu:76-152): s~_e = sum w rho s /
+//     (sum w * rho_e), linear cone weight 1 - |d|/r on a (2*int(r+0.5)+1)^3
+//     window, normalised by the full-window weight sum, optionally periodic.
+//   symetrize_tensor_kernel (TensorExpression.cuh:72-): orbit averages with the
+//     reference's FP32 summation order, so results are bit-identical.
+#include "h3d_internal.cuh"
+
+namespace h3d {
+
+__global__ void k_density_in(int n0, int n1, int n2, const float *__restrict__ src, int pitch, float *dst) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long ne = (long long)n0 * n1 * n2;
+    if (e >= ne) return;
+    const int x = (int)(e % n0);
+    const long long t = e / n0;
+    const int y = (int)(t % n1), z = (int)(t / n1);
+    dst[e] = src[x + ((long long)y + (long long)z * n1) * pitch];
+}
+
+void launch_density_in(const int n[3], const float *src, int pitch, float *dst, cudaStream_t s) {
+    const long long ne = (long long)n[0] * n[1] * n[2];
+    k_density_in<<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(n[0], n[1], n[2], src, pitch, dst);
+}
+
+// ---- OC ----------------------------------------------------------------------
+// scratch layout: [0] lo, [1] hi, [2] done, [3] g, [4..] partial sums
+constexpr int OC_BS = 256;
+constexpr int OC_NB = 1184;  // 8 blocks per SM on 148 SMs
+
+__global__ void __launch_bounds__(OC_BS) k_oc_maxabs(const float *__restrict__ s, long long n, double *partial) {
+    double m = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        m = fmax(m, (double)fabsf(s[i]));
+    __shared__ double sm[32];
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) sm[threadIdx.x >> 5] = m;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        m = threadIdx.x < (blockDim.x >> 5) ? sm[threadIdx.x] : 0.0;
+        for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_down_sync(0xffffffffu, m, o));
+        if (threadIdx.x == 0) partial[4 + blockIdx.x] = m;
+    }
+}
+
+__global__ void k_oc_init(double *st, int nb) {
+    if (threadIdx.x == 0) {
+        double m = 0;
+        for (int b = 0; b < nb; b++) m = fmax(m, st[4 + b]);
+        st[0] = 0.0;
+        st[1] = (double)(float)m;
+        st[2] = 0.0;
+    }
+}
+
+__global__ void __launch_bounds__(OC_BS) k_oc_step(const float *__restrict__ sens, const float *__restrict__ rho,
+                                                   float *rho_new, long long n, float minrho, float step, float damp,
+                                                   double *st) {
+    if (st[2] != 0.0) return;  // converged in an earlier step: keep its densities
+    const float g = ((float)st[1] + (float)st[0]) / 2;
+    double s = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const float r = rho[i];
+        float B = -sens[i] / g;
+        if (B < 0) B = 0.01f;
+        float v = powf(B, damp) * r;
+        if (v - r < -step) v = r - step;
+        if (v - r > step) v = r + step;
+        if (v < minrho) v = minrho;
+        if (v > 1) v = 1;
+        rho_new[i] = v;
+        s += v;
+    }
+    double ss[1] = {s};
+    block_reduce<1>(ss, st + 4, blockIdx.x);
+}
+
+__global__ void k_oc_decide(double *st, int nb, long long n, float vol) {
+    if (threadIdx.x != 0 || st[2] != 0.0) return;
+    double s = 0;
+    for (int b = 0; b < nb; b++) s += st[4 + b];
+    const float cur = (float)(s / (double)n);
+    const float g = ((float)st[1] + (float)st[0]) / 2;
+    if (cur < vol - 0.0001f) st[1] = g;
+    else if (cur > vol + 0.0001f) st[0] = g;
+    else st[2] = 1.0;
+}
+
+void launch_oc(const float *sens, float *rho, float *rho_new, long long n, float vol, float minrho, float step,
+               float damp, double *scratch, cudaStream_t s) {
+    k_oc_maxabs<<<OC_NB, OC_BS, 0, s>>>(sens, n, scratch);
+    k_oc_init<<<1, 32, 0, s>>>(scratch, OC_NB);
+    for (int it = 0; it < 20; ++it) {
+        k_oc_step<<<OC_NB, OC_BS, 0, s>>>(sens, rho, rho_new, n, minrho, step, damp, scratch);
+        k_oc_decide<<<1, 32, 0, s>>>(scratch, OC_NB, n, vol);
+    }
+    cudaMemcpyAsync(rho, rho_new, sizeof(float) * n, cudaMemcpyDeviceToDevice, s);
+}
+
+// ---- sensitivity filter ------------------------------------------------------
+__global__ void __launch_bounds__(256) k_filter(int n0, int n1, int n2, int pitch, const float *__restrict__ sens,
+                                                const float *__restrict__ rho, float *out, float radius, int hw,
+                                                float wtot, int periodic) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long ne = (long long)n0 * n1 * n2;
+    if (e >= ne) return;
+    const int x = (int)(e % n0);
+    const long long t = e / n0;
+    const int y = (int)(t % n1), z = (int)(t / n1);
+    float sum = 0.f, ws = 0.f;
+    const int side = 2 * hw + 1;
+    for (int id = 0; id < side * side * side; ++id) {
+        const int ox = id % side - hw, oy = id / side % side - hw, oz = id / (side * side) - hw;
+        const float r2 = (float)(ox * ox + oy * oy + oz * oz) / (radius * radius);
+        float w = r2 < 1.f ? 1.f - sqrtf(r2) : 0.f;
+        w /= wtot;
+        int px = x + ox, py = y + oy, pz = z + oz;
+        if (periodic) { px = (px + n0) % n0; py = (py + n1) % n1; pz = (pz + n2) % n2; }
+        if (px < 0 || px >= n0 || py < 0 || py >= n1 || pz < 0 || pz >= n2) continue;
+        const long long nid = px + ((long long)py + (long long)pz * n1) * pitch;
+        sum += sens[nid] * rho[nid] * w;
+        ws += w;
+    }
+    const long long me = x + ((long long)y + (long long)z * n1) * pitch;
+    sum /= ws * rho[me];
+    out[me] = sum;
+}
+
+void launch_filter(const int n[3], int pitch, const float *sens, const float *rho, float *out, float radius,
+                   int periodic, cudaStream_t s) {
+    const int hw = (int)(radius + 0.5f);
+    float wtot = 0.f;
+    const int side = 2 * hw + 1;
+    for (int id = 0; id < side * side * side; ++id) {
+        const int ox = id % side - hw, oy = id / side % side - hw, oz = id / (side * side) - hw;
+        const float r2 = (float)(ox * ox + oy * oy + oz * oz) / (radius * radius);
+        wtot += r2 < 1.f ? 1.f - sqrtf(r2) : 0.f;
+    }
+    const long long ne = (long long)n[0] * n[1] * n[2];
+    k_filter<<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(n[0], n[1], n[2], pitch, sens, rho, out, radius, hw, wtot,
+                                                          periodic);
+}
+
+// ---- symmetrisation ------------------------------------------------------------
+__device__ __forceinline__ long long lid(const int n[3], int a, int b, int c) {
+    return a + (long long)n[0] * (b + (long long)n[1] * c);
+}
+
+__global__ void k_sym_reflect3(int n0, int n1, int n2, float *v) {
+    const int n[3] = {n0, n1, n2}, h[3] = {n0 / 2, n1 / 2, n2 / 2};
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= (long long)h[0] * h[1] * h[2]) return;
+    const int rp[3] = {(int)(t % h[0]), (int)(t / h[0] % h[1]), (int)(t / ((long long)h[0] * h[1]))};
+    int orb[8][3];
+    for (int i = 0; i < 8; i++)
+        for (int j = 0; j < 3; j++) orb[i][j] = ((i >> j) & 1) ? n[j] - 1 - rp[j] : rp[j];
+    float val = v[lid(n, orb[0][0], orb[0][1], orb[0][2])];
+    for (int i = 1; i < 8; i++) val += v[lid(n, orb[i][0], orb[i][1], orb[i][2])];
+    val /= 8;
+    for (int i = 0; i < 8; i++) v[lid(n, orb[i][0], orb[i][1], orb[i][2])] = val;
+}
+
+__global__ void k_sym_reflect6(int n0, int h, float *v, long long nrep) {
+    const int n[3] = {n0, n0, n0};
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= nrep) return;
+    // representative x <= y <= z < h, enumerated tetrahedrally
+    int z = (int)cbrtf(6.f * (float)t);
+    while (z > 0 && (long long)z * (z + 1) * (z + 2) / 6 > t) z--;
+    while ((long long)(z + 1) * (z + 2) * (z + 3) / 6 <= t) z++;
+    long long rem = t - (long long)z * (z + 1) * (z + 2) / 6;
+    int y = (int)sqrtf(2.f * (float)rem);
+    while (y > 0 && (long long)y * (y + 1) / 2 > rem) y--;
+    while ((long long)(y + 1) * (y + 2) / 2 <= rem) y++;
+    const int x = (int)(rem - (long long)y * (y + 1) / 2);
+    const int rp[3] = {x, y, z};
+    float s = 0;
+    for (int i = 0; i < 8; i++) {
+        int o[3];
+        for (int j = 0; j < 3; j++) o[j] = ((i >> j) & 1) ? n[j] - 1 - rp[j] : rp[j];
+        s += v[lid(n, o[0], o[1], o[2])];
+        s += v[lid(n, o[0], o[2], o[1])];
+        s += v[lid(n, o[2], o[0], o[1])];
+        s += v[lid(n, o[2], o[1], o[0])];
+        s += v[lid(n, o[1], o[0], o[2])];
+        s += v[lid(n, o[1], o[2], o[0])];
+    }
+    s /= 48;
+    for (int i = 0; i < 8; i++) {
+        int o[3];
+        for (int j = 0; j < 3; j++) o[j] = ((i >> j) & 1) ? n[j] - 1 - rp[j] : rp[j];
+        v[lid(n, o[0], o[1], o[2])] = s;
+        v[lid(n, o[0], o[2], o[1])] = s;
+        v[lid(n, o[2], o[0], o[1])] = s;
+        v[lid(n, o[2], o[1], o[0])] = s;
+        v[lid(n, o[1], o[0], o[2])] = s;
+        v[lid(n, o[1], o[2], o[0])] = s;
+    }
+}
+
+__global__ void k_sym_rotate3(int n0, int h, float *v, long long nrep) {
+    const int n[3] = {n0, n0, n0};
+    const int hh[3] = {h, h, h};
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= nrep) return;
+    // representative z in [0,h), x, y in [0, z]
+    int z = (int)cbrtf(3.f * (float)t);
+    while (z > 0 && (long long)z * (z + 1) * (2 * z + 1) / 6 > t) z--;
+    while ((long long)(z + 1) * (z + 2) * (2 * z + 3) / 6 <= t) z++;
+    const long long rem = t - (long long)z * (z + 1) * (2 * z + 1) / 6;
+    const int y = (int)(rem / (z + 1)), x = (int)(rem % (z + 1));
+    const int rp[3] = {x, y, z};
+    const int perm[6][3] = {{0, 2, 1}, {2, 1, 0}, {1, 0, 2}, {2, 0, 1}, {1, 2, 0}, {0, 1, 2}};
+    const int fo[4][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 1}};
+    const int fe[4][3] = {{0, 0, 0}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}};
+    float s = 0;
+    for (int i = 0; i < 6; i++) {
+        const int o[3] = {rp[perm[i][0]], rp[perm[i][1]], rp[perm[i][2]]};
+        for (int f = 0; f < 4; f++) {
+            const int *fl = i < 3 ? fo[f] : fe[f];
+            int p[3];
+            for (int j = 0; j < 3; j++) p[j] = fl[j] ? hh[j] - 1 - o[j] : hh[j] + o[j];
+            s += v[lid(n, p[0], p[1], p[2])];
+        }
+    }
+    s /= 24;
+    for (int i = 0; i < 6; i++) {
+        const int o[3] = {rp[perm[i][0]], rp[perm[i][1]], rp[perm[i][2]]};
+        for (int f = 0; f < 4; f++) {
+            const int *fl = i < 3 ? fo[f] : fe[f];
+            int p[3];
+            for (int j = 0; j < 3; j++) p[j] = fl[j] ? hh[j] - 1 - o[j] : hh[j] + o[j];
+            v[lid(n, p[0], p[1], p[2])] = s;
+        }
+    }
+}
+
+void launch_symmetrize(const int n[3], float *v, int sym, cudaStream_t s) {
+    const int h = n[0] / 2;
+    if (sym == 0) {
+        const long long nr = (long long)(n[0] / 2) * (n[1] / 2) * (n[2] / 2);
+        k_sym_reflect3<<<(unsigned)((nr + 255) / 256), 256, 0, s>>>(n[0], n[1], n[2], v);
+    } else if (sym == 1) {
+        const long long nr = (long long)h * (h + 1) * (h + 2) / 6;
+        k_sym_reflect6<<<(unsigned)((nr + 255) / 256), 256, 0, s>>>(n[0], h, v, nr);
+    } else if (sym == 2) {
+        const long long nr = (long long)h * (h + 1) * (2 * h + 1) / 6;
+        k_sym_rotate3<<<(unsigned)((nr + 255) / 256), 256, 0, s>>>(n[0], h, v, nr);
+    }
+}
+
+}  // namespace h3d

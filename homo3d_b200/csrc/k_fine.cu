@@ -1,0 +1,267 @@
+// k_fine.cu -- matrix-free fine-level operator: Gauss-Seidel colour sweeps,
+// residual with fused per-case norms, and the unit macro-strain right-hand side.
+//
+// Reference behaviour restated (homo3d grid.cu):
+//   gs_relaxation_otf_kernel (grid.cu:323-551): for each vertex of one colour,
+//     sum over its 8 elements of (1e-9 + rho_e) * Ke[own rows][other nodes] * u,
+//     then a 3x3 block Gauss-Seidel step on the components (x, then y, then z);
+//     neighbours at the pinned origin count as zero; the origin stays zero.
+//   update_residual_otf_kernel_1 (grid.cu:1277-1461): r = f - K(rho) u, r = 0 at
+//     the pinned origin.
+//   enforce_unit_macro_strain_kernel (grid.cu:1818-1919): f_i = K(rho) chi0_i.
+//
+// B200 design: all six load cases are fused into every sweep so each element
+// density and each neighbour address is fetched once for six right-hand sides.
+// The element loop is reorganised per neighbour: for each of the 26 neighbours
+// the 3x3 coupling block sum_e rho_e Ke[a_e][b_e] is formed once (Ke entries are
+// compile-time offsets into the kernel-parameter bank, so they are FFMA operands)
+// and applied to the six cases, 576 + 234*6 FMAs per vertex instead of 3240.
+#include "h3d_internal.cuh"
+
+namespace h3d {
+
+struct FineArgs {
+    const float *__restrict__ rho;
+    float *u;
+    const float *__restrict__ f;
+    float *r;
+    int n[3];
+    int h[3];
+    long long nv;  // vertices
+    long long P;   // vertices per colour plane
+    float w;
+};
+
+__device__ __forceinline__ void axis_nbrs(int i, int p, int h, int &im, int &ip) {
+    if (p) { im = i; ip = (i + 1 == h) ? 0 : i + 1; }
+    else { im = (i == 0) ? h - 1 : i - 1; ip = i; }
+}
+
+// acc[3c+r] = sum over neighbours (and the vertex itself when SELF) of the
+// assembled coupling block times u; ks = own 3x3 diagonal block
+template <int K, bool SELF>
+__device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, int i, int j, int l,
+                                           float acc[NF], float ks[9]) {
+    constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
+    const int x = 2 * i + px, y = 2 * j + py, z = 2 * l + pz;
+    const int xe0 = x == 0 ? a.n[0] - 1 : x - 1;
+    const int ye0 = y == 0 ? a.n[1] - 1 : y - 1;
+    const int ze0 = z == 0 ? a.n[2] - 1 : z - 1;
+    float rw[8];
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        const int ex = (w & 1) ? x : xe0, ey = ((w >> 1) & 1) ? y : ye0, ez = (w >> 2) ? z : ze0;
+        rw[w] = RHO_PENAL_MIN + __ldg(&a.rho[ex + (long long)a.n[0] * (ey + (long long)a.n[1] * ez)]);
+    }
+    int ii[3], jj[3], ll[3];
+    axis_nbrs(i, px, a.h[0], ii[0], ii[2]);
+    axis_nbrs(j, py, a.h[1], jj[0], jj[2]);
+    axis_nbrs(l, pz, a.h[2], ll[0], ll[2]);
+    ii[1] = i; jj[1] = j; ll[1] = l;
+#pragma unroll
+    for (int q = 0; q < NF; ++q) acc[q] = 0.f;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
+        if (d == 13 && !SELF) continue;
+        float A[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) A[k] = 0.f;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            const int ex = w & 1, ey = (w >> 1) & 1, ez = w >> 2;
+            const int bx = 1 - ex + dx, by = 1 - ey + dy, bz = 1 - ez + dz;
+            if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+            const int an = 7 - w, bn = bx + 2 * by + 4 * bz;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    A[3 * r + c] = fmaf(rw[w], ke.k[(3 * an + r) * 24 + 3 * bn + c], A[3 * r + c]);
+        }
+        const int Kn = K ^ ((dx & 1) | ((dy & 1) << 1) | ((dz & 1) << 2));
+        const int ni = ii[dx + 1], nj = jj[dy + 1], nl = ll[dz + 1];
+        if (Kn == 7 && (ni | nj | nl) == 0) continue;  // pinned origin: u = 0
+        const long long nid = (long long)Kn * a.P + ni + (long long)a.h[0] * (nj + (long long)a.h[1] * nl);
+        const float *up = a.u + nid;
+#pragma unroll
+        for (int c = 0; c < NCASE; ++c) {
+            const float u0 = __ldg(up + (3 * c) * a.nv);
+            const float u1 = __ldg(up + (3 * c + 1) * a.nv);
+            const float u2 = __ldg(up + (3 * c + 2) * a.nv);
+            acc[3 * c + 0] = fmaf(A[0], u0, fmaf(A[1], u1, fmaf(A[2], u2, acc[3 * c + 0])));
+            acc[3 * c + 1] = fmaf(A[3], u0, fmaf(A[4], u1, fmaf(A[5], u2, acc[3 * c + 1])));
+            acc[3 * c + 2] = fmaf(A[6], u0, fmaf(A[7], u1, fmaf(A[8], u2, acc[3 * c + 2])));
+        }
+    }
+    if (!SELF) {
+#pragma unroll
+        for (int k = 0; k < 9; ++k) ks[k] = 0.f;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            const int an = 7 - w;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    ks[3 * r + c] = fmaf(rw[w], ke.k[(3 * an + r) * 24 + 3 * an + c], ks[3 * r + c]);
+        }
+    }
+}
+
+__device__ __forceinline__ void plane_coords(long long p, const int h[3], int &i, int &j, int &l) {
+    i = (int)(p % h[0]);
+    long long t = p / h[0];
+    j = (int)(t % h[1]);
+    l = (int)(t / h[1]);
+}
+
+template <int K>
+__global__ void __launch_bounds__(128) k_fine_gs(FineArgs a, const __grid_constant__ KeMat ke) {
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= a.P) return;
+    const long long me = (long long)K * a.P + p;
+    if (K == 7 && p == 0) {  // the pinned origin (grid.cu:445-447, 545)
+#pragma unroll
+        for (int q = 0; q < NF; ++q) a.u[q * a.nv + me] = 0.f;
+        return;
+    }
+    int i, j, l;
+    plane_coords(p, a.h, i, j, l);
+    float acc[NF], ks[9];
+    fine_apply<K, false>(a, ke, i, j, l, acc, ks);
+    const float w = a.w;
+#pragma unroll
+    for (int c = 0; c < NCASE; ++c) {
+        float *u = a.u + me + (3 * c) * a.nv;
+        const float *f = a.f + me + (3 * c) * a.nv;
+        float u0 = u[0], u1 = u[a.nv], u2 = u[2 * a.nv];
+        u0 = w * (f[0] - acc[3 * c] - ks[1] * u1 - ks[2] * u2) / ks[0] + (1.f - w) * u0;
+        u1 = w * (f[a.nv] - acc[3 * c + 1] - ks[3] * u0 - ks[5] * u2) / ks[4] + (1.f - w) * u1;
+        u2 = w * (f[2 * a.nv] - acc[3 * c + 2] - ks[6] * u0 - ks[7] * u1) / ks[8] + (1.f - w) * u2;
+        u[0] = u0;
+        u[a.nv] = u1;
+        u[2 * a.nv] = u2;
+    }
+}
+
+template <int K>
+__device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const KeMat &ke, long long p,
+                                                     double nrm[NCASE]) {
+    const long long me = (long long)K * a.P + p;
+    int i, j, l;
+    plane_coords(p, a.h, i, j, l);
+    float acc[NF];
+    if (K == 7 && p == 0) {
+#pragma unroll
+        for (int q = 0; q < NF; ++q) a.r[q * a.nv + me] = 0.f;
+        return;
+    }
+    fine_apply<K, true>(a, ke, i, j, l, acc, nullptr);
+    constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
+    const double mult = (double)(axis_mult(2 * i + px, a.n[0]) * axis_mult(2 * j + py, a.n[1]) *
+                                 axis_mult(2 * l + pz, a.n[2]));
+#pragma unroll
+    for (int c = 0; c < NCASE; ++c) {
+        double s2 = 0;
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            const long long o = (3 * c + m) * a.nv + me;
+            const float rv = a.f[o] - acc[3 * c + m];
+            a.r[o] = rv;
+            s2 += (double)rv * rv;
+        }
+        nrm[c] += mult * s2;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_fine_residual(FineArgs a, const __grid_constant__ KeMat ke,
+                                                       double *partial) {
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int K = blockIdx.y;
+    double nrm[NCASE] = {0, 0, 0, 0, 0, 0};
+    if (p < a.P) {
+        switch (K) {
+        case 0: fine_residual_vertex<0>(a, ke, p, nrm); break;
+        case 1: fine_residual_vertex<1>(a, ke, p, nrm); break;
+        case 2: fine_residual_vertex<2>(a, ke, p, nrm); break;
+        case 3: fine_residual_vertex<3>(a, ke, p, nrm); break;
+        case 4: fine_residual_vertex<4>(a, ke, p, nrm); break;
+        case 5: fine_residual_vertex<5>(a, ke, p, nrm); break;
+        case 6: fine_residual_vertex<6>(a, ke, p, nrm); break;
+        default: fine_residual_vertex<7>(a, ke, p, nrm); break;
+        }
+    }
+    if (partial) block_reduce<NCASE>(nrm, partial, (long long)blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// f(case c) = sum_w (1e-9 + rho_w) * (Ke chi0_c)[rows of the vertex's local node in element w]
+__global__ void __launch_bounds__(256) k_rhs(Planes P, const float *__restrict__ rho, float *f,
+                                             const __grid_constant__ RhsTab g) {
+    const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (v >= P.nv) return;
+    const int k = color_of_index(P, v);
+    int x, y, z;
+    vpos(P, k, v - P.base[k], x, y, z);
+    const int n0 = P.n[0], n1 = P.n[1], n2 = P.n[2];
+    const int xe0 = x == 0 ? n0 - 1 : x - 1, ye0 = y == 0 ? n1 - 1 : y - 1, ze0 = z == 0 ? n2 - 1 : z - 1;
+    float acc[NF];
+#pragma unroll
+    for (int q = 0; q < NF; ++q) acc[q] = 0.f;
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        const int ex = (w & 1) ? x : xe0, ey = ((w >> 1) & 1) ? y : ye0, ez = (w >> 2) ? z : ze0;
+        const float rp = RHO_PENAL_MIN + __ldg(&rho[ex + (long long)n0 * (ey + (long long)n1 * ez)]);
+        const int an = 7 - w;
+#pragma unroll
+        for (int c = 0; c < NCASE; ++c)
+#pragma unroll
+            for (int m = 0; m < 3; ++m) acc[3 * c + m] = fmaf(rp, g.g[c][3 * an + m], acc[3 * c + m]);
+    }
+#pragma unroll
+    for (int q = 0; q < NF; ++q) f[q * P.nv + v] = acc[q];
+}
+
+static FineArgs make_args(const Level &L, const float *rho) {
+    FineArgs a;
+    a.rho = rho;
+    a.u = L.u;
+    a.f = L.f;
+    a.r = L.r;
+    for (int d = 0; d < 3; ++d) { a.n[d] = L.P.n[d]; a.h[d] = L.P.n[d] / 2; }
+    a.nv = L.P.nv;
+    a.P = L.P.nv / 8;
+    a.w = 1.f;
+    return a;
+}
+
+void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, cudaStream_t s) {
+    FineArgs a = make_args(L, rho);
+    a.w = w;
+    const int bs = 128;
+    const unsigned nb = (unsigned)((a.P + bs - 1) / bs);
+    k_fine_gs<0><<<nb, bs, 0, s>>>(a, ke);
+    k_fine_gs<1><<<nb, bs, 0, s>>>(a, ke);
+    k_fine_gs<2><<<nb, bs, 0, s>>>(a, ke);
+    k_fine_gs<3><<<nb, bs, 0, s>>>(a, ke);
+    k_fine_gs<4><<<nb, bs, 0, s>>>(a, ke);
+    k_fine_gs<5><<<nb, bs, 0, s>>>(a, ke);
+    k_fine_gs<6><<<nb, bs, 0, s>>>(a, ke);
+    k_fine_gs<7><<<nb, bs, 0, s>>>(a, ke);
+}
+
+void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, double *norm_partial, int nblk_norm,
+                          cudaStream_t s) {
+    FineArgs a = make_args(L, rho);
+    const int bs = 128;
+    const unsigned nb = (unsigned)((a.P + bs - 1) / bs);
+    (void)nblk_norm;
+    k_fine_residual<<<dim3(nb, 8), bs, 0, s>>>(a, ke, norm_partial);
+}
+
+void launch_rhs(const Level &L, const float *rho, const RhsTab &g, cudaStream_t s) {
+    const int bs = 256;
+    k_rhs<<<(unsigned)((L.P.nv + bs - 1) / bs), bs, 0, s>>>(L.P, rho, L.f, g);
+}
+
+}  // namespace h3d

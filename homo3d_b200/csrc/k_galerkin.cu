@@ -1,0 +1,375 @@
+// k_galerkin.cu -- Galerkin coarse operators and the coarsest-grid dense solve.
+//
+// Reference behaviour restated (homo3d):
+//   restrict_stencil_otf_aos_kernel_1 (grid_ex.cu:936-1060): level-1 stencils
+//     R K(rho) P computed from the fine densities (rho^p, no 1e-9 floor) for the
+//     lexicographic vertices 0..n_c per axis, elements clipped to the domain, the
+//     self block's diagonal clamped to >= 1e-4, stored FP16; the periodic images
+//     of a vertex on a min face are then summed in FP16 (grid.cu:2741-2772 ->
+//     grid.cu:3103-3176).  On B200 the triple loop over fine elements is replaced
+//     by the exact refactoring into coarse element matrices
+//     K_E = sum_s rho_s P_s^T Ke P_s (Q_s = P_s^T Ke P_s precomputed), and the
+//     images become the subsets of the 8 coarse elements around the vertex.
+//   restrict_stencil_arround_dirichelt_boundary (grid.cpp:1184-1325): the 27
+//     coarse vertices around the pinned fine origin use the pinned fine operator
+//     (identity at the origin node, 1e-9 floor) in double precision.  With
+//     pin_identity = 0 the identity is left out, which makes the coarse operator
+//     the exact Galerkin product of the pinned fine operator.
+//   restrict_stencil_aos_kernel_1 (grid_ex.cu:1065-1160): deeper levels R A P
+//     from the FP16 finer stencil.
+//   solveHostEquation / assembleHostMatrix (grid.cpp:349-424): coarsest level.
+//     Replaced by a dense FP64 inverse built on the device (Gauss-Jordan with
+//     partial pivoting) and applied as a GEMV per load case.
+#include "h3d_internal.cuh"
+
+namespace h3d {
+
+__device__ __forceinline__ int modp(int a, int n) { return ((a % n) + n) % n; }
+
+__device__ __forceinline__ void put_half(uint4 *st, long long nv, long long v, int e, __half h) {
+    __half *p = reinterpret_cast<__half *>(st + (long long)(e >> 3) * nv + v) + (e & 7);
+    *p = h;
+}
+__device__ __forceinline__ float get_half(const uint4 *st, long long nv, long long v, int e) {
+    const __half *p = reinterpret_cast<const __half *>(st + (long long)(e >> 3) * nv + v) + (e & 7);
+    return __half2float(*p);
+}
+
+// ---- level 1 from densities ---------------------------------------------------
+// R = 2 on every axis is compiled with the sub-element loop unrolled; R = 0 is
+// the generic path for ratio 4 (or mixed ratios).
+template <int R>
+__global__ void __launch_bounds__(128) k_galerkin_l1(Planes F, Planes C, int r0, int r1, int r2,
+                                                     const float *__restrict__ rho, const float *__restrict__ q,
+                                                     int nsub, uint4 *st) {
+    extern __shared__ float sq[];
+    for (int i = threadIdx.x; i < nsub * 576; i += blockDim.x) sq[i] = q[i];
+    __syncthreads();
+    const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (v >= C.nv) return;
+    if (R == 2) { r0 = r1 = r2 = 2; nsub = 8; }
+    const int k = color_of_index(C, v);
+    int X[3];
+    vpos(C, k, v - C.base[k], X[0], X[1], X[2]);
+    const int bmask = (X[0] == 0 ? 4 : 0) | (X[1] == 0 ? 2 : 0) | (X[2] == 0 ? 1 : 0);
+    // lexicographic index of fine element (E*r + s) for the coarse element E = X - l
+    long long ebase[8];
+#pragma unroll
+    for (int l = 0; l < 8; ++l) {
+        const int ex = wrap(X[0] - (l & 1), C.n[0]) * r0, ey = wrap(X[1] - ((l >> 1) & 1), C.n[1]) * r1,
+                  ez = wrap(X[2] - (l >> 2), C.n[2]) * r2;
+        ebase[l] = ex + (long long)F.n[0] * (ey + (long long)F.n[1] * ez);
+    }
+    uint32_t cbuf[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
+        __half res[9];
+#pragma unroll
+        for (int e = 0; e < 9; ++e) res[e] = __float2half_rn(0.f);
+        for (int img = 0; img < 8; ++img) {
+            if (img & ~bmask) continue;
+            float p[9];
+#pragma unroll
+            for (int e = 0; e < 9; ++e) p[e] = 0.f;
+#pragma unroll
+            for (int l = 0; l < 8; ++l) {
+                const int lx = l & 1, ly = (l >> 1) & 1, lz = l >> 2;
+                const int mx = lx + dx, my = ly + dy, mz = lz + dz;
+                if (mx < 0 || mx > 1 || my < 0 || my > 1 || mz < 0 || mz > 1) continue;
+                const int m = mx + 2 * my + 4 * mz;
+                const int limg = ((lx << 2) | (ly << 1) | lz) & bmask;
+                if (limg != img) continue;
+                if (R == 2) {
+#pragma unroll
+                    for (int s = 0; s < 8; ++s) {
+                        const long long fe = ebase[l] + (s & 1) + (long long)F.n[0] * (((s >> 1) & 1) + (long long)F.n[1] * (s >> 2));
+                        const float rp = __ldg(&rho[fe]);
+                        const float *Q = sq + s * 576;
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int j = 0; j < 3; ++j) p[3 * i + j] = fmaf(rp, Q[(3 * l + i) * 24 + 3 * m + j], p[3 * i + j]);
+                    }
+                } else {
+                    for (int s = 0; s < nsub; ++s) {
+                        const int sx = s % r0, sy = (s / r0) % r1, sz = s / (r0 * r1);
+                        const long long fe = ebase[l] + sx + (long long)F.n[0] * (sy + (long long)F.n[1] * sz);
+                        const float rp = __ldg(&rho[fe]);
+                        const float *Q = sq + s * 576;
+#pragma unroll
+                        for (int i = 0; i < 3; ++i)
+#pragma unroll
+                            for (int j = 0; j < 3; ++j) p[3 * i + j] = fmaf(rp, Q[(3 * l + i) * 24 + 3 * m + j], p[3 * i + j]);
+                    }
+                }
+            }
+            if (d == 13) {
+#pragma unroll
+                for (int t = 0; t < 3; ++t)
+                    if (fabsf(p[4 * t]) < 1e-4f) p[4 * t] = 1e-4f;
+            }
+#pragma unroll
+            for (int e = 0; e < 9; ++e) res[e] = __hadd(res[e], __float2half_rn(p[e]));
+        }
+        // stream the 9 halves into the packed chunks
+#pragma unroll
+        for (int e = 0; e < 9; ++e) {
+            const int g = 9 * d + e;
+            const uint32_t hv = (uint32_t)__half_as_ushort(res[e]);
+            const int slot = (g & 7) >> 1;
+            if (g & 1) cbuf[slot] |= hv << 16;
+            else cbuf[slot] = hv;
+            if ((g & 7) == 7 || g == 242) {
+                if (g == 242) { cbuf[1] &= 0xffffu; cbuf[2] = 0; cbuf[3] = 0; }
+                st[(long long)(g >> 3) * C.nv + v] = make_uint4(cbuf[0], cbuf[1], cbuf[2], cbuf[3]);
+            }
+        }
+    }
+}
+
+void launch_galerkin_l1(const Level &F, const Level &C, const float *rho, const float *q, int nsub, cudaStream_t s) {
+    const int bs = 128;
+    const unsigned nb = (unsigned)((C.P.nv + bs - 1) / bs);
+    const size_t smem = (size_t)nsub * 576 * sizeof(float);
+    if (C.ratio[0] == 2 && C.ratio[1] == 2 && C.ratio[2] == 2) {
+        k_galerkin_l1<2><<<nb, bs, smem, s>>>(F.P, C.P, 2, 2, 2, rho, q, nsub, C.st);
+    } else {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(k_galerkin_l1<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            attr = true;
+        }
+        k_galerkin_l1<0><<<nb, bs, smem, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], rho, q, nsub, C.st);
+    }
+}
+
+// ---- the 27 coarse vertices around the pinned fine origin -----------------------
+__device__ __forceinline__ double hat_w(int ox, int oy, int oz, int r0, int r1, int r2) {
+    ox = abs(ox); oy = abs(oy); oz = abs(oz);
+    if (ox >= r0 || oy >= r1 || oz >= r2) return 0.0;
+    return (double)((r0 - ox) * (r1 - oy) * (r2 - oz)) / (double)(r0 * r1 * r2);
+}
+
+// one thread per (coarse vertex offset vi in {-1,0,1}^3, neighbour d)
+__global__ void k_dirichlet_patch(Planes F, Planes C, int r0, int r1, int r2, const float *__restrict__ rho,
+                                  const double *__restrict__ ked, int pin_identity, uint4 *st) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= 27 * 27) return;
+    const int vi = t / 27, d = t % 27;
+    const int vio[3] = {(vi % 3 - 1), (vi / 3 % 3 - 1), (vi / 9 - 1)};
+    const int pi[3] = {vio[0] * r0, vio[1] * r1, vio[2] * r2};
+    const int pj[3] = {pi[0] + (d % 3 - 1) * r0, pi[1] + (d / 3 % 3 - 1) * r1, pi[2] + (d / 9 - 1) * r2};
+    double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    for (int ex = -r0; ex < r0; ex++)
+        for (int ey = -r1; ey < r1; ey++)
+            for (int ez = -r2; ez < r2; ez++) {
+                const int ep[3] = {pj[0] + ex, pj[1] + ey, pj[2] + ez};
+                const int eo[3] = {ep[0] - pi[0], ep[1] - pi[1], ep[2] - pi[2]};
+                if (eo[0] >= r0 || eo[0] < -r0 || eo[1] >= r1 || eo[1] < -r1 || eo[2] >= r2 || eo[2] < -r2) continue;
+                const long long fe =
+                    modp(ep[0], F.n[0]) + (long long)F.n[0] * (modp(ep[1], F.n[1]) + (long long)F.n[1] * modp(ep[2], F.n[2]));
+                const double rp = 1e-9 + (double)rho[fe];
+                for (int a = 0; a < 8; a++) {
+                    const int ap[3] = {ep[0] + (a & 1), ep[1] + ((a >> 1) & 1), ep[2] + (a >> 2)};
+                    const double wi = hat_w(ap[0] - pi[0], ap[1] - pi[1], ap[2] - pi[2], r0, r1, r2);
+                    if (wi == 0) continue;
+                    const bool ad = ap[0] == 0 && ap[1] == 0 && ap[2] == 0;
+                    for (int b = 0; b < 8; b++) {
+                        const int bp[3] = {ep[0] + (b & 1), ep[1] + ((b >> 1) & 1), ep[2] + (b >> 2)};
+                        const double wj = hat_w(bp[0] - pj[0], bp[1] - pj[1], bp[2] - pj[2], r0, r1, r2);
+                        if (wj == 0) continue;
+                        const bool bd = bp[0] == 0 && bp[1] == 0 && bp[2] == 0;
+                        if (ad || bd) {
+                            if (a == b && pin_identity)
+                                for (int i = 0; i < 3; i++) s[4 * i] += wi * wj;
+                        } else {
+                            for (int i = 0; i < 3; i++)
+                                for (int j = 0; j < 3; j++) s[3 * i + j] += wi * wj * rp * ked[(3 * a + i) * 24 + 3 * b + j];
+                        }
+                    }
+                }
+            }
+    if (d == 13)
+        for (int i = 0; i < 3; i++)
+            if (fabs(s[4 * i]) < 1e-4) s[4 * i] = 1e-4;
+    const long long v = vidx(C, modp(vio[0], C.n[0]), modp(vio[1], C.n[1]), modp(vio[2], C.n[2]));
+    for (int e = 0; e < 9; e++) put_half(st, C.nv, v, 9 * d + e, __double2half(s[e]));
+}
+
+void launch_dirichlet_patch(const Level &F, const Level &C, const float *rho, const double *ked, int pin_identity,
+                            cudaStream_t s) {
+    k_dirichlet_patch<<<(27 * 27 + 127) / 128, 128, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], rho, ked,
+                                                            pin_identity, C.st);
+}
+
+// ---- deeper levels: R A P from the finer FP16 stencil ----------------------------
+__global__ void __launch_bounds__(128) k_galerkin(Planes F, Planes C, int r0, int r1, int r2,
+                                                  const uint4 *__restrict__ fst, uint4 *cst) {
+    const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (v >= C.nv) return;
+    const int k = color_of_index(C, v);
+    int X[3];
+    vpos(C, k, v - C.base[k], X[0], X[1], X[2]);
+    const float pr = (float)(r0 * r1 * r2);
+    for (int d = 0; d < 27; d++) {
+        const int dj[3] = {r0 * (d % 3 - 1), r1 * (d / 3 % 3 - 1), r2 * (d / 9 - 1)};
+        float s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+        for (int fx = -r0; fx <= r0; fx++)
+            for (int fy = -r1; fy <= r1; fy++)
+                for (int fz = -r2; fz <= r2; fz++) {
+                    const int oi[3] = {fx + dj[0], fy + dj[1], fz + dj[2]};
+                    if (!(oi[0] > -r0 && oi[0] < r0 && oi[1] > -r1 && oi[1] < r1 && oi[2] > -r2 && oi[2] < r2)) continue;
+                    const long long fv = vidx(F, modp(X[0] * r0 + oi[0], F.n[0]), modp(X[1] * r1 + oi[1], F.n[1]),
+                                              modp(X[2] * r2 + oi[2], F.n[2]));
+                    const float wi = (float)((r0 - abs(oi[0])) * (r1 - abs(oi[1])) * (r2 - abs(oi[2]))) / pr;
+                    for (int j = 0; j < 27; j++) {
+                        const int o0 = abs(oi[0] + j % 3 - 1 - dj[0]), o1 = abs(oi[1] + j / 3 % 3 - 1 - dj[1]),
+                                  o2 = abs(oi[2] + j / 9 - 1 - dj[2]);
+                        if (o0 >= r0 || o1 >= r1 || o2 >= r2) continue;
+                        const float wj = (float)((r0 - o0) * (r1 - o1) * (r2 - o2)) / pr;
+                        const float ww = wi * wj;
+#pragma unroll
+                        for (int e = 0; e < 9; e++) s[e] = fmaf(ww, get_half(fst, F.nv, fv, 9 * j + e), s[e]);
+                    }
+                }
+        if (d == 13)
+            for (int t = 0; t < 3; t++)
+                if (fabsf(s[4 * t]) < 1e-4f) s[4 * t] = 1e-4f;
+        for (int e = 0; e < 9; e++) put_half(cst, C.nv, v, 9 * d + e, __float2half_rn(s[e]));
+    }
+}
+
+void launch_galerkin(const Level &F, const Level &C, cudaStream_t s) {
+    const int bs = 128;
+    k_galerkin<<<(unsigned)((C.P.nv + bs - 1) / bs), bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.st,
+                                                                  C.st);
+}
+
+// ---- coarsest level ---------------------------------------------------------------
+// aug: [n][2n] row-major, left = K over unique DOFs (3*lexid + comp), right = I
+__global__ void k_coarse_assemble(Planes C, const uint4 *__restrict__ st, double *aug, int n) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= C.nv * 27) return;
+    const long long lex = t / 27;
+    const int d = (int)(t % 27);
+    const int x = (int)(lex % C.n[0]);
+    const int y = (int)((lex / C.n[0]) % C.n[1]), z = (int)(lex / ((long long)C.n[0] * C.n[1]));
+    const long long v = vidx(C, x, y, z);
+    const int wx = wrap(x + d % 3 - 1, C.n[0]), wy = wrap(y + d / 3 % 3 - 1, C.n[1]), wz = wrap(z + d / 9 - 1, C.n[2]);
+    const long long w = wx + (long long)C.n[0] * (wy + (long long)C.n[1] * wz);
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++)
+            atomicAdd(&aug[(3 * lex + i) * (2LL * n) + 3 * w + j], (double)get_half(st, C.nv, v, 9 * d + 3 * i + j));
+    if (d == 0)
+        for (int i = 0; i < 3; i++) aug[(3 * lex + i) * (2LL * n) + n + 3 * lex + i] = 1.0;
+}
+
+void launch_coarse_assemble(const Level &C, double *aug, cudaStream_t s) {
+    const int n = (int)(3 * C.P.nv);
+    cudaMemsetAsync(aug, 0, sizeof(double) * (size_t)n * 2 * n, s);
+    const long long nt = C.P.nv * 27;
+    k_coarse_assemble<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(C.P, C.st, aug, n);
+}
+
+// single-CTA Gauss-Jordan elimination with partial pivoting on [K | I]
+__global__ void __launch_bounds__(1024) k_gauss_jordan(double *a, int n, int *flag) {
+    extern __shared__ double col[];  // n factors
+    __shared__ double rmax[32];
+    __shared__ int ridx[32];
+    __shared__ int piv;
+    const int tid = threadIdx.x, nt = blockDim.x, m = 2 * n;
+    for (int k = 0; k < n; k++) {
+        // pivot search over rows k..n-1
+        double best = -1.0;
+        int bi = k;
+        for (int i = k + tid; i < n; i += nt) {
+            const double v = fabs(a[(long long)i * m + k]);
+            if (v > best) { best = v; bi = i; }
+        }
+        for (int o = 16; o > 0; o >>= 1) {
+            const double ob = __shfl_down_sync(0xffffffffu, best, o);
+            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+            if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+        }
+        if ((tid & 31) == 0) { rmax[tid >> 5] = best; ridx[tid >> 5] = bi; }
+        __syncthreads();
+        if (tid == 0) {
+            double b = -1.0;
+            int p = k;
+            for (int w = 0; w < (nt + 31) / 32; w++)
+                if (rmax[w] > b || (rmax[w] == b && ridx[w] < p)) { b = rmax[w]; p = ridx[w]; }
+            piv = p;
+            if (!(b > 0.0)) *flag = 1;
+        }
+        __syncthreads();
+        const int p = piv;
+        if (p != k)
+            for (int j = tid; j < m; j += nt) {
+                const double t = a[(long long)k * m + j];
+                a[(long long)k * m + j] = a[(long long)p * m + j];
+                a[(long long)p * m + j] = t;
+            }
+        __syncthreads();
+        const double inv = 1.0 / a[(long long)k * m + k];
+        __syncthreads();
+        for (int j = tid; j < m; j += nt) a[(long long)k * m + j] *= inv;
+        for (int i = tid; i < n; i += nt) col[i] = (i == k) ? 0.0 : a[(long long)i * m + k];
+        __syncthreads();
+        const long long total = (long long)n * (m - k);
+        for (long long t = tid; t < total; t += nt) {
+            const int i = (int)(t / (m - k)), j = k + (int)(t % (m - k));
+            if (i != k) a[(long long)i * m + j] -= col[i] * a[(long long)k * m + j];
+        }
+        __syncthreads();
+    }
+}
+
+void launch_gauss_jordan(double *aug, int n, int *flag, cudaStream_t s) {
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
+        attr = true;
+    }
+    k_gauss_jordan<<<1, 1024, (size_t)n * sizeof(double), s>>>(aug, n, flag);
+}
+
+// one block per load case: b (optionally minus its mean per component), x = K^-1 b
+__global__ void __launch_bounds__(256) k_coarse_apply(Planes C, const double *__restrict__ aug, int n, int project,
+                                                      const float *__restrict__ f, float *u) {
+    extern __shared__ double b[];
+    __shared__ double mean[3];
+    const int c = blockIdx.x;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const long long lex = i / 3;
+        const int comp = i % 3;
+        const int x = (int)(lex % C.n[0]), y = (int)((lex / C.n[0]) % C.n[1]), z = (int)(lex / ((long long)C.n[0] * C.n[1]));
+        b[i] = f[(3 * c + comp) * C.nv + vidx(C, x, y, z)];
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        double s = 0;
+        if (project)
+            for (int i = threadIdx.x; i < n; i += 3) s += b[i];
+        mean[threadIdx.x] = s / (double)(n / 3);
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) b[i] -= mean[i % 3];
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double *row = aug + (long long)i * 2 * n + n;
+        double s = 0;
+        for (int j = 0; j < n; j++) s = fma(row[j], b[j], s);
+        const long long lex = i / 3;
+        const int comp = i % 3;
+        const int x = (int)(lex % C.n[0]), y = (int)((lex / C.n[0]) % C.n[1]), z = (int)(lex / ((long long)C.n[0] * C.n[1]));
+        u[(3 * c + comp) * C.nv + vidx(C, x, y, z)] = (float)s;
+    }
+}
+
+void launch_coarse_apply(const Level &C, const double *aug, int project, cudaStream_t s) {
+    const int n = (int)(3 * C.P.nv);
+    k_coarse_apply<<<NCASE, 256, (size_t)n * sizeof(double), s>>>(C.P, aug, n, project, C.f, C.u);
+}
+
+}  // namespace h3d

@@ -1,0 +1,154 @@
+/*
+ * h3d.h -- C ABI of the B200 periodic-homogenization solver (libh3d.so).
+ *
+ * The library replaces the hot path of lavenklau/homo3d: the multigrid grid
+ * operations, the V-cycle, the homogenized elastic tensor and its sensitivities,
+ * and the OC design update.  Every entry point returns an h3d_status; none
+ * exits, throws or prints.  Device pointers passed in are owned by the caller;
+ * all solver memory is owned by the handle.  Calls on one handle are ordered on
+ * the handle's CUDA stream; calls that return host data synchronise that stream.
+ * Distinct handles are independent and may be used from different threads.
+ *
+ * Data formats at this boundary
+ *   density / sensitivity : float, lexicographic cell order, element (x,y,z) at
+ *                           x + (y + z*ny)*pitchT  (pitchT >= nx; -1 means nx)
+ *   vertex fields         : float [6][nz][ny][nx][3]  (load case, vertex, comp)
+ *   stencils              : float [nz][ny][nx][27][9], neighbour d = (dx+1) +
+ *                           3(dy+1) + 9(dz+1), entry 3*row + col
+ *   elastic tensor C      : double[36] row-major, Voigt order xx yy zz yz xz xy
+ *                           with engineering shear strains
+ */
+#ifndef H3D_H
+#define H3D_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define H3D_API __attribute__((visibility("default")))
+#else
+#define H3D_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct h3d_handle h3d_handle;
+
+typedef enum {
+    H3D_OK = 0,
+    H3D_ERR_ARG = 1,          /* invalid argument or unsupported size */
+    H3D_ERR_CUDA = 2,         /* a CUDA call failed; see h3d_last_error */
+    H3D_ERR_NOMEM = 3,        /* device allocation failed */
+    H3D_NOT_CONVERGED = 4,    /* iteration cap reached above the tolerance */
+    H3D_DIVERGED = 5,         /* relative residual above 10 twice, or NaN */
+    H3D_ERR_STATE = 6,        /* call order violated (e.g. solve before density) */
+    H3D_ERR_SINGULAR = 7      /* coarsest-grid matrix could not be inverted */
+} h3d_status;
+
+/* how the coarsest-grid right-hand side is treated before the dense solve */
+typedef enum {
+    H3D_COARSE_EXACT = 0,       /* solve the pinned Galerkin system as is */
+    H3D_COARSE_PROJECT = 1      /* first remove the mean (rigid translations) */
+} h3d_coarse_mode;
+
+/* how the pinned origin vertex enters the level-1 Galerkin operator */
+typedef enum {
+    H3D_PIN_IDENTITY = 0,       /* identity block at the pinned node, as the reference does */
+    H3D_PIN_GALERKIN = 1        /* exact Galerkin product of the pinned fine operator */
+} h3d_pin_mode;
+
+typedef struct {
+    int reso[3];                /* requested cells per axis; corrected like the reference */
+    double youngs_modulus;      /* E of the base material */
+    double poisson_ratio;       /* nu of the base material */
+    int coarse_mode;            /* h3d_coarse_mode */
+    int pin_mode;               /* h3d_pin_mode */
+    int device;                 /* CUDA device ordinal */
+} h3d_config;
+
+typedef struct {
+    int vcycles;                /* V-cycles run (max over the active load cases) */
+    int status;                 /* h3d_status of the solve */
+    double rel_res[6];          /* final ||r||/||f|| per load case */
+    double solve_ms;            /* device time of the V-cycle loop */
+} h3d_solve_stats;
+
+/* fields addressable through h3d_get_field / h3d_set_field */
+typedef enum {
+    H3D_FIELD_U = 0,            /* displacement */
+    H3D_FIELD_F = 1,            /* right-hand side */
+    H3D_FIELD_R = 2,            /* residual */
+    H3D_FIELD_STENCIL = 3,      /* coarse-level stencil (levels >= 1) */
+    H3D_FIELD_CHI = 4           /* stored solutions of the six cases (level 0) */
+} h3d_field;
+
+/* ---- lifetime (homogenization.cpp:40-66 Homogenization::build) ---------- */
+H3D_API int h3d_create(const h3d_config *cfg, h3d_handle **out);
+H3D_API int h3d_destroy(h3d_handle *h);
+H3D_API const char *h3d_last_error(const h3d_handle *h);
+H3D_API int h3d_sync(h3d_handle *h);
+/* the handle's CUDA stream (cudaStream_t) for callers that order their own work */
+H3D_API void *h3d_stream(h3d_handle *h);
+
+/* ---- hierarchy queries (grid.cpp:21-151 buildRoot / coarse2) -------------- */
+H3D_API int h3d_num_levels(const h3d_handle *h);
+H3D_API int h3d_level_dims(const h3d_handle *h, int level, int dims[3], int ratio[3]);
+/* the 24x24 element matrix in double, row-major (templateMatrix.cpp:95-201) */
+H3D_API int h3d_element_matrix(const h3d_handle *h, double ke[576]);
+
+/* ---- design input (homogenization.cpp:79-85 Homogenization::update) ------- */
+/* rho_dev: physical density rho^p on the device (grid.cu:4208-4240 Grid::update) */
+H3D_API int h3d_update_density(h3d_handle *h, const float *rho_dev, int pitchT);
+/* Galerkin coarse operators + coarsest factorisation (MG.cpp:341-354) */
+H3D_API int h3d_update_stencils(h3d_handle *h);
+/* one coarse level's stencil from the next finer level (grid.cu:2383-2439);
+ * coarse_level 1 is built from the densities */
+H3D_API int h3d_restrict_stencil(h3d_handle *h, int coarse_level);
+/* dense inverse of the coarsest-level operator (grid.cpp:385-424) */
+H3D_API int h3d_factor_coarsest(h3d_handle *h);
+
+/* ---- grid entry points, all six load cases at once (grid.h:225-275) ------ */
+H3D_API int h3d_enforce_unit_macro_strain(h3d_handle *h);            /* grid.cu:1921 */
+H3D_API int h3d_gs_relaxation(h3d_handle *h, int level, float w, int times); /* grid.cu:1192 */
+H3D_API int h3d_update_residual(h3d_handle *h, int level);           /* grid.cu:1566 */
+H3D_API int h3d_restrict_residual(h3d_handle *h, int coarse_level);  /* grid.cu:1257 */
+H3D_API int h3d_prolongate_correction(h3d_handle *h, int fine_level);/* grid.cu:1238 */
+H3D_API int h3d_coarse_solve(h3d_handle *h);                         /* grid.cpp:349 */
+H3D_API int h3d_reset_displacement(h3d_handle *h, int level);        /* grid.h:246; -1 = all */
+/* per-case norm of a level-0 field with the reference's padded-storage
+ * multiplicities (grid.cu:1954-1966 v3_norm) */
+H3D_API int h3d_field_norms(h3d_handle *h, int field, double out[6]);
+
+/* ---- multigrid (MG.cpp:46-203) ------------------------------------------- */
+H3D_API int h3d_v_cycle(h3d_handle *h, float w, int pre, int post);
+/* V-cycles until every case in case_mask has ||r||/||f|| <= tol; with_guess = 0
+ * starts from zero (MG::solveEquation) */
+H3D_API int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solve_stats *stats);
+
+/* ---- homogenization (homogenization.cu:464-948) -------------------------- */
+/* the six solves (warm-started from the previous design's solutions, mean
+ * removed) followed by C; tol is the relative residual threshold */
+H3D_API int h3d_elastic_matrix(h3d_handle *h, double tol, double C[36], h3d_solve_stats *stats);
+/* sens = d obj / d rho_phys from dC = d obj / d C (float[36] row-major) */
+H3D_API int h3d_sensitivity(h3d_handle *h, const float dC[36], float *sens_dev, int pitchT);
+/* forget the stored solutions (warm start) */
+H3D_API int h3d_reset_solutions(h3d_handle *h);
+
+/* ---- design update (OCOptimizer.cu:38-247, TensorExpression.cuh:72-) ----- */
+H3D_API int h3d_oc_update(h3d_handle *h, const float *sens_dev, float *rho_dev, int64_t n, float volratio,
+                  float min_rho, float step_limit, float damp);
+H3D_API int h3d_oc_filter(h3d_handle *h, float *sens_dev, const float *rho_dev, const int reso[3], int pitchT,
+                  float radius, int periodic);
+/* sym: 0 reflect3, 1 reflect6, 2 rotate3; lexicographic, pitch nx */
+H3D_API int h3d_symmetrize(h3d_handle *h, float *field_dev, const int reso[3], int sym);
+
+/* ---- data exchange (host pointers) ---------------------------------------- */
+H3D_API int h3d_get_field(h3d_handle *h, int level, int field, float *host);
+H3D_API int h3d_set_field(h3d_handle *h, int level, int field, const float *host);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* H3D_H */

@@ -1,0 +1,170 @@
+"""GPU end-to-end parity: solves, homogenized tensor, sensitivities, design update
+and symmetrisation against the FP64 oracle; error paths of the C ABI."""
+import numpy as np
+import pytest
+
+import homo3d_b200 as H
+from oracle import oracle as O
+from tests.conftest import smooth_density
+from tests.test_gpu_parity import make_pair, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def oracle_C(n, rho, tol=1e-10, **kw):
+    m = O.MG((n, n, n))
+    m.set_density(rho.astype(np.float32).astype(np.float64))
+    if kw.get("pin_mode", 0) == H.PIN_GALERKIN:
+        m.set_pin_identity(False)
+    m.update_stencils()
+    m.rhs()
+    m.solve(tol, 400)
+    return m
+
+
+@pytest.mark.parametrize("pin", [H.PIN_IDENTITY, H.PIN_GALERKIN])
+def test_elastic_matrix_1e5_matches_fp64(torch_cuda, pin):
+    """relthres 1e-5: C within 1e-4 relative of the FP64 oracle solved to 1e-10"""
+    n = 32
+    hd, _, t = make_pair(torch_cuda, n=n, seed=11, pin_mode=pin)
+    C = hd.elasticMatrix(1e-5)
+    st = hd.last_stats
+    assert st["status"] == H.H3D_OK and max(st["rel_res"]) <= 1e-5
+    m = oracle_C(n, smooth_density(n, seed=11), pin_mode=pin)
+    Cref = m.elastic_matrix()
+    assert rel_err(C, Cref) < 1e-4
+    assert np.abs(C - C.T).max() == 0
+
+
+def test_config1_32cube_relthres_1e2(torch_cuda):
+    """32^3, relthres 1e-2, zero start: C and sensitivities against the FP64 oracle at the
+    same number of V-cycles (the quantities the reference reports at this setting)"""
+    n = 32
+    hd, m, t = make_pair(torch_cuda, n=n, seed=0)
+    C = hd.elasticMatrix(1e-2)
+    k = hd.last_stats["vcycles"]
+    m.update_stencils()
+    m.rhs()
+    it, _ = m.solve(1e-2, 200)
+    assert abs(it - k) <= 1
+    Cref = m.elastic_matrix()
+    assert rel_err(C, Cref) < 5e-3
+    dC = np.zeros((6, 6), np.float32)
+    dC[0, 0] = dC[1, 1] = dC[2, 2] = -1 / 3.0
+    dC[0, 1] = dC[0, 2] = dC[1, 2] = -2 / 3.0
+    sens = torch_cuda.zeros(n ** 3, dtype=torch_cuda.float32, device="cuda")
+    hd.Sensitivity(dC, sens)
+    chi = hd.grid.get(H.FIELD_CHI)
+    s_ref = m.sensitivity(dC.astype(np.float64), chi=np.transpose(chi, (1, 0, 2)).astype(np.float64))
+    assert rel_err(sens.cpu().numpy().astype(np.float64), s_ref) < 2e-5
+
+
+def test_vcycle_counts_match_oracle(torch_cuda):
+    n = 32
+    hd, m, _ = make_pair(torch_cuda, n=n, seed=2)
+    hd.elasticMatrix(1e-5)
+    k = hd.last_stats["vcycles"]
+    m.update_stencils()
+    m.rhs()
+    it, _ = m.solve(1e-5, 200)
+    assert abs(it - k) <= 1, (it, k)
+
+
+def test_sensitivity_pitched_output(torch_cuda):
+    n = 16
+    hd, m, _ = make_pair(torch_cuda, n=n, seed=6)
+    hd.elasticMatrix(1e-6)
+    dC = np.random.default_rng(1).standard_normal((6, 6)).astype(np.float32)
+    pitch = 24
+    sens = torch_cuda.full((n * n * pitch,), 7.0, dtype=torch_cuda.float32, device="cuda")
+    hd.Sensitivity(dC, sens, pitch)
+    chi = np.transpose(hd.grid.get(H.FIELD_CHI), (1, 0, 2)).astype(np.float64)
+    m.update_stencils()
+    ref = m.sensitivity(dC.astype(np.float64), chi=chi, pitch=pitch)
+    got = sens.cpu().numpy().astype(np.float64)
+    assert rel_err(got, ref) < 2e-5
+    assert np.all(got.reshape(n, n, pitch)[:, :, n:] == 0)  # padding zeroed like the reference
+
+
+def test_warm_start_reuses_solutions(torch_cuda):
+    n = 16
+    hd, _, t = make_pair(torch_cuda, n=n, seed=8)
+    C1 = hd.elasticMatrix(1e-6)
+    k1 = hd.last_stats["vcycles"]
+    C2 = hd.elasticMatrix(1e-6)
+    k2 = hd.last_stats["vcycles"]
+    assert k2 < k1 and k2 <= 2
+    assert rel_err(C2, C1) < 1e-5
+
+
+def test_handles_are_independent(torch_cuda):
+    a, _, _ = make_pair(torch_cuda, n=16, seed=1)
+    b, _, _ = make_pair(torch_cuda, n=16, seed=2)
+    Ca = a.elasticMatrix(1e-6)
+    Cb = b.elasticMatrix(1e-6)
+    Ca2 = a.elasticMatrix(1e-6)
+    assert rel_err(Ca2, Ca) < 1e-5 and rel_err(Ca, Cb) > 1e-3
+
+
+def test_oc_update_matches_oracle(torch_cuda):
+    n = 32
+    rng = np.random.default_rng(3)
+    rho = np.clip(rng.random(n ** 3), 1e-3, 1).astype(np.float32)
+    sens = (-rng.random(n ** 3) * 2).astype(np.float32)
+    hd = H.Homogenization(16)
+    tr = torch_cuda.tensor(rho, device="cuda")
+    ts = torch_cuda.tensor(sens, device="cuda")
+    oc = H.OCOptimizer(n ** 3, 1e-3, 0.05, 0.5, handle=hd)
+    oc.update(ts, tr, 0.3)
+    got = tr.cpu().numpy()
+    ref, _ = O.oc_update(sens.astype(np.float64), rho.astype(np.float64), 0.3, 1e-3, 0.05, 0.5)
+    assert np.abs(got - ref).max() < 1e-5
+    assert abs(got.astype(np.float64).mean() - 0.3) <= 1.1e-4
+
+
+@pytest.mark.parametrize("periodic", [0, 1])
+def test_filter_matches_oracle(torch_cuda, periodic):
+    n = 20
+    rng = np.random.default_rng(4)
+    rho = np.clip(rng.random(n ** 3), 1e-3, 1).astype(np.float32)
+    sens = rng.standard_normal(n ** 3).astype(np.float32)
+    hd = H.Homogenization(16)
+    tr = torch_cuda.tensor(rho, device="cuda")
+    ts = torch_cuda.tensor(sens, device="cuda")
+    H.OCOptimizer(n ** 3, handle=hd).filterSens(ts, tr, n, (n, n, n), 2.0, bool(periodic))
+    ref = O.filter_sens((n, n, n), sens.astype(np.float64), rho.astype(np.float64), 2.0, periodic)
+    assert rel_err(ts.cpu().numpy().astype(np.float64), ref) < 1e-5
+
+
+@pytest.mark.parametrize("sym", ["reflect3", "reflect6", "rotate3"])
+@pytest.mark.parametrize("n", [8, 16, 30])
+def test_symmetrize_bit_exact(torch_cuda, sym, n):
+    rng = np.random.default_rng(n)
+    v = rng.standard_normal(n ** 3).astype(np.float32)
+    hd = H.Homogenization(8)
+    t = torch_cuda.tensor(v, device="cuda")
+    H.symmetrize(hd, t, (n, n, n), sym)
+    ref = O.symmetrize_f32((n, n, n), v, sym)
+    assert np.array_equal(t.cpu().numpy(), ref)
+
+
+def test_error_paths(torch_cuda):
+    with pytest.raises(H.H3DError) as e:
+        H.Homogenization(4)          # a single grid level
+    assert e.value.code == H.H3D_ERR_ARG
+    with pytest.raises(H.H3DError):
+        H.Homogenization(16, nu=0.5)
+    hd = H.Homogenization(16)
+    with pytest.raises(H.H3DError) as e:
+        hd.elasticMatrix(1e-2)       # no density yet
+    assert e.value.code == H.H3D_ERR_STATE
+    with pytest.raises(H.H3DError) as e:
+        hd.mg.grids[hd.nlevels - 1].gs_relaxation()
+    assert e.value.code == H.H3D_ERR_ARG
+    t = torch_cuda.ones(16 ** 3, device="cuda")
+    with pytest.raises(H.H3DError) as e:
+        hd.update(t, pitchT=8)
+    assert e.value.code == H.H3D_ERR_ARG
+    hd.update(t)
+    C = hd.elasticMatrix(1e-6)
+    assert np.abs(C - C.T).max() == 0

@@ -1,0 +1,118 @@
+"""GPU parity of the Galerkin coarse operators, coarse sweeps, transfers and the
+coarsest solve against the FP64 oracle (fed the library's own FP16 stencils
+where a kernel consumes them, so that only the arithmetic differs)."""
+import numpy as np
+import pytest
+
+import homo3d_b200 as H
+from oracle import oracle as O
+from tests.conftest import from_lib_field, half_ulp, random_field, to_lib_field
+from tests.test_gpu_parity import copy_stencils_to_oracle, make_pair, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def stencil_close(got, ref, ulps=4):
+    tol = ulps * half_ulp(ref) + 1e-7
+    bad = np.abs(got - ref) > tol
+    return int(bad.sum()), float(np.abs(got - ref).max())
+
+
+@pytest.mark.parametrize("n,pin", [(8, 0), (16, 0), (32, 0), (16, 1)])
+def test_level1_stencil(torch_cuda, n, pin):
+    hd, m, _ = make_pair(torch_cuda, n=n, seed=n, pin_mode=pin)
+    m.galerkin_l1(1)
+    got = hd.mg.grids[1].get(H.FIELD_STENCIL)
+    nbad, mx = stencil_close(got, m.stencil(1))
+    assert nbad == 0, (nbad, mx)
+
+
+def test_level1_stencil_reference_loop_nest(torch_cuda):
+    """the oracle's literal restatement of the reference kernel, not its refactoring"""
+    hd, m, _ = make_pair(torch_cuda, n=8, seed=7)
+    m.galerkin_l1(0)
+    nbad, mx = stencil_close(hd.mg.grids[1].get(H.FIELD_STENCIL), m.stencil(1))
+    assert nbad == 0, (nbad, mx)
+
+
+@pytest.mark.parametrize("n", [16, 32])
+def test_deeper_stencils(torch_cuda, n):
+    hd, m, _ = make_pair(torch_cuda, n=n, seed=1)
+    for l in range(2, hd.nlevels):
+        m.stencil(l - 1)[:] = hd.mg.grids[l - 1].get(H.FIELD_STENCIL).astype(np.float64)
+        m.galerkin(l)
+        nbad, mx = stencil_close(hd.mg.grids[l].get(H.FIELD_STENCIL), m.stencil(l))
+        assert nbad == 0, (l, nbad, mx)
+
+
+def test_coarse_gs_and_residual(torch_cuda):
+    n = 32
+    hd, m, _ = make_pair(torch_cuda, n=n, seed=2)
+    copy_stencils_to_oracle(hd, m)
+    for l in range(1, hd.nlevels - 1):
+        g = hd.mg.grids[l]
+        nv = hd.nv(l)
+        u0, f0 = random_field(nv, 10 + l), random_field(nv, 20 + l)
+        g.set(H.FIELD_U, to_lib_field(u0))
+        g.set(H.FIELD_F, to_lib_field(f0))
+        m.u(l)[:] = from_lib_field(to_lib_field(u0))
+        m.f(l)[:] = from_lib_field(to_lib_field(f0))
+        g.gs_relaxation(1.0)
+        m.gs(l, 1.0)
+        assert rel_err(from_lib_field(g.get(H.FIELD_U)), m.u(l)) < 2e-5
+        g.update_residual()
+        m.residual(l)
+        assert rel_err(from_lib_field(g.get(H.FIELD_R)), m.r(l)) < 2e-5
+
+
+def test_restrict_and_prolong(torch_cuda):
+    n = 32
+    hd, m, _ = make_pair(torch_cuda, n=n, seed=3)
+    for l in range(1, hd.nlevels):
+        gf, gc = hd.mg.grids[l - 1], hd.mg.grids[l]
+        r0 = random_field(hd.nv(l - 1), 30 + l)
+        gf.set(H.FIELD_R, to_lib_field(r0))
+        m.r(l - 1)[:] = from_lib_field(to_lib_field(r0))
+        gc.restrict_residual()
+        m.restrict(l)
+        assert rel_err(from_lib_field(gc.get(H.FIELD_F)), m.f(l)) < 2e-6
+        uc, uf = random_field(hd.nv(l), 40 + l), random_field(hd.nv(l - 1), 50 + l)
+        gc.set(H.FIELD_U, to_lib_field(uc))
+        gf.set(H.FIELD_U, to_lib_field(uf))
+        m.u(l)[:] = from_lib_field(to_lib_field(uc))
+        m.u(l - 1)[:] = from_lib_field(to_lib_field(uf))
+        gf.prolongate_correction()
+        m.prolong(l - 1)
+        got = from_lib_field(gf.get(H.FIELD_U))
+        assert rel_err(got, m.u(l - 1)) < 2e-6
+        if l == 1:
+            assert np.all(got[0] == to_lib_field(uf)[:, 0].astype(np.float64))  # pinned origin untouched
+
+
+@pytest.mark.parametrize("coarse_mode", [H.COARSE_EXACT, H.COARSE_PROJECT])
+def test_coarsest_solve(torch_cuda, coarse_mode):
+    n = 16
+    hd, m, _ = make_pair(torch_cuda, n=n, seed=4, coarse_mode=coarse_mode)
+    copy_stencils_to_oracle(hd, m)
+    L = hd.nlevels - 1
+    g = hd.mg.grids[L]
+    f0 = random_field(hd.nv(L), 60)
+    g.set(H.FIELD_F, to_lib_field(f0))
+    m.f(L)[:] = from_lib_field(to_lib_field(f0))
+    g.solveHostEquation()
+    m.coarse_solve()
+    assert rel_err(from_lib_field(g.get(H.FIELD_U)), m.u(L)) < 1e-5
+
+
+def test_vcycle_matches_oracle(torch_cuda):
+    n = 32
+    hd, m, _ = make_pair(torch_cuda, n=n, seed=5)
+    copy_stencils_to_oracle(hd, m)
+    hd.grid.enforce_unit_macro_strain()
+    m.rhs()
+    hd.mg.reset_displacement()
+    for it in range(3):
+        hd.mg.v_cycle()
+        m.vcycle(1.0)
+        u = from_lib_field(hd.grid.get(H.FIELD_U))
+        assert rel_err(u, m.u()) < 5e-5, it
