@@ -30,9 +30,10 @@ LIB_PATH = os.path.join(_HERE, "lib", "libh3d.so")
 
 H3D_OK, H3D_ERR_ARG, H3D_ERR_CUDA, H3D_ERR_NOMEM, H3D_NOT_CONVERGED, H3D_DIVERGED, H3D_ERR_STATE, \
     H3D_ERR_SINGULAR = range(8)
-FIELD_U, FIELD_F, FIELD_R, FIELD_STENCIL, FIELD_CHI = range(5)
+FIELD_U, FIELD_F, FIELD_R, FIELD_STENCIL, FIELD_CHI, FIELD_SOLUTION = range(6)
 COARSE_EXACT, COARSE_PROJECT = 0, 1
 PIN_IDENTITY, PIN_GALERKIN = 0, 1
+PREC_REFINE, PREC_FP32 = 0, 1
 SYMMETRY = {"reflect3": 0, "reflect6": 1, "rotate3": 2}
 
 _STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "not converged",
@@ -48,7 +49,7 @@ class H3DError(RuntimeError):
 class Config(ctypes.Structure):
     _fields_ = [("reso", ctypes.c_int * 3), ("youngs_modulus", ctypes.c_double),
                 ("poisson_ratio", ctypes.c_double), ("coarse_mode", ctypes.c_int), ("pin_mode", ctypes.c_int),
-                ("device", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("device", ctypes.c_int)]
 
 
 class SolveStats(ctypes.Structure):
@@ -126,6 +127,9 @@ def _ptr(x):
             raise ValueError("expected a CUDA tensor")
         if not x.is_contiguous():
             raise ValueError("expected a contiguous tensor")
+        # the handle's stream does not wait on torch's: finish the tensor's producers first
+        import torch
+        torch.cuda.current_stream(x.device).synchronize()
         return ctypes.c_void_p(x.data_ptr())
     raise TypeError("expected a CUDA tensor or a device pointer")
 
@@ -146,11 +150,14 @@ def reference_resolution(reso):
 
 
 class _Handle:
-    def __init__(self, reso, E=10.0, nu=0.3, coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY, device=0):
+    def __init__(self, reso, E=10.0, nu=0.3, coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY,
+                 precision=PREC_REFINE, device=0):
         L = lib()
         if isinstance(reso, int):
             reso = (reso, reso, reso)
-        cfg = Config((ctypes.c_int * 3)(*reso), float(E), float(nu), int(coarse_mode), int(pin_mode), int(device))
+        cfg = Config((ctypes.c_int * 3)(*reso), float(E), float(nu), int(coarse_mode), int(pin_mode),
+                     int(precision), int(device))
+        self.precision = precision
         h = ctypes.c_void_p()
         code = L.h3d_create(ctypes.byref(cfg), ctypes.byref(h))
         if code != H3D_OK:
@@ -277,8 +284,9 @@ class MG:
 class Homogenization(_Handle):
     """Homogenized elastic tensor of a periodic unit cell (homogenization.h:17-61)."""
 
-    def __init__(self, reso, E=10.0, nu=0.3, coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY, device=0):
-        super().__init__(reso, E, nu, coarse_mode, pin_mode, device)
+    def __init__(self, reso, E=10.0, nu=0.3, coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY,
+                 precision=PREC_REFINE, device=0):
+        super().__init__(reso, E, nu, coarse_mode, pin_mode, precision, device)
         self.mg = MG(self)
         self.grid = self.mg.grids[0]
         self.last_stats = None
@@ -307,6 +315,7 @@ class Homogenization(_Handle):
     def Sensitivity(self, dC, sens, pitchT=-1):
         d = np.ascontiguousarray(dC, dtype=np.float32).reshape(36)
         self.check(lib().h3d_sensitivity(self._h, d.ctypes.data_as(_fp), _ptr(sens), int(pitchT)))
+        self.sync()  # the caller's buffer is read on other streams
 
     def reset_solutions(self):
         self.check(lib().h3d_reset_solutions(self._h))
@@ -333,12 +342,15 @@ class OCOptimizer:
         hd = self._handle()
         hd.check(lib().h3d_oc_update(hd._h, _ptr(sens), _ptr(rho), self.ne, volratio, self.minRho,
                                      self.step_limit, self.damp))
+        hd.sync()
 
     def filterSens(self, sens, rho, pitchT, reso, radius=2.0, periodic=False):
         hd = self._handle()
         hd.check(lib().h3d_oc_filter(hd._h, _ptr(sens), _ptr(rho), _i3(reso), int(pitchT), radius, int(periodic)))
+        hd.sync()
 
 
 def symmetrize(handle, field, reso, sym="reflect6"):
     """Orbit-average a lexicographic CUDA field in place (TensorExpression.h:425-445)."""
     handle.check(lib().h3d_symmetrize(handle._h, _ptr(field), _i3(reso), SYMMETRY[sym]))
+    handle.sync()

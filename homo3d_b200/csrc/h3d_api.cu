@@ -147,7 +147,9 @@ struct h3d_handle {
     std::vector<float> qhost;
     int nsub = 0;
     float *rho = nullptr;       // physical density on level 0
-    float *chi = nullptr;       // stored solutions [18][nv0]
+    double *chi = nullptr;      // stored solutions [18][nv0], FP64
+    double *u64 = nullptr;      // level-0 solution in the refined mode [18][nv0]
+    float *f0 = nullptr;        // level-0 right-hand side of the refined mode [18][nv0]
     float *q = nullptr;         // level-1 Galerkin sub-element matrices
     double *d_ked = nullptr;
     double *aug = nullptr;      // coarsest [K | K^-1]
@@ -160,8 +162,10 @@ struct h3d_handle {
     float *tmp = nullptr;       // conversion / filter scratch
     size_t tmp_n = 0;
     cudaStream_t stream = nullptr;
-    cudaGraphExec_t vgraph = nullptr;
+    cudaGraphExec_t vgraph = nullptr;   // one V-cycle on the level-0 field u
+    cudaGraphExec_t rgraph = nullptr;   // one refinement cycle on u64
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    bool refine() const { return cfg.precision == H3D_PREC_REFINE; }
     bool have_density = false, have_stencils = false;
     std::string err;
 };
@@ -231,14 +235,21 @@ void build_q(const double ke[576], const int r[3], std::vector<float> &q, int &n
 
 int destroy_graph(h3d_handle *h) {
     if (h->vgraph) { cudaGraphExecDestroy(h->vgraph); h->vgraph = nullptr; }
+    if (h->rgraph) { cudaGraphExecDestroy(h->rgraph); h->rgraph = nullptr; }
     return H3D_OK;
 }
 
 // the V-cycle of MG::v_cycle (MG.cpp:46-70) on the handle's stream; the level-0
-// residual of the down leg also yields the per-case norms
-int enqueue_vcycle(h3d_handle *h, float w) {
+// residual of the down leg also yields the per-case norms.  With refine, the
+// cycle runs on the correction: level-0 f = f0 - K u64 (FP64-exact), u = 0 before
+// and u64 += u after (in exact arithmetic the same iterate as sweeping u64).
+int enqueue_vcycle(h3d_handle *h, float w, bool refine = false) {
     cudaStream_t s = h->stream;
     const int nblk_r = (int)(((h->lv[0].P.nv / 8) + 127) / 128) * 8;
+    if (refine) {
+        launch_fine_residual64(h->lv[0], h->rho, h->ke, h->f0, h->u64, h->lv[0].f, s);
+        cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * NF * h->lv[0].P.nv, s);
+    }
     for (int l = 0; l < h->nl; l++) {
         if (l > 0) {
             if (l - 1 == 0) launch_fine_residual(h->lv[0], h->rho, h->ke, h->partial, nblk_r, s);
@@ -255,20 +266,22 @@ int enqueue_vcycle(h3d_handle *h, float w) {
         if (l == 0) launch_fine_gs(h->lv[0], h->rho, h->ke, w, s);
         else launch_coarse_gs(h->lv[l], w, s);
     }
+    if (refine) launch_update64((long long)NF * h->lv[0].P.nv, h->u64, h->lv[0].u, s);
     launch_norm_finish(h->partial, nblk_r, h->d_small, s);
     cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, s);
     return H3D_OK;
 }
 
-int build_graph(h3d_handle *h) {
-    if (h->vgraph) return H3D_OK;
+int build_graph(h3d_handle *h, bool refine) {
+    cudaGraphExec_t &ge = refine ? h->rgraph : h->vgraph;
+    if (ge) return H3D_OK;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_vcycle(h, 1.f);
+    enqueue_vcycle(h, 1.f, refine);
     CK(cudaStreamEndCapture(h->stream, &g));
-    cudaError_t e = cudaGraphInstantiate(&h->vgraph, g, 0);
+    cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
-    if (e != cudaSuccess) { h->vgraph = nullptr; return fail(h, H3D_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e)); }
+    if (e != cudaSuccess) { ge = nullptr; return fail(h, H3D_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e)); }
     return H3D_OK;
 }
 
@@ -304,6 +317,8 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
         return fail(h, H3D_ERR_ARG, "invalid coarse_mode");
     if (cfg->pin_mode != H3D_PIN_IDENTITY && cfg->pin_mode != H3D_PIN_GALERKIN)
         return fail(h, H3D_ERR_ARG, "invalid pin_mode");
+    if (cfg->precision != H3D_PREC_REFINE && cfg->precision != H3D_PREC_FP32)
+        return fail(h, H3D_ERR_ARG, "invalid precision");
     h->cfg = *cfg;
     h->device = cfg->device;
     h->nl = nl;
@@ -327,8 +342,14 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
     }
     const long long nv0 = h->lv[0].P.nv;
     CK(cudaMalloc(&h->rho, sizeof(float) * nv0));
-    CK(cudaMalloc(&h->chi, sizeof(float) * NF * nv0));
-    CK(cudaMemset(h->chi, 0, sizeof(float) * NF * nv0));
+    CK(cudaMalloc(&h->chi, sizeof(double) * NF * nv0));
+    CK(cudaMemset(h->chi, 0, sizeof(double) * NF * nv0));
+    if (h->refine()) {
+        CK(cudaMalloc(&h->u64, sizeof(double) * NF * nv0));
+        CK(cudaMemset(h->u64, 0, sizeof(double) * NF * nv0));
+        CK(cudaMalloc(&h->f0, sizeof(float) * NF * nv0));
+        CK(cudaMemset(h->f0, 0, sizeof(float) * NF * nv0));
+    }
     // element matrix and derived tables
     element_matrix(cfg->youngs_modulus, cfg->poisson_ratio, h->ked);
     for (int i = 0; i < 576; i++) h->ke.k[i] = (float)h->ked[i];
@@ -385,7 +406,8 @@ int h3d_destroy(h3d_handle *h) {
     for (int l = 0; l < h->nl; l++) {
         cudaFree(h->lv[l].u); cudaFree(h->lv[l].f); cudaFree(h->lv[l].r); cudaFree(h->lv[l].st);
     }
-    cudaFree(h->rho); cudaFree(h->chi); cudaFree(h->q); cudaFree(h->d_ked); cudaFree(h->aug);
+    cudaFree(h->rho); cudaFree(h->chi); cudaFree(h->u64); cudaFree(h->f0);
+    cudaFree(h->q); cudaFree(h->d_ked); cudaFree(h->aug);
     cudaFree(h->d_flag); cudaFree(h->partial); cudaFree(h->d_small); cudaFree(h->tmp);
     if (h->h_small) cudaFreeHost(h->h_small);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -478,7 +500,10 @@ int h3d_update_stencils(h3d_handle *h) {
 int h3d_enforce_unit_macro_strain(h3d_handle *h) {
     if (!h) return H3D_ERR_ARG;
     if (!h->have_density) return fail(h, H3D_ERR_STATE, "no density");
-    launch_rhs(h->lv[0], h->rho, h->rhs, h->stream);
+    launch_rhs(h->lv[0], h->rho, h->rhs, h->lv[0].f, h->stream);
+    if (h->refine())
+        CK(cudaMemcpyAsync(h->f0, h->lv[0].f, sizeof(float) * NF * h->lv[0].P.nv, cudaMemcpyDeviceToDevice,
+                           h->stream));
     CKL();
     return H3D_OK;
 }
@@ -543,8 +568,14 @@ int h3d_reset_displacement(h3d_handle *h, int level) {
 int h3d_field_norms(h3d_handle *h, int field, double out[6]) {
     if (!h || !out) return H3D_ERR_ARG;
     const Level &L = h->lv[0];
-    const float *v = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r
-                   : field == H3D_FIELD_CHI ? h->chi : nullptr;
+    if (field == H3D_FIELD_CHI || field == H3D_FIELD_SOLUTION) {
+        const double *src = field == H3D_FIELD_CHI ? h->chi : h->u64;
+        if (!src) return fail(h, H3D_ERR_ARG, "no FP64 solution in this precision mode");
+        if (int e = ensure_tmp(h, (size_t)NF * L.P.nv)) return e;
+        launch_convert((long long)NF * L.P.nv, src, h->tmp, h->stream);
+        return weighted_norms(h, L.P, h->tmp, out);
+    }
+    const float *v = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r : nullptr;
     if (!v) return fail(h, H3D_ERR_ARG, "field has no norm");
     return weighted_norms(h, L.P, v, out);
 }
@@ -555,7 +586,7 @@ int h3d_v_cycle(h3d_handle *h, float w, int pre, int post) {
     if (pre != 1 || post != 1) return fail(h, H3D_ERR_ARG, "only V(1,1) is supported");
     CK(cudaSetDevice(h->device));
     if (w == 1.f) {
-        if (int e = build_graph(h)) return e;
+        if (int e = build_graph(h, false)) return e;
         CK(cudaGraphLaunch(h->vgraph, h->stream));
     } else {
         enqueue_vcycle(h, w);
@@ -569,10 +600,20 @@ int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solv
     if (!h->have_stencils) return fail(h, H3D_ERR_STATE, "no stencils");
     if (case_mask <= 0 || case_mask > 63) return fail(h, H3D_ERR_ARG, "case_mask must select load cases");
     CK(cudaSetDevice(h->device));
-    if (!with_guess) CK(cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * NF * h->lv[0].P.nv, h->stream));
-    if (int e = build_graph(h)) return e;
+    const bool refine = h->refine();
+    const Level &L0 = h->lv[0];
+    // the field that holds the solution: u64 (refined) or the swept u (FP32)
+    auto reset_solution = [&]() -> int {
+        if (refine) CK(cudaMemsetAsync(h->u64, 0, sizeof(double) * NF * L0.P.nv, h->stream));
+        else CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * NF * L0.P.nv, h->stream));
+        return H3D_OK;
+    };
+    if (!with_guess)
+        if (int e = reset_solution()) return e;
+    if (int e = build_graph(h, refine)) return e;
+    cudaGraphExec_t cycle = refine ? h->rgraph : h->vgraph;
     double fn[6], rel[6] = {1, 1, 1, 1, 1, 1};
-    if (int e = weighted_norms(h, h->lv[0].P, h->lv[0].f, fn)) return e;
+    if (int e = weighted_norms(h, L0.P, refine ? h->f0 : L0.f, fn)) return e;
     int it = 0, status = H3D_OK, explode_left = 2;
     CK(cudaEventRecord(h->ev0, h->stream));
     const int maxit = 200;
@@ -585,7 +626,7 @@ int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solv
             if (done) break;
         }
         if (it >= maxit) { status = H3D_NOT_CONVERGED; break; }
-        CK(cudaGraphLaunch(h->vgraph, h->stream));
+        CK(cudaGraphLaunch(cycle, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         it++;
         bool bad = false;
@@ -595,7 +636,7 @@ int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solv
         }
         if (bad) {  // MG.cpp:140-182: restart from zero once, then give up
             if (--explode_left <= 0) { status = H3D_DIVERGED; break; }
-            CK(cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * NF * h->lv[0].P.nv, h->stream));
+            if (int e = reset_solution()) return e;
         }
     }
     CK(cudaEventRecord(h->ev1, h->stream));
@@ -614,7 +655,7 @@ int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solv
 
 int h3d_reset_solutions(h3d_handle *h) {
     if (!h) return H3D_ERR_ARG;
-    CK(cudaMemsetAsync(h->chi, 0, sizeof(float) * NF * h->lv[0].P.nv, h->stream));
+    CK(cudaMemsetAsync(h->chi, 0, sizeof(double) * NF * h->lv[0].P.nv, h->stream));
     return H3D_OK;
 }
 
@@ -624,18 +665,27 @@ int h3d_elastic_matrix(h3d_handle *h, double tol, double C[36], h3d_solve_stats 
     CK(cudaSetDevice(h->device));
     Level &L = h->lv[0];
     cudaStream_t s = h->stream;
-    const size_t bytes = sizeof(float) * NF * L.P.nv;
-    launch_rhs(L, h->rho, h->rhs, s);
-    CK(cudaMemcpyAsync(L.u, h->chi, bytes, cudaMemcpyDeviceToDevice, s));
+    const long long n18 = (long long)NF * L.P.nv;
     const int nb = norm_blocks(L.P);
-    launch_mean_partial(L.P, L.u, h->partial, nb, s);
-    launch_remove_mean(L.P, L.u, h->partial, nb, s);
+    // right-hand sides and warm start from the stored solutions, mean removed
+    // (homogenization.cu:471-477, grid.cpp:1131-1141)
+    if (h->refine()) {
+        launch_rhs(L, h->rho, h->rhs, h->f0, s);
+        CK(cudaMemcpyAsync(h->u64, h->chi, sizeof(double) * n18, cudaMemcpyDeviceToDevice, s));
+        launch_remove_mean64(L.P, h->u64, h->partial, nb, s);
+    } else {
+        launch_rhs(L, h->rho, h->rhs, L.f, s);
+        launch_convert(n18, h->chi, L.u, s);
+        launch_mean_partial(L.P, L.u, h->partial, nb, s);
+        launch_remove_mean(L.P, L.u, h->partial, nb, s);
+    }
     CKL();
     h3d_solve_stats st;
     int e = h3d_solve(h, 63, tol, 1, &st);
     if (stats) *stats = st;
     if (e != H3D_OK && e != H3D_NOT_CONVERGED) return e;
-    CK(cudaMemcpyAsync(h->chi, L.u, bytes, cudaMemcpyDeviceToDevice, s));
+    if (h->refine()) CK(cudaMemcpyAsync(h->chi, h->u64, sizeof(double) * n18, cudaMemcpyDeviceToDevice, s));
+    else launch_convert(n18, L.u, h->chi, s);
     const int eb = elastic_blocks(L.P);
     launch_elastic_partials(L.P, h->chi, h->rho, h->ke, h->partial, eb, s);
     launch_elastic_finish(h->partial, eb, h->d_small, s);
@@ -712,13 +762,21 @@ int h3d_get_field(h3d_handle *h, int level, int field, float *host) {
         CK(cudaStreamSynchronize(h->stream));
         return H3D_OK;
     }
-    const float *src = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r
-                     : (field == H3D_FIELD_CHI && level == 0) ? h->chi : nullptr;
-    if (!src) return fail(h, H3D_ERR_ARG, "unknown field");
-    if (int e = ensure_tmp(h, (size_t)NF * L.P.nv)) return e;
-    launch_field_to_lex(L.P, src, h->tmp, h->stream);
+    const size_t n18 = (size_t)NF * L.P.nv;
+    if (field == H3D_FIELD_CHI || field == H3D_FIELD_SOLUTION) {
+        const double *src = level != 0 ? nullptr : field == H3D_FIELD_CHI ? h->chi : h->u64;
+        if (!src) return fail(h, H3D_ERR_ARG, "no such FP64 field on this level / precision mode");
+        if (int e = ensure_tmp(h, 2 * n18)) return e;
+        launch_convert((long long)n18, src, h->tmp + n18, h->stream);
+        launch_field_to_lex(L.P, h->tmp + n18, h->tmp, h->stream);
+    } else {
+        const float *src = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r : nullptr;
+        if (!src) return fail(h, H3D_ERR_ARG, "unknown field");
+        if (int e = ensure_tmp(h, n18)) return e;
+        launch_field_to_lex(L.P, src, h->tmp, h->stream);
+    }
     CKL();
-    CK(cudaMemcpyAsync(host, h->tmp, sizeof(float) * NF * L.P.nv, cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaMemcpyAsync(host, h->tmp, sizeof(float) * n18, cudaMemcpyDeviceToHost, h->stream));
     CK(cudaStreamSynchronize(h->stream));
     return H3D_OK;
 }
@@ -737,12 +795,24 @@ int h3d_set_field(h3d_handle *h, int level, int field, const float *host) {
         CK(cudaStreamSynchronize(h->stream));
         return H3D_OK;
     }
-    float *dst = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r
-               : (field == H3D_FIELD_CHI && level == 0) ? h->chi : nullptr;
-    if (!dst) return fail(h, H3D_ERR_ARG, "unknown field");
-    if (int e = ensure_tmp(h, (size_t)NF * L.P.nv)) return e;
-    CK(cudaMemcpyAsync(h->tmp, host, sizeof(float) * NF * L.P.nv, cudaMemcpyHostToDevice, h->stream));
-    launch_field_from_lex(L.P, h->tmp, dst, h->stream);
+    const size_t n18 = (size_t)NF * L.P.nv;
+    if (field == H3D_FIELD_CHI || field == H3D_FIELD_SOLUTION) {
+        double *dst = level != 0 ? nullptr : field == H3D_FIELD_CHI ? h->chi : h->u64;
+        if (!dst) return fail(h, H3D_ERR_ARG, "no such FP64 field on this level / precision mode");
+        if (int e = ensure_tmp(h, 2 * n18)) return e;
+        CK(cudaMemcpyAsync(h->tmp, host, sizeof(float) * n18, cudaMemcpyHostToDevice, h->stream));
+        launch_field_from_lex(L.P, h->tmp, h->tmp + n18, h->stream);
+        launch_convert((long long)n18, h->tmp + n18, dst, h->stream);
+    } else {
+        float *dst = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r : nullptr;
+        if (!dst) return fail(h, H3D_ERR_ARG, "unknown field");
+        if (int e = ensure_tmp(h, n18)) return e;
+        CK(cudaMemcpyAsync(h->tmp, host, sizeof(float) * n18, cudaMemcpyHostToDevice, h->stream));
+        launch_field_from_lex(L.P, h->tmp, dst, h->stream);
+        // in the refined mode the solve reads its right-hand side from f0
+        if (field == H3D_FIELD_F && level == 0 && h->refine())
+            CK(cudaMemcpyAsync(h->f0, dst, sizeof(float) * n18, cudaMemcpyDeviceToDevice, h->stream));
+    }
     CKL();
     CK(cudaStreamSynchronize(h->stream));
     return H3D_OK;

@@ -110,7 +110,14 @@ struct Level {
 void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, cudaStream_t s);
 void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, double *norm_partial,
                           int nblk_norm, cudaStream_t s);
-void launch_rhs(const Level &L, const float *rho, const RhsTab &g, cudaStream_t s);
+void launch_rhs(const Level &L, const float *rho, const RhsTab &g, float *f, cudaStream_t s);
+// r = f - K u with u in FP64, the operator in difference form (refined precision)
+void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const float *f, const double *u64,
+                            float *r, cudaStream_t s);
+void launch_update64(long long n, double *u64, const float *e, cudaStream_t s);
+void launch_convert(long long n, const float *src, double *dst, cudaStream_t s);
+void launch_convert(long long n, const double *src, float *dst, cudaStream_t s);
+void launch_remove_mean64(const Planes &P, double *v, double *partial, int nblk, cudaStream_t s);
 // coarse levels and transfers (k_coarse.cu)
 void launch_coarse_gs(const Level &L, float w, cudaStream_t s);
 void launch_coarse_residual(const Level &L, cudaStream_t s);
@@ -131,11 +138,11 @@ void launch_coarse_assemble(const Level &C, double *aug, cudaStream_t s);
 void launch_gauss_jordan(double *aug, int n, int *flag, cudaStream_t s);
 void launch_coarse_apply(const Level &C, const double *aug, int project, cudaStream_t s);
 // homogenized tensor, sensitivities (k_homog.cu)
-void launch_elastic_partials(const Planes &P, const float *chi, const float *rho, const KeMat &ke,
+void launch_elastic_partials(const Planes &P, const double *chi, const float *rho, const KeMat &ke,
                              double *partial, int nblk, cudaStream_t s);
 int elastic_blocks(const Planes &P);
 void launch_elastic_finish(const double *partial, int nblk, double *out21, cudaStream_t s);
-void launch_sensitivity(const Planes &P, const float *chi, const KeMat &ke, const float *dc36, float *sens,
+void launch_sensitivity(const Planes &P, const double *chi, const KeMat &ke, const float *dc36, float *sens,
                         int pitch, cudaStream_t s);
 // design (k_design.cu)
 void launch_density_in(const int n[3], const float *src, int pitch, float *dst, cudaStream_t s);

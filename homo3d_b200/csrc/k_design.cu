@@ -220,6 +220,20 @@ __global__ void k_sym_rotate3(int n0, int h, float *v, long long nrep) {
     const int perm[6][3] = {{0, 2, 1}, {2, 1, 0}, {1, 0, 2}, {2, 0, 1}, {1, 2, 0}, {0, 1, 2}};
     const int fo[4][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}, {1, 1, 1}};
     const int fe[4][3] = {{0, 0, 0}, {1, 1, 0}, {0, 1, 1}, {1, 0, 1}};
+    // representatives with x, y <= z can share an orbit; the reference lets their
+    // threads race, here each orbit is averaged once, by its first representative
+    for (int i = 0; i < 6; i++) {
+        const int o[3] = {rp[perm[i][0]], rp[perm[i][1]], rp[perm[i][2]]};
+        for (int f = 0; f < 4; f++) {
+            const int *fl = i < 3 ? fo[f] : fe[f];
+            int q[3];
+            for (int j = 0; j < 3; j++) q[j] = fl[j] ? -1 - o[j] : o[j];
+            if (q[0] >= 0 && q[1] >= 0 && q[2] >= 0 && q[0] <= q[2] && q[1] <= q[2]) {
+                const long long tq = (long long)q[2] * (q[2] + 1) * (2 * q[2] + 1) / 6 + (long long)q[1] * (q[2] + 1) + q[0];
+                if (tq < t) return;
+            }
+        }
+    }
     float s = 0;
     for (int i = 0; i < 6; i++) {
         const int o[3] = {rp[perm[i][0]], rp[perm[i][1]], rp[perm[i][2]]};

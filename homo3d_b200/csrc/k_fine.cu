@@ -259,9 +259,174 @@ void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, dou
     k_fine_residual<<<dim3(nb, 8), bs, 0, s>>>(a, ke, norm_partial);
 }
 
-void launch_rhs(const Level &L, const float *rho, const RhsTab &g, cudaStream_t s) {
+void launch_rhs(const Level &L, const float *rho, const RhsTab &g, float *f, cudaStream_t s) {
     const int bs = 256;
-    k_rhs<<<(unsigned)((L.P.nv + bs - 1) / bs), bs, 0, s>>>(L.P, rho, L.f, g);
+    k_rhs<<<(unsigned)((L.P.nv + bs - 1) / bs), bs, 0, s>>>(L.P, rho, f, g);
+}
+
+// ---- refined precision: residual of an FP64 solution ----------------------------
+// K u at vertex v equals sum_{d != 0} A_d (u_{v+d} - u_v), because the assembled
+// blocks of a row sum to zero (Ke annihilates rigid translations).  The
+// differences are taken in FP64 and are O(1) where u itself is O(N), so the FP32
+// products lose nothing to cancellation and the residual floor no longer grows
+// with the grid size.  The pinned origin enters as an ordinary neighbour: its
+// value is held fixed by the correction sweeps, so a nonzero value only
+// translates the solution.
+template <int K>
+__device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const KeMat &ke,
+                                                       const double *__restrict__ u64, long long p) {
+    constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
+    const long long me = (long long)K * a.P + p;
+    if (K == 7 && p == 0) {
+#pragma unroll
+        for (int q = 0; q < NF; ++q) a.r[q * a.nv + me] = 0.f;
+        return;
+    }
+    int i, j, l;
+    plane_coords(p, a.h, i, j, l);
+    const int x = 2 * i + px, y = 2 * j + py, z = 2 * l + pz;
+    const int xe0 = x == 0 ? a.n[0] - 1 : x - 1;
+    const int ye0 = y == 0 ? a.n[1] - 1 : y - 1;
+    const int ze0 = z == 0 ? a.n[2] - 1 : z - 1;
+    float rw[8];
+#pragma unroll
+    for (int w = 0; w < 8; ++w) {
+        const int ex = (w & 1) ? x : xe0, ey = ((w >> 1) & 1) ? y : ye0, ez = (w >> 2) ? z : ze0;
+        rw[w] = RHO_PENAL_MIN + __ldg(&a.rho[ex + (long long)a.n[0] * (ey + (long long)a.n[1] * ez)]);
+    }
+    int ii[3], jj[3], ll[3];
+    axis_nbrs(i, px, a.h[0], ii[0], ii[2]);
+    axis_nbrs(j, py, a.h[1], jj[0], jj[2]);
+    axis_nbrs(l, pz, a.h[2], ll[0], ll[2]);
+    ii[1] = i; jj[1] = j; ll[1] = l;
+    double uv[NF];
+#pragma unroll
+    for (int q = 0; q < NF; ++q) uv[q] = __ldg(u64 + q * a.nv + me);
+    float acc[NF];
+#pragma unroll
+    for (int q = 0; q < NF; ++q) acc[q] = 0.f;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        if (d == 13) continue;
+        const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
+        float A[9];
+#pragma unroll
+        for (int k = 0; k < 9; ++k) A[k] = 0.f;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            const int ex = w & 1, ey = (w >> 1) & 1, ez = w >> 2;
+            const int bx = 1 - ex + dx, by = 1 - ey + dy, bz = 1 - ez + dz;
+            if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+            const int an = 7 - w, bn = bx + 2 * by + 4 * bz;
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+#pragma unroll
+                for (int c = 0; c < 3; ++c)
+                    A[3 * r + c] = fmaf(rw[w], ke.k[(3 * an + r) * 24 + 3 * bn + c], A[3 * r + c]);
+        }
+        const int Kn = K ^ ((dx & 1) | ((dy & 1) << 1) | ((dz & 1) << 2));
+        const long long nid =
+            (long long)Kn * a.P + ii[dx + 1] + (long long)a.h[0] * (jj[dy + 1] + (long long)a.h[1] * ll[dz + 1]);
+        const double *up = u64 + nid;
+#pragma unroll
+        for (int c = 0; c < NCASE; ++c) {
+            const float d0 = (float)(__ldg(up + (3 * c) * a.nv) - uv[3 * c]);
+            const float d1 = (float)(__ldg(up + (3 * c + 1) * a.nv) - uv[3 * c + 1]);
+            const float d2 = (float)(__ldg(up + (3 * c + 2) * a.nv) - uv[3 * c + 2]);
+            acc[3 * c + 0] = fmaf(A[0], d0, fmaf(A[1], d1, fmaf(A[2], d2, acc[3 * c + 0])));
+            acc[3 * c + 1] = fmaf(A[3], d0, fmaf(A[4], d1, fmaf(A[5], d2, acc[3 * c + 1])));
+            acc[3 * c + 2] = fmaf(A[6], d0, fmaf(A[7], d1, fmaf(A[8], d2, acc[3 * c + 2])));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < NF; ++q) a.r[q * a.nv + me] = a.f[q * a.nv + me] - acc[q];
+}
+
+__global__ void __launch_bounds__(128) k_fine_residual64(FineArgs a, const __grid_constant__ KeMat ke,
+                                                         const double *__restrict__ u64) {
+    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (p >= a.P) return;
+    switch (blockIdx.y) {
+    case 0: fine_residual64_vertex<0>(a, ke, u64, p); break;
+    case 1: fine_residual64_vertex<1>(a, ke, u64, p); break;
+    case 2: fine_residual64_vertex<2>(a, ke, u64, p); break;
+    case 3: fine_residual64_vertex<3>(a, ke, u64, p); break;
+    case 4: fine_residual64_vertex<4>(a, ke, u64, p); break;
+    case 5: fine_residual64_vertex<5>(a, ke, u64, p); break;
+    case 6: fine_residual64_vertex<6>(a, ke, u64, p); break;
+    default: fine_residual64_vertex<7>(a, ke, u64, p); break;
+    }
+}
+
+void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const float *f, const double *u64,
+                            float *r, cudaStream_t s) {
+    FineArgs a = make_args(L, rho);
+    a.f = f;
+    a.r = r;
+    const int bs = 128;
+    const unsigned nb = (unsigned)((a.P + bs - 1) / bs);
+    k_fine_residual64<<<dim3(nb, 8), bs, 0, s>>>(a, ke, u64);
+}
+
+__global__ void k_update64(long long n, double *u, const float *__restrict__ e) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) u[i] += (double)e[i];
+}
+
+__global__ void k_f32_to_f64(long long n, const float *__restrict__ s, double *d) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) d[i] = (double)s[i];
+}
+
+__global__ void k_f64_to_f32(long long n, const double *__restrict__ s, float *d) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i < n) d[i] = (float)s[i];
+}
+
+void launch_update64(long long n, double *u64, const float *e, cudaStream_t s) {
+    k_update64<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, u64, e);
+}
+void launch_convert(long long n, const float *src, double *dst, cudaStream_t s) {
+    k_f32_to_f64<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, src, dst);
+}
+void launch_convert(long long n, const double *src, float *dst, cudaStream_t s) {
+    k_f64_to_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, src, dst);
+}
+
+// mean of each of the 18 planes over unique vertices, removed in place (FP64)
+__global__ void __launch_bounds__(256) k_sum18_64(long long nv, const double *__restrict__ v, double *partial) {
+    double s[NF];
+#pragma unroll
+    for (int q = 0; q < NF; ++q) s[q] = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x)
+#pragma unroll
+        for (int q = 0; q < NF; ++q) s[q] += v[q * nv + i];
+    block_reduce<NF>(s, partial, blockIdx.x);
+}
+
+__global__ void __launch_bounds__(256) k_sum18_finish(const double *__restrict__ partial, int nblk, double *out) {
+    double s[NF];
+#pragma unroll
+    for (int c = 0; c < NF; ++c) s[c] = 0;
+    for (int b = threadIdx.x; b < nblk; b += blockDim.x)
+#pragma unroll
+        for (int c = 0; c < NF; ++c) s[c] += partial[(long long)b * NF + c];
+    block_reduce<NF>(s, out, 0);
+}
+
+__global__ void k_sub_mean64(long long nv, double *v, const double *__restrict__ sum18) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    const double inv = 1.0 / (double)nv;
+#pragma unroll
+    for (int q = 0; q < NF; ++q) v[q * nv + i] -= sum18[q] * inv;
+}
+
+void launch_remove_mean64(const Planes &P, double *v, double *partial, int nblk, cudaStream_t s) {
+    double *tot = partial + (long long)nblk * NF;
+    k_sum18_64<<<nblk, 256, 0, s>>>(P.nv, v, partial);
+    k_sum18_finish<<<1, 256, 0, s>>>(partial, nblk, tot);
+    k_sub_mean64<<<(unsigned)((P.nv + 255) / 256), 256, 0, s>>>(P.nv, v, tot);
 }
 
 }  // namespace h3d

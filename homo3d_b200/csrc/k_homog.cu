@@ -8,8 +8,9 @@
 //     sum_{i<=j} (dC_ij + [i!=j] dC_ji) (chi0_i - chi_i)^T Ke (chi0_j - chi_j)
 //     * p rho^(p-1) / |Y| with p = 1, written at x + (y + z*ny)*pitchT.
 //   The reference rounds chi to FP16 before both reductions
-//   (homogenization.cu:433-462) and sums in FP32; here chi stays FP32 and the
-//   reduction is FP64 (per-thread partials, then a fixed-order two-stage sum).
+//   (homogenization.cu:433-462) and sums in FP32; here chi is read in FP64,
+//   taken relative to each element's node 0, and the reduction is FP64
+//   (per-thread partials, then a fixed-order two-stage sum).
 #include "h3d_internal.cuh"
 
 namespace h3d {
@@ -27,9 +28,18 @@ __host__ __device__ constexpr float macro_disp(int a, int c, int m) {
 }
 
 // E[t] for the 21 pairs (i <= j) of element e = (x,y,z)
-__device__ __forceinline__ void element_energy(const Planes &P, const float *__restrict__ chi, const KeMat &ke,
+// chi is FP64; the element's displacements are taken relative to its node 0
+// (Ke annihilates translations), so the FP32 products see O(1) values even
+// where chi itself is O(N)
+__device__ __forceinline__ void element_energy(const Planes &P, const double *__restrict__ chi, const KeMat &ke,
                                                int x, int y, int z, float E[21]) {
     float U[NCASE][24];
+    double c0[NF];
+    {
+        const long long v0 = vidx(P, x, y, z);
+#pragma unroll
+        for (int q = 0; q < NF; ++q) c0[q] = __ldg(&chi[q * P.nv + v0]);
+    }
 #pragma unroll
     for (int a = 0; a < 8; ++a) {
         const int vx = (a & 1) ? (x + 1 == P.n[0] ? 0 : x + 1) : x;
@@ -39,7 +49,8 @@ __device__ __forceinline__ void element_energy(const Planes &P, const float *__r
 #pragma unroll
         for (int c = 0; c < NCASE; ++c)
 #pragma unroll
-            for (int m = 0; m < 3; ++m) U[c][3 * a + m] = macro_disp(a, c, m) - __ldg(&chi[(3 * c + m) * P.nv + v]);
+            for (int m = 0; m < 3; ++m)
+                U[c][3 * a + m] = macro_disp(a, c, m) - (float)(__ldg(&chi[(3 * c + m) * P.nv + v]) - c0[3 * c + m]);
     }
     int t = 0;
 #pragma unroll
@@ -71,7 +82,7 @@ int elastic_blocks(const Planes &P) {
     return (int)(nb < 4096 ? nb : 4096);
 }
 
-__global__ void __launch_bounds__(EBS) k_elastic(Planes P, const float *__restrict__ chi, const float *__restrict__ rho,
+__global__ void __launch_bounds__(EBS) k_elastic(Planes P, const double *__restrict__ chi, const float *__restrict__ rho,
                                                  const __grid_constant__ KeMat ke, double *partial) {
     double acc[21];
 #pragma unroll
@@ -89,7 +100,7 @@ __global__ void __launch_bounds__(EBS) k_elastic(Planes P, const float *__restri
     block_reduce<21>(acc, partial, blockIdx.x);
 }
 
-void launch_elastic_partials(const Planes &P, const float *chi, const float *rho, const KeMat &ke, double *partial,
+void launch_elastic_partials(const Planes &P, const double *chi, const float *rho, const KeMat &ke, double *partial,
                              int nblk, cudaStream_t s) {
     k_elastic<<<nblk, EBS, 0, s>>>(P, chi, rho, ke, partial);
 }
@@ -111,7 +122,7 @@ void launch_elastic_finish(const double *partial, int nblk, double *out21, cudaS
 
 struct DcTab { float w[21]; };  // (dC_ij + [i!=j] dC_ji) / |Y| for the 21 pairs
 
-__global__ void __launch_bounds__(EBS) k_sensitivity(Planes P, const float *__restrict__ chi,
+__global__ void __launch_bounds__(EBS) k_sensitivity(Planes P, const double *__restrict__ chi,
                                                      const __grid_constant__ KeMat ke, DcTab dc, float *sens,
                                                      int pitch) {
     const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -127,7 +138,7 @@ __global__ void __launch_bounds__(EBS) k_sensitivity(Planes P, const float *__re
     sens[x + ((long long)y + (long long)z * P.n[1]) * pitch] = s;
 }
 
-void launch_sensitivity(const Planes &P, const float *chi, const KeMat &ke, const float *dc36, float *sens, int pitch,
+void launch_sensitivity(const Planes &P, const double *chi, const KeMat &ke, const float *dc36, float *sens, int pitch,
                         cudaStream_t s) {
     DcTab t;
     const double vol = (double)P.nv;

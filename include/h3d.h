@@ -59,12 +59,22 @@ typedef enum {
     H3D_PIN_GALERKIN = 1        /* exact Galerkin product of the pinned fine operator */
 } h3d_pin_mode;
 
+/* where the level-0 solution lives and how its residual is formed */
+typedef enum {
+    H3D_PREC_REFINE = 0,        /* FP64 solution; per cycle an FP64-exact residual in
+                                   translation-invariant difference form, then an FP32
+                                   V-cycle on the correction (iterative refinement) */
+    H3D_PREC_FP32 = 1           /* FP32 solution swept directly, as the reference does; its
+                                   relative residual floors near 1e-6 * N */
+} h3d_precision;
+
 typedef struct {
     int reso[3];                /* requested cells per axis; corrected like the reference */
     double youngs_modulus;      /* E of the base material */
     double poisson_ratio;       /* nu of the base material */
     int coarse_mode;            /* h3d_coarse_mode */
     int pin_mode;               /* h3d_pin_mode */
+    int precision;              /* h3d_precision */
     int device;                 /* CUDA device ordinal */
 } h3d_config;
 
@@ -81,7 +91,9 @@ typedef enum {
     H3D_FIELD_F = 1,            /* right-hand side */
     H3D_FIELD_R = 2,            /* residual */
     H3D_FIELD_STENCIL = 3,      /* coarse-level stencil (levels >= 1) */
-    H3D_FIELD_CHI = 4           /* stored solutions of the six cases (level 0) */
+    H3D_FIELD_CHI = 4,          /* stored solutions of the six cases (level 0, FP64) */
+    H3D_FIELD_SOLUTION = 5      /* the refined mode's FP64 solution (level 0); in that
+                                   mode level-0 U holds the last correction */
 } h3d_field;
 
 /* ---- lifetime (homogenization.cpp:40-66 Homogenization::build) ---------- */

@@ -1088,6 +1088,22 @@ void ora_symmetrize_f32(const int n[3], float *v, int type) {
             for (int y = 0; y <= z; y++)
                 for (int x = 0; x <= z; x++) {
                     int rp[3] = {x, y, z};
+                    /* representatives with x, y <= z can share an orbit (e.g. (0,1,1) and
+                     * (1,0,1)); average each orbit once, at its first representative */
+                    long t = (long)z * (z + 1) * (2 * z + 1) / 6 + (long)y * (z + 1) + x, tmin = t;
+                    for (int i = 0; i < 6; i++) {
+                        int o[3] = {rp[perm[i][0]], rp[perm[i][1]], rp[perm[i][2]]};
+                        for (int f = 0; f < 4; f++) {
+                            const int *fl = i < 3 ? flips_odd[f] : flips_even[f];
+                            int q[3];
+                            for (int j = 0; j < 3; j++) q[j] = fl[j] ? -1 - o[j] : o[j];
+                            if (q[0] >= 0 && q[1] >= 0 && q[2] >= 0 && q[0] <= q[2] && q[1] <= q[2]) {
+                                long tq = (long)q[2] * (q[2] + 1) * (2 * q[2] + 1) / 6 + (long)q[1] * (q[2] + 1) + q[0];
+                                if (tq < tmin) tmin = tq;
+                            }
+                        }
+                    }
+                    if (tmin < t) continue;
                     float s = 0;
                     for (int i = 0; i < 6; i++) {
                         int o[3] = {rp[perm[i][0]], rp[perm[i][1]], rp[perm[i][2]]};

@@ -42,6 +42,22 @@ def test_binding_signatures_cover_the_header():
     assert bound == set(declared_symbols())
 
 
+def test_cpp_shim_compiles_and_links(tmp_path):
+    src = tmp_path / "drv.cpp"
+    src.write_text(
+        '#include "h3d.hpp"\n'
+        "int main() {\n"
+        "  homo::HomoConfig c; c.reso[0] = c.reso[1] = c.reso[2] = 16;\n"
+        "  (void)c;\n"
+        "  void (homo::Homogenization::*f)(double (*)[6]) = &homo::Homogenization::elasticMatrix;\n"
+        "  (void)f; return 0;\n"
+        "}\n")
+    out = tmp_path / "drv"
+    r = subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(out),
+                        "-L", os.path.dirname(H.LIB_PATH), "-lh3d"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+
+
 def test_reference_resolution_rule():
     assert H.reference_resolution((80, 96, 100)) == (96, 96, 112)
     assert H.reference_resolution((320, 512, 1000)) == (320, 512, 1024)

@@ -36,6 +36,39 @@ def test_elastic_matrix_1e5_matches_fp64(torch_cuda, pin):
     assert np.abs(C - C.T).max() == 0
 
 
+def test_refined_precision_passes_the_fp32_floor(torch_cuda):
+    """An FP32 solution stalls near 1e-6 * N in ||r||/||f|| (chi is O(N) in grid units);
+    the refined mode (FP64 solution, difference-form residual) keeps converging."""
+    n = 32
+    rho = smooth_density(n, seed=12)
+    t = torch_cuda.tensor(rho, dtype=torch_cuda.float32, device="cuda")
+    fp32 = H.Homogenization(n, precision=H.PREC_FP32)
+    fp32.update(t)
+    fp32.elasticMatrix(1e-8)
+    assert fp32.last_stats["status"] == H.H3D_NOT_CONVERGED
+    assert min(fp32.last_stats["rel_res"]) > 1e-8
+    ref = H.Homogenization(n)
+    ref.update(t)
+    C = ref.elasticMatrix(1e-8)
+    st = ref.last_stats
+    assert st["status"] == H.H3D_OK and max(st["rel_res"]) <= 1e-8 and st["vcycles"] < 40
+    Cref = oracle_C(n, rho, tol=1e-11).elastic_matrix()
+    assert rel_err(C, Cref) < 1e-6
+
+
+def test_fp32_mode_matches_refined_mode_at_loose_tolerance(torch_cuda):
+    n = 32
+    rho = smooth_density(n, seed=13)
+    t = torch_cuda.tensor(rho, dtype=torch_cuda.float32, device="cuda")
+    out = {}
+    for prec in (H.PREC_FP32, H.PREC_REFINE):
+        hd = H.Homogenization(n, precision=prec)
+        hd.update(t)
+        out[prec] = (hd.elasticMatrix(1e-3), hd.last_stats["vcycles"])
+    assert abs(out[H.PREC_FP32][1] - out[H.PREC_REFINE][1]) <= 1
+    assert rel_err(out[H.PREC_FP32][0], out[H.PREC_REFINE][0]) < 1e-4
+
+
 def test_config1_32cube_relthres_1e2(torch_cuda):
     """32^3, relthres 1e-2, zero start: C and sensitivities against the FP64 oracle at the
     same number of V-cycles (the quantities the reference reports at this setting)"""
