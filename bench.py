@@ -45,6 +45,9 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--pin-mode", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--profile", action="store_true",
+                   help="only warm-up and timed steps (no e2e, setup or sweep side measurements), for ncu")
+    p.add_argument("--precision", type=int, default=0, help="0 refined (FP64 solution), 1 FP32")
     return p.parse_args()
 
 
@@ -136,7 +139,7 @@ def gpu_arm(args):
     rank, world, dist = dist_init(args.gpus)
     dev = torch.cuda.current_device()
     rho_h = make_density(args, rank)
-    hd = H.Homogenization(args.reso, pin_mode=args.pin_mode)
+    hd = H.Homogenization(args.reso, pin_mode=args.pin_mode, precision=args.precision)
     stream = torch.cuda.ExternalStream(hd.stream)
     rho_d = torch.tensor(rho_h, device="cuda")
     rho_pin = torch.from_numpy(rho_h).pin_memory()
@@ -179,6 +182,12 @@ def gpu_arm(args):
     t_ms = ev0.elapsed_time(ev1)
     t_max = max_over_ranks(dist, t_ms)
     ms_per_solve = t_max / (args.steps * world)
+    if args.profile:
+        hd.close()
+        if dist is not None:
+            dist.destroy_process_group()
+        return {"metric": metric_name(args), "value": round(ms_per_solve, 3), "unit": "ms", "profile_run": True,
+                "vcycles": cycles} if rank == 0 else None
 
     # end to end through the public API with host buffers
     torch.cuda.synchronize()
