@@ -152,8 +152,7 @@ def gpu_arm(args):
         return C
 
     def step_e2e():
-        with torch.cuda.stream(stream):
-            rho_e2e.copy_(rho_pin, non_blocking=True)
+        rho_e2e.copy_(rho_pin, non_blocking=True)   # ordered before the solve by the binding
         hd.update(rho_e2e)
         hd.reset_solutions()
         return hd.elasticMatrix(args.tol)

@@ -89,6 +89,8 @@ _SIGS = {
     "h3d_elastic_matrix": [_vp, ctypes.c_double, _dp, ctypes.POINTER(SolveStats)],
     "h3d_sensitivity": [_vp, _fp, _vp, ctypes.c_int],
     "h3d_reset_solutions": [_vp],
+    "h3d_penalize": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float],
+    "h3d_penalize_backward": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float],
     "h3d_oc_update": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
                       ctypes.c_float],
     "h3d_oc_filter": [_vp, _vp, _vp, _ip, ctypes.c_int, ctypes.c_float, ctypes.c_int],
@@ -319,6 +321,15 @@ class Homogenization(_Handle):
 
     def reset_solutions(self):
         self.check(lib().h3d_reset_solutions(self._h))
+
+    def penalize(self, rho, rho_phys, p=3.0):
+        """rho_phys = rho^p on the handle's stream (the reference's rho.pow(3))."""
+        self.check(lib().h3d_penalize(self._h, _ptr(rho), _ptr(rho_phys), rho.numel(), float(p)))
+
+    def penalize_backward(self, rho, grad, p=3.0):
+        """grad *= p rho^(p-1)."""
+        self.check(lib().h3d_penalize_backward(self._h, _ptr(rho), _ptr(grad), rho.numel(), float(p)))
+        self.sync()
 
     def field_norms(self, field):
         out = np.zeros(6)

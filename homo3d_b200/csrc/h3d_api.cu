@@ -163,7 +163,8 @@ struct h3d_handle {
     size_t tmp_n = 0;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t vgraph = nullptr;   // one V-cycle on the level-0 field u
-    cudaGraphExec_t rgraph = nullptr;   // one refinement cycle on u64
+    cudaGraphExec_t rgraph = nullptr;   // one refinement cycle on u64 (FP32 products)
+    cudaGraphExec_t xgraph = nullptr;   // the same with FP64-accumulated residual
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool refine() const { return cfg.precision == H3D_PREC_REFINE; }
     bool have_density = false, have_stencils = false;
@@ -236,6 +237,7 @@ void build_q(const double ke[576], const int r[3], std::vector<float> &q, int &n
 int destroy_graph(h3d_handle *h) {
     if (h->vgraph) { cudaGraphExecDestroy(h->vgraph); h->vgraph = nullptr; }
     if (h->rgraph) { cudaGraphExecDestroy(h->rgraph); h->rgraph = nullptr; }
+    if (h->xgraph) { cudaGraphExecDestroy(h->xgraph); h->xgraph = nullptr; }
     return H3D_OK;
 }
 
@@ -243,11 +245,11 @@ int destroy_graph(h3d_handle *h) {
 // residual of the down leg also yields the per-case norms.  With refine, the
 // cycle runs on the correction: level-0 f = f0 - K u64 (FP64-exact), u = 0 before
 // and u64 += u after (in exact arithmetic the same iterate as sweeping u64).
-int enqueue_vcycle(h3d_handle *h, float w, bool refine = false) {
+int enqueue_vcycle(h3d_handle *h, float w, bool refine = false, bool exact = false) {
     cudaStream_t s = h->stream;
-    const int nblk_r = (int)(((h->lv[0].P.nv / 8) + 127) / 128) * 8;
+    const int nblk_r = fine_residual_blocks(h->lv[0]);
     if (refine) {
-        launch_fine_residual64(h->lv[0], h->rho, h->ke, h->f0, h->u64, h->lv[0].f, s);
+        launch_fine_residual64(h->lv[0], h->rho, h->ke, h->f0, h->u64, h->lv[0].f, exact, s);
         cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * NF * h->lv[0].P.nv, s);
     }
     for (int l = 0; l < h->nl; l++) {
@@ -272,12 +274,12 @@ int enqueue_vcycle(h3d_handle *h, float w, bool refine = false) {
     return H3D_OK;
 }
 
-int build_graph(h3d_handle *h, bool refine) {
-    cudaGraphExec_t &ge = refine ? h->rgraph : h->vgraph;
+int build_graph(h3d_handle *h, bool refine, bool exact = false) {
+    cudaGraphExec_t &ge = !refine ? h->vgraph : exact ? h->xgraph : h->rgraph;
     if (ge) return H3D_OK;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_vcycle(h, 1.f, refine);
+    enqueue_vcycle(h, 1.f, refine, exact);
     CK(cudaStreamEndCapture(h->stream, &g));
     cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
@@ -370,7 +372,7 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
     CK(cudaMalloc(&h->aug, sizeof(double) * (size_t)h->ndof * 2 * h->ndof));
     CK(cudaMalloc(&h->d_flag, sizeof(int)));
     // reduction scratch: residual partials, norms, C partials, means, OC
-    size_t pn = (size_t)((((nv0 / 8) + 127) / 128) * 8) * NCASE;
+    size_t pn = (size_t)fine_residual_blocks(h->lv[0]) * NCASE;
     pn = std::max(pn, (size_t)4096 * 21);
     pn = std::max(pn, (size_t)2048 * NF + NF);
     pn = std::max(pn, (size_t)4 + 1184);
@@ -610,8 +612,11 @@ int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solv
     };
     if (!with_guess)
         if (int e = reset_solution()) return e;
-    if (int e = build_graph(h, refine)) return e;
-    cudaGraphExec_t cycle = refine ? h->rgraph : h->vgraph;
+    // below ~1e-4 the FP32 products of the difference-form residual would floor the
+    // iteration, so tight targets take the FP64-accumulating residual
+    const bool exact = refine && tol < 1e-4;
+    if (int e = build_graph(h, refine, exact)) return e;
+    cudaGraphExec_t cycle = !refine ? h->vgraph : exact ? h->xgraph : h->rgraph;
     double fn[6], rel[6] = {1, 1, 1, 1, 1, 1};
     if (int e = weighted_norms(h, L0.P, refine ? h->f0 : L0.f, fn)) return e;
     int it = 0, status = H3D_OK, explode_left = 2;
@@ -710,6 +715,22 @@ int h3d_sensitivity(h3d_handle *h, const float dC[36], float *sens_dev, int pitc
     if (pitchT < P.n[0]) return fail(h, H3D_ERR_ARG, "pitchT smaller than the x resolution");
     CK(cudaMemsetAsync(sens_dev, 0, sizeof(float) * (size_t)pitchT * P.n[1] * P.n[2], h->stream));
     launch_sensitivity(P, h->chi, h->ke, dC, sens_dev, pitchT, h->stream);
+    CKL();
+    return H3D_OK;
+}
+
+int h3d_penalize(h3d_handle *h, const float *rho_dev, float *rho_phys_dev, int64_t n, float p) {
+    if (!h || !rho_dev || !rho_phys_dev || n <= 0) return H3D_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    launch_penalize(n, rho_dev, rho_phys_dev, p, 0, h->stream);
+    CKL();
+    return H3D_OK;
+}
+
+int h3d_penalize_backward(h3d_handle *h, const float *rho_dev, float *grad_dev, int64_t n, float p) {
+    if (!h || !rho_dev || !grad_dev || n <= 0) return H3D_ERR_ARG;
+    CK(cudaSetDevice(h->device));
+    launch_penalize(n, rho_dev, grad_dev, p, 1, h->stream);
     CKL();
     return H3D_OK;
 }

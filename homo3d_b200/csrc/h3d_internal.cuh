@@ -110,10 +110,12 @@ struct Level {
 void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, cudaStream_t s);
 void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, double *norm_partial,
                           int nblk_norm, cudaStream_t s);
+// number of per-block norm partials launch_fine_residual writes
+int fine_residual_blocks(const Level &L);
 void launch_rhs(const Level &L, const float *rho, const RhsTab &g, float *f, cudaStream_t s);
 // r = f - K u with u in FP64, the operator in difference form (refined precision)
 void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const float *f, const double *u64,
-                            float *r, cudaStream_t s);
+                            float *r, bool exact, cudaStream_t s);
 void launch_update64(long long n, double *u64, const float *e, cudaStream_t s);
 void launch_convert(long long n, const float *src, double *dst, cudaStream_t s);
 void launch_convert(long long n, const double *src, float *dst, cudaStream_t s);
@@ -146,6 +148,7 @@ void launch_sensitivity(const Planes &P, const double *chi, const KeMat &ke, con
                         int pitch, cudaStream_t s);
 // design (k_design.cu)
 void launch_density_in(const int n[3], const float *src, int pitch, float *dst, cudaStream_t s);
+void launch_penalize(long long n, const float *rho, float *out, float p, int backward, cudaStream_t s);
 void launch_oc(const float *sens, float *rho, float *rho_new, long long n, float vol, float minrho, float step,
                float damp, double *scratch, cudaStream_t s);
 void launch_filter(const int n[3], int pitch, const float *sens, const float *rho, float *out, float radius,

@@ -25,6 +25,20 @@ __global__ void k_density_in(int n0, int n1, int n2, const float *__restrict__ s
     dst[e] = src[x + ((long long)y + (long long)z * n1) * pitch];
 }
 
+// SIMP penalisation rho_phys = rho^p and its backward grad *= p rho^(p-1)
+// (the reference builds these as the expression rho.pow(3), TensorExpression.h:517-531, 781-)
+__global__ void k_penalize(long long n, const float *__restrict__ rho, float *out, float p, int backward) {
+    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float r = rho[i];
+    if (backward) out[i] *= p * powf(r, p - 1.f);
+    else out[i] = powf(r, p);
+}
+
+void launch_penalize(long long n, const float *rho, float *out, float p, int backward, cudaStream_t s) {
+    k_penalize<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, rho, out, p, backward);
+}
+
 void launch_density_in(const int n[3], const float *src, int pitch, float *dst, cudaStream_t s) {
     const long long ne = (long long)n[0] * n[1] * n[2];
     k_density_in<<<(unsigned)((ne + 255) / 256), 256, 0, s>>>(n[0], n[1], n[2], src, pitch, dst);

@@ -1,5 +1,6 @@
 // k_fine.cu -- matrix-free fine-level operator: Gauss-Seidel colour sweeps,
-// residual with fused per-case norms, and the unit macro-strain right-hand side.
+// residuals (FP32 with fused per-case norms, and the refined FP64-solution form),
+// the unit macro-strain right-hand side, and FP64 helpers of the refined mode.
 //
 // Reference behaviour restated (homo3d grid.cu):
 //   gs_relaxation_otf_kernel (grid.cu:323-551): for each vertex of one colour,
@@ -10,15 +11,24 @@
 //     the pinned origin.
 //   enforce_unit_macro_strain_kernel (grid.cu:1818-1919): f_i = K(rho) chi0_i.
 //
-// B200 design: all six load cases are fused into every sweep so each element
-// density and each neighbour address is fetched once for six right-hand sides.
-// The element loop is reorganised per neighbour: for each of the 26 neighbours
-// the 3x3 coupling block sum_e rho_e Ke[a_e][b_e] is formed once (Ke entries are
-// compile-time offsets into the kernel-parameter bank, so they are FFMA operands)
-// and applied to the six cases, 576 + 234*6 FMAs per vertex instead of 3240.
+// B200 design.  The element loop is reorganised per neighbour: for each of the 26
+// neighbours the 3x3 coupling block sum_e rho_e Ke[a_e][b_e] is formed once (Ke
+// entries are compile-time offsets into the kernel-parameter bank, so they are
+// FFMA operands) and applied to the load cases.  Each vertex is served by three
+// threads with two load cases each (the three run in adjacent CTAs, so the shared
+// densities and neighbour rows hit L1/L2): two cases keep the register count near
+// 64 and the occupancy high enough to hide the neighbour-load latency, which is
+// what bounds this kernel; rebuilding the blocks per thread costs FMAs the
+// memory-bound sweep has to spare.
+#include <type_traits>
+
 #include "h3d_internal.cuh"
 
 namespace h3d {
+
+constexpr int CPT = 2;            // load cases per thread
+constexpr int NG = NCASE / CPT;   // threads per vertex
+constexpr int FBS = 128;          // threads per CTA
 
 struct FineArgs {
     const float *__restrict__ rho;
@@ -37,34 +47,39 @@ __device__ __forceinline__ void axis_nbrs(int i, int p, int h, int &im, int &ip)
     else { im = (i == 0) ? h - 1 : i - 1; ip = i; }
 }
 
-// acc[3c+r] = sum over neighbours (and the vertex itself when SELF) of the
-// assembled coupling block times u; ks = own 3x3 diagonal block
-template <int K, bool SELF>
-__device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, int i, int j, int l,
-                                           float acc[NF], float ks[9]) {
-    constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
-    const int x = 2 * i + px, y = 2 * j + py, z = 2 * l + pz;
-    const int xe0 = x == 0 ? a.n[0] - 1 : x - 1;
-    const int ye0 = y == 0 ? a.n[1] - 1 : y - 1;
-    const int ze0 = z == 0 ? a.n[2] - 1 : z - 1;
+__device__ __forceinline__ void plane_coords(long long p, const int h[3], int &i, int &j, int &l) {
+    i = (int)(p % h[0]);
+    long long t = p / h[0];
+    j = (int)(t % h[1]);
+    l = (int)(t / h[1]);
+}
+
+// geometry of one colour-K vertex: its element densities and neighbour plane coords
+template <int K>
+struct VertexGeo {
     float rw[8];
-#pragma unroll
-    for (int w = 0; w < 8; ++w) {
-        const int ex = (w & 1) ? x : xe0, ey = ((w >> 1) & 1) ? y : ye0, ez = (w >> 2) ? z : ze0;
-        rw[w] = RHO_PENAL_MIN + __ldg(&a.rho[ex + (long long)a.n[0] * (ey + (long long)a.n[1] * ez)]);
-    }
     int ii[3], jj[3], ll[3];
-    axis_nbrs(i, px, a.h[0], ii[0], ii[2]);
-    axis_nbrs(j, py, a.h[1], jj[0], jj[2]);
-    axis_nbrs(l, pz, a.h[2], ll[0], ll[2]);
-    ii[1] = i; jj[1] = j; ll[1] = l;
+    __device__ __forceinline__ VertexGeo(const FineArgs &a, long long p) {
+        constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
+        int i, j, l;
+        plane_coords(p, a.h, i, j, l);
+        const int x = 2 * i + px, y = 2 * j + py, z = 2 * l + pz;
+        const int xe0 = x == 0 ? a.n[0] - 1 : x - 1;
+        const int ye0 = y == 0 ? a.n[1] - 1 : y - 1;
+        const int ze0 = z == 0 ? a.n[2] - 1 : z - 1;
 #pragma unroll
-    for (int q = 0; q < NF; ++q) acc[q] = 0.f;
-#pragma unroll
-    for (int d = 0; d < 27; ++d) {
+        for (int w = 0; w < 8; ++w) {
+            const int ex = (w & 1) ? x : xe0, ey = ((w >> 1) & 1) ? y : ye0, ez = (w >> 2) ? z : ze0;
+            rw[w] = RHO_PENAL_MIN + __ldg(&a.rho[ex + (long long)a.n[0] * (ey + (long long)a.n[1] * ez)]);
+        }
+        axis_nbrs(i, px, a.h[0], ii[0], ii[2]);
+        axis_nbrs(j, py, a.h[1], jj[0], jj[2]);
+        axis_nbrs(l, pz, a.h[2], ll[0], ll[2]);
+        ii[1] = i; jj[1] = j; ll[1] = l;
+    }
+    // coupling block of neighbour d (compile-time d after unrolling)
+    __device__ __forceinline__ void block(const KeMat &ke, int d, float A[9]) const {
         const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
-        if (d == 13 && !SELF) continue;
-        float A[9];
 #pragma unroll
         for (int k = 0; k < 9; ++k) A[k] = 0.f;
 #pragma unroll
@@ -79,13 +94,35 @@ __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, i
                 for (int c = 0; c < 3; ++c)
                     A[3 * r + c] = fmaf(rw[w], ke.k[(3 * an + r) * 24 + 3 * bn + c], A[3 * r + c]);
         }
-        const int Kn = K ^ ((dx & 1) | ((dy & 1) << 1) | ((dz & 1) << 2));
+    }
+    __device__ __forceinline__ long long nbr(const FineArgs &a, int d, int &Kn, bool &pinned) const {
+        const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
+        Kn = K ^ ((dx & 1) | ((dy & 1) << 1) | ((dz & 1) << 2));
         const int ni = ii[dx + 1], nj = jj[dy + 1], nl = ll[dz + 1];
-        if (Kn == 7 && (ni | nj | nl) == 0) continue;  // pinned origin: u = 0
-        const long long nid = (long long)Kn * a.P + ni + (long long)a.h[0] * (nj + (long long)a.h[1] * nl);
-        const float *up = a.u + nid;
+        pinned = (Kn == 7) && ((ni | nj | nl) == 0);
+        return (long long)Kn * a.P + ni + (long long)a.h[0] * (nj + (long long)a.h[1] * nl);
+    }
+};
+
+// acc[3c+r] (c < CPT, cases cb..cb+CPT-1) = sum over neighbours (and the vertex
+// itself when SELF) of coupling block times u; u at the pinned origin counts as 0
+template <int K, bool SELF>
+__device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, const VertexGeo<K> &g, int cb,
+                                           float acc[3 * CPT]) {
 #pragma unroll
-        for (int c = 0; c < NCASE; ++c) {
+    for (int q = 0; q < 3 * CPT; ++q) acc[q] = 0.f;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        if (d == 13 && !SELF) continue;
+        int Kn;
+        bool pinned;
+        const long long nid = g.nbr(a, d, Kn, pinned);
+        if (pinned) continue;
+        float A[9];
+        g.block(ke, d, A);
+        const float *up = a.u + nid + (long long)(3 * cb) * a.nv;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
             const float u0 = __ldg(up + (3 * c) * a.nv);
             const float u1 = __ldg(up + (3 * c + 1) * a.nv);
             const float u2 = __ldg(up + (3 * c + 2) * a.nv);
@@ -94,47 +131,37 @@ __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, i
             acc[3 * c + 2] = fmaf(A[6], u0, fmaf(A[7], u1, fmaf(A[8], u2, acc[3 * c + 2])));
         }
     }
-    if (!SELF) {
-#pragma unroll
-        for (int k = 0; k < 9; ++k) ks[k] = 0.f;
-#pragma unroll
-        for (int w = 0; w < 8; ++w) {
-            const int an = 7 - w;
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    ks[3 * r + c] = fmaf(rw[w], ke.k[(3 * an + r) * 24 + 3 * an + c], ks[3 * r + c]);
-        }
-    }
 }
 
-__device__ __forceinline__ void plane_coords(long long p, const int h[3], int &i, int &j, int &l) {
-    i = (int)(p % h[0]);
-    long long t = p / h[0];
-    j = (int)(t % h[1]);
-    l = (int)(t / h[1]);
+// thread -> (vertex p in the colour plane, first case cb); the NG case groups of a
+// vertex block are adjacent CTAs
+__device__ __forceinline__ void thread_task(long long &p, int &cb) {
+    cb = (int)(blockIdx.x % NG) * CPT;
+    p = (long long)(blockIdx.x / NG) * blockDim.x + threadIdx.x;
 }
 
 template <int K>
-__global__ void __launch_bounds__(128) k_fine_gs(FineArgs a, const __grid_constant__ KeMat ke) {
-    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(FBS, 5) k_fine_gs(FineArgs a, const __grid_constant__ KeMat ke) {
+    long long p;
+    int cb;
+    thread_task(p, cb);
     if (p >= a.P) return;
     const long long me = (long long)K * a.P + p;
     if (K == 7 && p == 0) {  // the pinned origin (grid.cu:445-447, 545)
 #pragma unroll
-        for (int q = 0; q < NF; ++q) a.u[q * a.nv + me] = 0.f;
+        for (int q = 0; q < 3 * CPT; ++q) a.u[(3 * cb + q) * a.nv + me] = 0.f;
         return;
     }
-    int i, j, l;
-    plane_coords(p, a.h, i, j, l);
-    float acc[NF], ks[9];
-    fine_apply<K, false>(a, ke, i, j, l, acc, ks);
+    const VertexGeo<K> g(a, p);
+    float acc[3 * CPT];
+    fine_apply<K, false>(a, ke, g, cb, acc);
+    float ks[9];
+    g.block(ke, 13, ks);
     const float w = a.w;
 #pragma unroll
-    for (int c = 0; c < NCASE; ++c) {
-        float *u = a.u + me + (3 * c) * a.nv;
-        const float *f = a.f + me + (3 * c) * a.nv;
+    for (int c = 0; c < CPT; ++c) {
+        float *u = a.u + me + (long long)(3 * (cb + c)) * a.nv;
+        const float *f = a.f + me + (long long)(3 * (cb + c)) * a.nv;
         float u0 = u[0], u1 = u[a.nv], u2 = u[2 * a.nv];
         u0 = w * (f[0] - acc[3 * c] - ks[1] * u1 - ks[2] * u2) / ks[0] + (1.f - w) * u0;
         u1 = w * (f[a.nv] - acc[3 * c + 1] - ks[3] * u0 - ks[5] * u2) / ks[4] + (1.f - w) * u1;
@@ -146,53 +173,128 @@ __global__ void __launch_bounds__(128) k_fine_gs(FineArgs a, const __grid_consta
 }
 
 template <int K>
-__device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const KeMat &ke, long long p,
+__device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const KeMat &ke, long long p, int cb,
                                                      double nrm[NCASE]) {
     const long long me = (long long)K * a.P + p;
-    int i, j, l;
-    plane_coords(p, a.h, i, j, l);
-    float acc[NF];
     if (K == 7 && p == 0) {
 #pragma unroll
-        for (int q = 0; q < NF; ++q) a.r[q * a.nv + me] = 0.f;
+        for (int q = 0; q < 3 * CPT; ++q) a.r[(3 * cb + q) * a.nv + me] = 0.f;
         return;
     }
-    fine_apply<K, true>(a, ke, i, j, l, acc, nullptr);
+    const VertexGeo<K> g(a, p);
+    float acc[3 * CPT];
+    fine_apply<K, true>(a, ke, g, cb, acc);
     constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
+    int i, j, l;
+    plane_coords(p, a.h, i, j, l);
     const double mult = (double)(axis_mult(2 * i + px, a.n[0]) * axis_mult(2 * j + py, a.n[1]) *
                                  axis_mult(2 * l + pz, a.n[2]));
 #pragma unroll
-    for (int c = 0; c < NCASE; ++c) {
+    for (int c = 0; c < CPT; ++c) {
         double s2 = 0;
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-            const long long o = (3 * c + m) * a.nv + me;
+            const long long o = (long long)(3 * (cb + c) + m) * a.nv + me;
             const float rv = a.f[o] - acc[3 * c + m];
             a.r[o] = rv;
             s2 += (double)rv * rv;
         }
-        nrm[c] += mult * s2;
+#pragma unroll
+        for (int q = 0; q < NCASE; ++q)
+            if (q == cb + c) nrm[q] += mult * s2;
     }
 }
 
-__global__ void __launch_bounds__(128) k_fine_residual(FineArgs a, const __grid_constant__ KeMat ke,
+__global__ void __launch_bounds__(FBS, 5) k_fine_residual(FineArgs a, const __grid_constant__ KeMat ke,
                                                        double *partial) {
-    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    const int K = blockIdx.y;
+    long long p;
+    int cb;
+    thread_task(p, cb);
     double nrm[NCASE] = {0, 0, 0, 0, 0, 0};
     if (p < a.P) {
-        switch (K) {
-        case 0: fine_residual_vertex<0>(a, ke, p, nrm); break;
-        case 1: fine_residual_vertex<1>(a, ke, p, nrm); break;
-        case 2: fine_residual_vertex<2>(a, ke, p, nrm); break;
-        case 3: fine_residual_vertex<3>(a, ke, p, nrm); break;
-        case 4: fine_residual_vertex<4>(a, ke, p, nrm); break;
-        case 5: fine_residual_vertex<5>(a, ke, p, nrm); break;
-        case 6: fine_residual_vertex<6>(a, ke, p, nrm); break;
-        default: fine_residual_vertex<7>(a, ke, p, nrm); break;
+        switch (blockIdx.y) {
+        case 0: fine_residual_vertex<0>(a, ke, p, cb, nrm); break;
+        case 1: fine_residual_vertex<1>(a, ke, p, cb, nrm); break;
+        case 2: fine_residual_vertex<2>(a, ke, p, cb, nrm); break;
+        case 3: fine_residual_vertex<3>(a, ke, p, cb, nrm); break;
+        case 4: fine_residual_vertex<4>(a, ke, p, cb, nrm); break;
+        case 5: fine_residual_vertex<5>(a, ke, p, cb, nrm); break;
+        case 6: fine_residual_vertex<6>(a, ke, p, cb, nrm); break;
+        default: fine_residual_vertex<7>(a, ke, p, cb, nrm); break;
         }
     }
     if (partial) block_reduce<NCASE>(nrm, partial, (long long)blockIdx.y * gridDim.x + blockIdx.x);
+}
+
+// ---- refined precision: residual of an FP64 solution ----------------------------
+// K u at vertex v equals sum_{d != 0} A_d (u_{v+d} - u_v), because the assembled
+// blocks of a row sum to zero (Ke annihilates rigid translations).  The
+// differences are taken in FP64 and are O(1) where u itself is O(N), so the
+// residual floor no longer grows with the grid size.  The pinned origin enters as
+// an ordinary neighbour: its value is held fixed by the correction sweeps, so a
+// nonzero value only translates the solution.  EXACT accumulates the products in
+// FP64 too (the FP32-product form floors near 1e-6 of ||f||, independent of N).
+template <int K, bool EXACT>
+__device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const KeMat &ke,
+                                                       const double *__restrict__ u64, long long p, int cb) {
+    const long long me = (long long)K * a.P + p;
+    if (K == 7 && p == 0) {
+#pragma unroll
+        for (int q = 0; q < 3 * CPT; ++q) a.r[(3 * cb + q) * a.nv + me] = 0.f;
+        return;
+    }
+    const VertexGeo<K> g(a, p);
+    const double *uvp = u64 + me + (long long)(3 * cb) * a.nv;
+    double uv[3 * CPT];
+#pragma unroll
+    for (int q = 0; q < 3 * CPT; ++q) uv[q] = __ldg(uvp + q * a.nv);
+    using Acc = typename std::conditional<EXACT, double, float>::type;
+    Acc acc[3 * CPT];
+#pragma unroll
+    for (int q = 0; q < 3 * CPT; ++q) acc[q] = 0;
+#pragma unroll
+    for (int d = 0; d < 27; ++d) {
+        if (d == 13) continue;
+        int Kn;
+        bool pinned;
+        const long long nid = g.nbr(a, d, Kn, pinned);
+        float A[9];
+        g.block(ke, d, A);
+        const double *up = u64 + nid + (long long)(3 * cb) * a.nv;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            const Acc d0 = (Acc)(__ldg(up + (3 * c) * a.nv) - uv[3 * c]);
+            const Acc d1 = (Acc)(__ldg(up + (3 * c + 1) * a.nv) - uv[3 * c + 1]);
+            const Acc d2 = (Acc)(__ldg(up + (3 * c + 2) * a.nv) - uv[3 * c + 2]);
+            acc[3 * c + 0] = fma((Acc)A[0], d0, fma((Acc)A[1], d1, fma((Acc)A[2], d2, acc[3 * c + 0])));
+            acc[3 * c + 1] = fma((Acc)A[3], d0, fma((Acc)A[4], d1, fma((Acc)A[5], d2, acc[3 * c + 1])));
+            acc[3 * c + 2] = fma((Acc)A[6], d0, fma((Acc)A[7], d1, fma((Acc)A[8], d2, acc[3 * c + 2])));
+        }
+    }
+#pragma unroll
+    for (int q = 0; q < 3 * CPT; ++q) {
+        const long long o = (long long)(3 * cb + q) * a.nv + me;
+        a.r[o] = (float)((Acc)a.f[o] - acc[q]);
+    }
+}
+
+template <bool EXACT>
+__global__ void __launch_bounds__(FBS) k_fine_residual64(FineArgs a, const __grid_constant__ KeMat ke,
+                                                         const double *__restrict__ u64) {
+    long long p;
+    int cb;
+    thread_task(p, cb);
+    if (p >= a.P) return;
+    switch (blockIdx.y) {
+    case 0: fine_residual64_vertex<0, EXACT>(a, ke, u64, p, cb); break;
+    case 1: fine_residual64_vertex<1, EXACT>(a, ke, u64, p, cb); break;
+    case 2: fine_residual64_vertex<2, EXACT>(a, ke, u64, p, cb); break;
+    case 3: fine_residual64_vertex<3, EXACT>(a, ke, u64, p, cb); break;
+    case 4: fine_residual64_vertex<4, EXACT>(a, ke, u64, p, cb); break;
+    case 5: fine_residual64_vertex<5, EXACT>(a, ke, u64, p, cb); break;
+    case 6: fine_residual64_vertex<6, EXACT>(a, ke, u64, p, cb); break;
+    default: fine_residual64_vertex<7, EXACT>(a, ke, u64, p, cb); break;
+    }
 }
 
 // f(case c) = sum_w (1e-9 + rho_w) * (Ke chi0_c)[rows of the vertex's local node in element w]
@@ -235,28 +337,38 @@ static FineArgs make_args(const Level &L, const float *rho) {
     return a;
 }
 
+static unsigned task_blocks(const FineArgs &a) { return (unsigned)(((a.P + FBS - 1) / FBS) * NG); }
+
+int fine_residual_blocks(const Level &L) { return (int)(((L.P.nv / 8 + FBS - 1) / FBS) * NG * 8); }
+
 void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, cudaStream_t s) {
     FineArgs a = make_args(L, rho);
     a.w = w;
-    const int bs = 128;
-    const unsigned nb = (unsigned)((a.P + bs - 1) / bs);
-    k_fine_gs<0><<<nb, bs, 0, s>>>(a, ke);
-    k_fine_gs<1><<<nb, bs, 0, s>>>(a, ke);
-    k_fine_gs<2><<<nb, bs, 0, s>>>(a, ke);
-    k_fine_gs<3><<<nb, bs, 0, s>>>(a, ke);
-    k_fine_gs<4><<<nb, bs, 0, s>>>(a, ke);
-    k_fine_gs<5><<<nb, bs, 0, s>>>(a, ke);
-    k_fine_gs<6><<<nb, bs, 0, s>>>(a, ke);
-    k_fine_gs<7><<<nb, bs, 0, s>>>(a, ke);
+    const unsigned nb = task_blocks(a);
+    k_fine_gs<0><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<1><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<2><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<3><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<4><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<5><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<6><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<7><<<nb, FBS, 0, s>>>(a, ke);
 }
 
 void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, double *norm_partial, int nblk_norm,
                           cudaStream_t s) {
     FineArgs a = make_args(L, rho);
-    const int bs = 128;
-    const unsigned nb = (unsigned)((a.P + bs - 1) / bs);
     (void)nblk_norm;
-    k_fine_residual<<<dim3(nb, 8), bs, 0, s>>>(a, ke, norm_partial);
+    k_fine_residual<<<dim3(task_blocks(a), 8), FBS, 0, s>>>(a, ke, norm_partial);
+}
+
+void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const float *f, const double *u64,
+                            float *r, bool exact, cudaStream_t s) {
+    FineArgs a = make_args(L, rho);
+    a.f = f;
+    a.r = r;
+    if (exact) k_fine_residual64<true><<<dim3(task_blocks(a), 8), FBS, 0, s>>>(a, ke, u64);
+    else k_fine_residual64<false><<<dim3(task_blocks(a), 8), FBS, 0, s>>>(a, ke, u64);
 }
 
 void launch_rhs(const Level &L, const float *rho, const RhsTab &g, float *f, cudaStream_t s) {
@@ -264,110 +376,7 @@ void launch_rhs(const Level &L, const float *rho, const RhsTab &g, float *f, cud
     k_rhs<<<(unsigned)((L.P.nv + bs - 1) / bs), bs, 0, s>>>(L.P, rho, f, g);
 }
 
-// ---- refined precision: residual of an FP64 solution ----------------------------
-// K u at vertex v equals sum_{d != 0} A_d (u_{v+d} - u_v), because the assembled
-// blocks of a row sum to zero (Ke annihilates rigid translations).  The
-// differences are taken in FP64 and are O(1) where u itself is O(N), so the FP32
-// products lose nothing to cancellation and the residual floor no longer grows
-// with the grid size.  The pinned origin enters as an ordinary neighbour: its
-// value is held fixed by the correction sweeps, so a nonzero value only
-// translates the solution.
-template <int K>
-__device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const KeMat &ke,
-                                                       const double *__restrict__ u64, long long p) {
-    constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
-    const long long me = (long long)K * a.P + p;
-    if (K == 7 && p == 0) {
-#pragma unroll
-        for (int q = 0; q < NF; ++q) a.r[q * a.nv + me] = 0.f;
-        return;
-    }
-    int i, j, l;
-    plane_coords(p, a.h, i, j, l);
-    const int x = 2 * i + px, y = 2 * j + py, z = 2 * l + pz;
-    const int xe0 = x == 0 ? a.n[0] - 1 : x - 1;
-    const int ye0 = y == 0 ? a.n[1] - 1 : y - 1;
-    const int ze0 = z == 0 ? a.n[2] - 1 : z - 1;
-    float rw[8];
-#pragma unroll
-    for (int w = 0; w < 8; ++w) {
-        const int ex = (w & 1) ? x : xe0, ey = ((w >> 1) & 1) ? y : ye0, ez = (w >> 2) ? z : ze0;
-        rw[w] = RHO_PENAL_MIN + __ldg(&a.rho[ex + (long long)a.n[0] * (ey + (long long)a.n[1] * ez)]);
-    }
-    int ii[3], jj[3], ll[3];
-    axis_nbrs(i, px, a.h[0], ii[0], ii[2]);
-    axis_nbrs(j, py, a.h[1], jj[0], jj[2]);
-    axis_nbrs(l, pz, a.h[2], ll[0], ll[2]);
-    ii[1] = i; jj[1] = j; ll[1] = l;
-    double uv[NF];
-#pragma unroll
-    for (int q = 0; q < NF; ++q) uv[q] = __ldg(u64 + q * a.nv + me);
-    float acc[NF];
-#pragma unroll
-    for (int q = 0; q < NF; ++q) acc[q] = 0.f;
-#pragma unroll
-    for (int d = 0; d < 27; ++d) {
-        if (d == 13) continue;
-        const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
-        float A[9];
-#pragma unroll
-        for (int k = 0; k < 9; ++k) A[k] = 0.f;
-#pragma unroll
-        for (int w = 0; w < 8; ++w) {
-            const int ex = w & 1, ey = (w >> 1) & 1, ez = w >> 2;
-            const int bx = 1 - ex + dx, by = 1 - ey + dy, bz = 1 - ez + dz;
-            if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
-            const int an = 7 - w, bn = bx + 2 * by + 4 * bz;
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    A[3 * r + c] = fmaf(rw[w], ke.k[(3 * an + r) * 24 + 3 * bn + c], A[3 * r + c]);
-        }
-        const int Kn = K ^ ((dx & 1) | ((dy & 1) << 1) | ((dz & 1) << 2));
-        const long long nid =
-            (long long)Kn * a.P + ii[dx + 1] + (long long)a.h[0] * (jj[dy + 1] + (long long)a.h[1] * ll[dz + 1]);
-        const double *up = u64 + nid;
-#pragma unroll
-        for (int c = 0; c < NCASE; ++c) {
-            const float d0 = (float)(__ldg(up + (3 * c) * a.nv) - uv[3 * c]);
-            const float d1 = (float)(__ldg(up + (3 * c + 1) * a.nv) - uv[3 * c + 1]);
-            const float d2 = (float)(__ldg(up + (3 * c + 2) * a.nv) - uv[3 * c + 2]);
-            acc[3 * c + 0] = fmaf(A[0], d0, fmaf(A[1], d1, fmaf(A[2], d2, acc[3 * c + 0])));
-            acc[3 * c + 1] = fmaf(A[3], d0, fmaf(A[4], d1, fmaf(A[5], d2, acc[3 * c + 1])));
-            acc[3 * c + 2] = fmaf(A[6], d0, fmaf(A[7], d1, fmaf(A[8], d2, acc[3 * c + 2])));
-        }
-    }
-#pragma unroll
-    for (int q = 0; q < NF; ++q) a.r[q * a.nv + me] = a.f[q * a.nv + me] - acc[q];
-}
-
-__global__ void __launch_bounds__(128) k_fine_residual64(FineArgs a, const __grid_constant__ KeMat ke,
-                                                         const double *__restrict__ u64) {
-    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (p >= a.P) return;
-    switch (blockIdx.y) {
-    case 0: fine_residual64_vertex<0>(a, ke, u64, p); break;
-    case 1: fine_residual64_vertex<1>(a, ke, u64, p); break;
-    case 2: fine_residual64_vertex<2>(a, ke, u64, p); break;
-    case 3: fine_residual64_vertex<3>(a, ke, u64, p); break;
-    case 4: fine_residual64_vertex<4>(a, ke, u64, p); break;
-    case 5: fine_residual64_vertex<5>(a, ke, u64, p); break;
-    case 6: fine_residual64_vertex<6>(a, ke, u64, p); break;
-    default: fine_residual64_vertex<7>(a, ke, u64, p); break;
-    }
-}
-
-void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const float *f, const double *u64,
-                            float *r, cudaStream_t s) {
-    FineArgs a = make_args(L, rho);
-    a.f = f;
-    a.r = r;
-    const int bs = 128;
-    const unsigned nb = (unsigned)((a.P + bs - 1) / bs);
-    k_fine_residual64<<<dim3(nb, 8), bs, 0, s>>>(a, ke, u64);
-}
-
+// ---- FP64 helpers of the refined mode ---------------------------------------------
 __global__ void k_update64(long long n, double *u, const float *__restrict__ e) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i < n) u[i] += (double)e[i];

@@ -316,10 +316,15 @@ __global__ void __launch_bounds__(1024) k_gauss_jordan(double *a, int n, int *fl
         for (int j = tid; j < m; j += nt) a[(long long)k * m + j] *= inv;
         for (int i = tid; i < n; i += nt) col[i] = (i == k) ? 0.0 : a[(long long)i * m + k];
         __syncthreads();
-        const long long total = (long long)n * (m - k);
-        for (long long t = tid; t < total; t += nt) {
-            const int i = (int)(t / (m - k)), j = k + (int)(t % (m - k));
-            if (i != k) a[(long long)i * m + j] -= col[i] * a[(long long)k * m + j];
+        // lanes cover 32 consecutive columns (coalesced), warps stride over rows; the
+        // pivot-row entry stays in a register for all rows of a column chunk
+        {
+            const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
+            for (int j = k + lane; j < m; j += 32) {
+                const double akj = a[(long long)k * m + j];
+                for (int i = warp; i < n; i += nw)
+                    if (i != k) a[(long long)i * m + j] -= col[i] * akj;
+            }
         }
         __syncthreads();
     }

@@ -1,0 +1,111 @@
+"""Bulk-modulus maximisation with OC, the loop of homo3d's optiBulk
+(homogenization/testAutoDiff.cu:282-331), on the library's entry points.
+
+Per iteration: rho_phys = rho^3; update the hierarchy; six solves and C (warm
+start from the previous iteration); obj = -(C00+C11+C22 + 2(C01+C02+C12))/3;
+sensitivities wrt rho_phys, chain rule 3 rho^2; symmetrise; filter; OC update;
+symmetrise the density.  Every step runs on the handle's stream.
+
+    python -m homo3d_b200.optimize --reso 128 --iters 50
+"""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import (COARSE_EXACT, PIN_IDENTITY, PREC_REFINE, Homogenization, OCOptimizer, symmetrize)
+from .density import synthetic_density
+
+
+def bulk_gradient():
+    """d obj / d C of obj = -(C00 + C11 + C22 + 2 (C01 + C02 + C12)) / 3 (upper entries only,
+    as the expression Ch(0,1) etc. records them)."""
+    dC = np.zeros((6, 6), np.float32)
+    for i in range(3):
+        dC[i, i] = -1.0 / 3.0
+    dC[0, 1] = dC[0, 2] = dC[1, 2] = -2.0 / 3.0
+    return dC
+
+
+def bulk_objective(C):
+    return -(C[0, 0] + C[1, 1] + C[2, 2] + 2 * (C[0, 1] + C[0, 2] + C[1, 2])) / 3.0
+
+
+class ConvergeChecker:
+    """Stops when the relative objective change stays below thres for three
+    consecutive iterations after iteration 11 (Framework.cuh:312-343)."""
+
+    def __init__(self, thres=5e-4, length=10):
+        self.thres, self.obj, self.length = thres, [0.0] * length, length
+
+    def is_converge(self, it, obj):
+        self.obj[it % self.length] = obj
+        if it <= 11:
+            return False
+        g = lambda k: self.obj[(it - k) % self.length]
+        return all(abs(g(i) - g(i + 1)) / abs(g(i + 1)) <= self.thres for i in range(3))
+
+
+def optimize_bulk(reso, vol=0.3, iters=50, seed=0, relthres=1e-2, filter_radius=2.0, step=0.05, damp=0.5,
+                  sym="reflect6", finthres=5e-4, stop_on_converge=False, rho0=None, E=10.0, nu=0.3,
+                  coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY, precision=PREC_REFINE, device=0):
+    import torch
+
+    hom = Homogenization(reso, E, nu, coarse_mode, pin_mode, precision, device)
+    n = hom.dims[0]
+    ne = n[0] * n[1] * n[2]
+    dev = torch.device("cuda", device)
+    if rho0 is None:
+        rho0 = synthetic_density(n[0], seed=seed, vol=vol).ravel()
+    rho = torch.tensor(np.asarray(rho0, dtype=np.float32).ravel(), device=dev)
+    rhop = torch.empty_like(rho)
+    sens = torch.empty_like(rho)
+    oc = OCOptimizer(ne, 1e-3, step, damp, handle=hom)
+    dC = bulk_gradient()
+    stream = torch.cuda.ExternalStream(hom.stream, device=dev)
+    checker = ConvergeChecker(finthres)
+    records = []
+    for it in range(iters):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0 = time.perf_counter()
+        e0.record(stream)
+        hom.penalize(rho, rhop, 3.0)
+        hom.update(rhop)
+        C = hom.elasticMatrix(relthres)
+        st = hom.last_stats
+        obj = float(bulk_objective(C))
+        hom.Sensitivity(dC, sens)
+        hom.penalize_backward(rho, sens, 3.0)
+        done = checker.is_converge(it, obj)
+        symmetrize(hom, sens, n, sym)
+        oc.filterSens(sens, rho, n[0], n, filter_radius)
+        oc.update(sens, rho, vol)
+        symmetrize(hom, rho, n, sym)
+        e1.record(stream)
+        e1.synchronize()
+        records.append({"iter": it, "obj": obj, "vcycles": st["vcycles"], "solve_ms": st["solve_ms"],
+                        "iter_ms": e0.elapsed_time(e1), "wall_ms": (time.perf_counter() - t0) * 1e3,
+                        "vol": float(rho.double().mean())})
+        if done and stop_on_converge:
+            break
+    C = hom.elasticMatrix(relthres)
+    out = rho.cpu().numpy()
+    hom.close()
+    return out, C, records
+
+
+def main():
+    p = argparse.ArgumentParser()
+    p.add_argument("--reso", type=int, default=128)
+    p.add_argument("--iters", type=int, default=50)
+    p.add_argument("--vol", type=float, default=0.3)
+    p.add_argument("--seed", type=int, default=0)
+    p.add_argument("--relthres", type=float, default=1e-2)
+    a = p.parse_args()
+    rho, C, rec = optimize_bulk(a.reso, a.vol, a.iters, a.seed, a.relthres)
+    print(json.dumps({"final_C": C.tolist(), "iterations": rec}))
+
+
+if __name__ == "__main__":
+    main()

@@ -148,6 +148,12 @@ H3D_API int h3d_sensitivity(h3d_handle *h, const float dC[36], float *sens_dev, 
 /* forget the stored solutions (warm start) */
 H3D_API int h3d_reset_solutions(h3d_handle *h);
 
+/* ---- SIMP penalisation, the expression rho.pow(p) (TensorExpression.h:517-531) */
+/* rho_phys = rho^p */
+H3D_API int h3d_penalize(h3d_handle *h, const float *rho_dev, float *rho_phys_dev, int64_t n, float p);
+/* grad *= p rho^(p-1): d obj / d rho_phys -> d obj / d rho */
+H3D_API int h3d_penalize_backward(h3d_handle *h, const float *rho_dev, float *grad_dev, int64_t n, float p);
+
 /* ---- design update (OCOptimizer.cu:38-247, TensorExpression.cuh:72-) ----- */
 H3D_API int h3d_oc_update(h3d_handle *h, const float *sens_dev, float *rho_dev, int64_t n, float volratio,
                   float min_rho, float step_limit, float damp);
