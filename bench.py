@@ -115,12 +115,22 @@ def max_over_ranks(dist, value):
     return float(t.item())
 
 
-def launches_per_step(nl, vcycles):
-    """kernel launches of this library in one step (counted from the code paths)"""
-    per_cycle = 8 * 2 + (nl - 2) * 8 * 2 + (nl - 1) + (nl - 1) + (nl - 1) + 1 + 1
-    setup = 1 + 1 + 1 + (nl - 2) + 1 + 1          # density, L1, pin patch, deeper, assemble, inverse
-    solve = 1 + 3 + 2 + vcycles * per_cycle + 2    # rhs, mean removal, f norms, cycles, C
-    return setup + solve
+PRECISION_NAME = {0: "FP32 V-cycles on the correction of an FP64 solution (iterative refinement)",
+                  1: "FP32 solution (the reference's scheme)"}
+
+
+def launches_per_step(nl, vcycles, reso, refine, refinements):
+    """kernel launches of this library in one step, counted from the code paths
+    (checked against an ncu launch list of the same step)"""
+    nblk = -(-(reso ** 3 // 8) // 128) * 3 * 8                  # fine residual norm partials
+    finish = 2 if nblk > 4096 else 1
+    fine = 8 + 1 + 8 + finish                                   # GS, residual, GS, norm
+    coarse = (nl - 2) * (8 + 8 + 8)                             # GS, residual, GS per colour
+    per_cycle = fine + coarse + 2 * (nl - 1) + 1                # restrict, prolong, coarsest apply
+    per_refine = 4                                              # u64 += u, residual64, norm, finish
+    setup = 1 + 1 + 1 + (nl - 2) + 1 + 1                        # density, level 1, pin patch, deeper, assemble, inverse
+    pre, post = (4, 2) if refine else (5, 3)                   # rhs + mean removal (+ convert); (convert +) C
+    return setup + pre + 2 + vcycles * per_cycle + refinements * per_refine + post
 
 
 def make_density(args, rank):
@@ -169,10 +179,11 @@ def gpu_arm(args):
         dist.barrier()
     torch.cuda.synchronize()
     ev0.record(stream)
-    cycles = []
+    cycles, refs = [], []
     for _ in range(args.steps):
         C = step()
         cycles.append(hd.last_stats["vcycles"])
+        refs.append(hd.last_stats["refinements"])
     ev1.record(stream)
     torch.cuda.synchronize()
     if dist is not None:
@@ -185,7 +196,7 @@ def gpu_arm(args):
         hd.close()
         if dist is not None:
             dist.destroy_process_group()
-        return {"metric": metric_name(args), "value": round(ms_per_solve, 3), "unit": "ms", "profile_run": True,
+        return {"metric": metric_name(args), "value": round(ms_per_solve, 3), "unit": "ms", "profile_run": True, "refinements": refs,
                 "vcycles": cycles} if rank == 0 else None
 
     # end to end through the public API with host buffers
@@ -229,7 +240,8 @@ def gpu_arm(args):
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded trig-basis density, reflect6, vol %.2f, rho^3 (SIMP p=3)" % args.vol,
             "config": {"workload": "6-case periodic homogenization solve, %d^3, E=10 nu=0.3, relthres %g, "
-                                   "zero start, plain FP32 MG with FP16 coarse stencils" % (args.reso, args.tol),
+                                   "zero start, MG V(1,1) with 8-colour GS and FP16 coarse stencils, %s" % (
+                                       args.reso, args.tol, PRECISION_NAME[args.precision]),
                        "reso": args.reso, "load_cases": 6, "relthres": args.tol, "levels": hd.nlevels,
                        "pin_mode": args.pin_mode, "parallelism": "replicas" if world > 1 else "single",
                        "l2": "inputs larger than L2 (fields %.1f GB)" % (3 * 18 * 4 * n3 / 1e9)},
@@ -238,7 +250,9 @@ def gpu_arm(args):
             "C00": float(C[0, 0]), "C_e2e_match": bool(np.abs(Ce - C).max() <= 1e-6 * np.abs(C).max()),
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(rho_h.nbytes),
                     "d2h_bytes_per_step": 36 * 8},
-            "gpu_launches": launches_per_step(hd.nlevels, vc) * args.steps,
+            "refinements": refs[-1],
+            "gpu_launches": sum(launches_per_step(hd.nlevels, c, args.reso, args.precision == 0, r)
+                                for c, r in zip(cycles, refs)),
             "roofline": {"kernel": "k_fine_gs (8 colour launches = one sweep)", "bound": "hbm",
                          "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                          "frac": round(achieved / peaks.get("hbm_gbs"), 4), "traffic": None,
@@ -310,7 +324,8 @@ def reference_arm(args):
             "vs_baseline": None, "dtype": "f64", "impl": "reference",
             "data": "synthetic: seeded trig-basis density, reflect6, vol %.2f, rho^3 (SIMP p=3)" % args.vol,
             "config": {"workload": "6-case periodic homogenization solve, %d^3, E=10 nu=0.3, relthres %g, "
-                                   "zero start, plain FP32 MG with FP16 coarse stencils" % (args.reso, args.tol),
+                                   "zero start, MG V(1,1) with 8-colour GS and FP16 coarse stencils, %s" % (
+                                       args.reso, args.tol, PRECISION_NAME[args.precision]),
                        "reso": args.reso, "load_cases": 6, "relthres": args.tol},
             "cpu_baseline": cb,
             "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

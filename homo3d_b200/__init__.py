@@ -22,7 +22,7 @@ import os
 
 import numpy as np
 
-__all__ = ["Homogenization", "MG", "Grid", "OCOptimizer", "H3DError", "symmetrize", "lib", "LIB_PATH",
+__all__ = ["Homogenization", "MG", "Grid", "OCOptimizer", "MMAOptimizer", "H3DError", "symmetrize", "lib", "LIB_PATH",
            "reference_resolution"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -54,11 +54,11 @@ class Config(ctypes.Structure):
 
 class SolveStats(ctypes.Structure):
     _fields_ = [("vcycles", ctypes.c_int), ("status", ctypes.c_int), ("rel_res", ctypes.c_double * 6),
-                ("solve_ms", ctypes.c_double)]
+                ("solve_ms", ctypes.c_double), ("refinements", ctypes.c_int)]
 
     def as_dict(self):
         return {"vcycles": self.vcycles, "status": self.status, "rel_res": list(self.rel_res),
-                "solve_ms": self.solve_ms}
+                "solve_ms": self.solve_ms, "refinements": self.refinements}
 
 
 _lib = None
@@ -97,6 +97,12 @@ _SIGS = {
     "h3d_symmetrize": [_vp, _vp, _ip, ctypes.c_int],
     "h3d_get_field": [_vp, ctypes.c_int, ctypes.c_int, _fp],
     "h3d_set_field": [_vp, ctypes.c_int, ctypes.c_int, _fp],
+    "h3d_mma_create": [ctypes.c_int, ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
+                       ctypes.c_double, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+    "h3d_mma_destroy": [_vp],
+    "h3d_mma_set_bounds": [_vp, _vp, _vp],
+    "h3d_mma_set_bounds_scalar": [_vp, ctypes.c_float, ctypes.c_float],
+    "h3d_mma_update": [_vp, ctypes.c_int, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_void_p), _ip],
 }
 
 
@@ -115,6 +121,8 @@ def lib():
         L.h3d_last_error.restype = ctypes.c_char_p
         L.h3d_stream.argtypes = [_vp]
         L.h3d_stream.restype = ctypes.c_void_p
+        L.h3d_mma_last_error.argtypes = [_vp]
+        L.h3d_mma_last_error.restype = ctypes.c_char_p
         _lib = L
     return _lib
 
@@ -359,6 +367,49 @@ class OCOptimizer:
         hd = self._handle()
         hd.check(lib().h3d_oc_filter(hd._h, _ptr(sens), _ptr(rho), _i3(reso), int(pitchT), radius, int(periodic)))
         hd.sync()
+
+
+class MMAOptimizer:
+    """Method of moving asymptotes (MMAOptimizer, optimization/mmaOptimizer.h:12-36):
+    ``MMAOptimizer(nconstrain, nvar, a0, a, c, d)``, ``setBound``, ``update``.  The
+    design, objective gradient, constraint values and gradients are float32 CUDA
+    tensors; the optimiser keeps its FP64 state on the device."""
+
+    def __init__(self, nconstrain, nvar, a0=1.0, a=0.0, c=1000.0, d=1.0, device=0):
+        h = ctypes.c_void_p()
+        st = lib().h3d_mma_create(int(nconstrain), int(nvar), a0, a, c, d, int(device), ctypes.byref(h))
+        if st != H3D_OK:
+            raise H3DError(st, "h3d_mma_create failed (1 <= nconstrain <= 4, nvar >= 1)")
+        self._h = h
+        self.m, self.n = int(nconstrain), int(nvar)
+        self.newton_steps = 0
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().h3d_mma_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def check(self, st):
+        if st != H3D_OK:
+            raise H3DError(st, lib().h3d_mma_last_error(self._h).decode())
+
+    def setBound(self, xmin, xmax):
+        if hasattr(xmin, "data_ptr"):
+            self.check(lib().h3d_mma_set_bounds(self._h, _ptr(xmin), _ptr(xmax)))
+        else:
+            self.check(lib().h3d_mma_set_bounds_scalar(self._h, float(xmin), float(xmax)))
+
+    def update(self, itn, x, dfdx, gval, dgdx):
+        """x is replaced in place by the new design; dgdx is a sequence of m tensors"""
+        if len(dgdx) != self.m:
+            raise ValueError("dgdx needs one gradient per constraint")
+        ptrs = (ctypes.c_void_p * self.m)(*[_ptr(g).value for g in dgdx])
+        steps = ctypes.c_int(0)
+        self.check(lib().h3d_mma_update(self._h, int(itn), _ptr(x), _ptr(dfdx), _ptr(gval), ptrs,
+                                        ctypes.byref(steps)))
+        self.newton_steps = steps.value
 
 
 def symmetrize(handle, field, reso, sym="reflect6"):

@@ -163,8 +163,8 @@ struct h3d_handle {
     size_t tmp_n = 0;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t vgraph = nullptr;   // one V-cycle on the level-0 field u
-    cudaGraphExec_t rgraph = nullptr;   // one refinement cycle on u64 (FP32 products)
-    cudaGraphExec_t xgraph = nullptr;   // the same with FP64-accumulated residual
+    cudaGraphExec_t rgraph = nullptr;   // refinement step: u64 += u, f = f0 - K u64 (FP32 products)
+    cudaGraphExec_t xgraph = nullptr;   // the same with the FP64-accumulated residual
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool refine() const { return cfg.precision == H3D_PREC_REFINE; }
     bool have_density = false, have_stencils = false;
@@ -242,16 +242,12 @@ int destroy_graph(h3d_handle *h) {
 }
 
 // the V-cycle of MG::v_cycle (MG.cpp:46-70) on the handle's stream; the level-0
-// residual of the down leg also yields the per-case norms.  With refine, the
-// cycle runs on the correction: level-0 f = f0 - K u64 (FP64-exact), u = 0 before
-// and u64 += u after (in exact arithmetic the same iterate as sweeping u64).
-int enqueue_vcycle(h3d_handle *h, float w, bool refine = false, bool exact = false) {
+// residual of the down leg also yields the per-case norms (the stale residual the
+// stopping test of MG.cpp:130-139 reads).  The refined solve runs the same cycle on
+// the FP32 correction u, with level-0 f holding f0 - K u64.
+int enqueue_vcycle(h3d_handle *h, float w) {
     cudaStream_t s = h->stream;
     const int nblk_r = fine_residual_blocks(h->lv[0]);
-    if (refine) {
-        launch_fine_residual64(h->lv[0], h->rho, h->ke, h->f0, h->u64, h->lv[0].f, exact, s);
-        cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * NF * h->lv[0].P.nv, s);
-    }
     for (int l = 0; l < h->nl; l++) {
         if (l > 0) {
             if (l - 1 == 0) launch_fine_residual(h->lv[0], h->rho, h->ke, h->partial, nblk_r, s);
@@ -268,18 +264,37 @@ int enqueue_vcycle(h3d_handle *h, float w, bool refine = false, bool exact = fal
         if (l == 0) launch_fine_gs(h->lv[0], h->rho, h->ke, w, s);
         else launch_coarse_gs(h->lv[l], w, s);
     }
-    if (refine) launch_update64((long long)NF * h->lv[0].P.nv, h->u64, h->lv[0].u, s);
     launch_norm_finish(h->partial, nblk_r, h->d_small, s);
     cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, s);
     return H3D_OK;
 }
 
+// the refinement step of the refined solve: fold the correction into the FP64
+// solution (u64 += u, u = 0), recompute level-0 f = f0 - K u64 from it and read
+// the per-case weighted norms of that (current, not stale) residual
+int enqueue_refine(h3d_handle *h, bool exact) {
+    cudaStream_t s = h->stream;
+    const Level &L0 = h->lv[0];
+    const long long n18 = (long long)NF * L0.P.nv;
+    launch_update64(n18, h->u64, L0.u, s);
+    cudaMemsetAsync(L0.u, 0, sizeof(float) * n18, s);
+    launch_fine_residual64(L0, h->rho, h->ke, h->f0, h->u64, L0.f, exact, s);
+    const int nb = norm_blocks(L0.P);
+    launch_weighted_norm(L0.P, L0.f, h->partial, nb, s);
+    launch_norm_finish(h->partial, nb, h->d_small, s);
+    cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, s);
+    return H3D_OK;
+}
+
+// vgraph: one V-cycle; rgraph / xgraph: the refinement step with FP32 / FP64
+// accumulation of the residual
 int build_graph(h3d_handle *h, bool refine, bool exact = false) {
     cudaGraphExec_t &ge = !refine ? h->vgraph : exact ? h->xgraph : h->rgraph;
     if (ge) return H3D_OK;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    enqueue_vcycle(h, 1.f, refine, exact);
+    if (refine) enqueue_refine(h, exact);
+    else enqueue_vcycle(h, 1.f);
     CK(cudaStreamEndCapture(h->stream, &g));
     cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
@@ -372,7 +387,7 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
     CK(cudaMalloc(&h->aug, sizeof(double) * (size_t)h->ndof * 2 * h->ndof));
     CK(cudaMalloc(&h->d_flag, sizeof(int)));
     // reduction scratch: residual partials, norms, C partials, means, OC
-    size_t pn = (size_t)fine_residual_blocks(h->lv[0]) * NCASE;
+    size_t pn = ((size_t)fine_residual_blocks(h->lv[0]) + NORM_FINISH_CHUNKS) * NCASE;
     pn = std::max(pn, (size_t)4096 * 21);
     pn = std::max(pn, (size_t)2048 * NF + NF);
     pn = std::max(pn, (size_t)4 + 1184);
@@ -604,50 +619,85 @@ int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solv
     CK(cudaSetDevice(h->device));
     const bool refine = h->refine();
     const Level &L0 = h->lv[0];
+    const long long n18 = (long long)NF * L0.P.nv;
     // the field that holds the solution: u64 (refined) or the swept u (FP32)
     auto reset_solution = [&]() -> int {
-        if (refine) CK(cudaMemsetAsync(h->u64, 0, sizeof(double) * NF * L0.P.nv, h->stream));
-        else CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * NF * L0.P.nv, h->stream));
+        if (refine) CK(cudaMemsetAsync(h->u64, 0, sizeof(double) * n18, h->stream));
+        else CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * n18, h->stream));
         return H3D_OK;
     };
     if (!with_guess)
         if (int e = reset_solution()) return e;
+    if (int e = build_graph(h, false)) return e;
     // below ~1e-4 the FP32 products of the difference-form residual would floor the
     // iteration, so tight targets take the FP64-accumulating residual
     const bool exact = refine && tol < 1e-4;
-    if (int e = build_graph(h, refine, exact)) return e;
-    cudaGraphExec_t cycle = !refine ? h->vgraph : exact ? h->xgraph : h->rgraph;
-    double fn[6], rel[6] = {1, 1, 1, 1, 1, 1};
+    if (refine)
+        if (int e = build_graph(h, true, exact)) return e;
+    cudaGraphExec_t refine_step = exact ? h->xgraph : h->rgraph;
+    double fn[6], rel[6] = {1, 1, 1, 1, 1, 1}, base[6] = {1, 1, 1, 1, 1, 1};
     if (int e = weighted_norms(h, L0.P, refine ? h->f0 : L0.f, fn)) return e;
-    int it = 0, status = H3D_OK, explode_left = 2;
+    auto selected = [&](int c) { return ((case_mask >> c) & 1) != 0; };
+    // refined mode: the FP32 V-cycles on the correction measure the stale residual
+    // accurately down to ~1e-6 N of the correction's right-hand side; the correction
+    // is folded into u64 and the residual recomputed exactly once the estimate has
+    // dropped by theta (10x above that floor) or reached the tolerance, and the
+    // solve only stops when that exact residual meets the tolerance too
+    const int nmax = std::max(L0.P.n[0], std::max(L0.P.n[1], L0.P.n[2]));
+    const double theta = std::max(1e-3, 1e-5 * nmax);
+    int nref = 0;
+    auto refine_now = [&]() -> int {
+        nref++;
+        CK(cudaGraphLaunch(refine_step, h->stream));
+        CK(cudaStreamSynchronize(h->stream));
+        for (int c = 0; c < NCASE; c++) base[c] = std::sqrt(h->h_small[c]) / (fn[c] + 1e-10);
+        return H3D_OK;
+    };
     CK(cudaEventRecord(h->ev0, h->stream));
+    if (refine) {
+        CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * n18, h->stream));
+        if (int e = refine_now()) return e;
+    }
+    int it = 0, status = H3D_OK, explode_left = 2;
     const int maxit = 200;
     for (;;) {
-        if (it > 0) {
-            bool done = true;
-            for (int c = 0; c < NCASE; c++)
-                if ((case_mask >> c) & 1)
-                    if (!(rel[c] <= tol)) done = false;
-            if (done) break;
-        }
         if (it >= maxit) { status = H3D_NOT_CONVERGED; break; }
-        CK(cudaGraphLaunch(cycle, h->stream));
+        CK(cudaGraphLaunch(h->vgraph, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         it++;
-        bool bad = false;
+        bool bad = false, done = true, trigger = true;
         for (int c = 0; c < NCASE; c++) {
             rel[c] = std::sqrt(h->h_small[c]) / (fn[c] + 1e-10);
-            if (((case_mask >> c) & 1) && (!(rel[c] <= 10.0))) bad = true;
+            if (!selected(c)) continue;
+            if (!(rel[c] <= 10.0)) bad = true;
+            if (!(rel[c] <= tol)) done = false;
+            if (!(rel[c] <= tol || rel[c] <= theta * base[c])) trigger = false;
         }
         if (bad) {  // MG.cpp:140-182: restart from zero once, then give up
             if (--explode_left <= 0) { status = H3D_DIVERGED; break; }
             if (int e = reset_solution()) return e;
+            if (refine) {
+                CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * n18, h->stream));
+                if (int e = refine_now()) return e;
+            }
+            continue;
         }
+        if (refine && trigger) {
+            if (int e = refine_now()) return e;
+            if (done)
+                for (int c = 0; c < NCASE; c++)
+                    if (selected(c) && !(base[c] <= tol)) done = false;
+        }
+        if (done) break;
     }
+    // a solve that ends without converging still leaves its iterate in u64
+    if (refine && status != H3D_OK)
+        if (int e = refine_now()) return e;
     CK(cudaEventRecord(h->ev1, h->stream));
     CK(cudaEventSynchronize(h->ev1));
     if (stats) {
         stats->vcycles = it;
+        stats->refinements = nref;
         stats->status = status;
         for (int c = 0; c < NCASE; c++) stats->rel_res[c] = rel[c];
         float ms = 0;

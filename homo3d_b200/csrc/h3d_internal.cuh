@@ -127,6 +127,10 @@ void launch_restrict(const Level &F, const Level &C, cudaStream_t s);
 void launch_prolong(const Level &F, const Level &C, int is_root, cudaStream_t s);
 void launch_weighted_norm(const Planes &P, const float *v, double *partial, int nblk, cudaStream_t s);
 int norm_blocks(const Planes &P);
+// sums nblk x 6 partials into out6; above NORM_FINISH_DIRECT blocks it runs in two
+// stages and needs NORM_FINISH_CHUNKS x 6 doubles of scratch behind the partials
+constexpr int NORM_FINISH_DIRECT = 4096;
+constexpr int NORM_FINISH_CHUNKS = 592;
 void launch_norm_finish(const double *partial, int nblk, double *out6, cudaStream_t s);
 void launch_mean_partial(const Planes &P, const float *v, double *partial, int nblk, cudaStream_t s);
 void launch_remove_mean(const Planes &P, float *v, const double *partial, int nblk, cudaStream_t s);

@@ -54,8 +54,14 @@ __device__ __forceinline__ void load_block(const CoarseArgs &a, long long me, fl
     for (int k = 0; k < 9; ++k) s[k] = v[e0 + k - 8 * q0];
 }
 
+// load cases per thread on the coarse levels; the two threads of a vertex run in
+// adjacent CTAs, so the second read of its stencil hits L2
+constexpr int CPTC = 3;
+constexpr int NGC = NCASE / CPTC;
+
 template <int K, bool SELF>
-__device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, int i, int j, int l, float acc[NF]) {
+__device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, int i, int j, int l, int cb,
+                                             float acc[3 * CPTC]) {
     constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
     int ii[3], jj[3], ll[3];
     axis_nbrs_c(i, px, a.h[0], ii[0], ii[2]);
@@ -63,7 +69,7 @@ __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, 
     axis_nbrs_c(l, pz, a.h[2], ll[0], ll[2]);
     ii[1] = i; jj[1] = j; ll[1] = l;
 #pragma unroll
-    for (int q = 0; q < NF; ++q) acc[q] = 0.f;
+    for (int q = 0; q < 3 * CPTC; ++q) acc[q] = 0.f;
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         if (d == 13 && !SELF) continue;
@@ -80,9 +86,9 @@ __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, 
         const int Kn = K ^ ((dx & 1) | ((dy & 1) << 1) | ((dz & 1) << 2));
         const long long nid =
             (long long)Kn * a.P + ii[dx + 1] + (long long)a.h[0] * (jj[dy + 1] + (long long)a.h[1] * ll[dz + 1]);
-        const float *up = a.u + nid;
+        const float *up = a.u + nid + (long long)(3 * cb) * a.nv;
 #pragma unroll
-        for (int c = 0; c < NCASE; ++c) {
+        for (int c = 0; c < CPTC; ++c) {
             const float u0 = up[(3 * c) * a.nv], u1 = up[(3 * c + 1) * a.nv], u2 = up[(3 * c + 2) * a.nv];
             acc[3 * c + 0] = fmaf(s[0], u0, fmaf(s[1], u1, fmaf(s[2], u2, acc[3 * c + 0])));
             acc[3 * c + 1] = fmaf(s[3], u0, fmaf(s[4], u1, fmaf(s[5], u2, acc[3 * c + 1])));
@@ -91,22 +97,31 @@ __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, 
     }
 }
 
+// thread -> (vertex p, first load case cb): CTAs g*NGC .. g*NGC+NGC-1 cover the
+// same 128 vertices with different load cases
+__device__ __forceinline__ void coarse_task(long long &p, int &cb) {
+    cb = (int)(blockIdx.x % NGC) * CPTC;
+    p = (long long)(blockIdx.x / NGC) * blockDim.x + threadIdx.x;
+}
+
 template <int K>
 __global__ void __launch_bounds__(128) k_coarse_gs(CoarseArgs a) {
-    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    long long p;
+    int cb;
+    coarse_task(p, cb);
     if (p >= a.P) return;
     const long long me = (long long)K * a.P + p;
     const int i = (int)(p % a.h[0]);
     const long long t = p / a.h[0];
     const int j = (int)(t % a.h[1]), l = (int)(t / a.h[1]);
-    float acc[NF], ks[9];
-    coarse_apply<K, false>(a, me, i, j, l, acc);
+    float acc[3 * CPTC], ks[9];
+    coarse_apply<K, false>(a, me, i, j, l, cb, acc);
     load_block<13>(a, me, ks);
     const float w = a.w;
 #pragma unroll
-    for (int c = 0; c < NCASE; ++c) {
-        float *u = a.u + me + (3 * c) * a.nv;
-        const float *f = a.f + me + (3 * c) * a.nv;
+    for (int c = 0; c < CPTC; ++c) {
+        float *u = a.u + me + (3 * (cb + c)) * a.nv;
+        const float *f = a.f + me + (3 * (cb + c)) * a.nv;
         float u0 = u[0], u1 = u[a.nv], u2 = u[2 * a.nv];
         u0 = w * (f[0] - acc[3 * c] - ks[1] * u1 - ks[2] * u2) / ks[0] + (1.f - w) * u0;
         u1 = w * (f[a.nv] - acc[3 * c + 1] - ks[3] * u0 - ks[5] * u2) / ks[4] + (1.f - w) * u1;
@@ -118,30 +133,27 @@ __global__ void __launch_bounds__(128) k_coarse_gs(CoarseArgs a) {
 }
 
 template <int K>
-__device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long p) {
+__device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long p, int cb) {
     const long long me = (long long)K * a.P + p;
     const int i = (int)(p % a.h[0]);
     const long long t = p / a.h[0];
     const int j = (int)(t % a.h[1]), l = (int)(t / a.h[1]);
-    float acc[NF];
-    coarse_apply<K, true>(a, me, i, j, l, acc);
+    float acc[3 * CPTC];
+    coarse_apply<K, true>(a, me, i, j, l, cb, acc);
 #pragma unroll
-    for (int q = 0; q < NF; ++q) a.r[q * a.nv + me] = a.f[q * a.nv + me] - acc[q];
+    for (int q = 0; q < 3 * CPTC; ++q) {
+        const long long o = (3 * cb + q) * a.nv + me;
+        a.r[o] = a.f[o] - acc[q];
+    }
 }
 
-__global__ void __launch_bounds__(128) k_coarse_residual(CoarseArgs a) {
-    const long long p = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+template <int K>
+__global__ void __launch_bounds__(128, 5) k_coarse_residual(CoarseArgs a) {
+    long long p;
+    int cb;
+    coarse_task(p, cb);
     if (p >= a.P) return;
-    switch (blockIdx.y) {
-    case 0: coarse_res_vertex<0>(a, p); break;
-    case 1: coarse_res_vertex<1>(a, p); break;
-    case 2: coarse_res_vertex<2>(a, p); break;
-    case 3: coarse_res_vertex<3>(a, p); break;
-    case 4: coarse_res_vertex<4>(a, p); break;
-    case 5: coarse_res_vertex<5>(a, p); break;
-    case 6: coarse_res_vertex<6>(a, p); break;
-    default: coarse_res_vertex<7>(a, p); break;
-    }
+    coarse_res_vertex<K>(a, p, cb);
 }
 
 static CoarseArgs make_cargs(const Level &L) {
@@ -161,7 +173,7 @@ void launch_coarse_gs(const Level &L, float w, cudaStream_t s) {
     CoarseArgs a = make_cargs(L);
     a.w = w;
     const int bs = 128;
-    const unsigned nb = (unsigned)((a.P + bs - 1) / bs);
+    const unsigned nb = (unsigned)((a.P + bs - 1) / bs) * NGC;
     k_coarse_gs<0><<<nb, bs, 0, s>>>(a);
     k_coarse_gs<1><<<nb, bs, 0, s>>>(a);
     k_coarse_gs<2><<<nb, bs, 0, s>>>(a);
@@ -175,8 +187,15 @@ void launch_coarse_gs(const Level &L, float w, cudaStream_t s) {
 void launch_coarse_residual(const Level &L, cudaStream_t s) {
     CoarseArgs a = make_cargs(L);
     const int bs = 128;
-    const unsigned nb = (unsigned)((a.P + bs - 1) / bs);
-    k_coarse_residual<<<dim3(nb, 8), bs, 0, s>>>(a);
+    const unsigned nb = (unsigned)((a.P + bs - 1) / bs) * NGC;
+    k_coarse_residual<0><<<nb, bs, 0, s>>>(a);
+    k_coarse_residual<1><<<nb, bs, 0, s>>>(a);
+    k_coarse_residual<2><<<nb, bs, 0, s>>>(a);
+    k_coarse_residual<3><<<nb, bs, 0, s>>>(a);
+    k_coarse_residual<4><<<nb, bs, 0, s>>>(a);
+    k_coarse_residual<5><<<nb, bs, 0, s>>>(a);
+    k_coarse_residual<6><<<nb, bs, 0, s>>>(a);
+    k_coarse_residual<7><<<nb, bs, 0, s>>>(a);
 }
 
 // ---- transfers ---------------------------------------------------------------
@@ -291,8 +310,31 @@ __global__ void __launch_bounds__(256) k_finish(const double *__restrict__ parti
     block_reduce<N>(s, out, 0);
 }
 
+// first stage of a long reduction: CTA g sums the partials of blocks
+// [g*per, (g+1)*per) into out[g*N + c]
+template <int N>
+__global__ void __launch_bounds__(256) k_finish_chunks(const double *__restrict__ partial, int nblk, int per,
+                                                       double *out) {
+    const int b0 = blockIdx.x * per, b1 = min(nblk, b0 + per);
+    double s[N];
+#pragma unroll
+    for (int c = 0; c < N; ++c) s[c] = 0;
+    for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x)
+#pragma unroll
+        for (int c = 0; c < N; ++c) s[c] += partial[(long long)b * N + c];
+    block_reduce<N>(s, out, blockIdx.x);
+}
+
 void launch_norm_finish(const double *partial, int nblk, double *out6, cudaStream_t s) {
-    k_finish<NCASE><<<1, 256, 0, s>>>(partial, nblk, out6);
+    if (nblk <= NORM_FINISH_DIRECT) {
+        k_finish<NCASE><<<1, 256, 0, s>>>(partial, nblk, out6);
+        return;
+    }
+    // two stages; the first writes NORM_FINISH_CHUNKS x 6 sums behind the partials
+    const int per = (nblk + NORM_FINISH_CHUNKS - 1) / NORM_FINISH_CHUNKS;
+    double *mid = const_cast<double *>(partial) + (long long)nblk * NCASE;
+    k_finish_chunks<NCASE><<<NORM_FINISH_CHUNKS, 256, 0, s>>>(partial, nblk, per, mid);
+    k_finish<NCASE><<<1, 256, 0, s>>>(mid, NORM_FINISH_CHUNKS, out6);
 }
 
 __global__ void __launch_bounds__(NORM_BS) k_sum18(Planes P, const float *__restrict__ v, double *partial) {

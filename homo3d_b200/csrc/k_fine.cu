@@ -19,7 +19,10 @@
 // densities and neighbour rows hit L1/L2): two cases keep the register count near
 // 64 and the occupancy high enough to hide the neighbour-load latency, which is
 // what bounds this kernel; rebuilding the blocks per thread costs FMAs the
-// memory-bound sweep has to spare.
+// memory-bound sweep has to spare.  The operator is applied in difference form,
+// sum_{d != 0} A_d (u_{v+d} - u_v), and the Gauss-Seidel step as u += D^-1 r with
+// the components in the reference's order: the same iteration in exact
+// arithmetic, and in FP32 it keeps rigid translations exact (see fine_apply).
 #include <type_traits>
 
 #include "h3d_internal.cuh"
@@ -104,31 +107,34 @@ struct VertexGeo {
     }
 };
 
-// acc[3c+r] (c < CPT, cases cb..cb+CPT-1) = sum over neighbours (and the vertex
-// itself when SELF) of coupling block times u; u at the pinned origin counts as 0
-template <int K, bool SELF>
+// acc[3c+r] (c < CPT, cases cb..cb+CPT-1) = (K u)_v in difference form,
+// sum over the 26 neighbours of A_d (u_{v+d} - u_v), with u at the pinned origin
+// counted as 0.  Equal to sum_d A_d u_{v+d} in exact arithmetic (the blocks of a
+// row sum to zero), and exact for rigid translations in FP32 too, so the FP32
+// operator agrees with the FP64 difference-form residual of the refined mode on
+// the near-null translation mode of the pinned problem.
+template <int K>
 __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, const VertexGeo<K> &g, int cb,
-                                           float acc[3 * CPT]) {
+                                           const float uv[3 * CPT], float acc[3 * CPT]) {
 #pragma unroll
     for (int q = 0; q < 3 * CPT; ++q) acc[q] = 0.f;
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
-        if (d == 13 && !SELF) continue;
+        if (d == 13) continue;
         int Kn;
         bool pinned;
         const long long nid = g.nbr(a, d, Kn, pinned);
-        if (pinned) continue;
         float A[9];
         g.block(ke, d, A);
         const float *up = a.u + nid + (long long)(3 * cb) * a.nv;
 #pragma unroll
         for (int c = 0; c < CPT; ++c) {
-            const float u0 = __ldg(up + (3 * c) * a.nv);
-            const float u1 = __ldg(up + (3 * c + 1) * a.nv);
-            const float u2 = __ldg(up + (3 * c + 2) * a.nv);
-            acc[3 * c + 0] = fmaf(A[0], u0, fmaf(A[1], u1, fmaf(A[2], u2, acc[3 * c + 0])));
-            acc[3 * c + 1] = fmaf(A[3], u0, fmaf(A[4], u1, fmaf(A[5], u2, acc[3 * c + 1])));
-            acc[3 * c + 2] = fmaf(A[6], u0, fmaf(A[7], u1, fmaf(A[8], u2, acc[3 * c + 2])));
+            const float d0 = (pinned ? 0.f : __ldg(up + (3 * c) * a.nv)) - uv[3 * c];
+            const float d1 = (pinned ? 0.f : __ldg(up + (3 * c + 1) * a.nv)) - uv[3 * c + 1];
+            const float d2 = (pinned ? 0.f : __ldg(up + (3 * c + 2) * a.nv)) - uv[3 * c + 2];
+            acc[3 * c + 0] = fmaf(A[0], d0, fmaf(A[1], d1, fmaf(A[2], d2, acc[3 * c + 0])));
+            acc[3 * c + 1] = fmaf(A[3], d0, fmaf(A[4], d1, fmaf(A[5], d2, acc[3 * c + 1])));
+            acc[3 * c + 2] = fmaf(A[6], d0, fmaf(A[7], d1, fmaf(A[8], d2, acc[3 * c + 2])));
         }
     }
 }
@@ -153,22 +159,27 @@ __global__ void __launch_bounds__(FBS, 5) k_fine_gs(FineArgs a, const __grid_con
         return;
     }
     const VertexGeo<K> g(a, p);
+    float uv[3 * CPT];
+#pragma unroll
+    for (int q = 0; q < 3 * CPT; ++q) uv[q] = a.u[(3 * cb + q) * a.nv + me];
     float acc[3 * CPT];
-    fine_apply<K, false>(a, ke, g, cb, acc);
+    fine_apply<K>(a, ke, g, cb, uv, acc);
     float ks[9];
     g.block(ke, 13, ks);
     const float w = a.w;
+    // the reference's component-wise block Gauss-Seidel step (x, then y, then z,
+    // each with the relaxed values of the earlier components) written as an
+    // update of u by the residual r = f - K u
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
-        float *u = a.u + me + (long long)(3 * (cb + c)) * a.nv;
-        const float *f = a.f + me + (long long)(3 * (cb + c)) * a.nv;
-        float u0 = u[0], u1 = u[a.nv], u2 = u[2 * a.nv];
-        u0 = w * (f[0] - acc[3 * c] - ks[1] * u1 - ks[2] * u2) / ks[0] + (1.f - w) * u0;
-        u1 = w * (f[a.nv] - acc[3 * c + 1] - ks[3] * u0 - ks[5] * u2) / ks[4] + (1.f - w) * u1;
-        u2 = w * (f[2 * a.nv] - acc[3 * c + 2] - ks[6] * u0 - ks[7] * u1) / ks[8] + (1.f - w) * u2;
-        u[0] = u0;
-        u[a.nv] = u1;
-        u[2 * a.nv] = u2;
+        const long long o = me + (long long)(3 * (cb + c)) * a.nv;
+        const float r0 = a.f[o] - acc[3 * c], r1 = a.f[o + a.nv] - acc[3 * c + 1], r2 = a.f[o + 2 * a.nv] - acc[3 * c + 2];
+        const float d0 = w * r0 / ks[0];
+        const float d1 = w * (r1 - ks[3] * d0) / ks[4];
+        const float d2 = w * (r2 - ks[6] * d0 - ks[7] * d1) / ks[8];
+        a.u[o] = uv[3 * c] + d0;
+        a.u[o + a.nv] = uv[3 * c + 1] + d1;
+        a.u[o + 2 * a.nv] = uv[3 * c + 2] + d2;
     }
 }
 
@@ -182,8 +193,11 @@ __device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const Ke
         return;
     }
     const VertexGeo<K> g(a, p);
+    float uv[3 * CPT];
+#pragma unroll
+    for (int q = 0; q < 3 * CPT; ++q) uv[q] = __ldg(a.u + (3 * cb + q) * a.nv + me);
     float acc[3 * CPT];
-    fine_apply<K, true>(a, ke, g, cb, acc);
+    fine_apply<K>(a, ke, g, cb, uv, acc);
     constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
     int i, j, l;
     plane_coords(p, a.h, i, j, l);

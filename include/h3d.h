@@ -83,6 +83,7 @@ typedef struct {
     int status;                 /* h3d_status of the solve */
     double rel_res[6];          /* final ||r||/||f|| per load case */
     double solve_ms;            /* device time of the V-cycle loop */
+    int refinements;            /* refinement steps (u64 += u, exact residual) of the refined mode */
 } h3d_solve_stats;
 
 /* fields addressable through h3d_get_field / h3d_set_field */
@@ -161,6 +162,26 @@ H3D_API int h3d_oc_filter(h3d_handle *h, float *sens_dev, const float *rho_dev, 
                   float radius, int periodic);
 /* sym: 0 reflect3, 1 reflect6, 2 rotate3; lexicographic, pitch nx */
 H3D_API int h3d_symmetrize(h3d_handle *h, float *field_dev, const int reso[3], int sym);
+
+/* ---- MMA optimiser (MMAOptimizer, mmaOptimizer.h:12-36, mmaOpt.cu:429-1062) -
+ * Method of moving asymptotes with m constraints g_i(x) <= 0 (1 <= m <= 4) on n
+ * design variables; FP64 state on the device, float design and gradients at the
+ * boundary.  An MMA handle has its own stream and is independent of h3d_handle. */
+typedef struct h3d_mma h3d_mma;
+/* MMAOptimizer(m, n, a0, a, c, d) (mmaOptimizer.h:20-25) */
+H3D_API int h3d_mma_create(int m, int64_t n, double a0, double a, double c, double d, int device, h3d_mma **out);
+H3D_API int h3d_mma_destroy(h3d_mma *o);
+H3D_API const char *h3d_mma_last_error(const h3d_mma *o);
+/* MMAOptimizer::setBound(float *xmin, float *xmax) (mmaOptimizer.cu:44-48), device arrays */
+H3D_API int h3d_mma_set_bounds(h3d_mma *o, const float *xmin_dev, const float *xmax_dev);
+/* MMAOptimizer::setBound(float xmin, float xmax) (mmaOptimizer.cu:50-54) */
+H3D_API int h3d_mma_set_bounds_scalar(h3d_mma *o, float xmin, float xmax);
+/* MMAOptimizer::update(itn, x, dfdx, gval, dgdx) (mmaOptimizer.cu:61-78): x_dev is
+ * replaced by the new design; gval_dev holds m floats, dgdx_dev is a host array of
+ * m device pointers to n floats; newton_steps (may be NULL) receives the Newton
+ * steps of the subproblem solve */
+H3D_API int h3d_mma_update(h3d_mma *o, int itn, float *x_dev, const float *dfdx_dev, const float *gval_dev,
+                           const float *const *dgdx_dev, int *newton_steps);
 
 /* ---- data exchange (host pointers) ---------------------------------------- */
 H3D_API int h3d_get_field(h3d_handle *h, int level, int field, float *host);

@@ -142,6 +142,28 @@ struct OCOptimizer {
     }
 };
 
+// method of moving asymptotes (mmaOptimizer.h:12-36); device pointers throughout
+struct MMAOptimizer {
+    h3d_mma *o = nullptr;
+    int n, m;
+    MMAOptimizer(int nconstrain, int nvar, double a0_, double a_, double c_, double d_, int device = 0)
+        : n(nvar), m(nconstrain) {
+        if (h3d_mma_create(nconstrain, nvar, a0_, a_, c_, d_, device, &o) != H3D_OK)
+            throw std::runtime_error("h3d_mma_create failed");
+    }
+    ~MMAOptimizer() { h3d_mma_destroy(o); }
+    MMAOptimizer(const MMAOptimizer &) = delete;
+    MMAOptimizer &operator=(const MMAOptimizer &) = delete;
+    void check(int st) {
+        if (st != H3D_OK) throw std::runtime_error(h3d_mma_last_error(o));
+    }
+    void setBound(float *xmin, float *xmax) { check(h3d_mma_set_bounds(o, xmin, xmax)); }
+    void setBound(float xmin, float xmax) { check(h3d_mma_set_bounds_scalar(o, xmin, xmax)); }
+    void update(int itn, float *x, float *dfdx, float *gval, float **dgdx) {
+        check(h3d_mma_update(o, itn, x, dfdx, gval, dgdx, nullptr));
+    }
+};
+
 enum TensorSym { Reflection3 = 0, Reflection6 = 1, Rotate3 = 2 };
 inline void symmetrize(Homogenization &hom, float *field, const int reso[3], TensorSym sym) {
     h3d_check(hom.h, h3d_symmetrize(hom.h, field, reso, (int)sym));

@@ -1,4 +1,4 @@
-"""Python binding of the FP64 CPU oracle (h3d_oracle.c).
+"""Python binding of the FP64 CPU oracle (h3d_oracle.c, mma_oracle.c).
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, by ``__graft_entry__.smoke()`` and by
 the CPU-baseline leg of ``bench.py``.  The product (``homo3d_b200``) never imports it.
@@ -31,6 +31,9 @@ def lib():
         if not os.path.exists(path):
             build()
         L = ctypes.CDLL(path)
+        L.ora_mma_update.restype = ctypes.c_int
+        L.ora_mma_update.argtypes = [ctypes.c_int, ctypes.c_long, ctypes.c_int] + [_dp] * 10 + [
+            ctypes.c_double, _dp, _dp, _dp, ctypes.c_double]
         L.ora_mg_create.restype = ctypes.c_void_p
         L.ora_mg_create.argtypes = [_ip, ctypes.c_double, ctypes.c_double]
         L.ora_mg_destroy.argtypes = [ctypes.c_void_p]
@@ -101,6 +104,39 @@ def hierarchy(reso):
     d = np.frombuffer(dims, dtype=np.int32).reshape(16, 3)[:nl].copy()
     r = np.frombuffer(rat, dtype=np.int32).reshape(16, 3)[:nl].copy()
     return d, r
+
+
+class MMA:
+    """State of one MMA optimiser (MMAOptimizer, optimization/mmaOptimizer.h:12-36):
+    the FP64 design, the two previous designs and the asymptotes."""
+
+    def __init__(self, m, n, a0=1.0, a=0.0, c=1000.0, d=1.0):
+        self.m, self.n, self.a0 = m, n, a0
+        self.a = np.full(m, a, np.float64)
+        self.c = np.full(m, c, np.float64)
+        self.d = np.full(m, d, np.float64)
+        self.xmin = np.zeros(n)
+        self.xmax = np.ones(n)
+        self.xold1 = np.zeros(n)
+        self.xold2 = np.zeros(n)
+        self.low = np.zeros(n)
+        self.upp = np.zeros(n)
+        self.newton = 0
+
+    def set_bound(self, xmin, xmax):
+        self.xmin = np.broadcast_to(np.asarray(xmin, np.float64), (self.n,)).copy()
+        self.xmax = np.broadcast_to(np.asarray(xmax, np.float64), (self.n,)).copy()
+
+    def update(self, itn, x, dfdx, gval, dgdx, move=1.0):
+        """returns the new design; x, dfdx are [n], gval [m], dgdx [m, n]"""
+        xv = np.ascontiguousarray(x, np.float64).copy()
+        df = np.ascontiguousarray(dfdx, np.float64)
+        gv = np.ascontiguousarray(gval, np.float64).reshape(self.m)
+        dg = np.ascontiguousarray(dgdx, np.float64).reshape(self.m, self.n)
+        self.newton = lib().ora_mma_update(self.m, self.n, itn, _d(xv), _d(self.xmin), _d(self.xmax), _d(self.xold1),
+                                           _d(self.xold2), _d(df), _d(gv), _d(dg), _d(self.low), _d(self.upp),
+                                           self.a0, _d(self.a), _d(self.c), _d(self.d), move)
+        return xv
 
 
 def weighted_norm(n, v):

@@ -38,22 +38,30 @@ def test_elastic_matrix_1e5_matches_fp64(torch_cuda, pin):
 
 def test_refined_precision_passes_the_fp32_floor(torch_cuda):
     """An FP32 solution stalls near 1e-6 * N in ||r||/||f|| (chi is O(N) in grid units);
-    the refined mode (FP64 solution, difference-form residual) keeps converging."""
+    the refined mode (FP64 solution, difference-form residual) keeps converging at the
+    FP64 oracle's rate: 12 V-cycles to 1e-7 here (oracle: 11).  With the identity
+    block at the pinned coarse vertex it slows below ~1e-8; the exact Galerkin pin
+    keeps the rate to 1e-9 (oracle: 16 V-cycles)."""
     n = 32
     rho = smooth_density(n, seed=12)
     t = torch_cuda.tensor(rho, dtype=torch_cuda.float32, device="cuda")
     fp32 = H.Homogenization(n, precision=H.PREC_FP32)
     fp32.update(t)
-    fp32.elasticMatrix(1e-8)
+    fp32.elasticMatrix(1e-7)
     assert fp32.last_stats["status"] == H.H3D_NOT_CONVERGED
-    assert min(fp32.last_stats["rel_res"]) > 1e-8
+    assert min(fp32.last_stats["rel_res"]) > 1e-7
     ref = H.Homogenization(n)
     ref.update(t)
-    C = ref.elasticMatrix(1e-8)
+    C = ref.elasticMatrix(1e-7)
     st = ref.last_stats
-    assert st["status"] == H.H3D_OK and max(st["rel_res"]) <= 1e-8 and st["vcycles"] < 40
+    assert st["status"] == H.H3D_OK and max(st["rel_res"]) <= 1e-7 and st["vcycles"] <= 14
     Cref = oracle_C(n, rho, tol=1e-11).elastic_matrix()
     assert rel_err(C, Cref) < 1e-6
+    gal = H.Homogenization(n, pin_mode=H.PIN_GALERKIN)
+    gal.update(t)
+    gal.elasticMatrix(1e-9)
+    st = gal.last_stats
+    assert st["status"] == H.H3D_OK and max(st["rel_res"]) <= 1e-9 and st["vcycles"] <= 18
 
 
 def test_fp32_mode_matches_refined_mode_at_loose_tolerance(torch_cuda):
