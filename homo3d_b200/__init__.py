@@ -84,6 +84,7 @@ _SIGS = {
     "h3d_coarse_solve": [_vp],
     "h3d_reset_displacement": [_vp, ctypes.c_int],
     "h3d_field_norms": [_vp, ctypes.c_int, _dp],
+    "h3d_field_norms_static": [_vp, ctypes.c_int, _dp],
     "h3d_v_cycle": [_vp, ctypes.c_float, ctypes.c_int, ctypes.c_int],
     "h3d_solve": [_vp, ctypes.c_int, ctypes.c_double, ctypes.c_int, ctypes.POINTER(SolveStats)],
     "h3d_elastic_matrix": [_vp, ctypes.c_double, _dp, ctypes.POINTER(SolveStats)],
@@ -342,6 +343,13 @@ class Homogenization(_Handle):
     def field_norms(self, field):
         out = np.zeros(6)
         self.check(lib().h3d_field_norms(self._h, field, out.ctypes.data_as(_dp)))
+        return out
+
+    def field_norms_static(self, field):
+        """field_norms of U, F or R with the reduction scratch in a fixed per-device
+        array (no reference counterpart; calls on one device must not overlap)"""
+        out = np.zeros(6)
+        self.check(lib().h3d_field_norms_static(self._h, field, out.ctypes.data_as(_dp)))
         return out
 
 

@@ -61,9 +61,11 @@ typedef enum {
 
 /* where the level-0 solution lives and how its residual is formed */
 typedef enum {
-    H3D_PREC_REFINE = 0,        /* FP64 solution; per cycle an FP64-exact residual in
-                                   translation-invariant difference form, then an FP32
-                                   V-cycle on the correction (iterative refinement) */
+    H3D_PREC_REFINE = 0,        /* FP64 solution; FP32 V-cycles on the correction, folded
+                                   in with an FP64-exact residual in translation-invariant
+                                   difference form whenever the stale residual has dropped
+                                   by max(1e-3, 1e-5 N) or met the tolerance (iterative
+                                   refinement) */
     H3D_PREC_FP32 = 1           /* FP32 solution swept directly, as the reference does; its
                                    relative residual floors near 1e-6 * N */
 } h3d_precision;
@@ -133,6 +135,12 @@ H3D_API int h3d_reset_displacement(h3d_handle *h, int level);        /* grid.h:2
 /* per-case norm of a level-0 field with the reference's padded-storage
  * multiplicities (grid.cu:1954-1966 v3_norm) */
 H3D_API int h3d_field_norms(h3d_handle *h, int field, double out[6]);
+/* No reference counterpart.  h3d_field_norms for the FP32 fields U, F, R without
+ * touching the handle's scratch: the reduction uses a fixed device array of 2048
+ * x 6 + 6 doubles per device and allocates nothing (H3D_ERR_ARG if a field would
+ * need more blocks).  Calls on handles of one device must not overlap in time;
+ * the first call on a device must not be made while a stream is being captured. */
+H3D_API int h3d_field_norms_static(h3d_handle *h, int field, double out[6]);
 
 /* ---- multigrid (MG.cpp:46-203) ------------------------------------------- */
 H3D_API int h3d_v_cycle(h3d_handle *h, float w, int pre, int post);
