@@ -741,12 +741,19 @@ int h3d_elastic_matrix(h3d_handle *h, double tol, double C[36], h3d_solve_stats 
     if (e != H3D_OK && e != H3D_NOT_CONVERGED) return e;
     if (h->refine()) CK(cudaMemcpyAsync(h->chi, h->u64, sizeof(double) * n18, cudaMemcpyDeviceToDevice, s));
     else launch_convert(n18, L.u, h->chi, s);
-    const int eb = elastic_blocks(L.P);
-    launch_elastic_partials(L.P, h->chi, h->rho, h->ke, h->partial, eb, s);
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    const int eb = energy_tc_blocks(L.P, nsm);
+    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), s));
+    if (launch_elastic_tc(L.P, h->chi, h->rho, h->ke, h->partial, eb, h->d_flag, s) != 0)
+        return fail(h, H3D_ERR_CUDA, "tensor-core energy kernel could not be configured");
     launch_elastic_finish(h->partial, eb, h->d_small, s);
     CKL();
     CK(cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * 21, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&h->h_small[63], h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
+    if (*reinterpret_cast<int *>(&h->h_small[63]))
+        return fail(h, H3D_ERR_CUDA, "tensor-core energy kernel: mbarrier wait timed out");
     const double vol = (double)L.P.nv;
     int t = 0;
     for (int i = 0; i < 6; i++)
@@ -764,8 +771,17 @@ int h3d_sensitivity(h3d_handle *h, const float dC[36], float *sens_dev, int pitc
     if (pitchT < 0) pitchT = P.n[0];
     if (pitchT < P.n[0]) return fail(h, H3D_ERR_ARG, "pitchT smaller than the x resolution");
     CK(cudaMemsetAsync(sens_dev, 0, sizeof(float) * (size_t)pitchT * P.n[1] * P.n[2], h->stream));
-    launch_sensitivity(P, h->chi, h->ke, dC, sens_dev, pitchT, h->stream);
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), h->stream));
+    if (launch_sensitivity_tc(P, h->chi, h->ke, dC, sens_dev, pitchT, energy_tc_blocks(P, nsm), h->d_flag,
+                              h->stream) != 0)
+        return fail(h, H3D_ERR_CUDA, "tensor-core energy kernel could not be configured");
     CKL();
+    CK(cudaMemcpyAsync(&h->h_small[63], h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (*reinterpret_cast<int *>(&h->h_small[63]))
+        return fail(h, H3D_ERR_CUDA, "tensor-core energy kernel: mbarrier wait timed out");
     return H3D_OK;
 }
 

@@ -143,13 +143,15 @@ void launch_galerkin(const Level &F, const Level &C, cudaStream_t s);
 void launch_coarse_assemble(const Level &C, double *aug, cudaStream_t s);
 void launch_gauss_jordan(double *aug, int n, int *flag, cudaStream_t s);
 void launch_coarse_apply(const Level &C, const double *aug, int project, cudaStream_t s);
-// homogenized tensor, sensitivities (k_homog.cu)
-void launch_elastic_partials(const Planes &P, const double *chi, const float *rho, const KeMat &ke,
-                             double *partial, int nblk, cudaStream_t s);
-int elastic_blocks(const Planes &P);
+// homogenized tensor and sensitivities on the tensor cores (k_homog_tc.cu):
+// a persistent grid of energy_tc_blocks CTAs; *flag is set if an mbarrier wait
+// timed out; the launchers return -1 when the kernel cannot be configured
+int energy_tc_blocks(const Planes &P, int num_sms);
+int launch_elastic_tc(const Planes &P, const double *chi, const float *rho, const KeMat &ke, double *partial,
+                      int nblk, int *flag, cudaStream_t s);
+int launch_sensitivity_tc(const Planes &P, const double *chi, const KeMat &ke, const float *dc36, float *sens,
+                          int pitch, int nblk, int *flag, cudaStream_t s);
 void launch_elastic_finish(const double *partial, int nblk, double *out21, cudaStream_t s);
-void launch_sensitivity(const Planes &P, const double *chi, const KeMat &ke, const float *dc36, float *sens,
-                        int pitch, cudaStream_t s);
 // design (k_design.cu)
 void launch_density_in(const int n[3], const float *src, int pitch, float *dst, cudaStream_t s);
 void launch_penalize(long long n, const float *rho, float *out, float p, int backward, cudaStream_t s);

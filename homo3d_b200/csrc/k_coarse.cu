@@ -199,17 +199,21 @@ void launch_coarse_residual(const Level &L, cudaStream_t s) {
 }
 
 // ---- transfers ---------------------------------------------------------------
+// Restriction: one thread per (coarse vertex, load case) (blockIdx.y = case), three
+// accumulators over the 27 (ratio 2) gathered fine vertices, so the large levels
+// have enough independent loads in flight.  Prolongation: one thread per fine
+// vertex and all 18 planes (at most 8 coarse parents, most with weight 0).
 __global__ void __launch_bounds__(256) k_restrict(Planes F, Planes C, int r0, int r1, int r2,
                                                   const float *__restrict__ rf, float *fc) {
     const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (v >= C.nv) return;
+    const int c = blockIdx.y;
     const int k = color_of_index(C, v);
     int x, y, z;
     vpos(C, k, v - C.base[k], x, y, z);
     const float pr = (float)(r0 * r1 * r2);
-    float acc[NF];
-#pragma unroll
-    for (int q = 0; q < NF; ++q) acc[q] = 0.f;
+    const float *src = rf + (long long)(3 * c) * F.nv;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
     for (int ox = -r0 + 1; ox < r0; ox++) {
         const int fx = wrap(r0 * x + ox, F.n[0]);
         for (int oy = -r1 + 1; oy < r1; oy++) {
@@ -218,13 +222,16 @@ __global__ void __launch_bounds__(256) k_restrict(Planes F, Planes C, int r0, in
                 const int fz = wrap(r2 * z + oz, F.n[2]);
                 const float w = (float)((r0 - abs(ox)) * (r1 - abs(oy)) * (r2 - abs(oz))) / pr;
                 const long long fi = vidx(F, fx, fy, fz);
-#pragma unroll
-                for (int q = 0; q < NF; ++q) acc[q] = fmaf(__ldg(&rf[q * F.nv + fi]), w, acc[q]);
+                a0 = fmaf(__ldg(&src[fi]), w, a0);
+                a1 = fmaf(__ldg(&src[F.nv + fi]), w, a1);
+                a2 = fmaf(__ldg(&src[2 * F.nv + fi]), w, a2);
             }
         }
     }
-#pragma unroll
-    for (int q = 0; q < NF; ++q) fc[q * C.nv + v] = acc[q];
+    float *dst = fc + (long long)(3 * c) * C.nv + v;
+    dst[0] = a0;
+    dst[C.nv] = a1;
+    dst[2 * C.nv] = a2;
 }
 
 __global__ void __launch_bounds__(256) k_prolong(Planes F, Planes C, int r0, int r1, int r2, int is_root,
@@ -256,8 +263,8 @@ __global__ void __launch_bounds__(256) k_prolong(Planes F, Planes C, int r0, int
 
 void launch_restrict(const Level &F, const Level &C, cudaStream_t s) {
     const int bs = 256;
-    k_restrict<<<(unsigned)((C.P.nv + bs - 1) / bs), bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.r,
-                                                                  C.f);
+    const dim3 grid((unsigned)((C.P.nv + bs - 1) / bs), NCASE);
+    k_restrict<<<grid, bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.r, C.f);
 }
 
 void launch_prolong(const Level &F, const Level &C, int is_root, cudaStream_t s) {

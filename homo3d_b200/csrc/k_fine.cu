@@ -57,11 +57,22 @@ __device__ __forceinline__ void plane_coords(long long p, const int h[3], int &i
     l = (int)(t / h[1]);
 }
 
-// geometry of one colour-K vertex: its element densities and neighbour plane coords
+// first element (bit pattern w = ex | ey<<1 | ez<<2 of the element's offset from
+// the vertex) shared by the vertex and its neighbour d, -1 if none
+__host__ __device__ constexpr int first_shared(int d) {
+    for (int w = 0; w < 8; ++w) {
+        const int bx = 1 - (w & 1) + d % 3 - 1, by = 1 - ((w >> 1) & 1) + d / 3 % 3 - 1, bz = 1 - (w >> 2) + d / 9 - 1;
+        if (bx >= 0 && bx <= 1 && by >= 0 && by <= 1 && bz >= 0 && bz <= 1) return w;
+    }
+    return -1;
+}
+
+// geometry of one colour-K vertex: its element densities and the offsets of its
+// neighbours inside a colour plane (32-bit: a field plane holds < 2^31 vertices)
 template <int K>
 struct VertexGeo {
     float rw[8];
-    int ii[3], jj[3], ll[3];
+    unsigned X[3], Y[3], Z[3];  // plane offsets of the neighbour rows: i, h0*j, h0*h1*l
     __device__ __forceinline__ VertexGeo(const FineArgs &a, long long p) {
         constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
         int i, j, l;
@@ -70,40 +81,63 @@ struct VertexGeo {
         const int xe0 = x == 0 ? a.n[0] - 1 : x - 1;
         const int ye0 = y == 0 ? a.n[1] - 1 : y - 1;
         const int ze0 = z == 0 ? a.n[2] - 1 : z - 1;
+        const unsigned n0 = (unsigned)a.n[0], n01 = (unsigned)a.n[0] * (unsigned)a.n[1];
 #pragma unroll
         for (int w = 0; w < 8; ++w) {
-            const int ex = (w & 1) ? x : xe0, ey = ((w >> 1) & 1) ? y : ye0, ez = (w >> 2) ? z : ze0;
-            rw[w] = RHO_PENAL_MIN + __ldg(&a.rho[ex + (long long)a.n[0] * (ey + (long long)a.n[1] * ez)]);
+            const unsigned ex = (w & 1) ? x : xe0, ey = ((w >> 1) & 1) ? y : ye0, ez = (w >> 2) ? z : ze0;
+            rw[w] = RHO_PENAL_MIN + __ldg(&a.rho[ex + n0 * ey + n01 * ez]);
         }
+        int ii[3], jj[3], ll[3];
         axis_nbrs(i, px, a.h[0], ii[0], ii[2]);
         axis_nbrs(j, py, a.h[1], jj[0], jj[2]);
         axis_nbrs(l, pz, a.h[2], ll[0], ll[2]);
         ii[1] = i; jj[1] = j; ll[1] = l;
-    }
-    // coupling block of neighbour d (compile-time d after unrolling)
-    __device__ __forceinline__ void block(const KeMat &ke, int d, float A[9]) const {
-        const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
+        const unsigned h0 = (unsigned)a.h[0], h01 = (unsigned)a.h[0] * (unsigned)a.h[1];
 #pragma unroll
-        for (int k = 0; k < 9; ++k) A[k] = 0.f;
-#pragma unroll
-        for (int w = 0; w < 8; ++w) {
-            const int ex = w & 1, ey = (w >> 1) & 1, ez = w >> 2;
-            const int bx = 1 - ex + dx, by = 1 - ey + dy, bz = 1 - ez + dz;
-            if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
-            const int an = 7 - w, bn = bx + 2 * by + 4 * bz;
-#pragma unroll
-            for (int r = 0; r < 3; ++r)
-#pragma unroll
-                for (int c = 0; c < 3; ++c)
-                    A[3 * r + c] = fmaf(rw[w], ke.k[(3 * an + r) * 24 + 3 * bn + c], A[3 * r + c]);
+        for (int t = 0; t < 3; ++t) {
+            X[t] = (unsigned)ii[t];
+            Y[t] = h0 * (unsigned)jj[t];
+            Z[t] = h01 * (unsigned)ll[t];
         }
     }
-    __device__ __forceinline__ long long nbr(const FineArgs &a, int d, int &Kn, bool &pinned) const {
+    // coupling block of neighbour d (compile-time d after unrolling):
+    // sum over the shared elements e of rho_e Ke[a_e][b_e].  The shared elements
+    // are mirror images of the first one across the axes where they differ, and
+    // an isotropic Ke is invariant under the mirrors up to the sign of the
+    // components mirrored, so entry (r,c) = Ke[a_0][b_0](r,c) * sum_e +-rho_e with
+    // the sign set by whether r and c lie on the mirrored axes: four signed
+    // density sums per block instead of 9 FMAs per shared element.
+    __device__ __forceinline__ void block(const KeMat &ke, int d, float A[9]) const {
+        const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
+        const int w0 = first_shared(d);
+        float cs[8];  // cs[m]: signed sum for the axis mask m = (1<<r) ^ (1<<c)
+#pragma unroll
+        for (int m = 0; m < 8; ++m) cs[m] = 0.f;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            const int bx = 1 - (w & 1) + dx, by = 1 - ((w >> 1) & 1) + dy, bz = 1 - (w >> 2) + dz;
+            if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+            const int mir = w ^ w0;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                if (m != 0 && m != 3 && m != 5 && m != 6) continue;
+                cs[m] += (__popc(mir & m) & 1) ? -rw[w] : rw[w];
+            }
+        }
+        const int an = 7 - w0;
+        const int bn = (1 - (w0 & 1) + dx) + 2 * (1 - ((w0 >> 1) & 1) + dy) + 4 * (1 - (w0 >> 2) + dz);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) A[3 * r + c] = ke.k[(3 * an + r) * 24 + 3 * bn + c] * cs[(1 << r) ^ (1 << c)];
+    }
+    // index of neighbour d in its colour plane set, and whether it is the pinned origin
+    __device__ __forceinline__ unsigned nbr(const FineArgs &a, int d, int &Kn, bool &pinned) const {
         const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
         Kn = K ^ ((dx & 1) | ((dy & 1) << 1) | ((dz & 1) << 2));
-        const int ni = ii[dx + 1], nj = jj[dy + 1], nl = ll[dz + 1];
-        pinned = (Kn == 7) && ((ni | nj | nl) == 0);
-        return (long long)Kn * a.P + ni + (long long)a.h[0] * (nj + (long long)a.h[1] * nl);
+        const unsigned off = X[dx + 1] + Y[dy + 1] + Z[dz + 1];
+        pinned = (Kn == 7) && (off == 0u);
+        return (unsigned)Kn * (unsigned)a.P + off;
     }
 };
 
@@ -123,7 +157,7 @@ __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, c
         if (d == 13) continue;
         int Kn;
         bool pinned;
-        const long long nid = g.nbr(a, d, Kn, pinned);
+        const unsigned nid = g.nbr(a, d, Kn, pinned);
         float A[9];
         g.block(ke, d, A);
         const float *up = a.u + nid + (long long)(3 * cb) * a.nv;
@@ -271,7 +305,7 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
         if (d == 13) continue;
         int Kn;
         bool pinned;
-        const long long nid = g.nbr(a, d, Kn, pinned);
+        const unsigned nid = g.nbr(a, d, Kn, pinned);
         float A[9];
         g.block(ke, d, A);
         const double *up = u64 + nid + (long long)(3 * cb) * a.nv;
@@ -293,7 +327,7 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
 }
 
 template <bool EXACT>
-__global__ void __launch_bounds__(FBS) k_fine_residual64(FineArgs a, const __grid_constant__ KeMat ke,
+__global__ void __launch_bounds__(FBS, 4) k_fine_residual64(FineArgs a, const __grid_constant__ KeMat ke,
                                                          const double *__restrict__ u64) {
     long long p;
     int cb;
