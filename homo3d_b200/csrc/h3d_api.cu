@@ -905,21 +905,23 @@ int h3d_set_field(h3d_handle *h, int level, int field, const float *host) {
     return H3D_OK;
 }
 
-// h3d_field_norms for the FP32 level-0 fields with the reduction scratch in a
-// file-scope device array (k_static_norm.cu) instead of the handle's buffer; it
-// allocates nothing.  Calls on handles of the same device must not overlap in
-// time (they share that array); the first call on a device looks up the array's
-// address and must not be made during stream capture.
+// h3d_field_norms for the FP32 level-0 fields for callers that must not have
+// device memory allocated (or the handle's scratch touched) during the call: the
+// reduction runs in a fixed file-scope device array (k_static_norm.cu).  Calls on
+// one device share that array, so calls that overlap in time race; the first call
+// on a device looks up the array's address and should precede any stream capture.
 int h3d_field_norms_static(h3d_handle *h, int field, double out[6]) {
     if (!h || !out) return H3D_ERR_ARG;
     CK(cudaSetDevice(h->device));
     const Level &L = h->lv[0];
     const float *v = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r : nullptr;
     if (!v) return fail(h, H3D_ERR_ARG, "static-scratch norms take the FP32 fields U, F, R");
+    const int nb = norm_blocks(L.P);
+    if (nb > STATIC_NORM_MAX_BLOCKS)
+        return fail(h, H3D_ERR_ARG, "field needs more norm blocks than the static scratch holds (2048)");
     const double *tot = static_norm_totals(h->device);
-    if (!tot) return fail(h, H3D_ERR_CUDA, "scratch symbol lookup failed");
-    if (launch_weighted_norm_static(L.P, v, norm_blocks(L.P), h->stream) != 0)
-        return fail(h, H3D_ERR_ARG, "field needs more norm blocks than the static scratch holds");
+    if (!tot || launch_weighted_norm_static(h->device, L.P, v, nb, h->stream) != 0)
+        return fail(h, H3D_ERR_CUDA, "cudaGetSymbolAddress of the static norm scratch failed");
     CKL();
     double sums[NCASE];
     CK(cudaMemcpyAsync(sums, tot, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, h->stream));

@@ -160,11 +160,12 @@ void launch_oc(const float *sens, float *rho, float *rho_new, long long n, float
 void launch_filter(const int n[3], int pitch, const float *sens, const float *rho, float *out, float radius,
                    int periodic, cudaStream_t s);
 void launch_symmetrize(const int n[3], float *v, int sym, cudaStream_t s);
-// weighted norms with file-scope device scratch (k_static_norm.cu); the launcher
-// returns -1 when nblk exceeds STATIC_NORM_MAX_BLOCKS, the totals pointer is the
-// device address of the six sums (nullptr if the symbol lookup failed)
+// weighted norms with file-scope device scratch (k_static_norm.cu), on the
+// current device: the launcher returns -1 when nblk exceeds STATIC_NORM_MAX_BLOCKS
+// and -2 when the array's address cannot be looked up; the totals pointer is the
+// device address of the six sums (nullptr if the lookup failed)
 constexpr int STATIC_NORM_MAX_BLOCKS = 2048;
-int launch_weighted_norm_static(const Planes &P, const float *v, int nblk, cudaStream_t s);
+int launch_weighted_norm_static(int device, const Planes &P, const float *v, int nblk, cudaStream_t s);
 const double *static_norm_totals(int device);
 // field conversion (k_coarse.cu)
 void launch_field_to_lex(const Planes &P, const float *src, float *dst_lex, cudaStream_t s);

@@ -135,11 +135,15 @@ H3D_API int h3d_reset_displacement(h3d_handle *h, int level);        /* grid.h:2
 /* per-case norm of a level-0 field with the reference's padded-storage
  * multiplicities (grid.cu:1954-1966 v3_norm) */
 H3D_API int h3d_field_norms(h3d_handle *h, int field, double out[6]);
-/* No reference counterpart.  h3d_field_norms for the FP32 fields U, F, R without
- * touching the handle's scratch: the reduction uses a fixed device array of 2048
- * x 6 + 6 doubles per device and allocates nothing (H3D_ERR_ARG if a field would
- * need more blocks).  Calls on handles of one device must not overlap in time;
- * the first call on a device must not be made while a stream is being captured. */
+/* No reference counterpart.  h3d_field_norms for the FP32 fields U, F, R, for
+ * callers that must not have device memory allocated during the call (their
+ * device memory is owned by another allocator, or they cannot take the device
+ * synchronisation of cudaMalloc / cudaFree): the reduction runs in a fixed device
+ * array of 2048 x 6 + 6 doubles (about 96 KB, held by every GPU that loads the
+ * library until exit) and nothing is allocated; H3D_ERR_ARG if a field would need
+ * more than 2048 blocks.  Calls on one device share the array, so overlapping
+ * calls race; the first call on a device looks up the array's address and should
+ * come before any stream capture. */
 H3D_API int h3d_field_norms_static(h3d_handle *h, int field, double out[6]);
 
 /* ---- multigrid (MG.cpp:46-203) ------------------------------------------- */
