@@ -22,7 +22,8 @@ import os
 
 import numpy as np
 
-__all__ = ["Homogenization", "MG", "Grid", "OCOptimizer", "MMAOptimizer", "H3DError", "symmetrize", "lib", "LIB_PATH",
+__all__ = ["Homogenization", "MG", "Grid", "OCOptimizer", "MMAOptimizer", "WarmNet", "H3DError", "symmetrize", "lib",
+           "LIB_PATH",
            "reference_resolution"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -104,6 +105,16 @@ _SIGS = {
     "h3d_mma_set_bounds": [_vp, _vp, _vp],
     "h3d_mma_set_bounds_scalar": [_vp, ctypes.c_float, ctypes.c_float],
     "h3d_mma_update": [_vp, ctypes.c_int, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_void_p), _ip],
+    "h3d_warmnet_create": [ctypes.c_int, ctypes.c_int, ctypes.c_uint64, ctypes.c_int, ctypes.POINTER(ctypes.c_void_p)],
+    "h3d_warmnet_destroy": [_vp],
+    "h3d_warmnet_num_params": [_vp, ctypes.POINTER(ctypes.c_int64)],
+    "h3d_warmnet_get_params": [_vp, _fp],
+    "h3d_warmnet_set_params": [_vp, _fp],
+    "h3d_warmnet_get_grads": [_vp, _fp],
+    "h3d_warmnet_forward": [_vp, _vp, ctypes.c_int, _vp],
+    "h3d_warmnet_gradients": [_vp, _vp, _vp, ctypes.c_int, _dp],
+    "h3d_warmnet_train_step": [_vp, _vp, _vp, ctypes.c_int, ctypes.c_float, _dp],
+    "h3d_warm_start_learned": [_vp, _vp],
 }
 
 
@@ -124,6 +135,8 @@ def lib():
         L.h3d_stream.restype = ctypes.c_void_p
         L.h3d_mma_last_error.argtypes = [_vp]
         L.h3d_mma_last_error.restype = ctypes.c_char_p
+        L.h3d_warmnet_last_error.argtypes = [_vp]
+        L.h3d_warmnet_last_error.restype = ctypes.c_char_p
         _lib = L
     return _lib
 
@@ -331,6 +344,10 @@ class Homogenization(_Handle):
     def reset_solutions(self):
         self.check(lib().h3d_reset_solutions(self._h))
 
+    def warm_start_learned(self, net):
+        """stored solutions from a WarmNet's prediction for the current density"""
+        self.check(lib().h3d_warm_start_learned(self._h, net._h))
+
     def penalize(self, rho, rho_phys, p=3.0):
         """rho_phys = rho^p on the handle's stream (the reference's rho.pow(3))."""
         self.check(lib().h3d_penalize(self._h, _ptr(rho), _ptr(rho_phys), rho.numel(), float(p)))
@@ -418,6 +435,76 @@ class MMAOptimizer:
         self.check(lib().h3d_mma_update(self._h, int(itn), _ptr(x), _ptr(dfdx), _ptr(gval), ptrs,
                                         ctypes.byref(steps)))
         self.newton_steps = steps.value
+
+
+class WarmNet:
+    """Learned warm start (no reference counterpart): a periodic 3-D conv
+    encoder-decoder from the density averaged to ``reso``^3 cells to chi / N at the
+    ``reso``^3 coarse vertices, with hand-written CUDA forward, backward and Adam.
+    Inputs are float32 CUDA tensors [batch, reso^3]; outputs [batch, 18, reso^3]."""
+
+    NOUT = 18
+
+    def __init__(self, reso=32, max_batch=8, seed=0, device=0):
+        h = ctypes.c_void_p()
+        st = lib().h3d_warmnet_create(int(reso), int(max_batch), int(seed), int(device), ctypes.byref(h))
+        if st != H3D_OK:
+            raise H3DError(st, "h3d_warmnet_create failed (reso: multiple of 8 in 8..128, max_batch 1..64)")
+        self._h, self.reso, self.max_batch = h, int(reso), int(max_batch)
+        n = ctypes.c_int64()
+        self.check(lib().h3d_warmnet_num_params(self._h, ctypes.byref(n)))
+        self.num_params = n.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().h3d_warmnet_destroy(self._h)
+            self._h = None
+
+    __del__ = close
+
+    def check(self, st):
+        if st != H3D_OK:
+            raise H3DError(st, lib().h3d_warmnet_last_error(self._h).decode())
+
+    def params(self):
+        out = np.empty(self.num_params, np.float32)
+        self.check(lib().h3d_warmnet_get_params(self._h, out.ctypes.data_as(_fp)))
+        return out
+
+    def set_params(self, p):
+        a = np.ascontiguousarray(p, np.float32)
+        if a.size != self.num_params:
+            raise ValueError("expected %d parameters" % self.num_params)
+        self.check(lib().h3d_warmnet_set_params(self._h, a.ctypes.data_as(_fp)))
+
+    def grads(self):
+        out = np.empty(self.num_params, np.float32)
+        self.check(lib().h3d_warmnet_get_grads(self._h, out.ctypes.data_as(_fp)))
+        return out
+
+    def forward(self, x):
+        import torch
+        b = x.shape[0]
+        y = torch.empty((b, self.NOUT, self.reso ** 3), dtype=torch.float32, device=x.device)
+        self.check(lib().h3d_warmnet_forward(self._h, _ptr(x), b, _ptr(y)))
+        return y
+
+    def gradients(self, x, t):
+        loss = ctypes.c_double()
+        self.check(lib().h3d_warmnet_gradients(self._h, _ptr(x), _ptr(t), x.shape[0], ctypes.byref(loss)))
+        return loss.value
+
+    def train_step(self, x, t, lr=1e-3):
+        loss = ctypes.c_double()
+        self.check(lib().h3d_warmnet_train_step(self._h, _ptr(x), _ptr(t), x.shape[0], float(lr),
+                                                ctypes.byref(loss)))
+        return loss.value
+
+    def save(self, path):
+        self.params().tofile(path)
+
+    def load(self, path):
+        self.set_params(np.fromfile(path, dtype=np.float32))
 
 
 def symmetrize(handle, field, reso, sym="reflect6"):

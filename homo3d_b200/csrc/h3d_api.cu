@@ -165,6 +165,8 @@ struct h3d_handle {
     cudaGraphExec_t vgraph = nullptr;   // one V-cycle on the level-0 field u
     cudaGraphExec_t rgraph = nullptr;   // refinement step: u64 += u, f = f0 - K u64 (FP32 products)
     cudaGraphExec_t xgraph = nullptr;   // the same with the FP64-accumulated residual
+    cudaGraphExec_t sgraph = nullptr;   // a solve's V-cycle: vgraph + rigid-translation deflation
+    double *pin_state = nullptr;        // deflation: F[18], pending shift T[18], plane sums[18]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool refine() const { return cfg.precision == H3D_PREC_REFINE; }
     bool have_density = false, have_stencils = false;
@@ -238,14 +240,16 @@ int destroy_graph(h3d_handle *h) {
     if (h->vgraph) { cudaGraphExecDestroy(h->vgraph); h->vgraph = nullptr; }
     if (h->rgraph) { cudaGraphExecDestroy(h->rgraph); h->rgraph = nullptr; }
     if (h->xgraph) { cudaGraphExecDestroy(h->xgraph); h->xgraph = nullptr; }
+    if (h->sgraph) { cudaGraphExecDestroy(h->sgraph); h->sgraph = nullptr; }
     return H3D_OK;
 }
 
 // the V-cycle of MG::v_cycle (MG.cpp:46-70) on the handle's stream; the level-0
 // residual of the down leg also yields the per-case norms (the stale residual the
 // stopping test of MG.cpp:130-139 reads).  The refined solve runs the same cycle on
-// the FP32 correction u, with level-0 f holding f0 - K u64.
-int enqueue_vcycle(h3d_handle *h, float w) {
+// the FP32 correction u, with level-0 f holding f0 - K u64.  Inside a solve the
+// cycle ends with the rigid-translation deflation (launch_pin_deflate).
+int enqueue_vcycle(h3d_handle *h, float w, bool deflate = false) {
     cudaStream_t s = h->stream;
     const int nblk_r = fine_residual_blocks(h->lv[0]);
     for (int l = 0; l < h->nl; l++) {
@@ -264,37 +268,52 @@ int enqueue_vcycle(h3d_handle *h, float w) {
         if (l == 0) launch_fine_gs(h->lv[0], h->rho, h->ke, w, s);
         else launch_coarse_gs(h->lv[l], w, s);
     }
+    if (deflate) launch_pin_deflate(h->lv[0], h->rho, h->ke, h->pin_state, s);
     launch_norm_finish(h->partial, nblk_r, h->d_small, s);
     cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, s);
     return H3D_OK;
 }
 
+// deflation state from the current level-0 f: F = sum of f over the vertices but
+// the origin, pending shift T = 0
+void enqueue_pin_init(h3d_handle *h) {
+    const Level &L0 = h->lv[0];
+    const int nb = norm_blocks(L0.P);
+    launch_mean_partial(L0.P, L0.f, h->partial, nb, h->stream);
+    launch_sum18_finish(h->partial, nb, h->pin_state + 2 * NF, h->stream);
+    launch_pin_init(L0, h->pin_state + 2 * NF, h->pin_state, h->stream);
+}
+
 // the refinement step of the refined solve: fold the correction into the FP64
-// solution (u64 += u, u = 0), recompute level-0 f = f0 - K u64 from it and read
-// the per-case weighted norms of that (current, not stale) residual
+// solution (u64 += u + T, u = 0), recompute level-0 f = f0 - K u64 from it, read
+// the per-case weighted norms of that (current, not stale) residual and restart
+// the deflation state from it
 int enqueue_refine(h3d_handle *h, bool exact) {
     cudaStream_t s = h->stream;
     const Level &L0 = h->lv[0];
     const long long n18 = (long long)NF * L0.P.nv;
-    launch_update64(n18, h->u64, L0.u, s);
+    launch_update64(L0, h->u64, L0.u, h->pin_state + NF, s);
     cudaMemsetAsync(L0.u, 0, sizeof(float) * n18, s);
     launch_fine_residual64(L0, h->rho, h->ke, h->f0, h->u64, L0.f, exact, s);
     const int nb = norm_blocks(L0.P);
     launch_weighted_norm(L0.P, L0.f, h->partial, nb, s);
     launch_norm_finish(h->partial, nb, h->d_small, s);
     cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, s);
+    enqueue_pin_init(h);
     return H3D_OK;
 }
 
-// vgraph: one V-cycle; rgraph / xgraph: the refinement step with FP32 / FP64
-// accumulation of the residual
-int build_graph(h3d_handle *h, bool refine, bool exact = false) {
-    cudaGraphExec_t &ge = !refine ? h->vgraph : exact ? h->xgraph : h->rgraph;
+// vgraph: one V-cycle (h3d_v_cycle); sgraph: the same with the deflation (solves);
+// rgraph / xgraph: the refinement step with FP32 / FP64 accumulation of the residual
+enum GraphKind { G_VCYCLE, G_SOLVE, G_REFINE, G_REFINE_EXACT };
+int build_graph(h3d_handle *h, GraphKind kind) {
+    cudaGraphExec_t &ge = kind == G_VCYCLE ? h->vgraph : kind == G_SOLVE ? h->sgraph
+                        : kind == G_REFINE_EXACT ? h->xgraph : h->rgraph;
     if (ge) return H3D_OK;
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal));
-    if (refine) enqueue_refine(h, exact);
-    else enqueue_vcycle(h, 1.f);
+    if (kind == G_REFINE || kind == G_REFINE_EXACT) enqueue_refine(h, kind == G_REFINE_EXACT);
+    else enqueue_vcycle(h, 1.f, kind == G_SOLVE);
     CK(cudaStreamEndCapture(h->stream, &g));
     cudaError_t e = cudaGraphInstantiate(&ge, g, 0);
     cudaGraphDestroy(g);
@@ -395,6 +414,8 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
     CK(cudaMalloc(&h->partial, sizeof(double) * pn));
     CK(cudaMalloc(&h->d_small, sizeof(double) * 64));
     CK(cudaMallocHost(&h->h_small, sizeof(double) * 64));
+    CK(cudaMalloc(&h->pin_state, sizeof(double) * 3 * NF));
+    CK(cudaMemset(h->pin_state, 0, sizeof(double) * 3 * NF));
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
     CK(cudaEventCreate(&h->ev0));
     CK(cudaEventCreate(&h->ev1));
@@ -425,7 +446,7 @@ int h3d_destroy(h3d_handle *h) {
     }
     cudaFree(h->rho); cudaFree(h->chi); cudaFree(h->u64); cudaFree(h->f0);
     cudaFree(h->q); cudaFree(h->d_ked); cudaFree(h->aug);
-    cudaFree(h->d_flag); cudaFree(h->partial); cudaFree(h->d_small); cudaFree(h->tmp);
+    cudaFree(h->d_flag); cudaFree(h->partial); cudaFree(h->d_small); cudaFree(h->tmp); cudaFree(h->pin_state);
     if (h->h_small) cudaFreeHost(h->h_small);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -603,7 +624,7 @@ int h3d_v_cycle(h3d_handle *h, float w, int pre, int post) {
     if (pre != 1 || post != 1) return fail(h, H3D_ERR_ARG, "only V(1,1) is supported");
     CK(cudaSetDevice(h->device));
     if (w == 1.f) {
-        if (int e = build_graph(h, false)) return e;
+        if (int e = build_graph(h, G_VCYCLE)) return e;
         CK(cudaGraphLaunch(h->vgraph, h->stream));
     } else {
         enqueue_vcycle(h, w);
@@ -628,12 +649,22 @@ int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solv
     };
     if (!with_guess)
         if (int e = reset_solution()) return e;
-    if (int e = build_graph(h, false)) return e;
+    // balance the right-hand side: a periodic load has zero net force, and the few
+    // ulps of net force left by FP32 rounding would, in the pinned problem, become a
+    // point load at the origin; remove each plane's mean over the unique vertices
+    {
+        float *rhs = refine ? h->f0 : L0.f;
+        const int nb = norm_blocks(L0.P);
+        launch_mean_partial(L0.P, rhs, h->partial, nb, h->stream);
+        launch_remove_mean(L0.P, rhs, h->partial, nb, h->stream);
+        CKL();
+    }
+    if (int e = build_graph(h, G_SOLVE)) return e;
     // below ~1e-4 the FP32 products of the difference-form residual would floor the
     // iteration, so tight targets take the FP64-accumulating residual
     const bool exact = refine && tol < 1e-4;
     if (refine)
-        if (int e = build_graph(h, true, exact)) return e;
+        if (int e = build_graph(h, exact ? G_REFINE_EXACT : G_REFINE)) return e;
     cudaGraphExec_t refine_step = exact ? h->xgraph : h->rgraph;
     double fn[6], rel[6] = {1, 1, 1, 1, 1, 1}, base[6] = {1, 1, 1, 1, 1, 1};
     if (int e = weighted_norms(h, L0.P, refine ? h->f0 : L0.f, fn)) return e;
@@ -654,15 +685,25 @@ int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solv
         return H3D_OK;
     };
     CK(cudaEventRecord(h->ev0, h->stream));
+    CK(cudaMemsetAsync(h->pin_state + NF, 0, sizeof(double) * NF, h->stream));  // no pending shift
+    if (!refine) enqueue_pin_init(h);
     if (refine) {
         CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * n18, h->stream));
         if (int e = refine_now()) return e;
+        // a starting guess worse than zero (relative residual above 1) is dropped
+        bool worse = false;
+        for (int c = 0; c < NCASE; c++)
+            if (selected(c) && !(base[c] <= 1.0)) worse = true;
+        if (with_guess && worse) {
+            if (int e = reset_solution()) return e;
+            if (int e = refine_now()) return e;
+        }
     }
     int it = 0, status = H3D_OK, explode_left = 2;
     const int maxit = 200;
     for (;;) {
         if (it >= maxit) { status = H3D_NOT_CONVERGED; break; }
-        CK(cudaGraphLaunch(h->vgraph, h->stream));
+        CK(cudaGraphLaunch(h->sgraph, h->stream));
         CK(cudaStreamSynchronize(h->stream));
         it++;
         bool bad = false, done = true, trigger = true;
@@ -675,10 +716,14 @@ int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solv
         }
         if (bad) {  // MG.cpp:140-182: restart from zero once, then give up
             if (--explode_left <= 0) { status = H3D_DIVERGED; break; }
+            if (!refine) launch_pin_fold(L0, h->rho, h->ke, h->pin_state, h->stream);  // restores f
             if (int e = reset_solution()) return e;
+            CK(cudaMemsetAsync(h->pin_state + NF, 0, sizeof(double) * NF, h->stream));
             if (refine) {
                 CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * n18, h->stream));
                 if (int e = refine_now()) return e;
+            } else {
+                enqueue_pin_init(h);
             }
             continue;
         }
@@ -690,9 +735,11 @@ int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solv
         }
         if (done) break;
     }
-    // a solve that ends without converging still leaves its iterate in u64
+    // a solve that ends without converging still leaves its iterate in u64; the FP32
+    // solution takes the pending shift and f is restored
     if (refine && status != H3D_OK)
         if (int e = refine_now()) return e;
+    if (!refine) launch_pin_fold(L0, h->rho, h->ke, h->pin_state, h->stream);
     CK(cudaEventRecord(h->ev1, h->stream));
     CK(cudaEventSynchronize(h->ev1));
     if (stats) {
@@ -900,6 +947,25 @@ int h3d_set_field(h3d_handle *h, int level, int field, const float *host) {
         if (field == H3D_FIELD_F && level == 0 && h->refine())
             CK(cudaMemcpyAsync(h->f0, dst, sizeof(float) * n18, cudaMemcpyDeviceToDevice, h->stream));
     }
+    CKL();
+    CK(cudaStreamSynchronize(h->stream));
+    return H3D_OK;
+}
+
+int h3d_warm_start_learned(h3d_handle *h, h3d_warmnet *net) {
+    if (!h || !net) return H3D_ERR_ARG;
+    const Level &L = h->lv[0];
+    const int N = L.P.n[0], R = warmnet_reso(net);
+    if (L.P.n[1] != N || L.P.n[2] != N || N % R != 0)
+        return fail(h, H3D_ERR_ARG, "learned warm start needs a cubic grid whose size is a multiple of the network's");
+    if (warmnet_device(net) != h->device) return fail(h, H3D_ERR_ARG, "network and handle on different devices");
+    if (!h->rho) return fail(h, H3D_ERR_STATE, "no density");
+    CK(cudaSetDevice(h->device));
+    if (int e = ensure_tmp(h, (size_t)R * R * R)) return e;
+    launch_warmnet_density_pool(h->rho, N, R, h->tmp, h->stream);
+    const float *y = nullptr;
+    if (warmnet_forward_on(net, h->tmp, h->stream, &y) != H3D_OK) return fail(h, H3D_ERR_CUDA, "network forward failed");
+    launch_warmnet_to_chi(L.P, y, R, h->chi, h->stream);
     CKL();
     CK(cudaStreamSynchronize(h->stream));
     return H3D_OK;

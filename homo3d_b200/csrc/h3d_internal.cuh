@@ -116,7 +116,15 @@ void launch_rhs(const Level &L, const float *rho, const RhsTab &g, float *f, cud
 // r = f - K u with u in FP64, the operator in difference form (refined precision)
 void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const float *f, const double *u64,
                             float *r, bool exact, cudaStream_t s);
-void launch_update64(long long n, double *u64, const float *e, cudaStream_t s);
+// u64 += e + T over the level-0 vertices but the pinned origin
+void launch_update64(const Level &L, double *u64, const float *e, const double *T, cudaStream_t s);
+// rigid-translation deflation of the pinned level-0 problem (k_fine.cu); state is
+// 36 doubles: F (sum of f over the vertices but the origin) and the pending shift T
+void launch_pin_deflate(const Level &L, const float *rho, const KeMat &ke, double *state, cudaStream_t s);
+// state from the 18 plane sums of level-0 f: F = sums - f(origin), T = 0
+void launch_pin_init(const Level &L, const double *sums, double *state, cudaStream_t s);
+// FP32 solutions: u += T (but the origin), f restored near the origin, T = 0
+void launch_pin_fold(const Level &L, const float *rho, const KeMat &ke, double *state, cudaStream_t s);
 void launch_convert(long long n, const float *src, double *dst, cudaStream_t s);
 void launch_convert(long long n, const double *src, float *dst, cudaStream_t s);
 void launch_remove_mean64(const Planes &P, double *v, double *partial, int nblk, cudaStream_t s);
@@ -134,6 +142,7 @@ constexpr int NORM_FINISH_CHUNKS = 592;
 void launch_norm_finish(const double *partial, int nblk, double *out6, cudaStream_t s);
 void launch_mean_partial(const Planes &P, const float *v, double *partial, int nblk, cudaStream_t s);
 void launch_remove_mean(const Planes &P, float *v, const double *partial, int nblk, cudaStream_t s);
+void launch_sum18_finish(const double *partial, int nblk, double *out, cudaStream_t s);
 // Galerkin and coarsest solve (k_galerkin.cu)
 void launch_galerkin_l1(const Level &F, const Level &C, const float *rho, const float *q, int nsub,
                         cudaStream_t s);
@@ -167,6 +176,15 @@ void launch_symmetrize(const int n[3], float *v, int sym, cudaStream_t s);
 constexpr int STATIC_NORM_MAX_BLOCKS = 2048;
 int launch_weighted_norm_static(int device, const Planes &P, const float *v, int nblk, cudaStream_t s);
 const double *static_norm_totals(int device);
+// learned warm start (k_warmnet.cu)
+}  // namespace h3d
+struct h3d_warmnet;
+namespace h3d {
+int warmnet_reso(const h3d_warmnet *n);
+int warmnet_device(const h3d_warmnet *n);
+int warmnet_forward_on(h3d_warmnet *n, const float *x, cudaStream_t s, const float **y);
+void launch_warmnet_density_pool(const float *rho, int N, int R, float *out, cudaStream_t s);
+void launch_warmnet_to_chi(const Planes &P, const float *y, int R, double *chi, cudaStream_t s);
 // field conversion (k_coarse.cu)
 void launch_field_to_lex(const Planes &P, const float *src, float *dst_lex, cudaStream_t s);
 void launch_field_from_lex(const Planes &P, const float *src_lex, float *dst, cudaStream_t s);

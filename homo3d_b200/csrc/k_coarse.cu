@@ -366,6 +366,11 @@ void launch_mean_partial(const Planes &P, const float *v, double *partial, int n
     k_sum18<<<nblk, NORM_BS, 0, s>>>(P, v, partial);
 }
 
+// the 18 plane sums of launch_mean_partial's partials into out
+void launch_sum18_finish(const double *partial, int nblk, double *out, cudaStream_t s) {
+    k_finish<NF><<<1, 256, 0, s>>>(partial, nblk, out);
+}
+
 // partial holds nblk rows of 18 sums; the total goes to partial[nblk*18 ..]
 void launch_remove_mean(const Planes &P, float *v, const double *partial, int nblk, cudaStream_t s) {
     double *tot = const_cast<double *>(partial) + (long long)nblk * NF;

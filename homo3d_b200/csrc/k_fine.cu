@@ -425,9 +425,130 @@ void launch_rhs(const Level &L, const float *rho, const RhsTab &g, float *f, cud
 }
 
 // ---- FP64 helpers of the refined mode ---------------------------------------------
-__global__ void k_update64(long long n, double *u, const float *__restrict__ e) {
+// u64 += e + T (T: the pending rigid translation of each of the 18 planes, see
+// k_pin_deflate); the pinned origin (colour 7, first vertex) keeps its value
+__global__ void k_update64(long long nv, double *u, const float *__restrict__ e, const double *__restrict__ T,
+                           long long pin) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n) u[i] += (double)e[i];
+    if (i >= nv * NF) return;
+    const long long v = i % nv;
+    if (v == pin) return;
+    u[i] += (double)e[i] + T[i / nv];
+}
+
+// ---- rigid-translation deflation of the pinned problem -------------------------
+// In the pinned system (rows v != origin, u_origin = 0) the rigid translation t'
+// (1 on every vertex but the origin) is the lowest-energy mode: t'^T K t' is only
+// the origin's 3x3 self block A_pp.  The FP16 coarse operators misjudge that tiny
+// eigenvalue, and once the solution itself is small (near-uniform designs, where
+// f nearly cancels) the V-cycle's error in this mode can grow from cycle to cycle.
+// After every V-cycle of a solve the translation error is therefore removed
+// exactly: s = sum_{v != origin} r_v = F + q with F = sum_{v != origin} f_v and
+// q = sum_{d != 0} A_{p,d} u_{p+d} (because the columns of the periodic K sum to
+// zero), alpha = A_pp^-1 s per case.  Instead of adding alpha to every vertex the
+// shift is kept pending in T and folded into f (f_v += K_{v,p} alpha at the 26
+// neighbours of the origin, F -= A_pp alpha), which is the same iteration; T joins
+// the solution when it is next folded (k_update64, k_pin_fold).
+// state[0..17] = F per (case, component), state[18..35] = T.
+__global__ void k_pin_deflate(FineArgs a, const __grid_constant__ KeMat ke, double *state) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const VertexGeo<7> g(a, 0);
+    double q[NF];
+#pragma unroll
+    for (int i = 0; i < NF; ++i) q[i] = 0.0;
+    for (int d = 0; d < 27; ++d) {
+        if (d == 13) continue;
+        int Kn;
+        bool pinned;
+        const unsigned nid = g.nbr(a, d, Kn, pinned);
+        if (pinned) continue;
+        float A[9];
+        g.block(ke, d, A);
+        for (int c = 0; c < NCASE; ++c)
+            for (int r = 0; r < 3; ++r) {
+                double t = 0;
+                for (int k = 0; k < 3; ++k) t += (double)A[3 * r + k] * (double)a.u[(3 * c + k) * a.nv + nid];
+                q[3 * c + r] += t;
+            }
+    }
+    float Af[9];
+    g.block(ke, 13, Af);
+    double M[9];
+    for (int k = 0; k < 9; ++k) M[k] = (double)Af[k];
+    // inverse of the 3x3 self block by cofactors
+    const double c00 = M[4] * M[8] - M[5] * M[7], c01 = M[5] * M[6] - M[3] * M[8], c02 = M[3] * M[7] - M[4] * M[6];
+    const double det = M[0] * c00 + M[1] * c01 + M[2] * c02;
+    if (!(det > 0.0)) return;  // not positive definite: leave the iterate alone
+    const double inv[9] = {c00 / det, (M[2] * M[7] - M[1] * M[8]) / det, (M[1] * M[5] - M[2] * M[4]) / det,
+                           c01 / det, (M[0] * M[8] - M[2] * M[6]) / det, (M[2] * M[3] - M[0] * M[5]) / det,
+                           c02 / det, (M[1] * M[6] - M[0] * M[7]) / det, (M[0] * M[4] - M[1] * M[3]) / det};
+    double al[NF];
+    for (int c = 0; c < NCASE; ++c) {
+        double sres[3];
+        for (int r = 0; r < 3; ++r) sres[r] = state[3 * c + r] + q[3 * c + r];
+        for (int r = 0; r < 3; ++r) al[3 * c + r] = inv[3 * r] * sres[0] + inv[3 * r + 1] * sres[1] + inv[3 * r + 2] * sres[2];
+        for (int r = 0; r < 3; ++r) {
+            state[NF + 3 * c + r] += al[3 * c + r];
+            state[3 * c + r] -= M[3 * r] * al[3 * c] + M[3 * r + 1] * al[3 * c + 1] + M[3 * r + 2] * al[3 * c + 2];
+        }
+    }
+    // f at the origin's neighbours: K_{v,p} alpha = A_{p,d}^T alpha
+    for (int d = 0; d < 27; ++d) {
+        if (d == 13) continue;
+        int Kn;
+        bool pinned;
+        const unsigned nid = g.nbr(a, d, Kn, pinned);
+        if (pinned) continue;
+        float A[9];
+        g.block(ke, d, A);
+        for (int c = 0; c < NCASE; ++c)
+            for (int r = 0; r < 3; ++r) {
+                const double t = (double)A[r] * al[3 * c] + (double)A[3 + r] * al[3 * c + 1] + (double)A[6 + r] * al[3 * c + 2];
+                float *fp = const_cast<float *>(a.f) + (3 * c + r) * a.nv + nid;
+                *fp = (float)((double)*fp + t);
+            }
+    }
+}
+
+// state: F = (plane sums of f) - f at the origin, T = 0
+__global__ void k_pin_init(const double *__restrict__ sums, const float *__restrict__ f, long long nv, long long pin,
+                           double *state) {
+    const int i = threadIdx.x;
+    if (i >= NF) return;
+    state[i] = sums[i] - (double)f[(long long)i * nv + pin];
+    state[NF + i] = 0.0;
+}
+
+// FP32 solutions: u += T on every vertex but the origin (grid-stride)
+__global__ void k_pin_fold_u(long long nv, float *u, const double *__restrict__ state, long long pin) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv * NF;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long v = i % nv;
+        if (v != pin) u[i] = (float)((double)u[i] + state[NF + i / nv]);
+    }
+}
+
+// undo the fold of T into f at the origin's neighbours, then T = 0
+__global__ void k_pin_restore_f(FineArgs a, const __grid_constant__ KeMat ke, double *state) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const VertexGeo<7> g(a, 0);
+    for (int d = 0; d < 27; ++d) {
+        if (d == 13) continue;
+        int Kn;
+        bool pinned;
+        const unsigned nid = g.nbr(a, d, Kn, pinned);
+        if (pinned) continue;
+        float A[9];
+        g.block(ke, d, A);
+        for (int c = 0; c < NCASE; ++c)
+            for (int r = 0; r < 3; ++r) {
+                const double *T = state + NF + 3 * c;
+                const double t = (double)A[r] * T[0] + (double)A[3 + r] * T[1] + (double)A[6 + r] * T[2];
+                float *fp = const_cast<float *>(a.f) + (3 * c + r) * a.nv + nid;
+                *fp = (float)((double)*fp - t);
+            }
+    }
+    for (int i = 0; i < NF; ++i) state[NF + i] = 0.0;
 }
 
 __global__ void k_f32_to_f64(long long n, const float *__restrict__ s, double *d) {
@@ -440,8 +561,19 @@ __global__ void k_f64_to_f32(long long n, const double *__restrict__ s, float *d
     if (i < n) d[i] = (float)s[i];
 }
 
-void launch_update64(long long n, double *u64, const float *e, cudaStream_t s) {
-    k_update64<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, u64, e);
+void launch_update64(const Level &L, double *u64, const float *e, const double *T, cudaStream_t s) {
+    const long long n = (long long)NF * L.P.nv;
+    k_update64<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(L.P.nv, u64, e, T, L.P.base[7]);
+}
+void launch_pin_deflate(const Level &L, const float *rho, const KeMat &ke, double *state, cudaStream_t s) {
+    k_pin_deflate<<<1, 32, 0, s>>>(make_args(L, rho), ke, state);
+}
+void launch_pin_init(const Level &L, const double *sums, double *state, cudaStream_t s) {
+    k_pin_init<<<1, 32, 0, s>>>(sums, L.f, L.P.nv, L.P.base[7], state);
+}
+void launch_pin_fold(const Level &L, const float *rho, const KeMat &ke, double *state, cudaStream_t s) {
+    k_pin_fold_u<<<1184, 256, 0, s>>>(L.P.nv, L.u, state, L.P.base[7]);
+    k_pin_restore_f<<<1, 32, 0, s>>>(make_args(L, rho), ke, state);
 }
 void launch_convert(long long n, const float *src, double *dst, cudaStream_t s) {
     k_f32_to_f64<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, src, dst);

@@ -49,7 +49,10 @@ class ConvergeChecker:
 
 def optimize_bulk(reso, vol=0.3, iters=50, seed=0, relthres=1e-2, filter_radius=2.0, step=0.05, damp=0.5,
                   sym="reflect6", finthres=5e-4, stop_on_converge=False, rho0=None, E=10.0, nu=0.3,
-                  coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY, precision=PREC_REFINE, device=0):
+                  coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY, precision=PREC_REFINE, device=0,
+                  on_solve=None):
+    """The OC loop of testAutoDiff.cu:282-331 (bulk modulus); on_solve(hom, rho_phys)
+    is called after every solve (e.g. to record training pairs)."""
     import torch
 
     hom = Homogenization(reso, E, nu, coarse_mode, pin_mode, precision, device)
@@ -74,6 +77,8 @@ def optimize_bulk(reso, vol=0.3, iters=50, seed=0, relthres=1e-2, filter_radius=
         hom.update(rhop)
         C = hom.elasticMatrix(relthres)
         st = hom.last_stats
+        if on_solve is not None:
+            on_solve(hom, rhop)
         obj = float(bulk_objective(C))
         hom.Sensitivity(dC, sens)
         hom.penalize_backward(rho, sens, 3.0)

@@ -195,6 +195,34 @@ H3D_API int h3d_mma_set_bounds_scalar(h3d_mma *o, float xmin, float xmax);
 H3D_API int h3d_mma_update(h3d_mma *o, int itn, float *x_dev, const float *dfdx_dev, const float *gval_dev,
                            const float *const *dgdx_dev, int *newton_steps);
 
+/* ---- learned warm start (no reference counterpart) ------------------------
+ * A periodic 3-D convolutional encoder-decoder (channels 16-32-64-64, ~0.26 M
+ * FP32 parameters) from the density averaged to reso^3 cells to the six cell
+ * solutions chi / N at the reso^3 coarse vertices, trained with its own CUDA
+ * forward / backward / Adam kernels.  Tensors are float [batch][channel][reso^3],
+ * voxel x + reso*(y + reso*z); targets have 18 channels (case, component). */
+typedef struct h3d_warmnet h3d_warmnet;
+/* reso: multiple of 8 in 8..128; max_batch: 1..64 */
+H3D_API int h3d_warmnet_create(int reso, int max_batch, uint64_t seed, int device, h3d_warmnet **out);
+H3D_API int h3d_warmnet_destroy(h3d_warmnet *n);
+H3D_API const char *h3d_warmnet_last_error(const h3d_warmnet *n);
+H3D_API int h3d_warmnet_num_params(const h3d_warmnet *n, int64_t *count);
+H3D_API int h3d_warmnet_get_params(h3d_warmnet *n, float *host);
+H3D_API int h3d_warmnet_set_params(h3d_warmnet *n, const float *host);
+H3D_API int h3d_warmnet_get_grads(h3d_warmnet *n, float *host);
+H3D_API int h3d_warmnet_forward(h3d_warmnet *n, const float *x_dev, int batch, float *y_dev);
+/* gradients of the mean squared error of one batch (replacing stored gradients) */
+H3D_API int h3d_warmnet_gradients(h3d_warmnet *n, const float *x_dev, const float *t_dev, int batch, double *loss);
+/* one Adam step on one batch; *loss = the batch's error before the step */
+H3D_API int h3d_warmnet_train_step(h3d_warmnet *n, const float *x_dev, const float *t_dev, int batch, float lr,
+                                   double *loss);
+/* replace the handle's stored solutions (the starting point of the next
+ * h3d_elastic_matrix) by the network's prediction for the handle's density, on
+ * cubic grids whose size is a multiple of the network's reso.  In the refined
+ * precision mode a solve whose starting residual exceeds that of a zero start
+ * restarts from zero. */
+H3D_API int h3d_warm_start_learned(h3d_handle *h, h3d_warmnet *net);
+
 /* ---- data exchange (host pointers) ---------------------------------------- */
 H3D_API int h3d_get_field(h3d_handle *h, int level, int field, float *host);
 H3D_API int h3d_set_field(h3d_handle *h, int level, int field, const float *host);

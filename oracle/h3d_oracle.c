@@ -870,9 +870,53 @@ void ora_mg_remove_mean(ora_mg *m) {
 /* repeat V-cycles until every case has ||r||/||f|| <= tol (stale residual taken
  * after pre-smoothing, as the reference does); returns the number of cycles;
  * hist receives [cycle][6] relative residuals (up to maxit rows) */
+/* Rigid-translation deflation after each V-cycle of a solve (the CUDA library's
+ * k_pin_deflate): in the pinned system the translation t' (1 on every vertex but
+ * the origin) has energy t'^T K t' = A_pp, the origin's unpinned self block, and
+ * the residual's translation component is s = sum_{v != 0} f_v + (K u)_origin
+ * (the columns of the periodic operator sum to zero).  u += A_pp^-1 s on every
+ * vertex but the origin removes the error in that mode exactly.  The reference
+ * has no such step (it projects the translations out of the coarsest right-hand
+ * side, grid.cpp:349-374). */
+static void pin_deflate(ora_mg *m) {
+    ora_level *L = &m->lv[0];
+    const int *n = L->n;
+    double F[NF] = {0};
+    for (long v = 1; v < L->nv; v++)
+        for (int i = 0; i < NF; i++) F[i] += L->f[v * NF + i];
+    double q[NF], A[9];
+    fine_apply(m, L->u, 0, 0, 0, 0, q, A);
+    const double c00 = A[4] * A[8] - A[5] * A[7], c01 = A[5] * A[6] - A[3] * A[8], c02 = A[3] * A[7] - A[4] * A[6];
+    const double det = A[0] * c00 + A[1] * c01 + A[2] * c02;
+    if (!(det > 0)) return;
+    const double inv[9] = {c00 / det, (A[2] * A[7] - A[1] * A[8]) / det, (A[1] * A[5] - A[2] * A[4]) / det,
+                           c01 / det, (A[0] * A[8] - A[2] * A[6]) / det, (A[2] * A[3] - A[0] * A[5]) / det,
+                           c02 / det, (A[1] * A[6] - A[0] * A[7]) / det, (A[0] * A[4] - A[1] * A[3]) / det};
+    double al[NF];
+    for (int c = 0; c < NCASE; c++)
+        for (int r = 0; r < 3; r++) {
+            al[3 * c + r] = 0;
+            for (int k = 0; k < 3; k++) al[3 * c + r] += inv[3 * r + k] * (F[3 * c + k] + q[3 * c + k]);
+        }
+#pragma omp parallel for
+    for (long v = 1; v < L->nv; v++)
+        for (int i = 0; i < NF; i++) L->u[v * NF + i] += al[i];
+    (void)n;
+}
+
 int ora_mg_solve(ora_mg *m, double tol, int maxit, double *hist) {
     ora_level *L = &m->lv[0];
     double fn[NCASE], rn[NCASE];
+    /* balanced right-hand side (zero net force per case and component), as the
+     * CUDA library enforces before every solve */
+    {
+        double mean[NF] = {0};
+        for (long v = 0; v < L->nv; v++)
+            for (int i = 0; i < NF; i++) mean[i] += L->f[v * NF + i];
+        for (int i = 0; i < NF; i++) mean[i] /= (double)L->nv;
+        for (long v = 0; v < L->nv; v++)
+            for (int i = 0; i < NF; i++) L->f[v * NF + i] -= mean[i];
+    }
     ora_weighted_norm(L->n, L->f, fn);
     int it = 0;
     for (;;) {
@@ -883,6 +927,7 @@ int ora_mg_solve(ora_mg *m, double tol, int maxit, double *hist) {
         }
         if (it >= maxit) break;
         ora_mg_vcycle(m, 1.0);
+        pin_deflate(m);
         it++;
         /* the level-0 residual left by the down leg */
         ora_weighted_norm(L->n, L->r, rn);

@@ -38,7 +38,7 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_binding_signatures_cover_the_header():
-    bound = set(H._SIGS) | {"h3d_last_error", "h3d_stream", "h3d_mma_last_error"}
+    bound = set(H._SIGS) | {"h3d_last_error", "h3d_stream", "h3d_mma_last_error", "h3d_warmnet_last_error"}
     assert bound == set(declared_symbols())
 
 
