@@ -51,6 +51,12 @@ static inline int vcolor(int x, int y, int z) {
     return ((x + 1) & 1) | (((y + 1) & 1) << 1) | (((z + 1) & 1) << 2);
 }
 static inline double to_half(double v) { return (double)(_Float16)v; }
+/* fp16 == 3: FP32 storage of the coarse stencils (not the reference's scheme;
+ * used to show that FP16 storage is what makes the V-cycle diverge on
+ * high-contrast designs) */
+static void round_row_f32(double *st) {
+    for (int q = 0; q < 243; q++) st[q] = (double)(float)st[q];
+}
 
 /* ------------------------------------------------------------------------- */
 /* element matrix (templateMatrix.cpp:95-201)                                 */
@@ -192,7 +198,7 @@ typedef struct {
     int ndof;
     double *lu;
     int *piv;
-    int fp16; /* store coarse stencils rounded to FP16 */
+    int fp16; /* coarse stencil storage: 1 FP16 (the reference's), 0 FP64, 3 FP32 */
     int project; /* remove rigid translations from the coarsest right-hand side */
     int pin_identity; /* add the identity block at the pinned node (reference patch) */
 } ora_mg;
@@ -549,7 +555,7 @@ static void l1_combine(const ora_mg *m, int lc, int x, int y, int z, double out[
                 double p[243];
                 partial(m, lc, X, p);
                 clamp_diag(p + 9 * 13);
-                if (m->fp16) {
+                if (m->fp16 == 1) {
                     for (int q = 0; q < 243; q++) {
                         p[q] = to_half(p[q]);
                         /* FP16 accumulation: each sum correctly rounded to half (native
@@ -562,6 +568,7 @@ static void l1_combine(const ora_mg *m, int lc, int x, int y, int z, double out[
                 first = 0;
             }
     (void)first;
+    if (m->fp16 == 3) round_row_f32(acc);
     memcpy(out, acc, sizeof(acc));
 }
 
@@ -611,8 +618,10 @@ static void l1_dirichlet_patch(const ora_mg *m, int lc, const int Xoff[3], doubl
                 }
     }
     clamp_diag(st + 9 * 13);
-    if (m->fp16)
+    if (m->fp16 == 1)
         for (int q = 0; q < 243; q++) st[q] = to_half(st[q]);
+    else if (m->fp16 == 3)
+        round_row_f32(st);
 }
 
 /* fast restatement of l1_partial: coarse element matrices
@@ -731,8 +740,9 @@ void ora_mg_galerkin(ora_mg *m, int lc) {
                                 }
                             }
                     if (d == 13) clamp_diag(s);
-                    for (int k = 0; k < 9; k++) st[9 * d + k] = m->fp16 ? to_half(s[k]) : s[k];
+                    for (int k = 0; k < 9; k++) st[9 * d + k] = m->fp16 == 1 ? to_half(s[k]) : s[k];
                 }
+                if (m->fp16 == 3) round_row_f32(st);
             }
 }
 
