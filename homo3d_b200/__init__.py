@@ -23,7 +23,7 @@ import os
 import numpy as np
 
 __all__ = ["Homogenization", "MG", "Grid", "OCOptimizer", "MMAOptimizer", "WarmNet", "H3DError", "symmetrize", "lib",
-           "LIB_PATH",
+           "LIB_PATH", "batch_update", "batch_elasticMatrix",
            "reference_resolution"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -91,6 +91,9 @@ _SIGS = {
     "h3d_elastic_matrix": [_vp, ctypes.c_double, _dp, ctypes.POINTER(SolveStats)],
     "h3d_sensitivity": [_vp, _fp, _vp, ctypes.c_int],
     "h3d_reset_solutions": [_vp],
+    "h3d_batch_update_density": [ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.c_int],
+    "h3d_batch_elastic_matrix": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_double, _dp,
+                                 ctypes.POINTER(SolveStats), _ip],
     "h3d_penalize": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float],
     "h3d_penalize_backward": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float],
     "h3d_oc_update": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
@@ -505,6 +508,47 @@ class WarmNet:
 
     def load(self, path):
         self.set_params(np.fromfile(path, dtype=np.float32))
+
+
+def _handle_array(homs):
+    arr = (_vp * len(homs))(*[h._h for h in homs])
+    return arr
+
+
+def batch_update(homs, rho_phys):
+    """Homogenization.update on several designs, their stencil assemblies running
+    concurrently; rho_phys: one contiguous CUDA tensor per design."""
+    if len(homs) != len(rho_phys):
+        raise ValueError("one density per design")
+    ptrs = (_vp * len(homs))(*[_ptr(r).value for r in rho_phys])
+    code = lib().h3d_batch_update_density(_handle_array(homs), ptrs, len(homs))
+    if code != H3D_OK:
+        for h in homs:
+            msg = lib().h3d_last_error(h._h).decode()
+            if msg:
+                raise H3DError(code, msg)
+        raise H3DError(code, "batch update failed")
+
+
+def batch_elasticMatrix(homs, tol=1e-2):
+    """Homogenization.elasticMatrix on several designs solved together (each on its
+    own stream).  Returns the [n, 6, 6] C; each design's solve statistics land in
+    its last_stats.  A design that fails raises after all have been attempted."""
+    n = len(homs)
+    C = np.zeros((n, 36))
+    st = (SolveStats * n)()
+    status = np.zeros(n, dtype=np.int32)
+    status[:] = -1
+    code = lib().h3d_batch_elastic_matrix(_handle_array(homs), n, float(tol), C.ctypes.data_as(_dp), st,
+                                          status.ctypes.data_as(_ip))
+    if code not in (H3D_OK, H3D_NOT_CONVERGED) and (status == -1).any():  # refused before any design ran
+        raise H3DError(code, lib().h3d_last_error(homs[0]._h).decode() if n else "")
+    for i, h in enumerate(homs):
+        h.last_stats = st[i].as_dict()
+    for i, h in enumerate(homs):
+        if status[i] not in (H3D_OK, H3D_NOT_CONVERGED):
+            raise H3DError(int(status[i]), "design %d: %s" % (i, lib().h3d_last_error(h._h).decode()))
+    return C.reshape(n, 6, 6)
 
 
 def symmetrize(handle, field, reso, sym="reflect6"):

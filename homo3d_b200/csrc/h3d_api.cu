@@ -19,6 +19,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "../../include/h3d.h"
@@ -341,6 +342,278 @@ int check_level(h3d_handle *h, int level, bool coarse_only = false) {
 
 }  // namespace
 
+namespace {
+
+// The solve loop of MG::solveEquation (MG.cpp:113-203) as a resumable state
+// machine: begin() enqueues the first step on the handle's stream; after that
+// stream has drained, advance() reads the step's result and enqueues the next
+// one, until finished().  h3d_solve drives one handle; h3d_batch_elastic_matrix
+// drives several, each on its own stream, so their kernels overlap on the GPU.
+//
+// Refined mode: the FP32 V-cycles on the correction measure the stale residual
+// accurately down to ~1e-6 N of the correction's right-hand side; the correction
+// is folded into u64 and the residual recomputed exactly once the estimate has
+// dropped by theta (10x above that floor) or reached the tolerance, and the solve
+// only stops when that exact residual meets the tolerance too.
+struct SolveRun {
+    enum Pending { P_NONE, P_START_REFINE, P_CYCLE, P_TRIGGER_REFINE, P_FINAL_REFINE, P_DONE };
+    h3d_handle *h = nullptr;
+    int mask = 63, it = 0, nref = 0, status = H3D_OK, explode_left = 2, maxit = 200;
+    double tol = 1e-2, theta = 1e-3;
+    bool refine = false, exact = false, with_guess = false, fallback_tried = false, done_flag = false;
+    double fn[6] = {}, rel[6] = {1, 1, 1, 1, 1, 1}, base[6] = {1, 1, 1, 1, 1, 1};
+    Pending pending = P_NONE;
+    cudaGraphExec_t refine_step = nullptr;
+
+    bool selected(int c) const { return ((mask >> c) & 1) != 0; }
+    bool finished() const { return pending == P_DONE; }
+    long long n18() const { return (long long)NF * h->lv[0].P.nv; }
+
+    int reset_solution() {
+        if (refine) CK(cudaMemsetAsync(h->u64, 0, sizeof(double) * n18(), h->stream));
+        else CK(cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * n18(), h->stream));
+        return H3D_OK;
+    }
+    int launch_refine(Pending next) {
+        nref++;
+        CK(cudaGraphLaunch(refine_step, h->stream));
+        pending = next;
+        return H3D_OK;
+    }
+    int launch_cycle() {
+        if (it >= maxit) return finish(H3D_NOT_CONVERGED);
+        CK(cudaGraphLaunch(h->sgraph, h->stream));
+        pending = P_CYCLE;
+        return H3D_OK;
+    }
+    void read_base() {
+        for (int c = 0; c < NCASE; c++) base[c] = std::sqrt(h->h_small[c]) / (fn[c] + 1e-10);
+    }
+    // a solve that ends without converging still leaves its iterate in u64; the
+    // FP32 solution takes the pending shift and f is restored
+    int finish(int st) {
+        status = st;
+        if (refine && st != H3D_OK) return launch_refine(P_FINAL_REFINE);
+        if (!refine) launch_pin_fold(h->lv[0], h->rho, h->ke, h->pin_state, h->stream);
+        CK(cudaEventRecord(h->ev1, h->stream));
+        pending = P_DONE;
+        return H3D_OK;
+    }
+
+    int begin(h3d_handle *hh, int case_mask, double tolerance, int guess) {
+        h = hh;
+        if (!h) return H3D_ERR_ARG;
+        if (!h->have_stencils) return fail(h, H3D_ERR_STATE, "no stencils");
+        if (case_mask <= 0 || case_mask > 63) return fail(h, H3D_ERR_ARG, "case_mask must select load cases");
+        CK(cudaSetDevice(h->device));
+        mask = case_mask;
+        tol = tolerance;
+        with_guess = guess != 0;
+        refine = h->refine();
+        const Level &L0 = h->lv[0];
+        if (!with_guess)
+            if (int e = reset_solution()) return e;
+        // balance the right-hand side: a periodic load has zero net force, and the few
+        // ulps of net force left by FP32 rounding would, in the pinned problem, become
+        // a point load at the origin; remove each plane's mean over the unique vertices
+        {
+            float *rhs = refine ? h->f0 : L0.f;
+            const int nb = norm_blocks(L0.P);
+            launch_mean_partial(L0.P, rhs, h->partial, nb, h->stream);
+            launch_remove_mean(L0.P, rhs, h->partial, nb, h->stream);
+            CKL();
+        }
+        if (int e = build_graph(h, G_SOLVE)) return e;
+        // below ~1e-4 the FP32 products of the difference-form residual would floor
+        // the iteration, so tight targets take the FP64-accumulating residual
+        exact = refine && tol < 1e-4;
+        if (refine)
+            if (int e = build_graph(h, exact ? G_REFINE_EXACT : G_REFINE)) return e;
+        refine_step = exact ? h->xgraph : h->rgraph;
+        if (int e = weighted_norms(h, L0.P, refine ? h->f0 : L0.f, fn)) return e;
+        const int nmax = std::max(L0.P.n[0], std::max(L0.P.n[1], L0.P.n[2]));
+        theta = std::max(1e-3, 1e-5 * nmax);
+        CK(cudaEventRecord(h->ev0, h->stream));
+        CK(cudaMemsetAsync(h->pin_state + NF, 0, sizeof(double) * NF, h->stream));  // no pending shift
+        if (refine) {
+            CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * n18(), h->stream));
+            return launch_refine(P_START_REFINE);
+        }
+        enqueue_pin_init(h);
+        return launch_cycle();
+    }
+
+    // the step enqueued last has completed on the handle's stream
+    int advance() {
+        switch (pending) {
+        case P_START_REFINE: {
+            read_base();
+            // a starting guess worse than zero (relative residual above 1) is dropped
+            bool worse = false;
+            for (int c = 0; c < NCASE; c++)
+                if (selected(c) && !(base[c] <= 1.0)) worse = true;
+            if (with_guess && worse && !fallback_tried) {
+                fallback_tried = true;
+                if (int e = reset_solution()) return e;
+                return launch_refine(P_START_REFINE);
+            }
+            return launch_cycle();
+        }
+        case P_CYCLE: {
+            it++;
+            bool bad = false, done = true, trigger = true;
+            for (int c = 0; c < NCASE; c++) {
+                rel[c] = std::sqrt(h->h_small[c]) / (fn[c] + 1e-10);
+                if (!selected(c)) continue;
+                if (!(rel[c] <= 10.0)) bad = true;
+                if (!(rel[c] <= tol)) done = false;
+                if (!(rel[c] <= tol || rel[c] <= theta * base[c])) trigger = false;
+            }
+            if (bad) {  // MG.cpp:140-182: restart from zero once, then give up
+                if (--explode_left <= 0) return finish(H3D_DIVERGED);
+                if (!refine) launch_pin_fold(h->lv[0], h->rho, h->ke, h->pin_state, h->stream);  // restores f
+                if (int e = reset_solution()) return e;
+                CK(cudaMemsetAsync(h->pin_state + NF, 0, sizeof(double) * NF, h->stream));
+                fallback_tried = true;
+                if (refine) {
+                    CK(cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * n18(), h->stream));
+                    return launch_refine(P_START_REFINE);
+                }
+                enqueue_pin_init(h);
+                return launch_cycle();
+            }
+            if (refine && trigger) {
+                done_flag = done;
+                return launch_refine(P_TRIGGER_REFINE);
+            }
+            if (done) return finish(H3D_OK);
+            return launch_cycle();
+        }
+        case P_TRIGGER_REFINE: {
+            read_base();
+            bool done = done_flag;
+            if (done)
+                for (int c = 0; c < NCASE; c++)
+                    if (selected(c) && !(base[c] <= tol)) done = false;
+            if (done) return finish(H3D_OK);
+            return launch_cycle();
+        }
+        case P_FINAL_REFINE:
+            read_base();
+            CK(cudaEventRecord(h->ev1, h->stream));
+            pending = P_DONE;
+            return H3D_OK;
+        default:
+            return fail(h, H3D_ERR_STATE, "solve advanced in a wrong state");
+        }
+    }
+
+    int end(h3d_solve_stats *stats) {
+        CK(cudaEventSynchronize(h->ev1));
+        if (stats) {
+            stats->vcycles = it;
+            stats->refinements = nref;
+            stats->status = status;
+            for (int c = 0; c < NCASE; c++) stats->rel_res[c] = rel[c];
+            float ms = 0;
+            cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+            stats->solve_ms = ms;
+        }
+        if (status != H3D_OK) return fail(h, status, status == H3D_DIVERGED ? "multigrid diverged" : "not converged");
+        return H3D_OK;
+    }
+};
+
+
+// the coarsest level's assembly and Gauss-Jordan inversion with the
+// singular-matrix flag copied to the host; factor_coarsest_check reads it once
+// the stream has drained
+int factor_coarsest_enqueue(h3d_handle *h) {
+    cudaStream_t s = h->stream;
+    launch_coarse_assemble(h->lv[h->nl - 1], h->aug, s);
+    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), s));
+    launch_gauss_jordan(h->aug, h->ndof, h->d_flag, s);
+    CKL();
+    CK(cudaMemcpyAsync(&h->h_small[63], h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    return H3D_OK;
+}
+
+int factor_coarsest_check(h3d_handle *h) {
+    int flag = 0;
+    std::memcpy(&flag, &h->h_small[63], sizeof(int));
+    if (flag) return fail(h, H3D_ERR_SINGULAR, "coarsest-grid matrix is singular");
+    h->have_stencils = true;
+    return H3D_OK;
+}
+
+// right-hand sides and warm start from the stored solutions, mean removed
+// (homogenization.cu:471-477, grid.cpp:1131-1141)
+int elastic_prepare(h3d_handle *h) {
+    Level &L = h->lv[0];
+    cudaStream_t s = h->stream;
+    const long long n18 = (long long)NF * L.P.nv;
+    const int nb = norm_blocks(L.P);
+    if (h->refine()) {
+        launch_rhs(L, h->rho, h->rhs, h->f0, s);
+        CK(cudaMemcpyAsync(h->u64, h->chi, sizeof(double) * n18, cudaMemcpyDeviceToDevice, s));
+        launch_remove_mean64(L.P, h->u64, h->partial, nb, s);
+    } else {
+        launch_rhs(L, h->rho, h->rhs, L.f, s);
+        launch_convert(n18, h->chi, L.u, s);
+        launch_mean_partial(L.P, L.u, h->partial, nb, s);
+        launch_remove_mean(L.P, L.u, h->partial, nb, s);
+    }
+    CKL();
+    return H3D_OK;
+}
+
+// store the solutions as chi and enqueue the energy reduction of the 21 entries
+// of C, with the results and the kernel's wait flag copied to the host
+int elastic_enqueue_energy(h3d_handle *h) {
+    Level &L = h->lv[0];
+    cudaStream_t s = h->stream;
+    const long long n18 = (long long)NF * L.P.nv;
+    if (h->refine()) CK(cudaMemcpyAsync(h->chi, h->u64, sizeof(double) * n18, cudaMemcpyDeviceToDevice, s));
+    else launch_convert(n18, L.u, h->chi, s);
+    int nsm = 0;
+    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+    const int eb = energy_tc_blocks(L.P, nsm);
+    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), s));
+    if (launch_elastic_tc(L.P, h->chi, h->rho, h->ke, h->partial, eb, h->d_flag, s) != 0)
+        return fail(h, H3D_ERR_CUDA, "tensor-core energy kernel could not be configured");
+    launch_elastic_finish(h->partial, eb, h->d_small, s);
+    CKL();
+    CK(cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * 21, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(&h->h_small[63], h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
+    return H3D_OK;
+}
+
+// C from the reduced energies once the stream has drained
+int elastic_read(h3d_handle *h, double *C) {
+    if (*reinterpret_cast<int *>(&h->h_small[63]))
+        return fail(h, H3D_ERR_CUDA, "tensor-core energy kernel: mbarrier wait timed out");
+    const double vol = (double)h->lv[0].P.nv;
+    int t = 0;
+    for (int i = 0; i < 6; i++)
+        for (int j = i; j < 6; j++) {
+            C[i * 6 + j] = C[j * 6 + i] = h->h_small[t] / vol;
+            t++;
+        }
+    return H3D_OK;
+}
+
+// a batch drives each design's stream and host mirror separately, so a handle
+// may appear only once
+int distinct_handles(h3d_handle *const *hs, int n) {
+    std::vector<const h3d_handle *> v(hs, hs + n);
+    std::sort(v.begin(), v.end());
+    for (int i = 1; i < n; i++)
+        if (v[i] == v[i - 1]) return fail(hs[0], H3D_ERR_ARG, "a handle appears twice in the batch");
+    return H3D_OK;
+}
+
+}  // namespace
+
 extern "C" {
 
 static int create_impl(h3d_handle *h, const h3d_config *cfg) {
@@ -513,18 +786,9 @@ int h3d_restrict_stencil(h3d_handle *h, int coarse_level) {
 int h3d_factor_coarsest(h3d_handle *h) {
     if (!h) return H3D_ERR_ARG;
     CK(cudaSetDevice(h->device));
-    cudaStream_t s = h->stream;
-    launch_coarse_assemble(h->lv[h->nl - 1], h->aug, s);
-    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), s));
-    launch_gauss_jordan(h->aug, h->ndof, h->d_flag, s);
-    CKL();
-    int flag = 0;
-    CK(cudaMemcpyAsync(&h->h_small[63], h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    std::memcpy(&flag, &h->h_small[63], sizeof(int));
-    if (flag) return fail(h, H3D_ERR_SINGULAR, "coarsest-grid matrix is singular");
-    h->have_stencils = true;
-    return H3D_OK;
+    if (int e = factor_coarsest_enqueue(h)) return e;
+    CK(cudaStreamSynchronize(h->stream));
+    return factor_coarsest_check(h);
 }
 
 int h3d_update_stencils(h3d_handle *h) {
@@ -634,125 +898,13 @@ int h3d_v_cycle(h3d_handle *h, float w, int pre, int post) {
 }
 
 int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solve_stats *stats) {
-    if (!h) return H3D_ERR_ARG;
-    if (!h->have_stencils) return fail(h, H3D_ERR_STATE, "no stencils");
-    if (case_mask <= 0 || case_mask > 63) return fail(h, H3D_ERR_ARG, "case_mask must select load cases");
-    CK(cudaSetDevice(h->device));
-    const bool refine = h->refine();
-    const Level &L0 = h->lv[0];
-    const long long n18 = (long long)NF * L0.P.nv;
-    // the field that holds the solution: u64 (refined) or the swept u (FP32)
-    auto reset_solution = [&]() -> int {
-        if (refine) CK(cudaMemsetAsync(h->u64, 0, sizeof(double) * n18, h->stream));
-        else CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * n18, h->stream));
-        return H3D_OK;
-    };
-    if (!with_guess)
-        if (int e = reset_solution()) return e;
-    // balance the right-hand side: a periodic load has zero net force, and the few
-    // ulps of net force left by FP32 rounding would, in the pinned problem, become a
-    // point load at the origin; remove each plane's mean over the unique vertices
-    {
-        float *rhs = refine ? h->f0 : L0.f;
-        const int nb = norm_blocks(L0.P);
-        launch_mean_partial(L0.P, rhs, h->partial, nb, h->stream);
-        launch_remove_mean(L0.P, rhs, h->partial, nb, h->stream);
-        CKL();
-    }
-    if (int e = build_graph(h, G_SOLVE)) return e;
-    // below ~1e-4 the FP32 products of the difference-form residual would floor the
-    // iteration, so tight targets take the FP64-accumulating residual
-    const bool exact = refine && tol < 1e-4;
-    if (refine)
-        if (int e = build_graph(h, exact ? G_REFINE_EXACT : G_REFINE)) return e;
-    cudaGraphExec_t refine_step = exact ? h->xgraph : h->rgraph;
-    double fn[6], rel[6] = {1, 1, 1, 1, 1, 1}, base[6] = {1, 1, 1, 1, 1, 1};
-    if (int e = weighted_norms(h, L0.P, refine ? h->f0 : L0.f, fn)) return e;
-    auto selected = [&](int c) { return ((case_mask >> c) & 1) != 0; };
-    // refined mode: the FP32 V-cycles on the correction measure the stale residual
-    // accurately down to ~1e-6 N of the correction's right-hand side; the correction
-    // is folded into u64 and the residual recomputed exactly once the estimate has
-    // dropped by theta (10x above that floor) or reached the tolerance, and the
-    // solve only stops when that exact residual meets the tolerance too
-    const int nmax = std::max(L0.P.n[0], std::max(L0.P.n[1], L0.P.n[2]));
-    const double theta = std::max(1e-3, 1e-5 * nmax);
-    int nref = 0;
-    auto refine_now = [&]() -> int {
-        nref++;
-        CK(cudaGraphLaunch(refine_step, h->stream));
+    SolveRun run;
+    if (int e = run.begin(h, case_mask, tol, with_guess)) return e;
+    while (!run.finished()) {
         CK(cudaStreamSynchronize(h->stream));
-        for (int c = 0; c < NCASE; c++) base[c] = std::sqrt(h->h_small[c]) / (fn[c] + 1e-10);
-        return H3D_OK;
-    };
-    CK(cudaEventRecord(h->ev0, h->stream));
-    CK(cudaMemsetAsync(h->pin_state + NF, 0, sizeof(double) * NF, h->stream));  // no pending shift
-    if (!refine) enqueue_pin_init(h);
-    if (refine) {
-        CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * n18, h->stream));
-        if (int e = refine_now()) return e;
-        // a starting guess worse than zero (relative residual above 1) is dropped
-        bool worse = false;
-        for (int c = 0; c < NCASE; c++)
-            if (selected(c) && !(base[c] <= 1.0)) worse = true;
-        if (with_guess && worse) {
-            if (int e = reset_solution()) return e;
-            if (int e = refine_now()) return e;
-        }
+        if (int e = run.advance()) return e;
     }
-    int it = 0, status = H3D_OK, explode_left = 2;
-    const int maxit = 200;
-    for (;;) {
-        if (it >= maxit) { status = H3D_NOT_CONVERGED; break; }
-        CK(cudaGraphLaunch(h->sgraph, h->stream));
-        CK(cudaStreamSynchronize(h->stream));
-        it++;
-        bool bad = false, done = true, trigger = true;
-        for (int c = 0; c < NCASE; c++) {
-            rel[c] = std::sqrt(h->h_small[c]) / (fn[c] + 1e-10);
-            if (!selected(c)) continue;
-            if (!(rel[c] <= 10.0)) bad = true;
-            if (!(rel[c] <= tol)) done = false;
-            if (!(rel[c] <= tol || rel[c] <= theta * base[c])) trigger = false;
-        }
-        if (bad) {  // MG.cpp:140-182: restart from zero once, then give up
-            if (--explode_left <= 0) { status = H3D_DIVERGED; break; }
-            if (!refine) launch_pin_fold(L0, h->rho, h->ke, h->pin_state, h->stream);  // restores f
-            if (int e = reset_solution()) return e;
-            CK(cudaMemsetAsync(h->pin_state + NF, 0, sizeof(double) * NF, h->stream));
-            if (refine) {
-                CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * n18, h->stream));
-                if (int e = refine_now()) return e;
-            } else {
-                enqueue_pin_init(h);
-            }
-            continue;
-        }
-        if (refine && trigger) {
-            if (int e = refine_now()) return e;
-            if (done)
-                for (int c = 0; c < NCASE; c++)
-                    if (selected(c) && !(base[c] <= tol)) done = false;
-        }
-        if (done) break;
-    }
-    // a solve that ends without converging still leaves its iterate in u64; the FP32
-    // solution takes the pending shift and f is restored
-    if (refine && status != H3D_OK)
-        if (int e = refine_now()) return e;
-    if (!refine) launch_pin_fold(L0, h->rho, h->ke, h->pin_state, h->stream);
-    CK(cudaEventRecord(h->ev1, h->stream));
-    CK(cudaEventSynchronize(h->ev1));
-    if (stats) {
-        stats->vcycles = it;
-        stats->refinements = nref;
-        stats->status = status;
-        for (int c = 0; c < NCASE; c++) stats->rel_res[c] = rel[c];
-        float ms = 0;
-        cudaEventElapsedTime(&ms, h->ev0, h->ev1);
-        stats->solve_ms = ms;
-    }
-    if (status != H3D_OK) return fail(h, status, status == H3D_DIVERGED ? "multigrid diverged" : "not converged");
-    return H3D_OK;
+    return run.end(stats);
 }
 
 int h3d_reset_solutions(h3d_handle *h) {
@@ -765,50 +917,117 @@ int h3d_elastic_matrix(h3d_handle *h, double tol, double C[36], h3d_solve_stats 
     if (!h || !C) return H3D_ERR_ARG;
     if (!h->have_stencils) return fail(h, H3D_ERR_STATE, "no stencils");
     CK(cudaSetDevice(h->device));
-    Level &L = h->lv[0];
-    cudaStream_t s = h->stream;
-    const long long n18 = (long long)NF * L.P.nv;
-    const int nb = norm_blocks(L.P);
-    // right-hand sides and warm start from the stored solutions, mean removed
-    // (homogenization.cu:471-477, grid.cpp:1131-1141)
-    if (h->refine()) {
-        launch_rhs(L, h->rho, h->rhs, h->f0, s);
-        CK(cudaMemcpyAsync(h->u64, h->chi, sizeof(double) * n18, cudaMemcpyDeviceToDevice, s));
-        launch_remove_mean64(L.P, h->u64, h->partial, nb, s);
-    } else {
-        launch_rhs(L, h->rho, h->rhs, L.f, s);
-        launch_convert(n18, h->chi, L.u, s);
-        launch_mean_partial(L.P, L.u, h->partial, nb, s);
-        launch_remove_mean(L.P, L.u, h->partial, nb, s);
-    }
-    CKL();
+    if (int e = elastic_prepare(h)) return e;
     h3d_solve_stats st;
     int e = h3d_solve(h, 63, tol, 1, &st);
     if (stats) *stats = st;
     if (e != H3D_OK && e != H3D_NOT_CONVERGED) return e;
-    if (h->refine()) CK(cudaMemcpyAsync(h->chi, h->u64, sizeof(double) * n18, cudaMemcpyDeviceToDevice, s));
-    else launch_convert(n18, L.u, h->chi, s);
-    int nsm = 0;
-    CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
-    const int eb = energy_tc_blocks(L.P, nsm);
-    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), s));
-    if (launch_elastic_tc(L.P, h->chi, h->rho, h->ke, h->partial, eb, h->d_flag, s) != 0)
-        return fail(h, H3D_ERR_CUDA, "tensor-core energy kernel could not be configured");
-    launch_elastic_finish(h->partial, eb, h->d_small, s);
-    CKL();
-    CK(cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * 21, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(&h->h_small[63], h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
-    CK(cudaStreamSynchronize(s));
-    if (*reinterpret_cast<int *>(&h->h_small[63]))
-        return fail(h, H3D_ERR_CUDA, "tensor-core energy kernel: mbarrier wait timed out");
-    const double vol = (double)L.P.nv;
-    int t = 0;
-    for (int i = 0; i < 6; i++)
-        for (int j = i; j < 6; j++) {
-            C[i * 6 + j] = C[j * 6 + i] = h->h_small[t] / vol;
-            t++;
-        }
+    if (int e2 = elastic_enqueue_energy(h)) return e2;
+    CK(cudaStreamSynchronize(h->stream));
+    if (int e2 = elastic_read(h, C)) return e2;
     return e;
+}
+
+int h3d_batch_update_density(h3d_handle *const *hs, const float *const *rho_dev, int n) {
+    if (!hs || !rho_dev || n < 0) return H3D_ERR_ARG;
+    for (int i = 0; i < n; i++)
+        if (!hs[i] || !rho_dev[i]) return H3D_ERR_ARG;
+    if (int e = distinct_handles(hs, n)) return e;
+    // enqueue every design's assembly, then collect the singular-matrix flags, so
+    // the assemblies of different designs run concurrently on their own streams
+    int first = H3D_OK;
+    for (int i = 0; i < n; i++) {
+        h3d_handle *h = hs[i];
+        int e = [&]() -> int {
+            CK(cudaSetDevice(h->device));
+            launch_density_in(h->lv[0].P.n, rho_dev[i], h->lv[0].P.n[0], h->rho, h->stream);
+            CKL();
+            h->have_density = true;
+            for (int l = 1; l < h->nl; l++)
+                if (int e2 = h3d_restrict_stencil(h, l)) return e2;
+            return factor_coarsest_enqueue(h);
+        }();
+        if (e && first == H3D_OK) first = e;
+    }
+    for (int i = 0; i < n; i++) {
+        h3d_handle *h = hs[i];
+        int e = [&]() -> int {
+            CK(cudaSetDevice(h->device));
+            CK(cudaStreamSynchronize(h->stream));
+            return factor_coarsest_check(h);
+        }();
+        if (e && first == H3D_OK) first = e;
+    }
+    return first;
+}
+
+int h3d_batch_elastic_matrix(h3d_handle *const *hs, int n, double tol, double *C, h3d_solve_stats *stats,
+                             int *status) {
+    if (!hs || !C || n < 0) return H3D_ERR_ARG;
+    for (int i = 0; i < n; i++)
+        if (!hs[i]) return H3D_ERR_ARG;
+    if (int e = distinct_handles(hs, n)) return e;
+    std::vector<SolveRun> runs(n);
+    std::vector<int> st(n, H3D_OK);
+    std::vector<char> live(n, 0);
+    // start every solve (the graph captures happen here, before any polling)
+    for (int i = 0; i < n; i++) {
+        h3d_handle *h = hs[i];
+        if (!h->have_stencils) { st[i] = fail(h, H3D_ERR_STATE, "no stencils"); continue; }
+        st[i] = [&]() -> int {
+            CK(cudaSetDevice(h->device));
+            if (int e = elastic_prepare(h)) return e;
+            return runs[i].begin(h, 63, tol, 1);
+        }();
+        live[i] = st[i] == H3D_OK;
+    }
+    // advance whichever design's step has completed; each design's V-cycles and
+    // refinements run on its own stream, so small designs fill the GPU together
+    int nlive = 0;
+    for (int i = 0; i < n; i++) nlive += live[i];
+    while (nlive > 0) {
+        bool progressed = false;
+        for (int i = 0; i < n; i++) {
+            if (!live[i]) continue;
+            h3d_handle *h = hs[i];
+            cudaError_t q = cudaStreamQuery(h->stream);
+            if (q == cudaErrorNotReady) continue;
+            progressed = true;
+            int e = q == cudaSuccess ? runs[i].advance() : fail(h, H3D_ERR_CUDA, cudaGetErrorString(q));
+            if (e == H3D_OK && runs[i].finished()) {
+                h3d_solve_stats s1;
+                e = runs[i].end(&s1);
+                if (stats) stats[i] = s1;
+                if (e == H3D_OK || e == H3D_NOT_CONVERGED) {
+                    const int e2 = elastic_enqueue_energy(h);
+                    if (e2) e = e2;
+                }
+                st[i] = e;
+                live[i] = 0;
+                nlive--;
+            } else if (e != H3D_OK) {
+                st[i] = e;
+                live[i] = 0;
+                nlive--;
+            }
+        }
+        if (!progressed) std::this_thread::yield();
+    }
+    int first = H3D_OK;
+    for (int i = 0; i < n; i++) {
+        h3d_handle *h = hs[i];
+        if (st[i] == H3D_OK || st[i] == H3D_NOT_CONVERGED) {
+            const int e = [&]() -> int {
+                CK(cudaSetDevice(h->device));
+                CK(cudaStreamSynchronize(h->stream));
+                return elastic_read(h, C + 36 * (size_t)i);
+            }();
+            if (e) st[i] = e;
+        }
+        if (status) status[i] = st[i];
+        if (st[i] != H3D_OK && first == H3D_OK) first = st[i];
+    }
+    return first;
 }
 
 int h3d_sensitivity(h3d_handle *h, const float dC[36], float *sens_dev, int pitchT) {

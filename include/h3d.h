@@ -161,6 +161,20 @@ H3D_API int h3d_sensitivity(h3d_handle *h, const float dC[36], float *sens_dev, 
 /* forget the stored solutions (warm start) */
 H3D_API int h3d_reset_solutions(h3d_handle *h);
 
+/* ---- batched designs (no reference counterpart: the reference homogenizes one
+ * design per process) -------------------------------------------------------- */
+/* h3d_update_density on n distinct handles (lexicographic rho_phys, unpadded),
+ * with the stencil assemblies of all designs enqueued before any is waited on.
+ * Returns the first error; every handle is attempted. */
+H3D_API int h3d_batch_update_density(h3d_handle *const *hs, const float *const *rho_dev, int n);
+/* h3d_elastic_matrix on n distinct handles, solved together: each design's
+ * V-cycles run on its own stream and the host advances whichever design's step
+ * has completed.  C holds n row-major 6x6 blocks; stats (n entries) and status
+ * (n codes, H3D_NOT_CONVERGED keeps its C) may be NULL.  The handles may differ
+ * in resolution and precision mode.  Returns the first non-OK status. */
+H3D_API int h3d_batch_elastic_matrix(h3d_handle *const *hs, int n, double tol, double *C,
+                                     h3d_solve_stats *stats, int *status);
+
 /* ---- SIMP penalisation, the expression rho.pow(p) (TensorExpression.h:517-531) */
 /* rho_phys = rho^p */
 H3D_API int h3d_penalize(h3d_handle *h, const float *rho_dev, float *rho_phys_dev, int64_t n, float p);
