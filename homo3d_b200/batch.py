@@ -47,16 +47,20 @@ def run_pass(torch, homs, rhos, tol, batched):
         hd.sync()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
+    t_update = 0.0
     if batched:
         batch_update(homs, rhos)
+        t_update = time.perf_counter() - t0
         C = batch_elasticMatrix(homs, tol)
     else:
         C = np.zeros((len(homs), 6, 6))
         for i, hd in enumerate(homs):
+            t1 = time.perf_counter()
             hd.update(rhos[i])
+            t_update += time.perf_counter() - t1
             C[i] = hd.elasticMatrix(tol)
     dt = time.perf_counter() - t0
-    return dt, C, [dict(hd.last_stats) for hd in homs]
+    return dt, t_update, C, [dict(hd.last_stats) for hd in homs]
 
 
 def main():
@@ -80,11 +84,13 @@ def main():
     res = {}
     for arm, batched in (("sequential", False), ("batched", True)):
         run_pass(torch, homs, rhos, args.tol, batched)  # graph captures, first-touch
-        times, Cs, stats = [], None, None
+        times, upd, Cs, stats = [], [], None, None
         for _ in range(args.repeat):
-            dt, Cs, stats = run_pass(torch, homs, rhos, args.tol, batched)
+            dt, tu, Cs, stats = run_pass(torch, homs, rhos, args.tol, batched)
             times.append(dt)
-        res[arm] = {"s_per_pass": min(times), "s_all": times, "C": Cs, "stats": stats}
+            upd.append(tu)
+        k = int(np.argmin(times))
+        res[arm] = {"s_per_pass": times[k], "s_update": upd[k], "s_all": times, "C": Cs, "stats": stats}
     seq, bat = res["sequential"], res["batched"]
     rel = [float(np.abs(bat["C"][i] - seq["C"][i]).max() / np.abs(seq["C"][i]).max()) for i in range(len(sizes))]
     rep = {
@@ -94,6 +100,8 @@ def main():
         "designs_per_s_sequential": len(sizes) / seq["s_per_pass"],
         "speedup": seq["s_per_pass"] / bat["s_per_pass"],
         "s_per_pass": {"batched": bat["s_per_pass"], "sequential": seq["s_per_pass"]},
+        "s_stencils": {"batched": bat["s_update"], "sequential": seq["s_update"]},
+        "sum_solve_ms_sequential": sum(s["solve_ms"] for s in seq["stats"]),
         "max_rel_C_diff_batched_vs_sequential": max(rel),
         "vcycles": [s["vcycles"] for s in bat["stats"]],
         "vcycles_equal": [s["vcycles"] for s in bat["stats"]] == [s["vcycles"] for s in seq["stats"]],

@@ -167,6 +167,7 @@ struct h3d_handle {
     cudaGraphExec_t rgraph = nullptr;   // refinement step: u64 += u, f = f0 - K u64 (FP32 products)
     cudaGraphExec_t xgraph = nullptr;   // the same with the FP64-accumulated residual
     cudaGraphExec_t sgraph = nullptr;   // a solve's V-cycle: vgraph + rigid-translation deflation
+    cudaGraphExec_t fgraph = nullptr;   // coarsest assembly + Gauss-Jordan inverse (n + 1 launches)
     double *pin_state = nullptr;        // deflation: F[18], pending shift T[18], plane sums[18]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool refine() const { return cfg.precision == H3D_PREC_REFINE; }
@@ -242,6 +243,7 @@ int destroy_graph(h3d_handle *h) {
     if (h->rgraph) { cudaGraphExecDestroy(h->rgraph); h->rgraph = nullptr; }
     if (h->xgraph) { cudaGraphExecDestroy(h->xgraph); h->xgraph = nullptr; }
     if (h->sgraph) { cudaGraphExecDestroy(h->sgraph); h->sgraph = nullptr; }
+    if (h->fgraph) { cudaGraphExecDestroy(h->fgraph); h->fgraph = nullptr; }
     return H3D_OK;
 }
 
@@ -530,10 +532,21 @@ struct SolveRun {
 // the stream has drained
 int factor_coarsest_enqueue(h3d_handle *h) {
     cudaStream_t s = h->stream;
-    launch_coarse_assemble(h->lv[h->nl - 1], h->aug, s);
-    CK(cudaMemsetAsync(h->d_flag, 0, sizeof(int), s));
-    launch_gauss_jordan(h->aug, h->ndof, h->d_flag, s);
-    CKL();
+    if (!h->fgraph) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        launch_coarse_assemble(h->lv[h->nl - 1], h->aug, s);
+        cudaMemsetAsync(h->d_flag, 0, sizeof(int), s);
+        launch_gauss_jordan(h->aug, h->ndof, h->d_flag, s);
+        CK(cudaStreamEndCapture(s, &g));
+        cudaError_t e = cudaGraphInstantiate(&h->fgraph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            h->fgraph = nullptr;
+            return fail(h, H3D_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
+        }
+    }
+    CK(cudaGraphLaunch(h->fgraph, s));
     CK(cudaMemcpyAsync(&h->h_small[63], h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s));
     return H3D_OK;
 }
@@ -676,7 +689,7 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
     CK(cudaMemcpy(h->d_ked, h->ked, sizeof(double) * 576, cudaMemcpyHostToDevice));
     const Level &C = h->lv[nl - 1];
     h->ndof = (int)(3 * C.P.nv);
-    CK(cudaMalloc(&h->aug, sizeof(double) * (size_t)h->ndof * 2 * h->ndof));
+    CK(cudaMalloc(&h->aug, sizeof(double) * gauss_jordan_doubles(h->ndof)));
     CK(cudaMalloc(&h->d_flag, sizeof(int)));
     // reduction scratch: residual partials, norms, C partials, means, OC
     size_t pn = ((size_t)fine_residual_blocks(h->lv[0]) + NORM_FINISH_CHUNKS) * NCASE;

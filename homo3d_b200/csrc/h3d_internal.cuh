@@ -150,6 +150,9 @@ void launch_dirichlet_patch(const Level &F, const Level &C, const float *rho, co
                             cudaStream_t s);
 void launch_galerkin(const Level &F, const Level &C, cudaStream_t s);
 void launch_coarse_assemble(const Level &C, double *aug, cudaStream_t s);
+// aug must hold gauss_jordan_doubles(n) doubles: the [n][2n] matrix and the
+// elimination scratch behind it
+size_t gauss_jordan_doubles(int n);
 void launch_gauss_jordan(double *aug, int n, int *flag, cudaStream_t s);
 void launch_coarse_apply(const Level &C, const double *aug, int project, cudaStream_t s);
 // homogenized tensor and sensitivities on the tensor cores (k_homog_tc.cu):

@@ -150,8 +150,16 @@ struct VertexGeo {
 template <int K>
 __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, const VertexGeo<K> &g, int cb,
                                            const float uv[3 * CPT], float acc[3 * CPT]) {
+    static_assert(CPT == 2, "the two load cases of a thread share one packed FP32x2 lane pair");
+    // lane pair (case cb, case cb+1) of each component: Blackwell's packed FP32x2
+    // add and FMA do both cases in one instruction with the rounding of the
+    // scalar forms, so the sums are the same as the scalar per-case loop
+    float2 acc2[3], nuv2[3];
 #pragma unroll
-    for (int q = 0; q < 3 * CPT; ++q) acc[q] = 0.f;
+    for (int m = 0; m < 3; ++m) {
+        acc2[m] = make_float2(0.f, 0.f);
+        nuv2[m] = make_float2(-uv[m], -uv[3 + m]);
+    }
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         if (d == 13) continue;
@@ -161,15 +169,23 @@ __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, c
         float A[9];
         g.block(ke, d, A);
         const float *up = a.u + nid + (long long)(3 * cb) * a.nv;
+        float2 dd[3];
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-            const float d0 = (pinned ? 0.f : __ldg(up + (3 * c) * a.nv)) - uv[3 * c];
-            const float d1 = (pinned ? 0.f : __ldg(up + (3 * c + 1) * a.nv)) - uv[3 * c + 1];
-            const float d2 = (pinned ? 0.f : __ldg(up + (3 * c + 2) * a.nv)) - uv[3 * c + 2];
-            acc[3 * c + 0] = fmaf(A[0], d0, fmaf(A[1], d1, fmaf(A[2], d2, acc[3 * c + 0])));
-            acc[3 * c + 1] = fmaf(A[3], d0, fmaf(A[4], d1, fmaf(A[5], d2, acc[3 * c + 1])));
-            acc[3 * c + 2] = fmaf(A[6], d0, fmaf(A[7], d1, fmaf(A[8], d2, acc[3 * c + 2])));
+        for (int m = 0; m < 3; ++m) {
+            const float2 un = pinned ? make_float2(0.f, 0.f)
+                                     : make_float2(__ldg(up + m * a.nv), __ldg(up + (3 + m) * a.nv));
+            dd[m] = __fadd2_rn(un, nuv2[m]);
         }
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+            acc2[r] = __ffma2_rn(make_float2(A[3 * r], A[3 * r]), dd[0],
+                                 __ffma2_rn(make_float2(A[3 * r + 1], A[3 * r + 1]), dd[1],
+                                            __ffma2_rn(make_float2(A[3 * r + 2], A[3 * r + 2]), dd[2], acc2[r])));
+    }
+#pragma unroll
+    for (int m = 0; m < 3; ++m) {
+        acc[m] = acc2[m].x;
+        acc[3 + m] = acc2[m].y;
     }
 }
 

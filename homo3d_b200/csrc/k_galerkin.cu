@@ -272,71 +272,108 @@ void launch_coarse_assemble(const Level &C, double *aug, cudaStream_t s) {
     k_coarse_assemble<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(C.P, C.st, aug, n);
 }
 
-// single-CTA Gauss-Jordan elimination with partial pivoting on [K | I]
-__global__ void __launch_bounds__(1024) k_gauss_jordan(double *a, int n, int *flag) {
-    extern __shared__ double col[];  // n factors
-    __shared__ double rmax[32];
-    __shared__ int ridx[32];
+// Gauss-Jordan elimination with partial pivoting on [K | I] (n rows, 2n columns,
+// FP64; grid.cpp:385-424 inverts the same matrix on the host).  One launch per
+// pivot column spreads the rank-1 update over every SM; the pivot search, row
+// swap and scaling of the next column are done by whichever CTA of a launch
+// finishes last (an arrival counter, no waiting), so a factorisation is n + 1
+// launches.  Scratch behind the matrix: the n elimination factors of the current
+// column and the arrival counter.
+constexpr int GJ_THREADS = 256;
+constexpr int GJ_TC = 64;                          // tile columns (lanes of a row)
+constexpr int GJ_RPT = 8;                          // rows per thread
+constexpr int GJ_TR = GJ_RPT * GJ_THREADS / GJ_TC; // tile rows
+
+// pivot step of column k by one CTA: the row among k..n-1 with the largest |a_ik|
+// (ties: the lowest row) swapped into row k and scaled by 1 / a_kk; col_i = a_ik
+// (0 for the pivot row) for the elimination launch of column k
+__device__ void gj_pivot(double *a, int n, int k, double *col, int *flag) {
+    __shared__ double rmax[GJ_THREADS / 32];
+    __shared__ int ridx[GJ_THREADS / 32];
     __shared__ int piv;
-    const int tid = threadIdx.x, nt = blockDim.x, m = 2 * n;
-    for (int k = 0; k < n; k++) {
-        // pivot search over rows k..n-1
-        double best = -1.0;
-        int bi = k;
-        for (int i = k + tid; i < n; i += nt) {
-            const double v = fabs(a[(long long)i * m + k]);
-            if (v > best) { best = v; bi = i; }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ob = __shfl_down_sync(0xffffffffu, best, o);
-            const int oi = __shfl_down_sync(0xffffffffu, bi, o);
-            if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
-        }
-        if ((tid & 31) == 0) { rmax[tid >> 5] = best; ridx[tid >> 5] = bi; }
-        __syncthreads();
-        if (tid == 0) {
-            double b = -1.0;
-            int p = k;
-            for (int w = 0; w < (nt + 31) / 32; w++)
-                if (rmax[w] > b || (rmax[w] == b && ridx[w] < p)) { b = rmax[w]; p = ridx[w]; }
-            piv = p;
-            if (!(b > 0.0)) *flag = 1;
-        }
-        __syncthreads();
-        const int p = piv;
-        if (p != k)
-            for (int j = tid; j < m; j += nt) {
-                const double t = a[(long long)k * m + j];
-                a[(long long)k * m + j] = a[(long long)p * m + j];
-                a[(long long)p * m + j] = t;
-            }
-        __syncthreads();
-        const double inv = 1.0 / a[(long long)k * m + k];
-        __syncthreads();
-        for (int j = tid; j < m; j += nt) a[(long long)k * m + j] *= inv;
-        for (int i = tid; i < n; i += nt) col[i] = (i == k) ? 0.0 : a[(long long)i * m + k];
-        __syncthreads();
-        // lanes cover 32 consecutive columns (coalesced), warps stride over rows; the
-        // pivot-row entry stays in a register for all rows of a column chunk
-        {
-            const int lane = tid & 31, warp = tid >> 5, nw = nt >> 5;
-            for (int j = k + lane; j < m; j += 32) {
-                const double akj = a[(long long)k * m + j];
-                for (int i = warp; i < n; i += nw)
-                    if (i != k) a[(long long)i * m + j] -= col[i] * akj;
-            }
-        }
-        __syncthreads();
+    const int tid = threadIdx.x, m = 2 * n;
+    double best = -1.0;
+    int bi = k;
+    for (int i = k + tid; i < n; i += GJ_THREADS) {
+        const double v = fabs(__ldcg(&a[(long long)i * m + k]));
+        if (v > best) { best = v; bi = i; }
     }
+    for (int o = 16; o > 0; o >>= 1) {
+        const double ob = __shfl_down_sync(0xffffffffu, best, o);
+        const int oi = __shfl_down_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) { best = ob; bi = oi; }
+    }
+    if ((tid & 31) == 0) { rmax[tid >> 5] = best; ridx[tid >> 5] = bi; }
+    __syncthreads();
+    if (tid == 0) {
+        double b = -1.0;
+        int p = k;
+        for (int w = 0; w < GJ_THREADS / 32; w++)
+            if (rmax[w] > b || (rmax[w] == b && ridx[w] < p)) { b = rmax[w]; p = ridx[w]; }
+        piv = p;
+        if (!(b > 0.0)) *flag = 1;
+    }
+    __syncthreads();
+    const int p = piv;
+    if (p != k)
+        for (int j = k + tid; j < m; j += GJ_THREADS) {
+            const double t = __ldcg(&a[(long long)k * m + j]);
+            a[(long long)k * m + j] = __ldcg(&a[(long long)p * m + j]);
+            a[(long long)p * m + j] = t;
+        }
+    __syncthreads();
+    const double inv = 1.0 / __ldcg(&a[(long long)k * m + k]);
+    __syncthreads();
+    for (int j = k + tid; j < m; j += GJ_THREADS) a[(long long)k * m + j] = __ldcg(&a[(long long)k * m + j]) * inv;
+    for (int i = tid; i < n; i += GJ_THREADS) col[i] = (i == k) ? 0.0 : __ldcg(&a[(long long)i * m + k]);
 }
 
-void launch_gauss_jordan(double *aug, int n, int *flag, cudaStream_t s) {
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(k_gauss_jordan, cudaFuncAttributeMaxDynamicSharedMemorySize, 160 * 1024);
-        attr = true;
+__global__ void __launch_bounds__(GJ_THREADS) k_gj_first(double *a, int n, double *col, int *flag) {
+    gj_pivot(a, n, 0, col, flag);
+}
+
+// elimination of column k from every other row over columns k..2n-1
+// (a_ij -= col_i a_kj), then the pivot step of column k + 1 by the last CTA
+__global__ void __launch_bounds__(GJ_THREADS) k_gj_step(double *a, int n, int k, double *col, int *flag,
+                                                        unsigned *arrived) {
+    const int m = 2 * n;
+    const int j = k + blockIdx.x * GJ_TC + (threadIdx.x % GJ_TC);
+    const int i0 = blockIdx.y * GJ_TR + threadIdx.x / GJ_TC;
+    if (j < m) {
+        const double akj = __ldcg(&a[(long long)k * m + j]);
+#pragma unroll
+        for (int r = 0; r < GJ_RPT; ++r) {
+            const int i = i0 + r * (GJ_THREADS / GJ_TC);
+            if (i < n && i != k) {
+                double *e = &a[(long long)i * m + j];
+                *e = fma(-__ldcg(&col[i]), akj, __ldcg(e));
+            }
+        }
     }
-    k_gauss_jordan<<<1, 1024, (size_t)n * sizeof(double), s>>>(aug, n, flag);
+    if (k + 1 >= n) return;
+    __shared__ bool last;
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) last = atomicAdd(arrived, 1u) == gridDim.x * gridDim.y - 1;
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    gj_pivot(a, n, k + 1, col, flag);
+    if (threadIdx.x == 0) *arrived = 0u;
+}
+
+size_t gauss_jordan_doubles(int n) { return (size_t)n * 2 * n + n + 1; }
+
+void launch_gauss_jordan(double *aug, int n, int *flag, cudaStream_t s) {
+    double *col = aug + (size_t)n * 2 * n;
+    unsigned *arrived = reinterpret_cast<unsigned *>(col + n);
+    cudaMemsetAsync(arrived, 0, sizeof(unsigned), s);
+    k_gj_first<<<1, GJ_THREADS, 0, s>>>(aug, n, col, flag);
+    const unsigned gy = (unsigned)((n + GJ_TR - 1) / GJ_TR);
+    for (int k = 0; k < n; k++) {
+        const unsigned gx = (unsigned)((2 * n - k + GJ_TC - 1) / GJ_TC);
+        k_gj_step<<<dim3(gx, gy), GJ_THREADS, 0, s>>>(aug, n, k, col, flag, arrived);
+    }
 }
 
 // one block per load case: b (optionally minus its mean per component), x = K^-1 b

@@ -89,9 +89,9 @@ def test_restrict_and_prolong(torch_cuda):
             assert np.all(got[0] == to_lib_field(uf)[:, 0].astype(np.float64))  # pinned origin untouched
 
 
-@pytest.mark.parametrize("coarse_mode", [H.COARSE_EXACT, H.COARSE_PROJECT])
-def test_coarsest_solve(torch_cuda, coarse_mode):
-    n = 16
+@pytest.mark.parametrize("coarse_mode,n", [(H.COARSE_EXACT, 16), (H.COARSE_PROJECT, 16), (H.COARSE_EXACT, 24)])
+def test_coarsest_solve(torch_cuda, coarse_mode, n):
+    # 16^3: 4^3 coarsest (192 unknowns); 24^3: 6^3 coarsest (648 unknowns, 21 x 21 elimination tiles)
     hd, m, _ = make_pair(torch_cuda, n=n, seed=4, coarse_mode=coarse_mode)
     copy_stencils_to_oracle(hd, m)
     L = hd.nlevels - 1
