@@ -235,7 +235,7 @@ __global__ void __launch_bounds__(FBS, 5) k_fine_gs(FineArgs a, const __grid_con
 
 template <int K>
 __device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const KeMat &ke, long long p, int cb,
-                                                     double nrm[NCASE]) {
+                                                     double nrm[CPT]) {
     const long long me = (long long)K * a.P + p;
     if (K == 7 && p == 0) {
 #pragma unroll
@@ -263,31 +263,38 @@ __device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const Ke
             a.r[o] = rv;
             s2 += (double)rv * rv;
         }
-#pragma unroll
-        for (int q = 0; q < NCASE; ++q)
-            if (q == cb + c) nrm[q] += mult * s2;
+        nrm[c] += mult * s2;
     }
 }
 
-__global__ void __launch_bounds__(FBS, 5) k_fine_residual(FineArgs a, const __grid_constant__ KeMat ke,
+// one colour per launch (the eight colour bodies in one kernel would not share
+// the instruction cache); the per-CTA norm partials of the CTA's two cases go to
+// row colour * gridDim.x + blockIdx.x, zeros for the other cases
+template <int K>
+__global__ void __launch_bounds__(FBS, 6) k_fine_residual(FineArgs a, const __grid_constant__ KeMat ke,
                                                        double *partial) {
     long long p;
     int cb;
     thread_task(p, cb);
-    double nrm[NCASE] = {0, 0, 0, 0, 0, 0};
-    if (p < a.P) {
-        switch (blockIdx.y) {
-        case 0: fine_residual_vertex<0>(a, ke, p, cb, nrm); break;
-        case 1: fine_residual_vertex<1>(a, ke, p, cb, nrm); break;
-        case 2: fine_residual_vertex<2>(a, ke, p, cb, nrm); break;
-        case 3: fine_residual_vertex<3>(a, ke, p, cb, nrm); break;
-        case 4: fine_residual_vertex<4>(a, ke, p, cb, nrm); break;
-        case 5: fine_residual_vertex<5>(a, ke, p, cb, nrm); break;
-        case 6: fine_residual_vertex<6>(a, ke, p, cb, nrm); break;
-        default: fine_residual_vertex<7>(a, ke, p, cb, nrm); break;
-        }
+    double nrm[CPT] = {0, 0};
+    if (p < a.P) fine_residual_vertex<K>(a, ke, p, cb, nrm);
+    if (!partial) return;
+    __shared__ double sm[CPT][FBS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        const double v = warp_sum(nrm[c]);
+        if (lane == 0) sm[c][wid] = v;
     }
-    if (partial) block_reduce<NCASE>(nrm, partial, (long long)blockIdx.y * gridDim.x + blockIdx.x);
+    __syncthreads();
+    if (threadIdx.x < NCASE) {
+        const int q = threadIdx.x;
+        double v = 0;
+        if (q >= cb && q < cb + CPT)
+#pragma unroll
+            for (int w = 0; w < FBS / 32; ++w) v += sm[q - cb][w];
+        partial[((long long)K * gridDim.x + blockIdx.x) * NCASE + q] = v;
+    }
 }
 
 // ---- refined precision: residual of an FP64 solution ----------------------------
@@ -423,7 +430,15 @@ void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, dou
                           cudaStream_t s) {
     FineArgs a = make_args(L, rho);
     (void)nblk_norm;
-    k_fine_residual<<<dim3(task_blocks(a), 8), FBS, 0, s>>>(a, ke, norm_partial);
+    const unsigned nb = task_blocks(a);
+    k_fine_residual<0><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
+    k_fine_residual<1><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
+    k_fine_residual<2><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
+    k_fine_residual<3><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
+    k_fine_residual<4><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
+    k_fine_residual<5><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
+    k_fine_residual<6><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
+    k_fine_residual<7><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
 }
 
 void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const float *f, const double *u64,
