@@ -42,11 +42,30 @@ __host__ __device__ inline long long vidx(const Planes &P, int x, int y, int z) 
 }
 
 // inverse of vidx for the vertex with plane offset p in colour k
+// unsigned 32-bit division by a divisor fixed at launch, as a multiply-high, an
+// add and a shift (Granlund and Montgomery's round-up method with the 33-bit
+// multiplier 2^32 + m, l = ceil(log2 d)); exact for every 32-bit dividend
+struct FastDiv {
+    unsigned d = 1, m = 1;
+    int l = 0;
+    FastDiv() = default;
+    __host__ explicit FastDiv(unsigned div) : d(div) {
+        l = 0;
+        while (l < 32 && (1ull << l) < div) ++l;
+        m = (unsigned)((((1ull << 32) * ((1ull << l) - div)) / div) + 1);
+    }
+    __device__ __forceinline__ unsigned div(unsigned n) const {
+        return (unsigned)(((unsigned long long)__umulhi(m, n) + n) >> l);
+    }
+};
+
+// position of index p (< 2^32) of colour plane k
 __host__ __device__ inline void vpos(const Planes &P, int k, long long p, int &x, int &y, int &z) {
-    int i = (int)(p % P.pn[k][0]);
-    long long t = p / P.pn[k][0];
-    int j = (int)(t % P.pn[k][1]);
-    int l = (int)(t / P.pn[k][1]);
+    const unsigned q = (unsigned)p, a = (unsigned)P.pn[k][0], b = (unsigned)P.pn[k][1];
+    const unsigned t = q / a;
+    const int i = (int)(q - t * a);
+    const int l = (int)(t / b);
+    const int j = (int)(t - (unsigned)l * b);
     x = 2 * i + ((k & 1) ^ 1);
     y = 2 * j + (((k >> 1) & 1) ^ 1);
     z = 2 * l + (((k >> 2) & 1) ^ 1);

@@ -26,7 +26,18 @@ struct CoarseArgs {
     long long nv;
     long long P;
     float w;
+    FastDiv dh0, dh1;  // division by h[0], h[1]
 };
+
+// (i, j, l) of index p (< 2^32) of a colour plane
+__device__ __forceinline__ void cplane_coords(const CoarseArgs &a, long long p, int &i, int &j, int &l) {
+    const unsigned q = (unsigned)p;
+    const unsigned t = a.dh0.div(q);
+    i = (int)(q - t * (unsigned)a.h[0]);
+    const unsigned z = a.dh1.div(t);
+    j = (int)(t - z * (unsigned)a.h[1]);
+    l = (int)z;
+}
 
 __device__ __forceinline__ void axis_nbrs_c(int i, int p, int h, int &im, int &ip) {
     if (p) { im = i; ip = (i + 1 == h) ? 0 : i + 1; }
@@ -68,6 +79,15 @@ __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, 
     axis_nbrs_c(j, py, a.h[1], jj[0], jj[2]);
     axis_nbrs_c(l, pz, a.h[2], ll[0], ll[2]);
     ii[1] = i; jj[1] = j; ll[1] = l;
+    // plane offsets of the neighbour rows (a colour plane holds < 2^32 vertices)
+    unsigned X[3], Y[3], Z[3];
+    const unsigned h0 = (unsigned)a.h[0], h01 = (unsigned)a.h[0] * (unsigned)a.h[1];
+#pragma unroll
+    for (int t = 0; t < 3; ++t) {
+        X[t] = (unsigned)ii[t];
+        Y[t] = h0 * (unsigned)jj[t];
+        Z[t] = h01 * (unsigned)ll[t];
+    }
 #pragma unroll
     for (int q = 0; q < 3 * CPTC; ++q) acc[q] = 0.f;
 #pragma unroll
@@ -84,8 +104,7 @@ __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, 
 #undef H3D_LB
         }
         const int Kn = K ^ ((dx & 1) | ((dy & 1) << 1) | ((dz & 1) << 2));
-        const long long nid =
-            (long long)Kn * a.P + ii[dx + 1] + (long long)a.h[0] * (jj[dy + 1] + (long long)a.h[1] * ll[dz + 1]);
+        const unsigned nid = (unsigned)Kn * (unsigned)a.P + X[dx + 1] + Y[dy + 1] + Z[dz + 1];
         const float *up = a.u + nid + (long long)(3 * cb) * a.nv;
 #pragma unroll
         for (int c = 0; c < CPTC; ++c) {
@@ -111,9 +130,8 @@ __global__ void __launch_bounds__(128) k_coarse_gs(CoarseArgs a) {
     coarse_task(p, cb);
     if (p >= a.P) return;
     const long long me = (long long)K * a.P + p;
-    const int i = (int)(p % a.h[0]);
-    const long long t = p / a.h[0];
-    const int j = (int)(t % a.h[1]), l = (int)(t / a.h[1]);
+    int i, j, l;
+    cplane_coords(a, p, i, j, l);
     float acc[3 * CPTC], ks[9];
     coarse_apply<K, false>(a, me, i, j, l, cb, acc);
     load_block<13>(a, me, ks);
@@ -135,9 +153,8 @@ __global__ void __launch_bounds__(128) k_coarse_gs(CoarseArgs a) {
 template <int K>
 __device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long p, int cb) {
     const long long me = (long long)K * a.P + p;
-    const int i = (int)(p % a.h[0]);
-    const long long t = p / a.h[0];
-    const int j = (int)(t % a.h[1]), l = (int)(t / a.h[1]);
+    int i, j, l;
+    cplane_coords(a, p, i, j, l);
     float acc[3 * CPTC];
     coarse_apply<K, true>(a, me, i, j, l, cb, acc);
 #pragma unroll
@@ -166,6 +183,8 @@ static CoarseArgs make_cargs(const Level &L) {
     a.nv = L.P.nv;
     a.P = L.P.nv / 8;
     a.w = 1.f;
+    a.dh0 = FastDiv((unsigned)a.h[0]);
+    a.dh1 = FastDiv((unsigned)a.h[1]);
     return a;
 }
 

@@ -43,6 +43,7 @@ struct FineArgs {
     long long nv;  // vertices
     long long P;   // vertices per colour plane
     float w;
+    FastDiv dh0, dh1;  // division by h[0], h[1]
 };
 
 __device__ __forceinline__ void axis_nbrs(int i, int p, int h, int &im, int &ip) {
@@ -50,11 +51,14 @@ __device__ __forceinline__ void axis_nbrs(int i, int p, int h, int &im, int &ip)
     else { im = (i == 0) ? h - 1 : i - 1; ip = i; }
 }
 
-__device__ __forceinline__ void plane_coords(long long p, const int h[3], int &i, int &j, int &l) {
-    i = (int)(p % h[0]);
-    long long t = p / h[0];
-    j = (int)(t % h[1]);
-    l = (int)(t / h[1]);
+// (i, j, l) of index p (< 2^32) of a colour plane
+__device__ __forceinline__ void plane_coords(const FineArgs &a, long long p, int &i, int &j, int &l) {
+    const unsigned q = (unsigned)p;
+    const unsigned t = a.dh0.div(q);
+    i = (int)(q - t * (unsigned)a.h[0]);
+    const unsigned z = a.dh1.div(t);
+    j = (int)(t - z * (unsigned)a.h[1]);
+    l = (int)z;
 }
 
 // first element (bit pattern w = ex | ey<<1 | ez<<2 of the element's offset from
@@ -76,7 +80,7 @@ struct VertexGeo {
     __device__ __forceinline__ VertexGeo(const FineArgs &a, long long p) {
         constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
         int i, j, l;
-        plane_coords(p, a.h, i, j, l);
+        plane_coords(a, p, i, j, l);
         const int x = 2 * i + px, y = 2 * j + py, z = 2 * l + pz;
         const int xe0 = x == 0 ? a.n[0] - 1 : x - 1;
         const int ye0 = y == 0 ? a.n[1] - 1 : y - 1;
@@ -250,7 +254,7 @@ __device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const Ke
     fine_apply<K>(a, ke, g, cb, uv, acc);
     constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
     int i, j, l;
-    plane_coords(p, a.h, i, j, l);
+    plane_coords(a, p, i, j, l);
     const double mult = (double)(axis_mult(2 * i + px, a.n[0]) * axis_mult(2 * j + py, a.n[1]) *
                                  axis_mult(2 * l + pz, a.n[2]));
 #pragma unroll
@@ -405,6 +409,8 @@ static FineArgs make_args(const Level &L, const float *rho) {
     a.nv = L.P.nv;
     a.P = L.P.nv / 8;
     a.w = 1.f;
+    a.dh0 = FastDiv((unsigned)a.h[0]);
+    a.dh1 = FastDiv((unsigned)a.h[1]);
     return a;
 }
 
