@@ -35,6 +35,7 @@ FIELD_U, FIELD_F, FIELD_R, FIELD_STENCIL, FIELD_CHI, FIELD_SOLUTION = range(6)
 COARSE_EXACT, COARSE_PROJECT = 0, 1
 PIN_IDENTITY, PIN_GALERKIN = 0, 1
 PREC_REFINE, PREC_FP32 = 0, 1
+STENCIL_FP16, STENCIL_FP32 = 0, 1
 SYMMETRY = {"reflect3": 0, "reflect6": 1, "rotate3": 2}
 
 _STATUS = {0: "ok", 1: "invalid argument", 2: "CUDA error", 3: "out of device memory", 4: "not converged",
@@ -50,7 +51,7 @@ class H3DError(RuntimeError):
 class Config(ctypes.Structure):
     _fields_ = [("reso", ctypes.c_int * 3), ("youngs_modulus", ctypes.c_double),
                 ("poisson_ratio", ctypes.c_double), ("coarse_mode", ctypes.c_int), ("pin_mode", ctypes.c_int),
-                ("precision", ctypes.c_int), ("device", ctypes.c_int)]
+                ("precision", ctypes.c_int), ("device", ctypes.c_int), ("stencil_precision", ctypes.c_int)]
 
 
 class SolveStats(ctypes.Structure):
@@ -178,13 +179,14 @@ def reference_resolution(reso):
 
 class _Handle:
     def __init__(self, reso, E=10.0, nu=0.3, coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY,
-                 precision=PREC_REFINE, device=0):
+                 precision=PREC_REFINE, device=0, stencil=STENCIL_FP16):
         L = lib()
         if isinstance(reso, int):
             reso = (reso, reso, reso)
         cfg = Config((ctypes.c_int * 3)(*reso), float(E), float(nu), int(coarse_mode), int(pin_mode),
-                     int(precision), int(device))
+                     int(precision), int(device), int(stencil))
         self.precision = precision
+        self.stencil = stencil
         h = ctypes.c_void_p()
         code = L.h3d_create(ctypes.byref(cfg), ctypes.byref(h))
         if code != H3D_OK:
@@ -312,8 +314,8 @@ class Homogenization(_Handle):
     """Homogenized elastic tensor of a periodic unit cell (homogenization.h:17-61)."""
 
     def __init__(self, reso, E=10.0, nu=0.3, coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY,
-                 precision=PREC_REFINE, device=0):
-        super().__init__(reso, E, nu, coarse_mode, pin_mode, precision, device)
+                 precision=PREC_REFINE, device=0, stencil=STENCIL_FP16):
+        super().__init__(reso, E, nu, coarse_mode, pin_mode, precision, device, stencil)
         self.mg = MG(self)
         self.grid = self.mg.grids[0]
         self.last_stats = None

@@ -10,7 +10,8 @@
 //   sweep therefore reads and writes contiguous runs, and the 26 neighbours of a
 //   vertex sit in the other colour planes at unit-stride offsets.
 //   Coarse stencils: 243 FP16 entries per vertex (27 neighbours x 3x3) packed
-//   eight to a uint4 chunk, chunk-major: st[q * nv + v], q = 0..30.
+//   eight to a uint4 chunk, chunk-major: st[q * nv + v], q = 0..30; or, with
+//   FP32 stencil storage, four to a chunk, q = 0..60.
 //   Density: float, lexicographic cells (the fine level only).
 #pragma once
 #include <cuda_runtime.h>
@@ -22,6 +23,7 @@ namespace h3d {
 constexpr int NCASE = 6;
 constexpr int NF = 18;          // floats per vertex (6 cases x 3 components)
 constexpr int NCHUNK = 31;      // uint4 chunks per stencil (243 halves -> 248)
+constexpr int NCHUNK32 = 61;    // the same with FP32 entries (243 floats -> 244)
 constexpr float RHO_PENAL_MIN = 1e-9f;  // grid.h:425
 
 struct Planes {
@@ -122,7 +124,55 @@ struct Level {
     int ratio[3];          // coarsening ratio from the finer level (0 on level 0)
     float *u = nullptr, *f = nullptr, *r = nullptr;
     uint4 *st = nullptr;   // coarse levels
+    bool st32 = false;     // FP32 stencil entries (FP16 otherwise)
 };
+
+#ifdef __CUDACC__
+// coarse-stencil storage: entry e of vertex v in chunk e / PER, slot e % PER
+template <bool F32>
+struct StencilStore;
+template <>
+struct StencilStore<false> {
+    static constexpr int PER = 8, CHUNKS = NCHUNK;
+    __device__ static float get(const uint4 *st, long long nv, long long v, int e) {
+        return __half2float(reinterpret_cast<const __half *>(st + (long long)(e >> 3) * nv + v)[e & 7]);
+    }
+    __device__ static void put(uint4 *st, long long nv, long long v, int e, float x) {
+        reinterpret_cast<__half *>(st + (long long)(e >> 3) * nv + v)[e & 7] = __float2half_rn(x);
+    }
+    __device__ static void putd(uint4 *st, long long nv, long long v, int e, double x) {
+        reinterpret_cast<__half *>(st + (long long)(e >> 3) * nv + v)[e & 7] = __double2half(x);
+    }
+    __device__ __forceinline__ static void unpack(const uint4 &c, float *o) {
+        const __half2 *h = reinterpret_cast<const __half2 *>(&c);
+#pragma unroll
+        for (int t = 0; t < 4; ++t) {
+            const float2 q = __half22float2(h[t]);
+            o[2 * t] = q.x;
+            o[2 * t + 1] = q.y;
+        }
+    }
+};
+template <>
+struct StencilStore<true> {
+    static constexpr int PER = 4, CHUNKS = NCHUNK32;
+    __device__ static float get(const uint4 *st, long long nv, long long v, int e) {
+        return reinterpret_cast<const float *>(st + (long long)(e >> 2) * nv + v)[e & 3];
+    }
+    __device__ static void put(uint4 *st, long long nv, long long v, int e, float x) {
+        reinterpret_cast<float *>(st + (long long)(e >> 2) * nv + v)[e & 3] = x;
+    }
+    __device__ static void putd(uint4 *st, long long nv, long long v, int e, double x) {
+        reinterpret_cast<float *>(st + (long long)(e >> 2) * nv + v)[e & 3] = (float)x;
+    }
+    __device__ __forceinline__ static void unpack(const uint4 &c, float *o) {
+        o[0] = __uint_as_float(c.x);
+        o[1] = __uint_as_float(c.y);
+        o[2] = __uint_as_float(c.z);
+        o[3] = __uint_as_float(c.w);
+    }
+};
+#endif
 
 // ---- launch wrappers (kernels in the .cu files) --------------------------
 // fine level (k_fine.cu)
@@ -210,7 +260,7 @@ void launch_warmnet_to_chi(const Planes &P, const float *y, int R, double *chi, 
 // field conversion (k_coarse.cu)
 void launch_field_to_lex(const Planes &P, const float *src, float *dst_lex, cudaStream_t s);
 void launch_field_from_lex(const Planes &P, const float *src_lex, float *dst, cudaStream_t s);
-void launch_stencil_to_lex(const Planes &P, const uint4 *st, float *dst_lex, cudaStream_t s);
-void launch_stencil_from_lex(const Planes &P, const float *src_lex, uint4 *st, cudaStream_t s);
+void launch_stencil_to_lex(const Level &L, float *dst_lex, cudaStream_t s);
+void launch_stencil_from_lex(const Level &L, const float *src_lex, cudaStream_t s);
 
 }  // namespace h3d

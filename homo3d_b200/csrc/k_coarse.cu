@@ -44,25 +44,16 @@ __device__ __forceinline__ void axis_nbrs_c(int i, int p, int h, int &im, int &i
     else { im = (i == 0) ? h - 1 : i - 1; ip = i; }
 }
 
-__device__ __forceinline__ void unpack8(const uint4 &c, float o[8]) {
-    const __half2 *h = reinterpret_cast<const __half2 *>(&c);
-#pragma unroll
-    for (int t = 0; t < 4; ++t) {
-        const float2 v = __half22float2(h[t]);
-        o[2 * t] = v.x;
-        o[2 * t + 1] = v.y;
-    }
-}
-
 // the 9 entries of neighbour block d of vertex me
-template <int D>
+template <int D, bool F32>
 __device__ __forceinline__ void load_block(const CoarseArgs &a, long long me, float s[9]) {
-    constexpr int e0 = 9 * D, q0 = e0 / 8, q1 = (e0 + 8) / 8;
-    float v[16];
-    unpack8(a.st[q0 * a.nv + me], v);
-    if (q1 != q0) unpack8(a.st[q1 * a.nv + me], v + 8);
+    using S = StencilStore<F32>;
+    constexpr int e0 = 9 * D, q0 = e0 / S::PER, q1 = (e0 + 8) / S::PER;
+    float v[3 * S::PER];
 #pragma unroll
-    for (int k = 0; k < 9; ++k) s[k] = v[e0 + k - 8 * q0];
+    for (int q = q0; q <= q1; ++q) S::unpack(a.st[q * a.nv + me], v + (q - q0) * S::PER);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) s[k] = v[e0 + k - S::PER * q0];
 }
 
 // load cases per thread on the coarse levels; the two threads of a vertex run in
@@ -70,7 +61,7 @@ __device__ __forceinline__ void load_block(const CoarseArgs &a, long long me, fl
 constexpr int CPTC = 3;
 constexpr int NGC = NCASE / CPTC;
 
-template <int K, bool SELF>
+template <int K, bool SELF, bool F32>
 __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, int i, int j, int l, int cb,
                                              float acc[3 * CPTC]) {
     constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
@@ -96,7 +87,7 @@ __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, 
         const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
         float s[9];
         switch (d) {  // compile-time block index for the chunk arithmetic
-#define H3D_LB(D) case D: load_block<D>(a, me, s); break;
+#define H3D_LB(D) case D: load_block<D, F32>(a, me, s); break;
             H3D_LB(0) H3D_LB(1) H3D_LB(2) H3D_LB(3) H3D_LB(4) H3D_LB(5) H3D_LB(6) H3D_LB(7) H3D_LB(8)
             H3D_LB(9) H3D_LB(10) H3D_LB(11) H3D_LB(12) H3D_LB(13) H3D_LB(14) H3D_LB(15) H3D_LB(16)
             H3D_LB(17) H3D_LB(18) H3D_LB(19) H3D_LB(20) H3D_LB(21) H3D_LB(22) H3D_LB(23) H3D_LB(24)
@@ -123,7 +114,7 @@ __device__ __forceinline__ void coarse_task(long long &p, int &cb) {
     p = (long long)(blockIdx.x / NGC) * blockDim.x + threadIdx.x;
 }
 
-template <int K>
+template <int K, bool F32>
 __global__ void __launch_bounds__(128) k_coarse_gs(CoarseArgs a) {
     long long p;
     int cb;
@@ -133,8 +124,8 @@ __global__ void __launch_bounds__(128) k_coarse_gs(CoarseArgs a) {
     int i, j, l;
     cplane_coords(a, p, i, j, l);
     float acc[3 * CPTC], ks[9];
-    coarse_apply<K, false>(a, me, i, j, l, cb, acc);
-    load_block<13>(a, me, ks);
+    coarse_apply<K, false, F32>(a, me, i, j, l, cb, acc);
+    load_block<13, F32>(a, me, ks);
     const float w = a.w;
 #pragma unroll
     for (int c = 0; c < CPTC; ++c) {
@@ -150,13 +141,13 @@ __global__ void __launch_bounds__(128) k_coarse_gs(CoarseArgs a) {
     }
 }
 
-template <int K>
+template <int K, bool F32>
 __device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long p, int cb) {
     const long long me = (long long)K * a.P + p;
     int i, j, l;
     cplane_coords(a, p, i, j, l);
     float acc[3 * CPTC];
-    coarse_apply<K, true>(a, me, i, j, l, cb, acc);
+    coarse_apply<K, true, F32>(a, me, i, j, l, cb, acc);
 #pragma unroll
     for (int q = 0; q < 3 * CPTC; ++q) {
         const long long o = (3 * cb + q) * a.nv + me;
@@ -164,13 +155,13 @@ __device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long
     }
 }
 
-template <int K>
+template <int K, bool F32>
 __global__ void __launch_bounds__(128, 5) k_coarse_residual(CoarseArgs a) {
     long long p;
     int cb;
     coarse_task(p, cb);
     if (p >= a.P) return;
-    coarse_res_vertex<K>(a, p, cb);
+    coarse_res_vertex<K, F32>(a, p, cb);
 }
 
 static CoarseArgs make_cargs(const Level &L) {
@@ -188,33 +179,43 @@ static CoarseArgs make_cargs(const Level &L) {
     return a;
 }
 
+template <bool F32>
+static void coarse_gs_sweep(const CoarseArgs &a, unsigned nb, cudaStream_t s) {
+    k_coarse_gs<0, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<1, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<2, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<3, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<4, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<5, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<6, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<7, F32><<<nb, 128, 0, s>>>(a);
+}
+
 void launch_coarse_gs(const Level &L, float w, cudaStream_t s) {
     CoarseArgs a = make_cargs(L);
     a.w = w;
-    const int bs = 128;
-    const unsigned nb = (unsigned)((a.P + bs - 1) / bs) * NGC;
-    k_coarse_gs<0><<<nb, bs, 0, s>>>(a);
-    k_coarse_gs<1><<<nb, bs, 0, s>>>(a);
-    k_coarse_gs<2><<<nb, bs, 0, s>>>(a);
-    k_coarse_gs<3><<<nb, bs, 0, s>>>(a);
-    k_coarse_gs<4><<<nb, bs, 0, s>>>(a);
-    k_coarse_gs<5><<<nb, bs, 0, s>>>(a);
-    k_coarse_gs<6><<<nb, bs, 0, s>>>(a);
-    k_coarse_gs<7><<<nb, bs, 0, s>>>(a);
+    const unsigned nb = (unsigned)((a.P + 127) / 128) * NGC;
+    if (L.st32) coarse_gs_sweep<true>(a, nb, s);
+    else coarse_gs_sweep<false>(a, nb, s);
+}
+
+template <bool F32>
+static void coarse_residual_all(const CoarseArgs &a, unsigned nb, cudaStream_t s) {
+    k_coarse_residual<0, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<1, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<2, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<3, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<4, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<5, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<6, F32><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<7, F32><<<nb, 128, 0, s>>>(a);
 }
 
 void launch_coarse_residual(const Level &L, cudaStream_t s) {
     CoarseArgs a = make_cargs(L);
-    const int bs = 128;
-    const unsigned nb = (unsigned)((a.P + bs - 1) / bs) * NGC;
-    k_coarse_residual<0><<<nb, bs, 0, s>>>(a);
-    k_coarse_residual<1><<<nb, bs, 0, s>>>(a);
-    k_coarse_residual<2><<<nb, bs, 0, s>>>(a);
-    k_coarse_residual<3><<<nb, bs, 0, s>>>(a);
-    k_coarse_residual<4><<<nb, bs, 0, s>>>(a);
-    k_coarse_residual<5><<<nb, bs, 0, s>>>(a);
-    k_coarse_residual<6><<<nb, bs, 0, s>>>(a);
-    k_coarse_residual<7><<<nb, bs, 0, s>>>(a);
+    const unsigned nb = (unsigned)((a.P + 127) / 128) * NGC;
+    if (L.st32) coarse_residual_all<true>(a, nb, s);
+    else coarse_residual_all<false>(a, nb, s);
 }
 
 // ---- transfers ---------------------------------------------------------------
@@ -422,34 +423,25 @@ void launch_field_from_lex(const Planes &P, const float *src_lex, float *dst, cu
     k_field_lex<<<(unsigned)((P.nv + 255) / 256), 256, 0, s>>>(P, src_lex, dst, 0);
 }
 
-__global__ void k_stencil_lex(Planes P, const uint4 *st, float *lexf, const float *lexin, uint4 *stout) {
+__global__ void k_stencil_lex(Planes P, const uint4 *st, float *lexf, const float *lexin, uint4 *stout, int f32) {
     const long long lex = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (lex >= P.nv) return;
     const int x = (int)(lex % P.n[0]);
     const long long t = lex / P.n[0];
     const int y = (int)(t % P.n[1]), z = (int)(t / P.n[1]);
     const long long v = vidx(P, x, y, z);
-    for (int q = 0; q < NCHUNK; ++q) {
-        if (lexf) {
-            uint4 c = st[q * P.nv + v];
-            const __half *h = reinterpret_cast<const __half *>(&c);
-            for (int e = 0; e < 8; ++e)
-                if (8 * q + e < 243) lexf[lex * 243 + 8 * q + e] = __half2float(h[e]);
-        } else {
-            uint4 c;
-            __half *h = reinterpret_cast<__half *>(&c);
-            for (int e = 0; e < 8; ++e)
-                h[e] = (8 * q + e < 243) ? __float2half_rn(lexin[lex * 243 + 8 * q + e]) : __float2half_rn(0.f);
-            stout[q * P.nv + v] = c;
-        }
+    for (int e = 0; e < 243; ++e) {
+        if (lexf) lexf[lex * 243 + e] = f32 ? StencilStore<true>::get(st, P.nv, v, e) : StencilStore<false>::get(st, P.nv, v, e);
+        else if (f32) StencilStore<true>::put(stout, P.nv, v, e, lexin[lex * 243 + e]);
+        else StencilStore<false>::put(stout, P.nv, v, e, lexin[lex * 243 + e]);
     }
 }
 
-void launch_stencil_to_lex(const Planes &P, const uint4 *st, float *dst_lex, cudaStream_t s) {
-    k_stencil_lex<<<(unsigned)((P.nv + 127) / 128), 128, 0, s>>>(P, st, dst_lex, nullptr, nullptr);
+void launch_stencil_to_lex(const Level &L, float *dst_lex, cudaStream_t s) {
+    k_stencil_lex<<<(unsigned)((L.P.nv + 127) / 128), 128, 0, s>>>(L.P, L.st, dst_lex, nullptr, nullptr, L.st32);
 }
-void launch_stencil_from_lex(const Planes &P, const float *src_lex, uint4 *st, cudaStream_t s) {
-    k_stencil_lex<<<(unsigned)((P.nv + 127) / 128), 128, 0, s>>>(P, nullptr, nullptr, src_lex, st);
+void launch_stencil_from_lex(const Level &L, const float *src_lex, cudaStream_t s) {
+    k_stencil_lex<<<(unsigned)((L.P.nv + 127) / 128), 128, 0, s>>>(L.P, nullptr, nullptr, src_lex, L.st, L.st32);
 }
 
 }  // namespace h3d

@@ -26,19 +26,10 @@ namespace h3d {
 
 __device__ __forceinline__ int modp(int a, int n) { return ((a % n) + n) % n; }
 
-__device__ __forceinline__ void put_half(uint4 *st, long long nv, long long v, int e, __half h) {
-    __half *p = reinterpret_cast<__half *>(st + (long long)(e >> 3) * nv + v) + (e & 7);
-    *p = h;
-}
-__device__ __forceinline__ float get_half(const uint4 *st, long long nv, long long v, int e) {
-    const __half *p = reinterpret_cast<const __half *>(st + (long long)(e >> 3) * nv + v) + (e & 7);
-    return __half2float(*p);
-}
-
 // ---- level 1 from densities ---------------------------------------------------
 // R = 2 on every axis is compiled with the sub-element loop unrolled; R = 0 is
 // the generic path for ratio 4 (or mixed ratios).
-template <int R>
+template <int R, bool F32>
 __global__ void __launch_bounds__(128) k_galerkin_l1(Planes F, Planes C, int r0, int r1, int r2,
                                                      const float *__restrict__ rho, const float *__restrict__ q,
                                                      int nsub, uint4 *st) {
@@ -64,9 +55,10 @@ __global__ void __launch_bounds__(128) k_galerkin_l1(Planes F, Planes C, int r0,
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
-        __half res[9];
+        // the images are summed in the storage precision (FP16: grid.cu:3103-3176)
+        float res[9];
 #pragma unroll
-        for (int e = 0; e < 9; ++e) res[e] = __float2half_rn(0.f);
+        for (int e = 0; e < 9; ++e) res[e] = 0.f;
         for (int img = 0; img < 8; ++img) {
             if (img & ~bmask) continue;
             float p[9];
@@ -110,19 +102,28 @@ __global__ void __launch_bounds__(128) k_galerkin_l1(Planes F, Planes C, int r0,
                     if (fabsf(p[4 * t]) < 1e-4f) p[4 * t] = 1e-4f;
             }
 #pragma unroll
-            for (int e = 0; e < 9; ++e) res[e] = __hadd(res[e], __float2half_rn(p[e]));
+            for (int e = 0; e < 9; ++e)
+                res[e] = F32 ? res[e] + p[e] : __half2float(__hadd(__float2half_rn(res[e]), __float2half_rn(p[e])));
         }
-        // stream the 9 halves into the packed chunks
+        // stream the 9 entries into the packed chunks
 #pragma unroll
         for (int e = 0; e < 9; ++e) {
             const int g = 9 * d + e;
-            const uint32_t hv = (uint32_t)__half_as_ushort(res[e]);
-            const int slot = (g & 7) >> 1;
-            if (g & 1) cbuf[slot] |= hv << 16;
-            else cbuf[slot] = hv;
-            if ((g & 7) == 7 || g == 242) {
-                if (g == 242) { cbuf[1] &= 0xffffu; cbuf[2] = 0; cbuf[3] = 0; }
-                st[(long long)(g >> 3) * C.nv + v] = make_uint4(cbuf[0], cbuf[1], cbuf[2], cbuf[3]);
+            if (F32) {
+                cbuf[g & 3] = __float_as_uint(res[e]);
+                if ((g & 3) == 3 || g == 242) {
+                    if (g == 242) cbuf[3] = 0;  // entries 240..242 and the pad
+                    st[(long long)(g >> 2) * C.nv + v] = make_uint4(cbuf[0], cbuf[1], cbuf[2], cbuf[3]);
+                }
+            } else {
+                const uint32_t hv = (uint32_t)__half_as_ushort(__float2half_rn(res[e]));
+                const int slot = (g & 7) >> 1;
+                if (g & 1) cbuf[slot] |= hv << 16;
+                else cbuf[slot] = hv;
+                if ((g & 7) == 7 || g == 242) {
+                    if (g == 242) { cbuf[1] &= 0xffffu; cbuf[2] = 0; cbuf[3] = 0; }
+                    st[(long long)(g >> 3) * C.nv + v] = make_uint4(cbuf[0], cbuf[1], cbuf[2], cbuf[3]);
+                }
             }
         }
     }
@@ -133,14 +134,20 @@ void launch_galerkin_l1(const Level &F, const Level &C, const float *rho, const 
     const unsigned nb = (unsigned)((C.P.nv + bs - 1) / bs);
     const size_t smem = (size_t)nsub * 576 * sizeof(float);
     if (C.ratio[0] == 2 && C.ratio[1] == 2 && C.ratio[2] == 2) {
-        k_galerkin_l1<2><<<nb, bs, smem, s>>>(F.P, C.P, 2, 2, 2, rho, q, nsub, C.st);
+        if (C.st32) k_galerkin_l1<2, true><<<nb, bs, smem, s>>>(F.P, C.P, 2, 2, 2, rho, q, nsub, C.st);
+        else k_galerkin_l1<2, false><<<nb, bs, smem, s>>>(F.P, C.P, 2, 2, 2, rho, q, nsub, C.st);
     } else {
         static bool attr = false;
         if (!attr) {
-            cudaFuncSetAttribute(k_galerkin_l1<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaFuncSetAttribute(k_galerkin_l1<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+            cudaFuncSetAttribute(k_galerkin_l1<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
             attr = true;
         }
-        k_galerkin_l1<0><<<nb, bs, smem, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], rho, q, nsub, C.st);
+        if (C.st32)
+            k_galerkin_l1<0, true><<<nb, bs, smem, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], rho, q, nsub, C.st);
+        else
+            k_galerkin_l1<0, false><<<nb, bs, smem, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], rho, q, nsub,
+                                                         C.st);
     }
 }
 
@@ -152,6 +159,7 @@ __device__ __forceinline__ double hat_w(int ox, int oy, int oz, int r0, int r1, 
 }
 
 // one thread per (coarse vertex offset vi in {-1,0,1}^3, neighbour d)
+template <bool F32>
 __global__ void k_dirichlet_patch(Planes F, Planes C, int r0, int r1, int r2, const float *__restrict__ rho,
                                   const double *__restrict__ ked, int pin_identity, uint4 *st) {
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
@@ -194,16 +202,21 @@ __global__ void k_dirichlet_patch(Planes F, Planes C, int r0, int r1, int r2, co
         for (int i = 0; i < 3; i++)
             if (fabs(s[4 * i]) < 1e-4) s[4 * i] = 1e-4;
     const long long v = vidx(C, modp(vio[0], C.n[0]), modp(vio[1], C.n[1]), modp(vio[2], C.n[2]));
-    for (int e = 0; e < 9; e++) put_half(st, C.nv, v, 9 * d + e, __double2half(s[e]));
+    for (int e = 0; e < 9; e++) StencilStore<F32>::putd(st, C.nv, v, 9 * d + e, s[e]);
 }
 
 void launch_dirichlet_patch(const Level &F, const Level &C, const float *rho, const double *ked, int pin_identity,
                             cudaStream_t s) {
-    k_dirichlet_patch<<<(27 * 27 + 127) / 128, 128, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], rho, ked,
-                                                            pin_identity, C.st);
+    if (C.st32)
+        k_dirichlet_patch<true><<<(27 * 27 + 127) / 128, 128, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2],
+                                                                      rho, ked, pin_identity, C.st);
+    else
+        k_dirichlet_patch<false><<<(27 * 27 + 127) / 128, 128, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2],
+                                                                       rho, ked, pin_identity, C.st);
 }
 
-// ---- deeper levels: R A P from the finer FP16 stencil ----------------------------
+// ---- deeper levels: R A P from the finer stencil -----------------------------------
+template <bool F32>
 __global__ void __launch_bounds__(128) k_galerkin(Planes F, Planes C, int r0, int r1, int r2,
                                                   const uint4 *__restrict__ fst, uint4 *cst) {
     const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
@@ -230,24 +243,27 @@ __global__ void __launch_bounds__(128) k_galerkin(Planes F, Planes C, int r0, in
                         const float wj = (float)((r0 - o0) * (r1 - o1) * (r2 - o2)) / pr;
                         const float ww = wi * wj;
 #pragma unroll
-                        for (int e = 0; e < 9; e++) s[e] = fmaf(ww, get_half(fst, F.nv, fv, 9 * j + e), s[e]);
+                        for (int e = 0; e < 9; e++)
+                            s[e] = fmaf(ww, StencilStore<F32>::get(fst, F.nv, fv, 9 * j + e), s[e]);
                     }
                 }
         if (d == 13)
             for (int t = 0; t < 3; t++)
                 if (fabsf(s[4 * t]) < 1e-4f) s[4 * t] = 1e-4f;
-        for (int e = 0; e < 9; e++) put_half(cst, C.nv, v, 9 * d + e, __float2half_rn(s[e]));
+        for (int e = 0; e < 9; e++) StencilStore<F32>::put(cst, C.nv, v, 9 * d + e, s[e]);
     }
 }
 
 void launch_galerkin(const Level &F, const Level &C, cudaStream_t s) {
     const int bs = 128;
-    k_galerkin<<<(unsigned)((C.P.nv + bs - 1) / bs), bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.st,
-                                                                  C.st);
+    const unsigned nb = (unsigned)((C.P.nv + bs - 1) / bs);
+    if (C.st32) k_galerkin<true><<<nb, bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.st, C.st);
+    else k_galerkin<false><<<nb, bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.st, C.st);
 }
 
 // ---- coarsest level ---------------------------------------------------------------
 // aug: [n][2n] row-major, left = K over unique DOFs (3*lexid + comp), right = I
+template <bool F32>
 __global__ void k_coarse_assemble(Planes C, const uint4 *__restrict__ st, double *aug, int n) {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (t >= C.nv * 27) return;
@@ -260,7 +276,7 @@ __global__ void k_coarse_assemble(Planes C, const uint4 *__restrict__ st, double
     const long long w = wx + (long long)C.n[0] * (wy + (long long)C.n[1] * wz);
     for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++)
-            atomicAdd(&aug[(3 * lex + i) * (2LL * n) + 3 * w + j], (double)get_half(st, C.nv, v, 9 * d + 3 * i + j));
+            atomicAdd(&aug[(3 * lex + i) * (2LL * n) + 3 * w + j], (double)StencilStore<F32>::get(st, C.nv, v, 9 * d + 3 * i + j));
     if (d == 0)
         for (int i = 0; i < 3; i++) aug[(3 * lex + i) * (2LL * n) + n + 3 * lex + i] = 1.0;
 }
@@ -269,7 +285,8 @@ void launch_coarse_assemble(const Level &C, double *aug, cudaStream_t s) {
     const int n = (int)(3 * C.P.nv);
     cudaMemsetAsync(aug, 0, sizeof(double) * (size_t)n * 2 * n, s);
     const long long nt = C.P.nv * 27;
-    k_coarse_assemble<<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(C.P, C.st, aug, n);
+    if (C.st32) k_coarse_assemble<true><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(C.P, C.st, aug, n);
+    else k_coarse_assemble<false><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(C.P, C.st, aug, n);
 }
 
 // Gauss-Jordan elimination with partial pivoting on [K | I] (n rows, 2n columns,

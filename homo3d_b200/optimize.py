@@ -14,7 +14,7 @@ import time
 
 import numpy as np
 
-from . import (COARSE_EXACT, PIN_IDENTITY, PREC_REFINE, Homogenization, OCOptimizer, symmetrize)
+from . import (COARSE_EXACT, PIN_IDENTITY, PREC_REFINE, STENCIL_FP16, Homogenization, OCOptimizer, symmetrize)
 from .density import synthetic_density
 
 
@@ -50,12 +50,12 @@ class ConvergeChecker:
 def optimize_bulk(reso, vol=0.3, iters=50, seed=0, relthres=1e-2, filter_radius=2.0, step=0.05, damp=0.5,
                   sym="reflect6", finthres=5e-4, stop_on_converge=False, rho0=None, E=10.0, nu=0.3,
                   coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY, precision=PREC_REFINE, device=0,
-                  on_solve=None):
+                  on_solve=None, stencil=STENCIL_FP16):
     """The OC loop of testAutoDiff.cu:282-331 (bulk modulus); on_solve(hom, rho_phys)
     is called after every solve (e.g. to record training pairs)."""
     import torch
 
-    hom = Homogenization(reso, E, nu, coarse_mode, pin_mode, precision, device)
+    hom = Homogenization(reso, E, nu, coarse_mode, pin_mode, precision, device, stencil)
     n = hom.dims[0]
     ne = n[0] * n[1] * n[2]
     dev = torch.device("cuda", device)

@@ -1,0 +1,92 @@
+"""Precision study of the six-case solve at large grids: the refined scheme
+(FP64 solution, FP32 V-cycles on the correction, FP64 C) at relthres 1e-5 and the
+plain FP32 scheme of the reference, each against a reference C from the same
+design solved to relthres 1e-9 with the FP64-accumulated residual.  No reference
+counterpart: the reference has only the FP32 scheme.
+
+At 256^3 and 512^3 the FP64 oracle cannot finish a solve in reasonable time on
+the host; the reference C here is the GPU's FP64-residual refinement driven to
+1e-9, whose FP64 arithmetic is checked against the oracle at small grids by the
+test suite.
+
+    python -m homo3d_b200.precision --reso 256 --vols 0.1,0.3,0.5
+"""
+import argparse
+import json
+import time
+
+import numpy as np
+
+from . import PREC_FP32, PREC_REFINE, STENCIL_FP16, STENCIL_FP32, H3DError, Homogenization
+from .density import synthetic_density
+
+
+def solve(torch, n, rho, precision, tol, stencil=STENCIL_FP16):
+    hd = Homogenization(n, precision=precision, stencil=stencil)
+    try:
+        hd.update(rho)
+        hd.reset_solutions()
+        hd.sync()
+        t0 = time.perf_counter()
+        try:
+            C = hd.elasticMatrix(tol)
+            err = None
+        except H3DError as e:
+            C, err = None, str(e)
+        dt = (time.perf_counter() - t0) * 1e3
+        st = dict(hd.last_stats or {})
+    finally:
+        hd.close()
+    return C, dt, st, err
+
+
+def study(n, vol, seed=0, fp32_tols=(1e-3, 1e-4, 1e-5), ref_stencil=STENCIL_FP16, stencil=STENCIL_FP16):
+    import torch
+    rho = torch.tensor((synthetic_density(n, seed=seed, vol=vol).ravel() ** 3).astype(np.float32), device="cuda")
+    Cref, tref, sref, eref = solve(torch, n, rho, PREC_REFINE, 1e-9, ref_stencil)
+    if Cref is None:
+        return {"reso": n, "vol": vol, "error": "reference solve failed: %s" % eref}
+    scale = np.abs(Cref).max()
+
+    def errs(C):
+        d = np.abs(C - Cref)
+        return {"diag_rel": [float(d[i, i] / abs(Cref[i, i])) for i in range(6)],
+                "max_abs_over_max_C": float(d.max() / scale)}
+
+    out = {"reso": n, "vol": vol, "seed": seed, "C_ref_diag": [float(Cref[i, i]) for i in range(6)],
+           "stencils": "fp32" if stencil == STENCIL_FP32 else "fp16",
+           "ref": {"relthres": 1e-9, "ms": tref, "vcycles": sref.get("vcycles"), "refinements": sref.get("refinements"),
+                   "status": sref.get("status"), "rel_res": max(sref.get("rel_res", [0])),
+                   "stencils": "fp32" if ref_stencil == STENCIL_FP32 else "fp16"}}
+    C, t, st, e = solve(torch, n, rho, PREC_REFINE, 1e-5, stencil)
+    out["refined_1e-5"] = {"ms": t, "vcycles": st.get("vcycles"), "refinements": st.get("refinements"),
+                           "rel_res": max(st.get("rel_res", [0])), "error": e, **(errs(C) if C is not None else {})}
+    for tol in fp32_tols:
+        C, t, st, e = solve(torch, n, rho, PREC_FP32, tol, stencil)
+        row = {"ms": t, "vcycles": st.get("vcycles"), "status": st.get("status"),
+               "rel_res": max(st.get("rel_res", [0])), "error": e}
+        if C is not None:
+            row.update(errs(C))
+        row["converged"] = st.get("status") == 0
+        out["fp32_%g" % tol] = row
+    return out
+
+
+def main():
+    ap = argparse.ArgumentParser(description=__doc__.splitlines()[0])
+    ap.add_argument("--reso", type=int, default=256)
+    ap.add_argument("--vols", default="0.1,0.3,0.5")
+    ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--fp32-tols", default="1e-3,1e-4,1e-5")
+    ap.add_argument("--stencils", choices=["fp16", "fp32"], default="fp16", help="coarse stencils of the timed solves")
+    ap.add_argument("--ref-stencils", choices=["fp16", "fp32"], default="fp32",
+                    help="coarse stencils of the 1e-9 reference solve")
+    args = ap.parse_args()
+    tols = tuple(float(t) for t in args.fp32_tols.split(",") if t)
+    st = {"fp16": STENCIL_FP16, "fp32": STENCIL_FP32}
+    for vol in (float(v) for v in args.vols.split(",")):
+        print(json.dumps(study(args.reso, vol, args.seed, tols, st[args.ref_stencils], st[args.stencils])), flush=True)
+
+
+if __name__ == "__main__":
+    main()

@@ -70,6 +70,14 @@ typedef enum {
                                    relative residual floors near 1e-6 * N */
 } h3d_precision;
 
+/* storage of the Galerkin coarse-level stencils */
+typedef enum {
+    H3D_STENCIL_FP16 = 0,       /* FP16 entries, images summed in FP16, as the reference does */
+    H3D_STENCIL_FP32 = 1        /* FP32 entries (twice the stencil bytes); keeps the V-cycle
+                                   convergent on high-contrast designs where FP16 rounding of
+                                   the coarse operators stalls or diverges it */
+} h3d_stencil_precision;
+
 typedef struct {
     int reso[3];                /* requested cells per axis; corrected like the reference */
     double youngs_modulus;      /* E of the base material */
@@ -78,6 +86,7 @@ typedef struct {
     int pin_mode;               /* h3d_pin_mode */
     int precision;              /* h3d_precision */
     int device;                 /* CUDA device ordinal */
+    int stencil_precision;      /* h3d_stencil_precision (0 = FP16) */
 } h3d_config;
 
 typedef struct {

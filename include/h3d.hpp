@@ -28,6 +28,7 @@ struct HomoConfig {               // the fields of cfg::HomoConfig this path rea
     int pinMode = H3D_PIN_IDENTITY;
     int precision = H3D_PREC_REFINE;
     int device = 0;
+    int stencilPrecision = H3D_STENCIL_FP16;
 };
 
 // one level of the hierarchy (grid.h:104-418); operates on all six load cases
@@ -92,6 +93,7 @@ struct Homogenization {
         cfg.pin_mode = c.pinMode;
         cfg.precision = c.precision;
         cfg.device = c.device;
+        cfg.stencil_precision = c.stencilPrecision;
         if (h3d_create(&cfg, &h) != H3D_OK) throw std::runtime_error("h3d_create failed");
         mg_.reset(new MG());
         mg_->h = h;
