@@ -487,64 +487,69 @@ __global__ void k_update64(long long nv, double *u, const float *__restrict__ e,
 // neighbours of the origin, F -= A_pp alpha), which is the same iteration; T joins
 // the solution when it is next folded (k_update64, k_pin_fold).
 // state[0..17] = F per (case, component), state[18..35] = T.
-__global__ void k_pin_deflate(FineArgs a, const __grid_constant__ KeMat ke, double *state) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+// One CTA of PIN_THREADS: thread (n, cr) with n < 26 the neighbour index (d = n,
+// or n + 1 past the origin's own d = 13) and cr = 3c + r; the products of each
+// neighbour are summed over d in ascending order by one thread per (c, r).
+constexpr int PIN_THREADS = 26 * NF;
+__global__ void __launch_bounds__(PIN_THREADS) k_pin_deflate(FineArgs a, const __grid_constant__ KeMat ke,
+                                                              double *state) {
+    __shared__ double qpart[26][NF];
+    __shared__ double al[NF];
+    __shared__ double Ms[9];
+    __shared__ int ok;
+    const int tid = threadIdx.x;
+    const int n = tid / NF, cr = tid % NF, c = cr / 3, r = cr % 3;
+    const int d = n < 13 ? n : n + 1;
     const VertexGeo<7> g(a, 0);
-    double q[NF];
-#pragma unroll
-    for (int i = 0; i < NF; ++i) q[i] = 0.0;
-    for (int d = 0; d < 27; ++d) {
-        if (d == 13) continue;
-        int Kn;
-        bool pinned;
-        const unsigned nid = g.nbr(a, d, Kn, pinned);
-        if (pinned) continue;
-        float A[9];
-        g.block(ke, d, A);
-        for (int c = 0; c < NCASE; ++c)
-            for (int r = 0; r < 3; ++r) {
-                double t = 0;
-                for (int k = 0; k < 3; ++k) t += (double)A[3 * r + k] * (double)a.u[(3 * c + k) * a.nv + nid];
-                q[3 * c + r] += t;
-            }
+    int Kn;
+    bool pinned;
+    const unsigned nid = g.nbr(a, d, Kn, pinned);
+    float A[9];
+    g.block(ke, d, A);
+    {
+        double t = 0;
+        if (!pinned)
+            for (int k = 0; k < 3; ++k) t += (double)A[3 * r + k] * (double)a.u[(3 * c + k) * a.nv + nid];
+        qpart[n][cr] = t;
     }
-    float Af[9];
-    g.block(ke, 13, Af);
-    double M[9];
-    for (int k = 0; k < 9; ++k) M[k] = (double)Af[k];
-    // inverse of the 3x3 self block by cofactors
-    const double c00 = M[4] * M[8] - M[5] * M[7], c01 = M[5] * M[6] - M[3] * M[8], c02 = M[3] * M[7] - M[4] * M[6];
-    const double det = M[0] * c00 + M[1] * c01 + M[2] * c02;
-    if (!(det > 0.0)) return;  // not positive definite: leave the iterate alone
-    const double inv[9] = {c00 / det, (M[2] * M[7] - M[1] * M[8]) / det, (M[1] * M[5] - M[2] * M[4]) / det,
-                           c01 / det, (M[0] * M[8] - M[2] * M[6]) / det, (M[2] * M[3] - M[0] * M[5]) / det,
-                           c02 / det, (M[1] * M[6] - M[0] * M[7]) / det, (M[0] * M[4] - M[1] * M[3]) / det};
-    double al[NF];
-    for (int c = 0; c < NCASE; ++c) {
-        double sres[3];
-        for (int r = 0; r < 3; ++r) sres[r] = state[3 * c + r] + q[3 * c + r];
-        for (int r = 0; r < 3; ++r) al[3 * c + r] = inv[3 * r] * sres[0] + inv[3 * r + 1] * sres[1] + inv[3 * r + 2] * sres[2];
-        for (int r = 0; r < 3; ++r) {
-            state[NF + 3 * c + r] += al[3 * c + r];
-            state[3 * c + r] -= M[3 * r] * al[3 * c] + M[3 * r + 1] * al[3 * c + 1] + M[3 * r + 2] * al[3 * c + 2];
+    if (tid == 0) {
+        float Af[9];
+        g.block(ke, 13, Af);
+        for (int k = 0; k < 9; ++k) Ms[k] = (double)Af[k];
+    }
+    __syncthreads();
+    if (tid < NCASE) {
+        const int cc = tid;
+        const double *M = Ms;
+        // inverse of the 3x3 self block by cofactors
+        const double c00 = M[4] * M[8] - M[5] * M[7], c01 = M[5] * M[6] - M[3] * M[8], c02 = M[3] * M[7] - M[4] * M[6];
+        const double det = M[0] * c00 + M[1] * c01 + M[2] * c02;
+        if (cc == 0) ok = det > 0.0;
+        if (det > 0.0) {  // otherwise not positive definite: leave the iterate alone
+            const double inv[9] = {c00 / det, (M[2] * M[7] - M[1] * M[8]) / det, (M[1] * M[5] - M[2] * M[4]) / det,
+                                   c01 / det, (M[0] * M[8] - M[2] * M[6]) / det, (M[2] * M[3] - M[0] * M[5]) / det,
+                                   c02 / det, (M[1] * M[6] - M[0] * M[7]) / det, (M[0] * M[4] - M[1] * M[3]) / det};
+            double sres[3];
+            for (int rr = 0; rr < 3; ++rr) {
+                double q = 0;
+                for (int m = 0; m < 26; ++m) q += qpart[m][3 * cc + rr];
+                sres[rr] = state[3 * cc + rr] + q;
+            }
+            double a3[3];
+            for (int rr = 0; rr < 3; ++rr) a3[rr] = inv[3 * rr] * sres[0] + inv[3 * rr + 1] * sres[1] + inv[3 * rr + 2] * sres[2];
+            for (int rr = 0; rr < 3; ++rr) {
+                al[3 * cc + rr] = a3[rr];
+                state[NF + 3 * cc + rr] += a3[rr];
+                state[3 * cc + rr] -= M[3 * rr] * a3[0] + M[3 * rr + 1] * a3[1] + M[3 * rr + 2] * a3[2];
+            }
         }
     }
+    __syncthreads();
+    if (!ok || pinned) return;
     // f at the origin's neighbours: K_{v,p} alpha = A_{p,d}^T alpha
-    for (int d = 0; d < 27; ++d) {
-        if (d == 13) continue;
-        int Kn;
-        bool pinned;
-        const unsigned nid = g.nbr(a, d, Kn, pinned);
-        if (pinned) continue;
-        float A[9];
-        g.block(ke, d, A);
-        for (int c = 0; c < NCASE; ++c)
-            for (int r = 0; r < 3; ++r) {
-                const double t = (double)A[r] * al[3 * c] + (double)A[3 + r] * al[3 * c + 1] + (double)A[6 + r] * al[3 * c + 2];
-                float *fp = const_cast<float *>(a.f) + (3 * c + r) * a.nv + nid;
-                *fp = (float)((double)*fp + t);
-            }
-    }
+    const double t = (double)A[r] * al[3 * c] + (double)A[3 + r] * al[3 * c + 1] + (double)A[6 + r] * al[3 * c + 2];
+    float *fp = const_cast<float *>(a.f) + (3 * c + r) * a.nv + nid;
+    *fp = (float)((double)*fp + t);
 }
 
 // state: F = (plane sums of f) - f at the origin, T = 0
@@ -603,7 +608,7 @@ void launch_update64(const Level &L, double *u64, const float *e, const double *
     k_update64<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(L.P.nv, u64, e, T, L.P.base[7]);
 }
 void launch_pin_deflate(const Level &L, const float *rho, const KeMat &ke, double *state, cudaStream_t s) {
-    k_pin_deflate<<<1, 32, 0, s>>>(make_args(L, rho), ke, state);
+    k_pin_deflate<<<1, PIN_THREADS, 0, s>>>(make_args(L, rho), ke, state);
 }
 void launch_pin_init(const Level &L, const double *sums, double *state, cudaStream_t s) {
     k_pin_init<<<1, 32, 0, s>>>(sums, L.f, L.P.nv, L.P.base[7], state);

@@ -216,49 +216,75 @@ void launch_dirichlet_patch(const Level &F, const Level &C, const float *rho, co
 }
 
 // ---- deeper levels: R A P from the finer stencil -----------------------------------
+// the 9 entries of block J of fine vertex fv (compile-time J: fixed chunk slots)
+template <int J, bool F32>
+__device__ __forceinline__ void fine_block(const uint4 *__restrict__ st, long long nv, long long fv, float b[9]) {
+    using S = StencilStore<F32>;
+    constexpr int e0 = 9 * J, q0 = e0 / S::PER, q1 = (e0 + 8) / S::PER;
+    float v[3 * S::PER];
+#pragma unroll
+    for (int q = q0; q <= q1; ++q) S::unpack(__ldg(st + q * nv + fv), v + (q - q0) * S::PER);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) b[k] = v[e0 + k - S::PER * q0];
+}
+
+// One thread per (coarse vertex, coarse neighbour d = blockIdx.y): block d of the
+// coarse stencil is sum over fine i in the support of the vertex and fine j in
+// the support of neighbour d of w_i w_j A_ij.  The fine offsets are visited in
+// the order x, y, z (z fastest) and the fine neighbours j in ascending order.
 template <bool F32>
 __global__ void __launch_bounds__(128) k_galerkin(Planes F, Planes C, int r0, int r1, int r2,
                                                   const uint4 *__restrict__ fst, uint4 *cst) {
     const long long v = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (v >= C.nv) return;
+    const int d = blockIdx.y;
     const int k = color_of_index(C, v);
     int X[3];
     vpos(C, k, v - C.base[k], X[0], X[1], X[2]);
     const float pr = (float)(r0 * r1 * r2);
-    for (int d = 0; d < 27; d++) {
-        const int dj[3] = {r0 * (d % 3 - 1), r1 * (d / 3 % 3 - 1), r2 * (d / 9 - 1)};
-        float s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-        for (int fx = -r0; fx <= r0; fx++)
-            for (int fy = -r1; fy <= r1; fy++)
-                for (int fz = -r2; fz <= r2; fz++) {
-                    const int oi[3] = {fx + dj[0], fy + dj[1], fz + dj[2]};
-                    if (!(oi[0] > -r0 && oi[0] < r0 && oi[1] > -r1 && oi[1] < r1 && oi[2] > -r2 && oi[2] < r2)) continue;
-                    const long long fv = vidx(F, modp(X[0] * r0 + oi[0], F.n[0]), modp(X[1] * r1 + oi[1], F.n[1]),
-                                              modp(X[2] * r2 + oi[2], F.n[2]));
-                    const float wi = (float)((r0 - abs(oi[0])) * (r1 - abs(oi[1])) * (r2 - abs(oi[2]))) / pr;
-                    for (int j = 0; j < 27; j++) {
-                        const int o0 = abs(oi[0] + j % 3 - 1 - dj[0]), o1 = abs(oi[1] + j / 3 % 3 - 1 - dj[1]),
-                                  o2 = abs(oi[2] + j / 9 - 1 - dj[2]);
-                        if (o0 >= r0 || o1 >= r1 || o2 >= r2) continue;
-                        const float wj = (float)((r0 - o0) * (r1 - o1) * (r2 - o2)) / pr;
-                        const float ww = wi * wj;
+    const int dj0 = r0 * (d % 3 - 1), dj1 = r1 * (d / 3 % 3 - 1), dj2 = r2 * (d / 9 - 1);
+    float s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    // fine offsets oi from the coarse vertex with |oi| < r and |oi - dj| <= r
+    const int a0 = max(-r0 + 1, dj0 - r0), b0 = min(r0 - 1, dj0 + r0);
+    const int a1 = max(-r1 + 1, dj1 - r1), b1 = min(r1 - 1, dj1 + r1);
+    const int a2 = max(-r2 + 1, dj2 - r2), b2 = min(r2 - 1, dj2 + r2);
+    for (int o0 = a0; o0 <= b0; o0++)
+        for (int o1 = a1; o1 <= b1; o1++)
+            for (int o2 = a2; o2 <= b2; o2++) {
+                const long long fv = vidx(F, modp(X[0] * r0 + o0, F.n[0]), modp(X[1] * r1 + o1, F.n[1]),
+                                          modp(X[2] * r2 + o2, F.n[2]));
+                const float wi = (float)((r0 - abs(o0)) * (r1 - abs(o1)) * (r2 - abs(o2))) / pr;
 #pragma unroll
-                        for (int e = 0; e < 9; e++)
-                            s[e] = fmaf(ww, StencilStore<F32>::get(fst, F.nv, fv, 9 * j + e), s[e]);
+                for (int j = 0; j < 27; j++) {
+                    const int q0 = abs(o0 + j % 3 - 1 - dj0), q1 = abs(o1 + j / 3 % 3 - 1 - dj1),
+                              q2 = abs(o2 + j / 9 - 1 - dj2);
+                    if (q0 >= r0 || q1 >= r1 || q2 >= r2) continue;
+                    const float wj = (float)((r0 - q0) * (r1 - q1) * (r2 - q2)) / pr;
+                    const float ww = wi * wj;
+                    float bl[9];
+                    switch (j) {  // compile-time block index for the chunk arithmetic
+#define H3D_FB(J) case J: fine_block<J, F32>(fst, F.nv, fv, bl); break;
+                        H3D_FB(0) H3D_FB(1) H3D_FB(2) H3D_FB(3) H3D_FB(4) H3D_FB(5) H3D_FB(6) H3D_FB(7) H3D_FB(8)
+                        H3D_FB(9) H3D_FB(10) H3D_FB(11) H3D_FB(12) H3D_FB(13) H3D_FB(14) H3D_FB(15) H3D_FB(16)
+                        H3D_FB(17) H3D_FB(18) H3D_FB(19) H3D_FB(20) H3D_FB(21) H3D_FB(22) H3D_FB(23) H3D_FB(24)
+                        H3D_FB(25) H3D_FB(26)
+#undef H3D_FB
                     }
+#pragma unroll
+                    for (int e = 0; e < 9; e++) s[e] = fmaf(ww, bl[e], s[e]);
                 }
-        if (d == 13)
-            for (int t = 0; t < 3; t++)
-                if (fabsf(s[4 * t]) < 1e-4f) s[4 * t] = 1e-4f;
-        for (int e = 0; e < 9; e++) StencilStore<F32>::put(cst, C.nv, v, 9 * d + e, s[e]);
-    }
+            }
+    if (d == 13)
+        for (int t = 0; t < 3; t++)
+            if (fabsf(s[4 * t]) < 1e-4f) s[4 * t] = 1e-4f;
+    for (int e = 0; e < 9; e++) StencilStore<F32>::put(cst, C.nv, v, 9 * d + e, s[e]);
 }
 
 void launch_galerkin(const Level &F, const Level &C, cudaStream_t s) {
     const int bs = 128;
-    const unsigned nb = (unsigned)((C.P.nv + bs - 1) / bs);
-    if (C.st32) k_galerkin<true><<<nb, bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.st, C.st);
-    else k_galerkin<false><<<nb, bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.st, C.st);
+    const dim3 grid((unsigned)((C.P.nv + bs - 1) / bs), 27);
+    if (C.st32) k_galerkin<true><<<grid, bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.st, C.st);
+    else k_galerkin<false><<<grid, bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.st, C.st);
 }
 
 // ---- coarsest level ---------------------------------------------------------------
