@@ -281,16 +281,101 @@ __global__ void __launch_bounds__(256) k_prolong(Planes F, Planes C, int r0, int
     for (int q = 0; q < NF; ++q) uf[q * F.nv + v] += acc[q];
 }
 
+// Ratio 2 on every axis (even grids): one thread per coarse vertex in
+// lexicographic order, so that consecutive threads read consecutive fine vertices
+// of each colour plane.  Fine vertex 2X + o has the colour of o's parities and, in
+// that colour's plane, the coordinates X - [o < 0] (wrapped) per axis; the sums
+// run in the general kernel's order, so the results are identical.
+__global__ void __launch_bounds__(256) k_restrict2(Planes F, Planes C, FastDiv dn0, FastDiv dn1,
+                                                   const float *__restrict__ rf, float *fc) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= C.nv) return;
+    const int c = blockIdx.y;
+    const unsigned q = (unsigned)t, tq = dn0.div(q), zq = dn1.div(tq);
+    const int x = (int)(q - tq * (unsigned)C.n[0]), y = (int)(tq - zq * (unsigned)C.n[1]), z = (int)zq;
+    const int xm = x == 0 ? C.n[0] - 1 : x - 1, ym = y == 0 ? C.n[1] - 1 : y - 1, zm = z == 0 ? C.n[2] - 1 : z - 1;
+    const long long cpl = F.nv / 8;  // vertices per fine colour plane
+    const float *src = rf + (long long)(3 * c) * F.nv;
+    float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+    for (int ox = -1; ox <= 1; ox++)
+#pragma unroll
+        for (int oy = -1; oy <= 1; oy++)
+#pragma unroll
+            for (int oz = -1; oz <= 1; oz++) {
+                const float w = (float)((2 - abs(ox)) * (2 - abs(oy)) * (2 - abs(oz))) / 8.f;
+                const int k = ((ox + 1) & 1) | (((oy + 1) & 1) << 1) | (((oz + 1) & 1) << 2);
+                const long long fi = k * cpl + (ox < 0 ? xm : x) +
+                                     (long long)C.n[0] * ((oy < 0 ? ym : y) + (long long)C.n[1] * (oz < 0 ? zm : z));
+                a0 = fmaf(__ldg(&src[fi]), w, a0);
+                a1 = fmaf(__ldg(&src[F.nv + fi]), w, a1);
+                a2 = fmaf(__ldg(&src[2 * F.nv + fi]), w, a2);
+            }
+    float *dst = fc + (long long)(3 * c) * C.nv + vidx(C, x, y, z);
+    dst[0] = a0;
+    dst[C.nv] = a1;
+    dst[2 * C.nv] = a2;
+}
+
+// Ratio 2: one thread per coarse cell X; its eight fine vertices 2X + e take
+// their corrections from the cell's eight corners, read once per plane.  Fine
+// vertex 2X + e sits at index X (lexicographic) of colour plane k(e).
+__global__ void __launch_bounds__(256) k_prolong2(Planes F, Planes C, FastDiv dn0, FastDiv dn1, int is_root,
+                                                  const float *__restrict__ uc, float *uf) {
+    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t >= C.nv) return;
+    const unsigned q = (unsigned)t, tq = dn0.div(q), zq = dn1.div(tq);
+    const int x = (int)(q - tq * (unsigned)C.n[0]), y = (int)(tq - zq * (unsigned)C.n[1]), z = (int)zq;
+    const int xp = x + 1 == C.n[0] ? 0 : x + 1, yp = y + 1 == C.n[1] ? 0 : y + 1, zp = z + 1 == C.n[2] ? 0 : z + 1;
+    long long ci[8];
+#pragma unroll
+    for (int id = 0; id < 8; ++id)
+        ci[id] = vidx(C, (id & 1) ? xp : x, ((id >> 1) & 1) ? yp : y, (id >> 2) ? zp : z);
+    const long long cpl = F.nv / 8;
+    const bool root = is_root && t == 0;
+#pragma unroll 1
+    for (int pl = 0; pl < NF; ++pl) {
+        float cv[8];
+#pragma unroll
+        for (int id = 0; id < 8; ++id) cv[id] = __ldg(&uc[pl * C.nv + ci[id]]);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            if (e == 0 && root) continue;  // the pinned origin keeps its value
+            const int ex = e & 1, ey = (e >> 1) & 1, ez = e >> 2;
+            float acc = 0.f;
+#pragma unroll
+            for (int id = 0; id < 8; ++id) {
+                const int ox = id & 1, oy = (id >> 1) & 1, oz = id >> 2;
+                const float w = (float)((2 - abs(ox * 2 - ex)) * (2 - abs(oy * 2 - ey)) * (2 - abs(oz * 2 - ez))) / 8.f;
+                if (w == 0.f) continue;
+                acc = fmaf(cv[id], w, acc);
+            }
+            // fine vertex (2x + ex, ...): colour of (ex, ey, ez), plane index t
+            const int k = ((ex + 1) & 1) | (((ey + 1) & 1) << 1) | (((ez + 1) & 1) << 2);
+            uf[pl * F.nv + k * cpl + t] += acc;
+        }
+    }
+}
+
+static bool ratio2(const Level &C) { return C.ratio[0] == 2 && C.ratio[1] == 2 && C.ratio[2] == 2; }
+
 void launch_restrict(const Level &F, const Level &C, cudaStream_t s) {
     const int bs = 256;
     const dim3 grid((unsigned)((C.P.nv + bs - 1) / bs), NCASE);
-    k_restrict<<<grid, bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.r, C.f);
+    if (ratio2(C) && F.P.even)
+        k_restrict2<<<grid, bs, 0, s>>>(F.P, C.P, FastDiv((unsigned)C.P.n[0]), FastDiv((unsigned)C.P.n[1]), F.r, C.f);
+    else
+        k_restrict<<<grid, bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], F.r, C.f);
 }
 
 void launch_prolong(const Level &F, const Level &C, int is_root, cudaStream_t s) {
     const int bs = 256;
-    k_prolong<<<(unsigned)((F.P.nv + bs - 1) / bs), bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2],
-                                                                  is_root, C.u, F.u);
+    if (ratio2(C) && F.P.even)
+        k_prolong2<<<(unsigned)((C.P.nv + bs - 1) / bs), bs, 0, s>>>(F.P, C.P, FastDiv((unsigned)C.P.n[0]),
+                                                                     FastDiv((unsigned)C.P.n[1]), is_root, C.u, F.u);
+    else
+        k_prolong<<<(unsigned)((F.P.nv + bs - 1) / bs), bs, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2],
+                                                                      is_root, C.u, F.u);
 }
 
 // ---- norms and means ---------------------------------------------------------
