@@ -260,7 +260,7 @@ int enqueue_vcycle(h3d_handle *h, float w, bool deflate = false) {
             if (l - 1 == 0) launch_fine_residual(h->lv[0], h->rho, h->ke, h->partial, nblk_r, s);
             else launch_coarse_residual(h->lv[l - 1], s);
             launch_restrict(h->lv[l - 1], h->lv[l], s);
-            cudaMemsetAsync(h->lv[l].u, 0, sizeof(float) * NF * h->lv[l].P.nv, s);
+            cudaMemsetAsync(h->lv[l].u, 0, sizeof(float) * field_floats(h->lv[l].P.nv), s);
         }
         if (l == h->nl - 1) launch_coarse_apply(h->lv[l], h->aug, h->cfg.coarse_mode == H3D_COARSE_PROJECT, s);
         else if (l == 0) launch_fine_gs(h->lv[0], h->rho, h->ke, w, s);
@@ -294,9 +294,8 @@ void enqueue_pin_init(h3d_handle *h) {
 int enqueue_refine(h3d_handle *h, bool exact) {
     cudaStream_t s = h->stream;
     const Level &L0 = h->lv[0];
-    const long long n18 = (long long)NF * L0.P.nv;
     launch_update64(L0, h->u64, L0.u, h->pin_state + NF, s);
-    cudaMemsetAsync(L0.u, 0, sizeof(float) * n18, s);
+    cudaMemsetAsync(L0.u, 0, sizeof(float) * field_floats(L0.P.nv), s);
     launch_fine_residual64(L0, h->rho, h->ke, h->f0, h->u64, L0.f, exact, s);
     const int nb = norm_blocks(L0.P);
     launch_weighted_norm(L0.P, L0.f, h->partial, nb, s);
@@ -371,11 +370,12 @@ struct SolveRun {
 
     bool selected(int c) const { return ((mask >> c) & 1) != 0; }
     bool finished() const { return pending == P_DONE; }
-    long long n18() const { return (long long)NF * h->lv[0].P.nv; }
+    long long n18() const { return (long long)NF * h->lv[0].P.nv; }      // FP64 planar field
+    long long nf32() const { return field_floats(h->lv[0].P.nv); }     // FP32 blocked field
 
     int reset_solution() {
         if (refine) CK(cudaMemsetAsync(h->u64, 0, sizeof(double) * n18(), h->stream));
-        else CK(cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * n18(), h->stream));
+        else CK(cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * nf32(), h->stream));
         return H3D_OK;
     }
     int launch_refine(Pending next) {
@@ -441,7 +441,7 @@ struct SolveRun {
         CK(cudaEventRecord(h->ev0, h->stream));
         CK(cudaMemsetAsync(h->pin_state + NF, 0, sizeof(double) * NF, h->stream));  // no pending shift
         if (refine) {
-            CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * n18(), h->stream));
+            CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * nf32(), h->stream));
             return launch_refine(P_START_REFINE);
         }
         enqueue_pin_init(h);
@@ -489,7 +489,7 @@ struct SolveRun {
                 CK(cudaMemsetAsync(h->pin_state + NF, 0, sizeof(double) * NF, h->stream));
                 fallback_tried = true;
                 if (refine) {
-                    CK(cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * n18(), h->stream));
+                    CK(cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * nf32(), h->stream));
                     return launch_refine(P_START_REFINE);
                 }
                 enqueue_pin_init(h);
@@ -583,7 +583,7 @@ int elastic_prepare(h3d_handle *h) {
         launch_remove_mean64(L.P, h->u64, h->partial, nb, s);
     } else {
         launch_rhs(L, h->rho, h->rhs, L.f, s);
-        launch_convert(n18, h->chi, L.u, s);
+        launch_convert_field(L.P.nv, h->chi, L.u, s);
         launch_mean_partial(L.P, L.u, h->partial, nb, s);
         launch_remove_mean(L.P, L.u, h->partial, nb, s);
     }
@@ -598,7 +598,7 @@ int elastic_enqueue_energy(h3d_handle *h) {
     cudaStream_t s = h->stream;
     const long long n18 = (long long)NF * L.P.nv;
     if (h->refine()) CK(cudaMemcpyAsync(h->chi, h->u64, sizeof(double) * n18, cudaMemcpyDeviceToDevice, s));
-    else launch_convert(n18, L.u, h->chi, s);
+    else launch_convert_field(L.P.nv, L.u, h->chi, s);
     int nsm = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
     const int eb = energy_tc_blocks(L.P, nsm);
@@ -663,7 +663,7 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
         L.P = make_planes(dims[l]);
         for (int a = 0; a < 3; a++) L.ratio[a] = rat[l][a];
         if (l < nl - 1 && !L.P.even) return fail(h, H3D_ERR_ARG, "every smoothed level needs even dimensions");
-        const size_t bytes = sizeof(float) * NF * (size_t)L.P.nv;
+        const size_t bytes = sizeof(float) * (size_t)field_floats(L.P.nv);
         CK(cudaMalloc(&L.u, bytes));
         CK(cudaMalloc(&L.f, bytes));
         CK(cudaMalloc(&L.r, bytes));
@@ -684,8 +684,8 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
     if (h->refine()) {
         CK(cudaMalloc(&h->u64, sizeof(double) * NF * nv0));
         CK(cudaMemset(h->u64, 0, sizeof(double) * NF * nv0));
-        CK(cudaMalloc(&h->f0, sizeof(float) * NF * nv0));
-        CK(cudaMemset(h->f0, 0, sizeof(float) * NF * nv0));
+        CK(cudaMalloc(&h->f0, sizeof(float) * field_floats(nv0)));
+        CK(cudaMemset(h->f0, 0, sizeof(float) * field_floats(nv0)));
     }
     // element matrix and derived tables
     element_matrix(cfg->youngs_modulus, cfg->poisson_ratio, h->ked);
@@ -832,7 +832,7 @@ int h3d_enforce_unit_macro_strain(h3d_handle *h) {
     if (!h->have_density) return fail(h, H3D_ERR_STATE, "no density");
     launch_rhs(h->lv[0], h->rho, h->rhs, h->lv[0].f, h->stream);
     if (h->refine())
-        CK(cudaMemcpyAsync(h->f0, h->lv[0].f, sizeof(float) * NF * h->lv[0].P.nv, cudaMemcpyDeviceToDevice,
+        CK(cudaMemcpyAsync(h->f0, h->lv[0].f, sizeof(float) * field_floats(h->lv[0].P.nv), cudaMemcpyDeviceToDevice,
                            h->stream));
     CKL();
     return H3D_OK;
@@ -891,7 +891,7 @@ int h3d_reset_displacement(h3d_handle *h, int level) {
     if (!h) return H3D_ERR_ARG;
     for (int l = 0; l < h->nl; l++)
         if (level < 0 || level == l)
-            CK(cudaMemsetAsync(h->lv[l].u, 0, sizeof(float) * NF * h->lv[l].P.nv, h->stream));
+            CK(cudaMemsetAsync(h->lv[l].u, 0, sizeof(float) * field_floats(h->lv[l].P.nv), h->stream));
     return H3D_OK;
 }
 
@@ -901,8 +901,8 @@ int h3d_field_norms(h3d_handle *h, int field, double out[6]) {
     if (field == H3D_FIELD_CHI || field == H3D_FIELD_SOLUTION) {
         const double *src = field == H3D_FIELD_CHI ? h->chi : h->u64;
         if (!src) return fail(h, H3D_ERR_ARG, "no FP64 solution in this precision mode");
-        if (int e = ensure_tmp(h, (size_t)NF * L.P.nv)) return e;
-        launch_convert((long long)NF * L.P.nv, src, h->tmp, h->stream);
+        if (int e = ensure_tmp(h, (size_t)field_floats(L.P.nv))) return e;
+        launch_convert_field(L.P.nv, src, h->tmp, h->stream);
         return weighted_norms(h, L.P, h->tmp, out);
     }
     const float *v = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r : nullptr;
@@ -1143,12 +1143,12 @@ int h3d_get_field(h3d_handle *h, int level, int field, float *host) {
         CK(cudaStreamSynchronize(h->stream));
         return H3D_OK;
     }
-    const size_t n18 = (size_t)NF * L.P.nv;
+    const size_t n18 = (size_t)NF * L.P.nv, nf = (size_t)field_floats(L.P.nv);
     if (field == H3D_FIELD_CHI || field == H3D_FIELD_SOLUTION) {
         const double *src = level != 0 ? nullptr : field == H3D_FIELD_CHI ? h->chi : h->u64;
         if (!src) return fail(h, H3D_ERR_ARG, "no such FP64 field on this level / precision mode");
-        if (int e = ensure_tmp(h, 2 * n18)) return e;
-        launch_convert((long long)n18, src, h->tmp + n18, h->stream);
+        if (int e = ensure_tmp(h, n18 + nf)) return e;
+        launch_convert_field(L.P.nv, src, h->tmp + n18, h->stream);
         launch_field_to_lex(L.P, h->tmp + n18, h->tmp, h->stream);
     } else {
         const float *src = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r : nullptr;
@@ -1176,14 +1176,14 @@ int h3d_set_field(h3d_handle *h, int level, int field, const float *host) {
         CK(cudaStreamSynchronize(h->stream));
         return H3D_OK;
     }
-    const size_t n18 = (size_t)NF * L.P.nv;
+    const size_t n18 = (size_t)NF * L.P.nv, nf = (size_t)field_floats(L.P.nv);
     if (field == H3D_FIELD_CHI || field == H3D_FIELD_SOLUTION) {
         double *dst = level != 0 ? nullptr : field == H3D_FIELD_CHI ? h->chi : h->u64;
         if (!dst) return fail(h, H3D_ERR_ARG, "no such FP64 field on this level / precision mode");
-        if (int e = ensure_tmp(h, 2 * n18)) return e;
+        if (int e = ensure_tmp(h, n18 + nf)) return e;
         CK(cudaMemcpyAsync(h->tmp, host, sizeof(float) * n18, cudaMemcpyHostToDevice, h->stream));
         launch_field_from_lex(L.P, h->tmp, h->tmp + n18, h->stream);
-        launch_convert((long long)n18, h->tmp + n18, dst, h->stream);
+        launch_convert_field(L.P.nv, h->tmp + n18, dst, h->stream);
     } else {
         float *dst = field == H3D_FIELD_U ? L.u : field == H3D_FIELD_F ? L.f : field == H3D_FIELD_R ? L.r : nullptr;
         if (!dst) return fail(h, H3D_ERR_ARG, "unknown field");
@@ -1192,7 +1192,7 @@ int h3d_set_field(h3d_handle *h, int level, int field, const float *host) {
         launch_field_from_lex(L.P, h->tmp, dst, h->stream);
         // in the refined mode the solve reads its right-hand side from f0
         if (field == H3D_FIELD_F && level == 0 && h->refine())
-            CK(cudaMemcpyAsync(h->f0, dst, sizeof(float) * n18, cudaMemcpyDeviceToDevice, h->stream));
+            CK(cudaMemcpyAsync(h->f0, dst, sizeof(float) * nf, cudaMemcpyDeviceToDevice, h->stream));
     }
     CKL();
     CK(cudaStreamSynchronize(h->stream));

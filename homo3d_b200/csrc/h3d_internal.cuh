@@ -26,6 +26,19 @@ constexpr int NCHUNK = 31;      // uint4 chunks per stencil (243 halves -> 248)
 constexpr int NCHUNK32 = 61;    // the same with FP32 entries (243 floats -> 244)
 constexpr float RHO_PENAL_MIN = 1e-9f;  // grid.h:425
 
+// FP32 vertex fields (u, f, r of every level): the 18 planes interleaved in
+// blocks of FVB vertices, value(plane q, vertex v) at fidx(q, v); the planes a
+// thread reads for one vertex are then immediate offsets from one address.  A
+// field holds field_floats(nv) floats (nv rounded up to a multiple of FVB).  The
+// FP64 fields (the refined solution, the stored solutions chi) stay planar:
+// value(q, v) at q * nv + v.
+constexpr int FVB = 128;
+static_assert(FVB == 128, "fidx shifts by log2(FVB) = 7");
+__host__ __device__ inline long long fidx(int q, long long v) {
+    return ((v >> 7) * NF + q) * FVB + (v & (FVB - 1));
+}
+__host__ __device__ inline long long field_floats(long long nv) { return ((nv + FVB - 1) / FVB) * FVB * NF; }
+
 struct Planes {
     int n[3];        // vertices (= cells) per axis
     int pn[8][3];    // plane dims of each colour
@@ -194,8 +207,9 @@ void launch_pin_deflate(const Level &L, const float *rho, const KeMat &ke, doubl
 void launch_pin_init(const Level &L, const double *sums, double *state, cudaStream_t s);
 // FP32 solutions: u += T (but the origin), f restored near the origin, T = 0
 void launch_pin_fold(const Level &L, const float *rho, const KeMat &ke, double *state, cudaStream_t s);
-void launch_convert(long long n, const float *src, double *dst, cudaStream_t s);
-void launch_convert(long long n, const double *src, float *dst, cudaStream_t s);
+// FP32 blocked field of nv vertices <-> FP64 planar field
+void launch_convert_field(long long nv, const float *src, double *dst, cudaStream_t s);
+void launch_convert_field(long long nv, const double *src, float *dst, cudaStream_t s);
 void launch_remove_mean64(const Planes &P, double *v, double *partial, int nblk, cudaStream_t s);
 // coarse levels and transfers (k_coarse.cu)
 void launch_coarse_gs(const Level &L, float w, cudaStream_t s);

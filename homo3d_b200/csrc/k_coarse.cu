@@ -96,10 +96,10 @@ __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, 
         }
         const int Kn = K ^ ((dx & 1) | ((dy & 1) << 1) | ((dz & 1) << 2));
         const unsigned nid = (unsigned)Kn * (unsigned)a.P + X[dx + 1] + Y[dy + 1] + Z[dz + 1];
-        const float *up = a.u + nid + (long long)(3 * cb) * a.nv;
+        const float *up = a.u + fidx(3 * cb, nid);  // planes 3cb.. of the neighbour, FVB apart
 #pragma unroll
         for (int c = 0; c < CPTC; ++c) {
-            const float u0 = up[(3 * c) * a.nv], u1 = up[(3 * c + 1) * a.nv], u2 = up[(3 * c + 2) * a.nv];
+            const float u0 = up[(3 * c) * FVB], u1 = up[(3 * c + 1) * FVB], u2 = up[(3 * c + 2) * FVB];
             acc[3 * c + 0] = fmaf(s[0], u0, fmaf(s[1], u1, fmaf(s[2], u2, acc[3 * c + 0])));
             acc[3 * c + 1] = fmaf(s[3], u0, fmaf(s[4], u1, fmaf(s[5], u2, acc[3 * c + 1])));
             acc[3 * c + 2] = fmaf(s[6], u0, fmaf(s[7], u1, fmaf(s[8], u2, acc[3 * c + 2])));
@@ -129,15 +129,15 @@ __global__ void __launch_bounds__(128) k_coarse_gs(CoarseArgs a) {
     const float w = a.w;
 #pragma unroll
     for (int c = 0; c < CPTC; ++c) {
-        float *u = a.u + me + (3 * (cb + c)) * a.nv;
-        const float *f = a.f + me + (3 * (cb + c)) * a.nv;
-        float u0 = u[0], u1 = u[a.nv], u2 = u[2 * a.nv];
+        float *u = a.u + fidx(3 * (cb + c), me);
+        const float *f = a.f + fidx(3 * (cb + c), me);
+        float u0 = u[0], u1 = u[FVB], u2 = u[2 * FVB];
         u0 = w * (f[0] - acc[3 * c] - ks[1] * u1 - ks[2] * u2) / ks[0] + (1.f - w) * u0;
-        u1 = w * (f[a.nv] - acc[3 * c + 1] - ks[3] * u0 - ks[5] * u2) / ks[4] + (1.f - w) * u1;
-        u2 = w * (f[2 * a.nv] - acc[3 * c + 2] - ks[6] * u0 - ks[7] * u1) / ks[8] + (1.f - w) * u2;
+        u1 = w * (f[FVB] - acc[3 * c + 1] - ks[3] * u0 - ks[5] * u2) / ks[4] + (1.f - w) * u1;
+        u2 = w * (f[2 * FVB] - acc[3 * c + 2] - ks[6] * u0 - ks[7] * u1) / ks[8] + (1.f - w) * u2;
         u[0] = u0;
-        u[a.nv] = u1;
-        u[2 * a.nv] = u2;
+        u[FVB] = u1;
+        u[2 * FVB] = u2;
     }
 }
 
@@ -150,7 +150,7 @@ __device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long
     coarse_apply<K, true, F32>(a, me, i, j, l, cb, acc);
 #pragma unroll
     for (int q = 0; q < 3 * CPTC; ++q) {
-        const long long o = (3 * cb + q) * a.nv + me;
+        const long long o = fidx(3 * cb + q, me);
         a.r[o] = a.f[o] - acc[q];
     }
 }
@@ -232,7 +232,6 @@ __global__ void __launch_bounds__(256) k_restrict(Planes F, Planes C, int r0, in
     int x, y, z;
     vpos(C, k, v - C.base[k], x, y, z);
     const float pr = (float)(r0 * r1 * r2);
-    const float *src = rf + (long long)(3 * c) * F.nv;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
     for (int ox = -r0 + 1; ox < r0; ox++) {
         const int fx = wrap(r0 * x + ox, F.n[0]);
@@ -241,17 +240,17 @@ __global__ void __launch_bounds__(256) k_restrict(Planes F, Planes C, int r0, in
             for (int oz = -r2 + 1; oz < r2; oz++) {
                 const int fz = wrap(r2 * z + oz, F.n[2]);
                 const float w = (float)((r0 - abs(ox)) * (r1 - abs(oy)) * (r2 - abs(oz))) / pr;
-                const long long fi = vidx(F, fx, fy, fz);
-                a0 = fmaf(__ldg(&src[fi]), w, a0);
-                a1 = fmaf(__ldg(&src[F.nv + fi]), w, a1);
-                a2 = fmaf(__ldg(&src[2 * F.nv + fi]), w, a2);
+                const float *src = rf + fidx(3 * c, vidx(F, fx, fy, fz));
+                a0 = fmaf(__ldg(&src[0]), w, a0);
+                a1 = fmaf(__ldg(&src[FVB]), w, a1);
+                a2 = fmaf(__ldg(&src[2 * FVB]), w, a2);
             }
         }
     }
-    float *dst = fc + (long long)(3 * c) * C.nv + v;
+    float *dst = fc + fidx(3 * c, v);
     dst[0] = a0;
-    dst[C.nv] = a1;
-    dst[2 * C.nv] = a2;
+    dst[FVB] = a1;
+    dst[2 * FVB] = a2;
 }
 
 __global__ void __launch_bounds__(256) k_prolong(Planes F, Planes C, int r0, int r1, int r2, int is_root,
@@ -275,10 +274,10 @@ __global__ void __launch_bounds__(256) k_prolong(Planes F, Planes C, int r0, int
         if (w == 0.f) continue;
         const long long ci = vidx(C, wrap(bx + ox, C.n[0]), wrap(by + oy, C.n[1]), wrap(bz + oz, C.n[2]));
 #pragma unroll
-        for (int q = 0; q < NF; ++q) acc[q] = fmaf(__ldg(&uc[q * C.nv + ci]), w, acc[q]);
+        for (int q = 0; q < NF; ++q) acc[q] = fmaf(__ldg(&uc[fidx(q, ci)]), w, acc[q]);
     }
 #pragma unroll
-    for (int q = 0; q < NF; ++q) uf[q * F.nv + v] += acc[q];
+    for (int q = 0; q < NF; ++q) uf[fidx(q, v)] += acc[q];
 }
 
 // Ratio 2 on every axis (even grids): one thread per coarse vertex in
@@ -295,7 +294,6 @@ __global__ void __launch_bounds__(256) k_restrict2(Planes F, Planes C, FastDiv d
     const int x = (int)(q - tq * (unsigned)C.n[0]), y = (int)(tq - zq * (unsigned)C.n[1]), z = (int)zq;
     const int xm = x == 0 ? C.n[0] - 1 : x - 1, ym = y == 0 ? C.n[1] - 1 : y - 1, zm = z == 0 ? C.n[2] - 1 : z - 1;
     const long long cpl = F.nv / 8;  // vertices per fine colour plane
-    const float *src = rf + (long long)(3 * c) * F.nv;
     float a0 = 0.f, a1 = 0.f, a2 = 0.f;
 #pragma unroll
     for (int ox = -1; ox <= 1; ox++)
@@ -307,14 +305,15 @@ __global__ void __launch_bounds__(256) k_restrict2(Planes F, Planes C, FastDiv d
                 const int k = ((ox + 1) & 1) | (((oy + 1) & 1) << 1) | (((oz + 1) & 1) << 2);
                 const long long fi = k * cpl + (ox < 0 ? xm : x) +
                                      (long long)C.n[0] * ((oy < 0 ? ym : y) + (long long)C.n[1] * (oz < 0 ? zm : z));
-                a0 = fmaf(__ldg(&src[fi]), w, a0);
-                a1 = fmaf(__ldg(&src[F.nv + fi]), w, a1);
-                a2 = fmaf(__ldg(&src[2 * F.nv + fi]), w, a2);
+                const float *src = rf + fidx(3 * c, fi);
+                a0 = fmaf(__ldg(&src[0]), w, a0);
+                a1 = fmaf(__ldg(&src[FVB]), w, a1);
+                a2 = fmaf(__ldg(&src[2 * FVB]), w, a2);
             }
-    float *dst = fc + (long long)(3 * c) * C.nv + vidx(C, x, y, z);
+    float *dst = fc + fidx(3 * c, vidx(C, x, y, z));
     dst[0] = a0;
-    dst[C.nv] = a1;
-    dst[2 * C.nv] = a2;
+    dst[FVB] = a1;
+    dst[2 * FVB] = a2;
 }
 
 // Ratio 2: one thread per coarse cell X; its eight fine vertices 2X + e take
@@ -337,7 +336,7 @@ __global__ void __launch_bounds__(256) k_prolong2(Planes F, Planes C, FastDiv dn
     for (int pl = 0; pl < NF; ++pl) {
         float cv[8];
 #pragma unroll
-        for (int id = 0; id < 8; ++id) cv[id] = __ldg(&uc[pl * C.nv + ci[id]]);
+        for (int id = 0; id < 8; ++id) cv[id] = __ldg(&uc[fidx(pl, ci[id])]);
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
             if (e == 0 && root) continue;  // the pinned origin keeps its value
@@ -352,7 +351,7 @@ __global__ void __launch_bounds__(256) k_prolong2(Planes F, Planes C, FastDiv dn
             }
             // fine vertex (2x + ex, ...): colour of (ex, ey, ez), plane index t
             const int k = ((ex + 1) & 1) | (((ey + 1) & 1) << 1) | (((ez + 1) & 1) << 2);
-            uf[pl * F.nv + k * cpl + t] += acc;
+            uf[fidx(pl, k * cpl + t)] += acc;
         }
     }
 }
@@ -398,7 +397,7 @@ __global__ void __launch_bounds__(NORM_BS) k_weighted_norm(Planes P, const float
             double a = 0;
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
-                const double t = v[(3 * c + q) * P.nv + i];
+                const double t = v[fidx(3 * c + q, i)];
                 a += t * t;
             }
             s[c] += m * a;
@@ -455,7 +454,7 @@ __global__ void __launch_bounds__(NORM_BS) k_sum18(Planes P, const float *__rest
     for (int q = 0; q < NF; ++q) s[q] = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < P.nv; i += (long long)gridDim.x * blockDim.x)
 #pragma unroll
-        for (int q = 0; q < NF; ++q) s[q] += v[q * P.nv + i];
+        for (int q = 0; q < NF; ++q) s[q] += v[fidx(q, i)];
     block_reduce<NF>(s, partial, blockIdx.x);
 }
 
@@ -464,7 +463,7 @@ __global__ void __launch_bounds__(256) k_sub_mean(Planes P, float *v, const doub
     if (i >= P.nv) return;
     const double inv = 1.0 / (double)P.nv;
 #pragma unroll
-    for (int q = 0; q < NF; ++q) v[q * P.nv + i] -= (float)(sum18[q] * inv);
+    for (int q = 0; q < NF; ++q) v[fidx(q, i)] -= (float)(sum18[q] * inv);
 }
 
 void launch_mean_partial(const Planes &P, const float *v, double *partial, int nblk, cudaStream_t s) {
@@ -483,7 +482,7 @@ void launch_remove_mean(const Planes &P, float *v, const double *partial, int nb
     k_sub_mean<<<(unsigned)((P.nv + 255) / 256), 256, 0, s>>>(P, v, tot);
 }
 
-// ---- layout conversion: lexicographic [6][nv][3] <-> colour planes [18][nv] ----
+// ---- layout conversion: lexicographic [6][nv][3] <-> the blocked colour-ordered field ----
 __global__ void k_field_lex(Planes P, const float *__restrict__ src, float *dst, int to_lex) {
     const long long lex = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (lex >= P.nv) return;
@@ -495,7 +494,7 @@ __global__ void k_field_lex(Planes P, const float *__restrict__ src, float *dst,
     for (int c = 0; c < NCASE; ++c)
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-            const long long li = ((long long)c * P.nv + lex) * 3 + m, pi = (3 * c + m) * P.nv + v;
+            const long long li = ((long long)c * P.nv + lex) * 3 + m, pi = fidx(3 * c + m, v);
             if (to_lex) dst[li] = src[pi];
             else dst[pi] = src[li];
         }

@@ -172,12 +172,12 @@ __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, c
         const unsigned nid = g.nbr(a, d, Kn, pinned);
         float A[9];
         g.block(ke, d, A);
-        const float *up = a.u + nid + (long long)(3 * cb) * a.nv;
+        const float *up = a.u + fidx(3 * cb, nid);  // planes 3cb.. of the neighbour, FVB apart
         float2 dd[3];
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
             const float2 un = pinned ? make_float2(0.f, 0.f)
-                                     : make_float2(__ldg(up + m * a.nv), __ldg(up + (3 + m) * a.nv));
+                                     : make_float2(__ldg(up + m * FVB), __ldg(up + (3 + m) * FVB));
             dd[m] = __fadd2_rn(un, nuv2[m]);
         }
 #pragma unroll
@@ -209,13 +209,13 @@ __global__ void __launch_bounds__(FBS, 5) k_fine_gs(FineArgs a, const __grid_con
     const long long me = (long long)K * a.P + p;
     if (K == 7 && p == 0) {  // the pinned origin (grid.cu:445-447, 545)
 #pragma unroll
-        for (int q = 0; q < 3 * CPT; ++q) a.u[(3 * cb + q) * a.nv + me] = 0.f;
+        for (int q = 0; q < 3 * CPT; ++q) a.u[fidx(3 * cb + q, me)] = 0.f;
         return;
     }
     const VertexGeo<K> g(a, p);
     float uv[3 * CPT];
 #pragma unroll
-    for (int q = 0; q < 3 * CPT; ++q) uv[q] = a.u[(3 * cb + q) * a.nv + me];
+    for (int q = 0; q < 3 * CPT; ++q) uv[q] = a.u[fidx(3 * cb + q, me)];
     float acc[3 * CPT];
     fine_apply<K>(a, ke, g, cb, uv, acc);
     float ks[9];
@@ -226,14 +226,14 @@ __global__ void __launch_bounds__(FBS, 5) k_fine_gs(FineArgs a, const __grid_con
     // update of u by the residual r = f - K u
 #pragma unroll
     for (int c = 0; c < CPT; ++c) {
-        const long long o = me + (long long)(3 * (cb + c)) * a.nv;
-        const float r0 = a.f[o] - acc[3 * c], r1 = a.f[o + a.nv] - acc[3 * c + 1], r2 = a.f[o + 2 * a.nv] - acc[3 * c + 2];
+        const long long o = fidx(3 * (cb + c), me);
+        const float r0 = a.f[o] - acc[3 * c], r1 = a.f[o + FVB] - acc[3 * c + 1], r2 = a.f[o + 2 * FVB] - acc[3 * c + 2];
         const float d0 = w * r0 / ks[0];
         const float d1 = w * (r1 - ks[3] * d0) / ks[4];
         const float d2 = w * (r2 - ks[6] * d0 - ks[7] * d1) / ks[8];
         a.u[o] = uv[3 * c] + d0;
-        a.u[o + a.nv] = uv[3 * c + 1] + d1;
-        a.u[o + 2 * a.nv] = uv[3 * c + 2] + d2;
+        a.u[o + FVB] = uv[3 * c + 1] + d1;
+        a.u[o + 2 * FVB] = uv[3 * c + 2] + d2;
     }
 }
 
@@ -243,13 +243,13 @@ __device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const Ke
     const long long me = (long long)K * a.P + p;
     if (K == 7 && p == 0) {
 #pragma unroll
-        for (int q = 0; q < 3 * CPT; ++q) a.r[(3 * cb + q) * a.nv + me] = 0.f;
+        for (int q = 0; q < 3 * CPT; ++q) a.r[fidx(3 * cb + q, me)] = 0.f;
         return;
     }
     const VertexGeo<K> g(a, p);
     float uv[3 * CPT];
 #pragma unroll
-    for (int q = 0; q < 3 * CPT; ++q) uv[q] = __ldg(a.u + (3 * cb + q) * a.nv + me);
+    for (int q = 0; q < 3 * CPT; ++q) uv[q] = __ldg(a.u + fidx(3 * cb + q, me));
     float acc[3 * CPT];
     fine_apply<K>(a, ke, g, cb, uv, acc);
     constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
@@ -262,7 +262,7 @@ __device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const Ke
         double s2 = 0;
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-            const long long o = (long long)(3 * (cb + c) + m) * a.nv + me;
+            const long long o = fidx(3 * (cb + c) + m, me);
             const float rv = a.f[o] - acc[3 * c + m];
             a.r[o] = rv;
             s2 += (double)rv * rv;
@@ -315,7 +315,7 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
     const long long me = (long long)K * a.P + p;
     if (K == 7 && p == 0) {
 #pragma unroll
-        for (int q = 0; q < 3 * CPT; ++q) a.r[(3 * cb + q) * a.nv + me] = 0.f;
+        for (int q = 0; q < 3 * CPT; ++q) a.r[fidx(3 * cb + q, me)] = 0.f;
         return;
     }
     const VertexGeo<K> g(a, p);
@@ -348,7 +348,7 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
     }
 #pragma unroll
     for (int q = 0; q < 3 * CPT; ++q) {
-        const long long o = (long long)(3 * cb + q) * a.nv + me;
+        const long long o = fidx(3 * cb + q, me);
         a.r[o] = (float)((Acc)a.f[o] - acc[q]);
     }
 }
@@ -396,7 +396,7 @@ __global__ void __launch_bounds__(256) k_rhs(Planes P, const float *__restrict__
             for (int m = 0; m < 3; ++m) acc[3 * c + m] = fmaf(rp, g.g[c][3 * an + m], acc[3 * c + m]);
     }
 #pragma unroll
-    for (int q = 0; q < NF; ++q) f[q * P.nv + v] = acc[q];
+    for (int q = 0; q < NF; ++q) f[fidx(q, v)] = acc[q];
 }
 
 static FineArgs make_args(const Level &L, const float *rho) {
@@ -468,9 +468,9 @@ __global__ void k_update64(long long nv, double *u, const float *__restrict__ e,
                            long long pin) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
     if (i >= nv * NF) return;
-    const long long v = i % nv;
+    const long long v = i % nv, q = i / nv;
     if (v == pin) return;
-    u[i] += (double)e[i] + T[i / nv];
+    u[i] += (double)e[fidx((int)q, v)] + T[q];
 }
 
 // ---- rigid-translation deflation of the pinned problem -------------------------
@@ -509,7 +509,7 @@ __global__ void __launch_bounds__(PIN_THREADS) k_pin_deflate(FineArgs a, const _
     {
         double t = 0;
         if (!pinned)
-            for (int k = 0; k < 3; ++k) t += (double)A[3 * r + k] * (double)a.u[(3 * c + k) * a.nv + nid];
+            for (int k = 0; k < 3; ++k) t += (double)A[3 * r + k] * (double)a.u[fidx(3 * c + k, nid)];
         qpart[n][cr] = t;
     }
     if (tid == 0) {
@@ -548,7 +548,7 @@ __global__ void __launch_bounds__(PIN_THREADS) k_pin_deflate(FineArgs a, const _
     if (!ok || pinned) return;
     // f at the origin's neighbours: K_{v,p} alpha = A_{p,d}^T alpha
     const double t = (double)A[r] * al[3 * c] + (double)A[3 + r] * al[3 * c + 1] + (double)A[6 + r] * al[3 * c + 2];
-    float *fp = const_cast<float *>(a.f) + (3 * c + r) * a.nv + nid;
+    float *fp = const_cast<float *>(a.f) + fidx(3 * c + r, nid);
     *fp = (float)((double)*fp + t);
 }
 
@@ -557,7 +557,7 @@ __global__ void k_pin_init(const double *__restrict__ sums, const float *__restr
                            double *state) {
     const int i = threadIdx.x;
     if (i >= NF) return;
-    state[i] = sums[i] - (double)f[(long long)i * nv + pin];
+    state[i] = sums[i] - (double)f[fidx(i, pin)];
     state[NF + i] = 0.0;
 }
 
@@ -565,8 +565,8 @@ __global__ void k_pin_init(const double *__restrict__ sums, const float *__restr
 __global__ void k_pin_fold_u(long long nv, float *u, const double *__restrict__ state, long long pin) {
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv * NF;
          i += (long long)gridDim.x * blockDim.x) {
-        const long long v = i % nv;
-        if (v != pin) u[i] = (float)((double)u[i] + state[NF + i / nv]);
+        const long long v = i % nv, q = i / nv;
+        if (v != pin) u[fidx((int)q, v)] = (float)((double)u[fidx((int)q, v)] + state[NF + q]);
     }
 }
 
@@ -586,21 +586,22 @@ __global__ void k_pin_restore_f(FineArgs a, const __grid_constant__ KeMat ke, do
             for (int r = 0; r < 3; ++r) {
                 const double *T = state + NF + 3 * c;
                 const double t = (double)A[r] * T[0] + (double)A[3 + r] * T[1] + (double)A[6 + r] * T[2];
-                float *fp = const_cast<float *>(a.f) + (3 * c + r) * a.nv + nid;
+                float *fp = const_cast<float *>(a.f) + fidx(3 * c + r, nid);
                 *fp = (float)((double)*fp - t);
             }
     }
     for (int i = 0; i < NF; ++i) state[NF + i] = 0.0;
 }
 
-__global__ void k_f32_to_f64(long long n, const float *__restrict__ s, double *d) {
+// FP32 blocked field <-> FP64 planar field (q * nv + v)
+__global__ void k_f32_to_f64(long long nv, const float *__restrict__ s, double *d) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n) d[i] = (double)s[i];
+    if (i < nv * NF) d[i] = (double)s[fidx((int)(i / nv), i % nv)];
 }
 
-__global__ void k_f64_to_f32(long long n, const double *__restrict__ s, float *d) {
+__global__ void k_f64_to_f32(long long nv, const double *__restrict__ s, float *d) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < n) d[i] = (float)s[i];
+    if (i < nv * NF) d[fidx((int)(i / nv), i % nv)] = (float)s[i];
 }
 
 void launch_update64(const Level &L, double *u64, const float *e, const double *T, cudaStream_t s) {
@@ -617,11 +618,11 @@ void launch_pin_fold(const Level &L, const float *rho, const KeMat &ke, double *
     k_pin_fold_u<<<1184, 256, 0, s>>>(L.P.nv, L.u, state, L.P.base[7]);
     k_pin_restore_f<<<1, 32, 0, s>>>(make_args(L, rho), ke, state);
 }
-void launch_convert(long long n, const float *src, double *dst, cudaStream_t s) {
-    k_f32_to_f64<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, src, dst);
+void launch_convert_field(long long nv, const float *src, double *dst, cudaStream_t s) {
+    k_f32_to_f64<<<(unsigned)((nv * NF + 255) / 256), 256, 0, s>>>(nv, src, dst);
 }
-void launch_convert(long long n, const double *src, float *dst, cudaStream_t s) {
-    k_f64_to_f32<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(n, src, dst);
+void launch_convert_field(long long nv, const double *src, float *dst, cudaStream_t s) {
+    k_f64_to_f32<<<(unsigned)((nv * NF + 255) / 256), 256, 0, s>>>(nv, src, dst);
 }
 
 // mean of each of the 18 planes over unique vertices, removed in place (FP64)

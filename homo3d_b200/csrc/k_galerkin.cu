@@ -429,7 +429,7 @@ __global__ void __launch_bounds__(256) k_coarse_apply(Planes C, const double *__
         const long long lex = i / 3;
         const int comp = i % 3;
         const int x = (int)(lex % C.n[0]), y = (int)((lex / C.n[0]) % C.n[1]), z = (int)(lex / ((long long)C.n[0] * C.n[1]));
-        b[i] = f[(3 * c + comp) * C.nv + vidx(C, x, y, z)];
+        b[i] = f[fidx(3 * c + comp, vidx(C, x, y, z))];
     }
     __syncthreads();
     if (threadIdx.x < 3) {
@@ -448,7 +448,7 @@ __global__ void __launch_bounds__(256) k_coarse_apply(Planes C, const double *__
         const long long lex = i / 3;
         const int comp = i % 3;
         const int x = (int)(lex % C.n[0]), y = (int)((lex / C.n[0]) % C.n[1]), z = (int)(lex / ((long long)C.n[0] * C.n[1]));
-        u[(3 * c + comp) * C.nv + vidx(C, x, y, z)] = (float)s;
+        u[fidx(3 * c + comp, vidx(C, x, y, z))] = (float)s;
     }
 }
 

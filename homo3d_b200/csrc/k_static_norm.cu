@@ -46,7 +46,7 @@ __global__ void __launch_bounds__(STATIC_NORM_BS) k_weighted_norm_static(Planes 
             double a = 0;
 #pragma unroll
             for (int q = 0; q < 3; ++q) {
-                const double t = v[(3 * c + q) * P.nv + i];
+                const double t = v[fidx(3 * c + q, i)];
                 a += t * t;
             }
             s[c] += m * a;
