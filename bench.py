@@ -119,18 +119,24 @@ PRECISION_NAME = {0: "FP32 V-cycles on the correction of an FP64 solution (itera
                   1: "FP32 solution (the reference's scheme)"}
 
 
-def launches_per_step(nl, vcycles, reso, refine, refinements):
+def launches_per_step(nl, vcycles, reso, refine, refinements, coarsest_nv):
     """kernel launches of this library in one step, counted from the code paths
-    (checked against an ncu launch list of the same step)"""
+    (equal to the ncu launch list of the 256^3 step: 1834)"""
     nblk = -(-(reso ** 3 // 8) // 128) * 3 * 8                  # fine residual norm partials
-    finish = 2 if nblk > 4096 else 1
-    fine = 8 + 1 + 8 + finish                                   # GS, residual, GS, norm
+    finish = 2 if nblk > 4096 else 1                            # one- or two-stage norm reduction
+    fine = 8 + 8 + finish + 8                                   # GS, residual (per colour), norms, GS
     coarse = (nl - 2) * (8 + 8 + 8)                             # GS, residual, GS per colour
-    per_cycle = fine + coarse + 2 * (nl - 1) + 1                # restrict, prolong, coarsest apply
-    per_refine = 4                                              # u64 += u, residual64, norm, finish
-    setup = 1 + 1 + 1 + (nl - 2) + 1 + 1                        # density, level 1, pin patch, deeper, assemble, inverse
-    pre, post = (4, 2) if refine else (5, 3)                   # rhs + mean removal (+ convert); (convert +) C
-    return setup + pre + 2 + vcycles * per_cycle + refinements * per_refine + post
+    per_cycle = fine + coarse + 2 * (nl - 1) + 1 + 1            # restrict, prolong, coarsest apply, deflation
+    per_refine = 1 + 1 + 2 + 3                                  # u64 += u, residual64, norms, deflation restart
+    setup = 1 + 1 + 1 + (nl - 2) + 1 + 1 + 3 * coarsest_nv      # density, level 1, pin patch, deeper, assemble,
+    #                                                             first pivot, one launch per pivot column
+    if refine:
+        pre = 1 + 3 + 3 + 2                                     # rhs, warm-start mean, balance, norms of f
+        post = 2                                                # C: energies, reduction
+    else:
+        pre = 1 + 1 + 3 + 3 + 2 + 3                             # rhs, convert, warm-start mean, balance, norms, deflation start
+        post = 1 + 1 + 2                                        # pending shift into u, convert, C
+    return setup + pre + vcycles * per_cycle + refinements * per_refine + post
 
 
 def make_density(args, rank):
@@ -150,6 +156,7 @@ def gpu_arm(args):
     dev = torch.cuda.current_device()
     rho_h = make_density(args, rank)
     hd = H.Homogenization(args.reso, pin_mode=args.pin_mode, precision=args.precision)
+    coarsest_nv = int(np.prod(hd.dims[-1]))
     stream = torch.cuda.ExternalStream(hd.stream)
     rho_d = torch.tensor(rho_h, device="cuda")
     rho_pin = torch.from_numpy(rho_h).pin_memory()
@@ -251,7 +258,7 @@ def gpu_arm(args):
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(rho_h.nbytes),
                     "d2h_bytes_per_step": 36 * 8},
             "refinements": refs[-1],
-            "gpu_launches": sum(launches_per_step(hd.nlevels, c, args.reso, args.precision == 0, r)
+            "gpu_launches": sum(launches_per_step(hd.nlevels, c, args.reso, args.precision == 0, r, coarsest_nv)
                                 for c, r in zip(cycles, refs)),
             "roofline": {"kernel": "k_fine_gs (8 colour launches = one sweep)", "bound": "hbm",
                          "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",

@@ -2,7 +2,9 @@
 //
 // Layout in HBM (every level):
 //   A vertex field holds the six load cases and three components as 18 planes
-//   of nv floats: value(case c, comp m, vertex v) = field[(3c + m) * nv + v].
+//   (q = 3c + m for case c, component m).  FP32 fields interleave the planes in
+//   blocks of 128 vertices, value(q, v) = field[fidx(q, v)]; FP64 fields are
+//   planar, value(q, v) = field[q * nv + v].
 //   Vertices are ordered by Gauss-Seidel colour, then lexicographically inside
 //   the colour: a vertex (x,y,z) has colour k = ((x+1)&1) | ((y+1)&1)<<1 |
 //   ((z+1)&1)<<2 (the reference's padded-position parity, grid.cu:143-200) and
