@@ -14,12 +14,13 @@
 // B200 design.  The element loop is reorganised per neighbour: for each of the 26
 // neighbours the 3x3 coupling block sum_e rho_e Ke[a_e][b_e] is formed once (Ke
 // entries are compile-time offsets into the kernel-parameter bank, so they are
-// FFMA operands) and applied to the load cases.  Each vertex is served by three
-// threads with two load cases each (the three run in adjacent CTAs, so the shared
-// densities and neighbour rows hit L1/L2): two cases keep the register count near
-// 64 and the occupancy high enough to hide the neighbour-load latency, which is
-// what bounds this kernel; rebuilding the blocks per thread costs FMAs the
-// memory-bound sweep has to spare.  The operator is applied in difference form,
+// FFMA operands) and applied to the load cases, two cases at a time as packed
+// FP32x2 lane pairs.  The colour sweep serves each vertex by one thread with all
+// six cases (the block is built once per vertex; the sweep is bound by instruction
+// issue, 128 registers, 4 CTAs/SM); the residuals serve it by three threads with
+// two cases each in adjacent CTAs (fewer registers: the residual also writes r and
+// reduces the norms), where the densities and neighbour rows the three share hit
+// L1/L2.  The operator is applied in difference form,
 // sum_{d != 0} A_d (u_{v+d} - u_v), and the Gauss-Seidel step as u += D^-1 r with
 // the components in the reference's order: the same iteration in exact
 // arithmetic, and in FP32 it keeps rigid translations exact (see fine_apply).
@@ -29,8 +30,8 @@
 
 namespace h3d {
 
-constexpr int CPT = 2;            // load cases per thread
-constexpr int NG = NCASE / CPT;   // threads per vertex
+constexpr int GS_CPT = 6;         // load cases per thread of the colour sweep (one thread per vertex)
+constexpr int CPT = 2;            // load cases per thread of the residuals (three threads per vertex)
 constexpr int FBS = 128;          // threads per CTA
 
 struct FineArgs {
@@ -151,19 +152,22 @@ struct VertexGeo {
 // row sum to zero), and exact for rigid translations in FP32 too, so the FP32
 // operator agrees with the FP64 difference-form residual of the refined mode on
 // the near-null translation mode of the pinned problem.
-template <int K>
+template <int K, int C>
 __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, const VertexGeo<K> &g, int cb,
-                                           const float uv[3 * CPT], float acc[3 * CPT]) {
-    static_assert(CPT == 2, "the two load cases of a thread share one packed FP32x2 lane pair");
-    // lane pair (case cb, case cb+1) of each component: Blackwell's packed FP32x2
-    // add and FMA do both cases in one instruction with the rounding of the
+                                           const float uv[3 * C], float acc[3 * C]) {
+    static_assert(C % 2 == 0, "the load cases of a thread go in packed FP32x2 lane pairs");
+    constexpr int NP = C / 2;  // case pairs per thread
+    // lane pair (case cb+2j, case cb+2j+1) of each component: Blackwell's packed
+    // FP32x2 add and FMA do both cases in one instruction with the rounding of the
     // scalar forms, so the sums are the same as the scalar per-case loop
-    float2 acc2[3], nuv2[3];
+    float2 acc2[3 * NP], nuv2[3 * NP];
 #pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        acc2[m] = make_float2(0.f, 0.f);
-        nuv2[m] = make_float2(-uv[m], -uv[3 + m]);
-    }
+    for (int j = 0; j < NP; ++j)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            acc2[3 * j + m] = make_float2(0.f, 0.f);
+            nuv2[3 * j + m] = make_float2(-uv[6 * j + m], -uv[6 * j + 3 + m]);
+        }
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         if (d == 13) continue;
@@ -173,51 +177,60 @@ __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, c
         float A[9];
         g.block(ke, d, A);
         const float *up = a.u + fidx(3 * cb, nid);  // planes 3cb.. of the neighbour, FVB apart
-        float2 dd[3];
+#pragma unroll
+        for (int j = 0; j < NP; ++j) {
+            float2 dd[3];
+#pragma unroll
+            for (int m = 0; m < 3; ++m) {
+                const float2 un = pinned ? make_float2(0.f, 0.f)
+                                         : make_float2(__ldg(up + (6 * j + m) * FVB), __ldg(up + (6 * j + 3 + m) * FVB));
+                dd[m] = __fadd2_rn(un, nuv2[3 * j + m]);
+            }
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+                acc2[3 * j + r] = __ffma2_rn(make_float2(A[3 * r], A[3 * r]), dd[0],
+                                             __ffma2_rn(make_float2(A[3 * r + 1], A[3 * r + 1]), dd[1],
+                                                        __ffma2_rn(make_float2(A[3 * r + 2], A[3 * r + 2]), dd[2],
+                                                                   acc2[3 * j + r])));
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < NP; ++j)
 #pragma unroll
         for (int m = 0; m < 3; ++m) {
-            const float2 un = pinned ? make_float2(0.f, 0.f)
-                                     : make_float2(__ldg(up + m * FVB), __ldg(up + (3 + m) * FVB));
-            dd[m] = __fadd2_rn(un, nuv2[m]);
+            acc[6 * j + m] = acc2[3 * j + m].x;
+            acc[6 * j + 3 + m] = acc2[3 * j + m].y;
         }
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-            acc2[r] = __ffma2_rn(make_float2(A[3 * r], A[3 * r]), dd[0],
-                                 __ffma2_rn(make_float2(A[3 * r + 1], A[3 * r + 1]), dd[1],
-                                            __ffma2_rn(make_float2(A[3 * r + 2], A[3 * r + 2]), dd[2], acc2[r])));
-    }
-#pragma unroll
-    for (int m = 0; m < 3; ++m) {
-        acc[m] = acc2[m].x;
-        acc[3 + m] = acc2[m].y;
-    }
 }
 
-// thread -> (vertex p in the colour plane, first case cb); the NG case groups of a
+// thread -> (vertex p in the colour plane, first case cb) for C cases per thread;
+// the NCASE / C case groups of a vertex block are adjacent CTAs
 // vertex block are adjacent CTAs
+template <int C>
 __device__ __forceinline__ void thread_task(long long &p, int &cb) {
-    cb = (int)(blockIdx.x % NG) * CPT;
+    constexpr int NG = NCASE / C;
+    cb = (int)(blockIdx.x % NG) * C;
     p = (long long)(blockIdx.x / NG) * blockDim.x + threadIdx.x;
 }
 
 template <int K>
-__global__ void __launch_bounds__(FBS, 5) k_fine_gs(FineArgs a, const __grid_constant__ KeMat ke) {
+__global__ void __launch_bounds__(FBS, 4) k_fine_gs(FineArgs a, const __grid_constant__ KeMat ke) {
     long long p;
     int cb;
-    thread_task(p, cb);
+    thread_task<GS_CPT>(p, cb);
     if (p >= a.P) return;
     const long long me = (long long)K * a.P + p;
     if (K == 7 && p == 0) {  // the pinned origin (grid.cu:445-447, 545)
 #pragma unroll
-        for (int q = 0; q < 3 * CPT; ++q) a.u[fidx(3 * cb + q, me)] = 0.f;
+        for (int q = 0; q < 3 * GS_CPT; ++q) a.u[fidx(3 * cb + q, me)] = 0.f;
         return;
     }
     const VertexGeo<K> g(a, p);
-    float uv[3 * CPT];
+    float uv[3 * GS_CPT];
 #pragma unroll
-    for (int q = 0; q < 3 * CPT; ++q) uv[q] = a.u[fidx(3 * cb + q, me)];
-    float acc[3 * CPT];
-    fine_apply<K>(a, ke, g, cb, uv, acc);
+    for (int q = 0; q < 3 * GS_CPT; ++q) uv[q] = a.u[fidx(3 * cb + q, me)];
+    float acc[3 * GS_CPT];
+    fine_apply<K, GS_CPT>(a, ke, g, cb, uv, acc);
     float ks[9];
     g.block(ke, 13, ks);
     const float w = a.w;
@@ -225,7 +238,7 @@ __global__ void __launch_bounds__(FBS, 5) k_fine_gs(FineArgs a, const __grid_con
     // each with the relaxed values of the earlier components) written as an
     // update of u by the residual r = f - K u
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) {
+    for (int c = 0; c < GS_CPT; ++c) {
         const long long o = fidx(3 * (cb + c), me);
         const float r0 = a.f[o] - acc[3 * c], r1 = a.f[o + FVB] - acc[3 * c + 1], r2 = a.f[o + 2 * FVB] - acc[3 * c + 2];
         const float d0 = w * r0 / ks[0];
@@ -251,7 +264,7 @@ __device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const Ke
 #pragma unroll
     for (int q = 0; q < 3 * CPT; ++q) uv[q] = __ldg(a.u + fidx(3 * cb + q, me));
     float acc[3 * CPT];
-    fine_apply<K>(a, ke, g, cb, uv, acc);
+    fine_apply<K, CPT>(a, ke, g, cb, uv, acc);
     constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
     int i, j, l;
     plane_coords(a, p, i, j, l);
@@ -279,7 +292,7 @@ __global__ void __launch_bounds__(FBS, 6) k_fine_residual(FineArgs a, const __gr
                                                        double *partial) {
     long long p;
     int cb;
-    thread_task(p, cb);
+    thread_task<CPT>(p, cb);
     double nrm[CPT] = {0, 0};
     if (p < a.P) fine_residual_vertex<K>(a, ke, p, cb, nrm);
     if (!partial) return;
@@ -358,7 +371,7 @@ __global__ void __launch_bounds__(FBS, 4) k_fine_residual64(FineArgs a, const __
                                                          const double *__restrict__ u64) {
     long long p;
     int cb;
-    thread_task(p, cb);
+    thread_task<CPT>(p, cb);
     if (p >= a.P) return;
     switch (blockIdx.y) {
     case 0: fine_residual64_vertex<0, EXACT>(a, ke, u64, p, cb); break;
@@ -414,14 +427,14 @@ static FineArgs make_args(const Level &L, const float *rho) {
     return a;
 }
 
-static unsigned task_blocks(const FineArgs &a) { return (unsigned)(((a.P + FBS - 1) / FBS) * NG); }
+static unsigned task_blocks(const FineArgs &a, int cpt) { return (unsigned)(((a.P + FBS - 1) / FBS) * (NCASE / cpt)); }
 
-int fine_residual_blocks(const Level &L) { return (int)(((L.P.nv / 8 + FBS - 1) / FBS) * NG * 8); }
+int fine_residual_blocks(const Level &L) { return (int)(((L.P.nv / 8 + FBS - 1) / FBS) * (NCASE / CPT) * 8); }
 
 void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, cudaStream_t s) {
     FineArgs a = make_args(L, rho);
     a.w = w;
-    const unsigned nb = task_blocks(a);
+    const unsigned nb = task_blocks(a, GS_CPT);
     k_fine_gs<0><<<nb, FBS, 0, s>>>(a, ke);
     k_fine_gs<1><<<nb, FBS, 0, s>>>(a, ke);
     k_fine_gs<2><<<nb, FBS, 0, s>>>(a, ke);
@@ -436,7 +449,7 @@ void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, dou
                           cudaStream_t s) {
     FineArgs a = make_args(L, rho);
     (void)nblk_norm;
-    const unsigned nb = task_blocks(a);
+    const unsigned nb = task_blocks(a, CPT);
     k_fine_residual<0><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
     k_fine_residual<1><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
     k_fine_residual<2><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
@@ -452,8 +465,8 @@ void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, c
     FineArgs a = make_args(L, rho);
     a.f = f;
     a.r = r;
-    if (exact) k_fine_residual64<true><<<dim3(task_blocks(a), 8), FBS, 0, s>>>(a, ke, u64);
-    else k_fine_residual64<false><<<dim3(task_blocks(a), 8), FBS, 0, s>>>(a, ke, u64);
+    if (exact) k_fine_residual64<true><<<dim3(task_blocks(a, CPT), 8), FBS, 0, s>>>(a, ke, u64);
+    else k_fine_residual64<false><<<dim3(task_blocks(a, CPT), 8), FBS, 0, s>>>(a, ke, u64);
 }
 
 void launch_rhs(const Level &L, const float *rho, const RhsTab &g, float *f, cudaStream_t s) {
