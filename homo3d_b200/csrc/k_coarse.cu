@@ -56,14 +56,17 @@ __device__ __forceinline__ void load_block(const CoarseArgs &a, long long me, fl
     for (int k = 0; k < 9; ++k) s[k] = v[e0 + k - S::PER * q0];
 }
 
-// load cases per thread on the coarse levels; the two threads of a vertex run in
-// adjacent CTAs, so the second read of its stencil hits L2
-constexpr int CPTC = 3;
-constexpr int NGC = NCASE / CPTC;
+// load cases per thread on the coarse levels (as packed FP32x2 case pairs) and the
+// CTAs per SM each kernel is compiled for; the threads of one vertex run in
+// adjacent CTAs, so the repeated reads of its stencil hit L2
+constexpr int CGS_CPT = 2, CGS_MINB = 6;
+constexpr int CRES_CPT = 2, CRES_MINB = 6;
 
-template <int K, bool SELF, bool F32>
+template <int K, bool SELF, bool F32, int C>
 __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, int i, int j, int l, int cb,
-                                             float acc[3 * CPTC]) {
+                                             float acc[3 * C]) {
+    static_assert(C % 2 == 0, "the load cases of a thread go in packed FP32x2 lane pairs");
+    constexpr int NP = C / 2;
     constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
     int ii[3], jj[3], ll[3];
     axis_nbrs_c(i, px, a.h[0], ii[0], ii[2]);
@@ -79,8 +82,10 @@ __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, 
         Y[t] = h0 * (unsigned)jj[t];
         Z[t] = h01 * (unsigned)ll[t];
     }
+    // lane pair (case cb+2j, case cb+2j+1): packed FP32x2 FMAs in the scalar per-case order
+    float2 acc2[3 * NP];
 #pragma unroll
-    for (int q = 0; q < 3 * CPTC; ++q) acc[q] = 0.f;
+    for (int q = 0; q < 3 * NP; ++q) acc2[q] = make_float2(0.f, 0.f);
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         if (d == 13 && !SELF) continue;
@@ -98,37 +103,51 @@ __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, 
         const unsigned nid = (unsigned)Kn * (unsigned)a.P + X[dx + 1] + Y[dy + 1] + Z[dz + 1];
         const float *up = a.u + fidx(3 * cb, nid);  // planes 3cb.. of the neighbour, FVB apart
 #pragma unroll
-        for (int c = 0; c < CPTC; ++c) {
-            const float u0 = up[(3 * c) * FVB], u1 = up[(3 * c + 1) * FVB], u2 = up[(3 * c + 2) * FVB];
-            acc[3 * c + 0] = fmaf(s[0], u0, fmaf(s[1], u1, fmaf(s[2], u2, acc[3 * c + 0])));
-            acc[3 * c + 1] = fmaf(s[3], u0, fmaf(s[4], u1, fmaf(s[5], u2, acc[3 * c + 1])));
-            acc[3 * c + 2] = fmaf(s[6], u0, fmaf(s[7], u1, fmaf(s[8], u2, acc[3 * c + 2])));
+        for (int jp = 0; jp < NP; ++jp) {
+            float2 uu[3];
+#pragma unroll
+            for (int m = 0; m < 3; ++m) uu[m] = make_float2(up[(6 * jp + m) * FVB], up[(6 * jp + 3 + m) * FVB]);
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+                acc2[3 * jp + r] = __ffma2_rn(make_float2(s[3 * r], s[3 * r]), uu[0],
+                                              __ffma2_rn(make_float2(s[3 * r + 1], s[3 * r + 1]), uu[1],
+                                                         __ffma2_rn(make_float2(s[3 * r + 2], s[3 * r + 2]), uu[2],
+                                                                    acc2[3 * jp + r])));
         }
     }
+#pragma unroll
+    for (int jp = 0; jp < NP; ++jp)
+#pragma unroll
+        for (int m = 0; m < 3; ++m) {
+            acc[6 * jp + m] = acc2[3 * jp + m].x;
+            acc[6 * jp + 3 + m] = acc2[3 * jp + m].y;
+        }
 }
 
-// thread -> (vertex p, first load case cb): CTAs g*NGC .. g*NGC+NGC-1 cover the
-// same 128 vertices with different load cases
+// thread -> (vertex p, first load case cb) for C cases per thread: the NCASE / C
+// CTAs of a case group cover the same 128 vertices with different load cases
+template <int C>
 __device__ __forceinline__ void coarse_task(long long &p, int &cb) {
-    cb = (int)(blockIdx.x % NGC) * CPTC;
-    p = (long long)(blockIdx.x / NGC) * blockDim.x + threadIdx.x;
+    constexpr int NG = NCASE / C;
+    cb = (int)(blockIdx.x % NG) * C;
+    p = (long long)(blockIdx.x / NG) * blockDim.x + threadIdx.x;
 }
 
 template <int K, bool F32>
-__global__ void __launch_bounds__(128) k_coarse_gs(CoarseArgs a) {
+__global__ void __launch_bounds__(128, CGS_MINB) k_coarse_gs(CoarseArgs a) {
     long long p;
     int cb;
-    coarse_task(p, cb);
+    coarse_task<CGS_CPT>(p, cb);
     if (p >= a.P) return;
     const long long me = (long long)K * a.P + p;
     int i, j, l;
     cplane_coords(a, p, i, j, l);
-    float acc[3 * CPTC], ks[9];
-    coarse_apply<K, false, F32>(a, me, i, j, l, cb, acc);
+    float acc[3 * CGS_CPT], ks[9];
+    coarse_apply<K, false, F32, CGS_CPT>(a, me, i, j, l, cb, acc);
     load_block<13, F32>(a, me, ks);
     const float w = a.w;
 #pragma unroll
-    for (int c = 0; c < CPTC; ++c) {
+    for (int c = 0; c < CGS_CPT; ++c) {
         float *u = a.u + fidx(3 * (cb + c), me);
         const float *f = a.f + fidx(3 * (cb + c), me);
         float u0 = u[0], u1 = u[FVB], u2 = u[2 * FVB];
@@ -146,20 +165,20 @@ __device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long
     const long long me = (long long)K * a.P + p;
     int i, j, l;
     cplane_coords(a, p, i, j, l);
-    float acc[3 * CPTC];
-    coarse_apply<K, true, F32>(a, me, i, j, l, cb, acc);
+    float acc[3 * CRES_CPT];
+    coarse_apply<K, true, F32, CRES_CPT>(a, me, i, j, l, cb, acc);
 #pragma unroll
-    for (int q = 0; q < 3 * CPTC; ++q) {
+    for (int q = 0; q < 3 * CRES_CPT; ++q) {
         const long long o = fidx(3 * cb + q, me);
         a.r[o] = a.f[o] - acc[q];
     }
 }
 
 template <int K, bool F32>
-__global__ void __launch_bounds__(128, 5) k_coarse_residual(CoarseArgs a) {
+__global__ void __launch_bounds__(128, CRES_MINB) k_coarse_residual(CoarseArgs a) {
     long long p;
     int cb;
-    coarse_task(p, cb);
+    coarse_task<CRES_CPT>(p, cb);
     if (p >= a.P) return;
     coarse_res_vertex<K, F32>(a, p, cb);
 }
@@ -194,7 +213,7 @@ static void coarse_gs_sweep(const CoarseArgs &a, unsigned nb, cudaStream_t s) {
 void launch_coarse_gs(const Level &L, float w, cudaStream_t s) {
     CoarseArgs a = make_cargs(L);
     a.w = w;
-    const unsigned nb = (unsigned)((a.P + 127) / 128) * NGC;
+    const unsigned nb = (unsigned)((a.P + 127) / 128) * (NCASE / CGS_CPT);
     if (L.st32) coarse_gs_sweep<true>(a, nb, s);
     else coarse_gs_sweep<false>(a, nb, s);
 }
@@ -213,7 +232,7 @@ static void coarse_residual_all(const CoarseArgs &a, unsigned nb, cudaStream_t s
 
 void launch_coarse_residual(const Level &L, cudaStream_t s) {
     CoarseArgs a = make_cargs(L);
-    const unsigned nb = (unsigned)((a.P + 127) / 128) * NGC;
+    const unsigned nb = (unsigned)((a.P + 127) / 128) * (NCASE / CRES_CPT);
     if (L.st32) coarse_residual_all<true>(a, nb, s);
     else coarse_residual_all<false>(a, nb, s);
 }
