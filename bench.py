@@ -258,6 +258,7 @@ def gpu_arm(args):
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(rho_h.nbytes),
                     "d2h_bytes_per_step": 36 * 8},
             "refinements": refs[-1],
+            "launch_shapes": hd.tuning(),
             "gpu_launches": sum(launches_per_step(hd.nlevels, c, args.reso, args.precision == 0, r, coarsest_nv)
                                 for c, r in zip(cycles, refs)),
             "roofline": {"kernel": "k_fine_gs (8 colour launches = one sweep)", "bound": "hbm",

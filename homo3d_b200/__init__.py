@@ -92,6 +92,9 @@ _SIGS = {
     "h3d_elastic_matrix": [_vp, ctypes.c_double, _dp, ctypes.POINTER(SolveStats)],
     "h3d_sensitivity": [_vp, _fp, _vp, ctypes.c_int],
     "h3d_reset_solutions": [_vp],
+    "h3d_autotune": [_vp],
+    "h3d_get_tuning": [_vp, ctypes.c_int, _ip],
+    "h3d_set_tuning": [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int],
     "h3d_batch_update_density": [ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.c_int],
     "h3d_batch_elastic_matrix": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_double, _dp,
                                  ctypes.POINTER(SolveStats), _ip],
@@ -348,6 +351,23 @@ class Homogenization(_Handle):
 
     def reset_solutions(self):
         self.check(lib().h3d_reset_solutions(self._h))
+
+    def autotune(self):
+        """time the launch shapes of every level now and keep the fastest"""
+        self.check(lib().h3d_autotune(self._h))
+        return self.tuning()
+
+    def tuning(self):
+        """[(sweep shape, residual shape)] per level"""
+        out = []
+        for l in range(self.nlevels):
+            sh = (ctypes.c_int * 2)()
+            self.check(lib().h3d_get_tuning(self._h, l, sh))
+            out.append((sh[0], sh[1]))
+        return out
+
+    def set_tuning(self, level, gs_shape, res_shape=0):
+        self.check(lib().h3d_set_tuning(self._h, int(level), int(gs_shape), int(res_shape)))
 
     def warm_start_learned(self, net):
         """stored solutions from a WarmNet's prediction for the current density"""

@@ -172,6 +172,7 @@ struct h3d_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool refine() const { return cfg.precision == H3D_PREC_REFINE; }
     bool have_density = false, have_stencils = false;
+    bool tuned = false;  // launch shapes chosen (autotuner or h3d_set_tuning)
     std::string err;
 };
 
@@ -345,6 +346,54 @@ int check_level(h3d_handle *h, int level, bool coarse_only = false) {
 
 namespace {
 
+// Autotuner (no reference counterpart).  Per smoothed level, each launch shape of
+// the colour sweep and, on the coarse levels, of the residual is timed with CUDA
+// events on the handle's stream (one untimed launch sequence, then three timed)
+// and the fastest is kept.  The sweeps iterate on the level's r, so u and f are
+// untouched (r is scratch that the next residual overwrites).  The shapes give
+// the same results to the last bit; tuning changes only the time.  Graphs
+// captured with the old shapes are dropped and re-captured on demand.
+int autotune(h3d_handle *h) {
+    CK(cudaSetDevice(h->device));
+    cudaStream_t s = h->stream;
+    constexpr int NSHAPE = 2, REPS = 3;
+    for (int l = 0; l < h->nl - 1; l++) {
+        Level &L = h->lv[l];
+        for (int kind = 0; kind < (l > 0 ? 2 : 1); kind++) {  // 0: sweep, 1: residual
+            float best = 0;
+            int pick = 0;
+            for (int v = 0; v < NSHAPE; v++) {
+                Level T = L;
+                T.gs_shape = T.res_shape = v;
+                if (kind == 0) T.u = L.r;  // the sweep iterates on scratch
+                auto run = [&]() {
+                    if (kind == 1) launch_coarse_residual(T, s);
+                    else if (l == 0) launch_fine_gs(T, h->rho, h->ke, 1.f, s);
+                    else launch_coarse_gs(T, 1.f, s);
+                };
+                run();
+                CK(cudaEventRecord(h->ev0, s));
+                for (int r = 0; r < REPS; r++) run();
+                CK(cudaEventRecord(h->ev1, s));
+                CK(cudaEventSynchronize(h->ev1));
+                CKL();
+                float ms = 0;
+                CK(cudaEventElapsedTime(&ms, h->ev0, h->ev1));
+                if (v == 0 || ms < best) { best = ms; pick = v; }
+            }
+            if (kind == 0) L.gs_shape = pick;
+            else L.res_shape = pick;
+        }
+    }
+    destroy_graph(h);
+    h->tuned = true;
+    return H3D_OK;
+}
+
+}  // namespace
+
+namespace {
+
 // The solve loop of MG::solveEquation (MG.cpp:113-203) as a resumable state
 // machine: begin() enqueues the first step on the handle's stream; after that
 // stream has drained, advance() reads the step's result and enqueues the next
@@ -428,6 +477,8 @@ struct SolveRun {
             launch_remove_mean(L0.P, rhs, h->partial, nb, h->stream);
             CKL();
         }
+        if (!h->tuned)
+            if (int e = autotune(h)) return e;
         if (int e = build_graph(h, G_SOLVE)) return e;
         // below ~1e-4 the FP32 products of the difference-form residual would floor
         // the iteration, so tight targets take the FP64-accumulating residual
@@ -933,6 +984,30 @@ int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solv
         if (int e = run.advance()) return e;
     }
     return run.end(stats);
+}
+
+int h3d_autotune(h3d_handle *h) {
+    if (!h) return H3D_ERR_ARG;
+    if (!h->have_stencils) return fail(h, H3D_ERR_STATE, "no stencils");
+    return autotune(h);
+}
+
+int h3d_get_tuning(const h3d_handle *h, int level, int shapes[2]) {
+    if (!h || !shapes || level < 0 || level >= h->nl) return H3D_ERR_ARG;
+    shapes[0] = h->lv[level].gs_shape;
+    shapes[1] = h->lv[level].res_shape;
+    return H3D_OK;
+}
+
+int h3d_set_tuning(h3d_handle *h, int level, int gs_shape, int res_shape) {
+    if (!h) return H3D_ERR_ARG;
+    if (level < 0 || level >= h->nl || gs_shape < 0 || gs_shape > 1 || res_shape < 0 || res_shape > 1)
+        return fail(h, H3D_ERR_ARG, "level or launch shape out of range");
+    h->lv[level].gs_shape = gs_shape;
+    h->lv[level].res_shape = res_shape;
+    destroy_graph(h);
+    h->tuned = true;
+    return H3D_OK;
 }
 
 int h3d_reset_solutions(h3d_handle *h) {

@@ -140,6 +140,9 @@ struct Level {
     float *u = nullptr, *f = nullptr, *r = nullptr;
     uint4 *st = nullptr;   // coarse levels
     bool st32 = false;     // FP32 stencil entries (FP16 otherwise)
+    // launch shapes of the level's sweep and residual (see the launchers); set by
+    // the autotuner, results do not depend on them
+    int gs_shape = 0, res_shape = 0;
 };
 
 #ifdef __CUDACC__

@@ -56,11 +56,11 @@ __device__ __forceinline__ void load_block(const CoarseArgs &a, long long me, fl
     for (int k = 0; k < 9; ++k) s[k] = v[e0 + k - S::PER * q0];
 }
 
-// load cases per thread on the coarse levels (as packed FP32x2 case pairs) and the
-// CTAs per SM each kernel is compiled for; the threads of one vertex run in
-// adjacent CTAs, so the repeated reads of its stencil hit L2
-constexpr int CGS_CPT = 2, CGS_MINB = 6;
-constexpr int CRES_CPT = 2, CRES_MINB = 6;
+// Launch shapes of the coarse kernels (load cases per thread as packed FP32x2
+// case pairs, CTAs per SM): shape 0 = three threads per vertex with two cases
+// each, 6 CTAs/SM; shape 1 = one thread per vertex with all six, 4 CTAs/SM.  The
+// threads of one vertex run in adjacent CTAs, so repeated stencil reads hit L2;
+// both shapes give the same result to the last bit.
 
 template <int K, bool SELF, bool F32, int C>
 __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, int i, int j, int l, int cb,
@@ -133,7 +133,7 @@ __device__ __forceinline__ void coarse_task(long long &p, int &cb) {
     p = (long long)(blockIdx.x / NG) * blockDim.x + threadIdx.x;
 }
 
-template <int K, bool F32>
+template <int K, bool F32, int CGS_CPT, int CGS_MINB>
 __global__ void __launch_bounds__(128, CGS_MINB) k_coarse_gs(CoarseArgs a) {
     long long p;
     int cb;
@@ -160,7 +160,7 @@ __global__ void __launch_bounds__(128, CGS_MINB) k_coarse_gs(CoarseArgs a) {
     }
 }
 
-template <int K, bool F32>
+template <int K, bool F32, int CRES_CPT>
 __device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long p, int cb) {
     const long long me = (long long)K * a.P + p;
     int i, j, l;
@@ -174,13 +174,13 @@ __device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long
     }
 }
 
-template <int K, bool F32>
+template <int K, bool F32, int CRES_CPT, int CRES_MINB>
 __global__ void __launch_bounds__(128, CRES_MINB) k_coarse_residual(CoarseArgs a) {
     long long p;
     int cb;
     coarse_task<CRES_CPT>(p, cb);
     if (p >= a.P) return;
-    coarse_res_vertex<K, F32>(a, p, cb);
+    coarse_res_vertex<K, F32, CRES_CPT>(a, p, cb);
 }
 
 static CoarseArgs make_cargs(const Level &L) {
@@ -198,43 +198,53 @@ static CoarseArgs make_cargs(const Level &L) {
     return a;
 }
 
-template <bool F32>
-static void coarse_gs_sweep(const CoarseArgs &a, unsigned nb, cudaStream_t s) {
-    k_coarse_gs<0, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<1, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<2, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<3, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<4, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<5, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<6, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<7, F32><<<nb, 128, 0, s>>>(a);
+template <bool F32, int C, int MINB>
+static void coarse_gs_sweep(const CoarseArgs &a, cudaStream_t s) {
+    const unsigned nb = (unsigned)((a.P + 127) / 128) * (NCASE / C);
+    k_coarse_gs<0, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<1, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<2, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<3, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<4, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<5, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<6, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<7, F32, C, MINB><<<nb, 128, 0, s>>>(a);
 }
 
 void launch_coarse_gs(const Level &L, float w, cudaStream_t s) {
     CoarseArgs a = make_cargs(L);
     a.w = w;
-    const unsigned nb = (unsigned)((a.P + 127) / 128) * (NCASE / CGS_CPT);
-    if (L.st32) coarse_gs_sweep<true>(a, nb, s);
-    else coarse_gs_sweep<false>(a, nb, s);
+    if (L.st32) {
+        if (L.gs_shape == 1) coarse_gs_sweep<true, 6, 4>(a, s);
+        else coarse_gs_sweep<true, 2, 6>(a, s);
+    } else {
+        if (L.gs_shape == 1) coarse_gs_sweep<false, 6, 4>(a, s);
+        else coarse_gs_sweep<false, 2, 6>(a, s);
+    }
 }
 
-template <bool F32>
-static void coarse_residual_all(const CoarseArgs &a, unsigned nb, cudaStream_t s) {
-    k_coarse_residual<0, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<1, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<2, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<3, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<4, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<5, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<6, F32><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<7, F32><<<nb, 128, 0, s>>>(a);
+template <bool F32, int C, int MINB>
+static void coarse_residual_all(const CoarseArgs &a, cudaStream_t s) {
+    const unsigned nb = (unsigned)((a.P + 127) / 128) * (NCASE / C);
+    k_coarse_residual<0, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<1, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<2, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<3, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<4, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<5, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<6, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<7, F32, C, MINB><<<nb, 128, 0, s>>>(a);
 }
 
 void launch_coarse_residual(const Level &L, cudaStream_t s) {
     CoarseArgs a = make_cargs(L);
-    const unsigned nb = (unsigned)((a.P + 127) / 128) * (NCASE / CRES_CPT);
-    if (L.st32) coarse_residual_all<true>(a, nb, s);
-    else coarse_residual_all<false>(a, nb, s);
+    if (L.st32) {
+        if (L.res_shape == 1) coarse_residual_all<true, 6, 4>(a, s);
+        else coarse_residual_all<true, 2, 6>(a, s);
+    } else {
+        if (L.res_shape == 1) coarse_residual_all<false, 6, 4>(a, s);
+        else coarse_residual_all<false, 2, 6>(a, s);
+    }
 }
 
 // ---- transfers ---------------------------------------------------------------

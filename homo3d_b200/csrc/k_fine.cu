@@ -30,7 +30,6 @@
 
 namespace h3d {
 
-constexpr int GS_CPT = 6;         // load cases per thread of the colour sweep (one thread per vertex)
 constexpr int CPT = 2;            // load cases per thread of the residuals (three threads per vertex)
 constexpr int FBS = 128;          // threads per CTA
 
@@ -213,24 +212,24 @@ __device__ __forceinline__ void thread_task(long long &p, int &cb) {
     p = (long long)(blockIdx.x / NG) * blockDim.x + threadIdx.x;
 }
 
-template <int K>
-__global__ void __launch_bounds__(FBS, 4) k_fine_gs(FineArgs a, const __grid_constant__ KeMat ke) {
+template <int K, int C, int MINB>
+__global__ void __launch_bounds__(FBS, MINB) k_fine_gs(FineArgs a, const __grid_constant__ KeMat ke) {
     long long p;
     int cb;
-    thread_task<GS_CPT>(p, cb);
+    thread_task<C>(p, cb);
     if (p >= a.P) return;
     const long long me = (long long)K * a.P + p;
     if (K == 7 && p == 0) {  // the pinned origin (grid.cu:445-447, 545)
 #pragma unroll
-        for (int q = 0; q < 3 * GS_CPT; ++q) a.u[fidx(3 * cb + q, me)] = 0.f;
+        for (int q = 0; q < 3 * C; ++q) a.u[fidx(3 * cb + q, me)] = 0.f;
         return;
     }
     const VertexGeo<K> g(a, p);
-    float uv[3 * GS_CPT];
+    float uv[3 * C];
 #pragma unroll
-    for (int q = 0; q < 3 * GS_CPT; ++q) uv[q] = a.u[fidx(3 * cb + q, me)];
-    float acc[3 * GS_CPT];
-    fine_apply<K, GS_CPT>(a, ke, g, cb, uv, acc);
+    for (int q = 0; q < 3 * C; ++q) uv[q] = a.u[fidx(3 * cb + q, me)];
+    float acc[3 * C];
+    fine_apply<K, C>(a, ke, g, cb, uv, acc);
     float ks[9];
     g.block(ke, 13, ks);
     const float w = a.w;
@@ -238,7 +237,7 @@ __global__ void __launch_bounds__(FBS, 4) k_fine_gs(FineArgs a, const __grid_con
     // each with the relaxed values of the earlier components) written as an
     // update of u by the residual r = f - K u
 #pragma unroll
-    for (int c = 0; c < GS_CPT; ++c) {
+    for (int c = 0; c < C; ++c) {
         const long long o = fidx(3 * (cb + c), me);
         const float r0 = a.f[o] - acc[3 * c], r1 = a.f[o + FVB] - acc[3 * c + 1], r2 = a.f[o + 2 * FVB] - acc[3 * c + 2];
         const float d0 = w * r0 / ks[0];
@@ -431,18 +430,27 @@ static unsigned task_blocks(const FineArgs &a, int cpt) { return (unsigned)(((a.
 
 int fine_residual_blocks(const Level &L) { return (int)(((L.P.nv / 8 + FBS - 1) / FBS) * (NCASE / CPT) * 8); }
 
+// the colour sweep in launch shape v: 0 = one thread per vertex with all six
+// cases (4 CTAs/SM), 1 = three threads per vertex with two cases each (5 CTAs/SM);
+// both give the same result to the last bit
+template <int C, int MINB>
+static void fine_gs_sweep(const FineArgs &a, const KeMat &ke, cudaStream_t s) {
+    const unsigned nb = task_blocks(a, C);
+    k_fine_gs<0, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<1, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<2, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<3, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<4, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<5, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<6, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<7, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
+}
+
 void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, cudaStream_t s) {
     FineArgs a = make_args(L, rho);
     a.w = w;
-    const unsigned nb = task_blocks(a, GS_CPT);
-    k_fine_gs<0><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<1><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<2><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<3><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<4><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<5><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<6><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<7><<<nb, FBS, 0, s>>>(a, ke);
+    if (L.gs_shape == 1) fine_gs_sweep<2, 5>(a, ke, s);
+    else fine_gs_sweep<6, 4>(a, ke, s);
 }
 
 void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, double *norm_partial, int nblk_norm,

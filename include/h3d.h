@@ -170,6 +170,19 @@ H3D_API int h3d_sensitivity(h3d_handle *h, const float dC[36], float *sens_dev, 
 /* forget the stored solutions (warm start) */
 H3D_API int h3d_reset_solutions(h3d_handle *h);
 
+/* ---- autotuner (no reference counterpart) ----------------------------------
+ * Each smoothed level has two launch shapes for its colour sweep and (coarse
+ * levels) its residual: shape 0 / 1 = one thread per vertex with all six load
+ * cases / three threads with two cases each on level 0, the reverse on the coarse
+ * levels.  Both give the same results to the last bit.  The first solve of a
+ * handle times them (CUDA events, a few sweeps per shape, iterating on the
+ * level's scratch residual field) and keeps the faster; h3d_autotune re-runs that
+ * now, h3d_set_tuning fixes the shapes (and turns the automatic tuning off),
+ * h3d_get_tuning reads them: shapes[0] = sweep, shapes[1] = residual. */
+H3D_API int h3d_autotune(h3d_handle *h);
+H3D_API int h3d_get_tuning(const h3d_handle *h, int level, int shapes[2]);
+H3D_API int h3d_set_tuning(h3d_handle *h, int level, int gs_shape, int res_shape);
+
 /* ---- batched designs (no reference counterpart: the reference homogenizes one
  * design per process) -------------------------------------------------------- */
 /* h3d_update_density on n distinct handles (lexicographic rho_phys, unpadded),
