@@ -17,7 +17,7 @@ import time
 
 import numpy as np
 
-from . import FIELD_CHI, H3DError, Homogenization, WarmNet
+from . import FIELD_CHI, STENCIL_FP16, STENCIL_FP32, H3DError, Homogenization, WarmNet
 from .density import synthetic_density
 from .optimize import optimize_bulk
 
@@ -76,12 +76,13 @@ def train(net, x, t, steps=2000, batch=8, lr=1e-3, seed=0, log_every=0):
     return hist
 
 
-def compare_starts(net, n, seeds, relthres=1e-5, vol_range=(0.1, 0.5), device=0):
+def compare_starts(net, n, seeds, relthres=1e-5, vol_range=(0.1, 0.5), device=0, stencil=STENCIL_FP16):
     """V-cycles and solve time of the plain zero start and of the learned start on
-    fresh designs (trig-basis densities, rho^3)"""
+    fresh designs (trig-basis densities, rho^3); a solve that fails is recorded in
+    the row's "error" and left out of the averages"""
     import torch
     out = []
-    hd = Homogenization(n, device=device)
+    hd = Homogenization(n, device=device, stencil=stencil)
     for seed in seeds:
         vol = float(np.random.default_rng(20011 + seed).uniform(*vol_range))
         rho = synthetic_density(n, seed=seed, vol=vol).ravel().astype(np.float64)
@@ -93,7 +94,11 @@ def compare_starts(net, n, seeds, relthres=1e-5, vol_range=(0.1, 0.5), device=0)
             t0 = time.perf_counter()
             if mode == "learned":
                 hd.warm_start_learned(net)
-            C = hd.elasticMatrix(relthres)
+            try:
+                C = hd.elasticMatrix(relthres)
+            except H3DError as e:
+                row["error"] = "%s start: %s" % (mode, e)
+                break
             row[mode + "_ms"] = (time.perf_counter() - t0) * 1e3
             row[mode + "_vcycles"] = hd.last_stats["vcycles"]
             row[mode + "_C00"] = float(C[0, 0])
@@ -116,8 +121,10 @@ def main():
     ap.add_argument("--steps", type=int, default=3000)
     ap.add_argument("--batch", type=int, default=8)
     ap.add_argument("--lr", type=float, default=2e-3)
-    ap.add_argument("--eval-reso", type=int, default=0, help="compare starts at this size after training")
+    ap.add_argument("--eval-reso", default="", help="compare starts at these sizes after training (e.g. 128,256)")
+    ap.add_argument("--eval-tols", default="1e-5", help="relative residual thresholds of the compared solves")
     ap.add_argument("--eval-seeds", default="1000-1003")
+    ap.add_argument("--stencils", choices=["fp16", "fp32"], default="fp16", help="coarse stencils of the compared solves")
     ap.add_argument("--out", default="")
     args = ap.parse_args()
     t0 = time.perf_counter()
@@ -132,10 +139,22 @@ def main():
            "data_s": round(t1 - t0, 1), "train_s": round(t2 - t1, 1), "loss_first": hist[0],
            "loss_last10": float(np.mean(hist[-10:]))}
     if args.eval_reso:
-        rows = compare_starts(net, args.eval_reso, _seeds(args.eval_seeds))
-        rep["eval"] = rows
-        rep["vcycles_zero"] = float(np.mean([r["zero_vcycles"] for r in rows]))
-        rep["vcycles_learned"] = float(np.mean([r["learned_vcycles"] for r in rows]))
+        rep["eval"] = []
+        for n in (int(v) for v in args.eval_reso.split(",")):
+            for tol in (float(v) for v in args.eval_tols.split(",")):
+                allrows = compare_starts(net, n, _seeds(args.eval_seeds), relthres=tol,
+                                         stencil=STENCIL_FP32 if args.stencils == "fp32" else STENCIL_FP16)
+                rows = [r for r in allrows if "error" not in r]
+                rep["eval"].append({
+                    "reso": n, "relthres": tol, "stencils": args.stencils, "designs": len(rows),
+                    "failed": [r["error"] for r in allrows if "error" in r],
+                    "vcycles_zero": float(np.mean([r["zero_vcycles"] for r in rows])),
+                    "vcycles_learned": float(np.mean([r["learned_vcycles"] for r in rows])),
+                    "ms_zero": float(np.mean([r["zero_ms"] for r in rows])),
+                    "ms_learned": float(np.mean([r["learned_ms"] for r in rows])),
+                    "max_rel_C00_diff": float(max(abs(r["learned_C00"] - r["zero_C00"]) / abs(r["zero_C00"])
+                                                  for r in rows))})
+                print(json.dumps(rep["eval"][-1]), flush=True)
     print(json.dumps(rep), flush=True)
 
 
