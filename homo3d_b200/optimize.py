@@ -1,12 +1,14 @@
-"""Bulk-modulus maximisation with OC, the loop of homo3d's optiBulk
-(homogenization/testAutoDiff.cu:282-331), on the library's entry points.
+"""OC design loops on the library's entry points: bulk-modulus maximisation (the
+loop of homo3d's optiBulk, homogenization/testAutoDiff.cu:282-331) and the
+negative-Poisson-ratio loop (example_opti_npr, Framework.cu:208-272).
 
 Per iteration: rho_phys = rho^3; update the hierarchy; six solves and C (warm
-start from the previous iteration); obj = -(C00+C11+C22 + 2(C01+C02+C12))/3;
+start from the previous iteration); the objective, bulk
+-(C00+C11+C22 + 2(C01+C02+C12))/3 or npr C01+C02+C12 - (C00+C11+C22) 0.8^iter;
 sensitivities wrt rho_phys, chain rule 3 rho^2; symmetrise; filter; OC update;
 symmetrise the density.  Every step runs on the handle's stream.
 
-    python -m homo3d_b200.optimize --reso 128 --iters 50
+    python -m homo3d_b200.optimize --reso 128 --iters 50 [--objective npr]
 """
 import argparse
 import json
@@ -32,6 +34,26 @@ def bulk_objective(C):
     return -(C[0, 0] + C[1, 1] + C[2, 2] + 2 * (C[0, 1] + C[0, 2] + C[1, 2])) / 3.0
 
 
+NPR_BETA = 0.8  # Framework.cu:241
+
+
+def npr_objective(C, it, beta=NPR_BETA):
+    return C[0, 1] + C[0, 2] + C[1, 2] - (C[0, 0] + C[1, 1] + C[2, 2]) * beta ** it
+
+
+def npr_gradient(it, beta=NPR_BETA):
+    """d obj / d C of the npr objective (upper entries, as recorded by Ch(0,1) etc.)"""
+    dC = np.zeros((6, 6), np.float32)
+    dC[0, 1] = dC[0, 2] = dC[1, 2] = 1.0
+    for i in range(3):
+        dC[i, i] = -np.float32(beta ** it)
+    return dC
+
+
+OBJECTIVES = {"bulk": (lambda C, it: bulk_objective(C), lambda it: bulk_gradient()),
+              "npr": (npr_objective, npr_gradient)}
+
+
 class ConvergeChecker:
     """Stops when the relative objective change stays below thres for three
     consecutive iterations after iteration 11 (Framework.cuh:312-343)."""
@@ -50,9 +72,11 @@ class ConvergeChecker:
 def optimize_bulk(reso, vol=0.3, iters=50, seed=0, relthres=1e-2, filter_radius=2.0, step=0.05, damp=0.5,
                   sym="reflect6", finthres=5e-4, stop_on_converge=False, rho0=None, E=10.0, nu=0.3,
                   coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY, precision=PREC_REFINE, device=0,
-                  on_solve=None, stencil=STENCIL_FP16):
-    """The OC loop of testAutoDiff.cu:282-331 (bulk modulus); on_solve(hom, rho_phys)
-    is called after every solve (e.g. to record training pairs)."""
+                  on_solve=None, stencil=STENCIL_FP16, objective="bulk"):
+    """The OC loop of testAutoDiff.cu:282-331 (objective "bulk") or of
+    Framework.cu:208-272 ("npr"); on_solve(hom, rho_phys) is called after every
+    solve (e.g. to record training pairs)."""
+    obj_fn, grad_fn = OBJECTIVES[objective]
     import torch
 
     hom = Homogenization(reso, E, nu, coarse_mode, pin_mode, precision, device, stencil)
@@ -65,7 +89,6 @@ def optimize_bulk(reso, vol=0.3, iters=50, seed=0, relthres=1e-2, filter_radius=
     rhop = torch.empty_like(rho)
     sens = torch.empty_like(rho)
     oc = OCOptimizer(ne, 1e-3, step, damp, handle=hom)
-    dC = bulk_gradient()
     stream = torch.cuda.ExternalStream(hom.stream, device=dev)
     checker = ConvergeChecker(finthres)
     records = []
@@ -79,8 +102,8 @@ def optimize_bulk(reso, vol=0.3, iters=50, seed=0, relthres=1e-2, filter_radius=
         st = hom.last_stats
         if on_solve is not None:
             on_solve(hom, rhop)
-        obj = float(bulk_objective(C))
-        hom.Sensitivity(dC, sens)
+        obj = float(obj_fn(C, it))
+        hom.Sensitivity(grad_fn(it), sens)
         hom.penalize_backward(rho, sens, 3.0)
         done = checker.is_converge(it, obj)
         symmetrize(hom, sens, n, sym)
@@ -107,8 +130,9 @@ def main():
     p.add_argument("--vol", type=float, default=0.3)
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--relthres", type=float, default=1e-2)
+    p.add_argument("--objective", choices=sorted(OBJECTIVES), default="bulk")
     a = p.parse_args()
-    rho, C, rec = optimize_bulk(a.reso, a.vol, a.iters, a.seed, a.relthres)
+    rho, C, rec = optimize_bulk(a.reso, a.vol, a.iters, a.seed, a.relthres, objective=a.objective)
     print(json.dumps({"final_C": C.tolist(), "iterations": rec}))
 
 

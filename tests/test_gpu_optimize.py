@@ -4,16 +4,16 @@ import numpy as np
 import pytest
 
 import homo3d_b200 as H
-from homo3d_b200.optimize import bulk_gradient, bulk_objective, optimize_bulk
+from homo3d_b200.optimize import OBJECTIVES, bulk_gradient, bulk_objective, optimize_bulk
 from homo3d_b200.density import synthetic_density
 from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
 
-def oracle_loop(n, rho, iters, vol=0.3):
+def oracle_loop(n, rho, iters, vol=0.3, objective="bulk"):
+    obj_fn, grad_fn = OBJECTIVES[objective]
     objs = []
-    chi = None
     for it in range(iters):
         m = O.MG((n, n, n))
         m.set_density(rho ** 3)
@@ -21,8 +21,8 @@ def oracle_loop(n, rho, iters, vol=0.3):
         m.rhs()
         m.solve(1e-10, 400)
         C = m.elastic_matrix()
-        objs.append(bulk_objective(C))
-        s = m.sensitivity(bulk_gradient().astype(np.float64)) * 3 * rho ** 2
+        objs.append(obj_fn(C, it))
+        s = m.sensitivity(grad_fn(it).astype(np.float64)) * 3 * rho ** 2
         s = O.symmetrize_f32((n, n, n), s, "reflect6").astype(np.float64)
         s = O.filter_sens((n, n, n), s, rho, 2.0, False)
         rho, _ = O.oc_update(s, rho, vol, 1e-3, 0.05, 0.5)
@@ -30,11 +30,12 @@ def oracle_loop(n, rho, iters, vol=0.3):
     return rho, objs
 
 
-def test_oc_loop_matches_oracle(torch_cuda):
+@pytest.mark.parametrize("objective", ["bulk", "npr"])
+def test_oc_loop_matches_oracle(torch_cuda, objective):
     n = 16
     rho0 = synthetic_density(n, seed=5, vol=0.3).ravel().astype(np.float32).astype(np.float64)
-    rho, C, rec = optimize_bulk(n, iters=3, rho0=rho0, relthres=1e-8)
-    ref_rho, ref_objs = oracle_loop(n, rho0.copy(), 3)
+    rho, C, rec = optimize_bulk(n, iters=3, rho0=rho0, relthres=1e-8, objective=objective)
+    ref_rho, ref_objs = oracle_loop(n, rho0.copy(), 3, objective=objective)
     objs = [r["obj"] for r in rec]
     for a, b in zip(objs, ref_objs):
         assert abs(a - b) / abs(b) < 1e-4, (objs, ref_objs)
@@ -48,3 +49,16 @@ def test_oc_loop_improves_bulk_modulus(torch_cuda):
     assert objs[-1] < objs[0]  # obj = -bulk modulus decreases
     assert all(r["vcycles"] >= 1 for r in rec)
     assert rec[-1]["vcycles"] <= rec[0]["vcycles"]  # warm start pays off
+
+
+def test_npr_loop_lowers_poisson_coupling(torch_cuda):
+    torch = torch_cuda
+    n = 32
+    rho0 = synthetic_density(n, seed=2, vol=0.3).ravel()
+    hd = H.Homogenization(n)
+    hd.update(torch.tensor((rho0 ** 3).astype(np.float32), device="cuda"))
+    C0 = hd.elasticMatrix(1e-4)
+    hd.close()
+    rho, C, rec = optimize_bulk(n, iters=10, rho0=rho0, relthres=1e-2, objective="npr")
+    ratio = lambda c: (c[0, 1] + c[0, 2] + c[1, 2]) / (c[0, 0] + c[1, 1] + c[2, 2])
+    assert ratio(C) < ratio(C0)  # the coupling falls relative to the diagonal
