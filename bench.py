@@ -107,10 +107,12 @@ def dist_init(n):
 
 
 def max_over_ranks(dist, value):
+    """the largest value over the ranks (the job's time is its slowest rank's)"""
     if dist is None:
         return value
     import torch
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 

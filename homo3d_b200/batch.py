@@ -40,6 +40,40 @@ def make_designs(sizes, seed0=0, vol_range=(0.1, 0.5)):
     return out
 
 
+def shard(n_designs, rank, world):
+    """round-robin share of the designs for one rank (no exchange between ranks
+    until the final gather)"""
+    return list(range(rank, n_designs, world))
+
+
+def gather_designs(dist, n_designs, local_idx, local_rows):
+    """rows of every rank's designs in design order, on every rank (one object
+    all-gather; None without a process group)"""
+    if dist is None:
+        out = [None] * n_designs
+        for i, r in zip(local_idx, local_rows):
+            out[i] = r
+        return out
+    parts = [None] * dist.get_world_size()
+    dist.all_gather_object(parts, list(zip(local_idx, local_rows)))
+    out = [None] * n_designs
+    for part in parts:
+        for i, r in part:
+            out[i] = r
+    return out
+
+
+def max_over_ranks(dist, values):
+    """elementwise maximum of a list of floats over the ranks"""
+    if dist is None:
+        return list(values)
+    import torch
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor(list(values), dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
 def run_pass(torch, homs, rhos, tol, batched):
     """one pass over all designs from a zero start; returns (seconds, C [n,6,6], stats)"""
     for hd in homs:
@@ -71,10 +105,24 @@ def main():
     ap.add_argument("--repeat", type=int, default=3, help="timed passes per arm (after one untimed)")
     ap.add_argument("--device", type=int, default=0)
     args = ap.parse_args()
+    import os
+
     import torch
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    dist = None
+    if world > 1:  # one rank per GPU (torchrun); designs shard round-robin
+        import datetime
+
+        import torch.distributed as dist
+        args.device = int(os.environ.get("LOCAL_RANK", "0"))
+        torch.cuda.set_device(args.device)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     torch.cuda.set_device(args.device)
-    sizes = parse_sizes(args.sizes)
-    designs = make_designs(sizes)
+    sizes_all = parse_sizes(args.sizes)
+    mine = shard(len(sizes_all), rank, world)
+    sizes = [sizes_all[i] for i in mine]
+    designs = [make_designs(sizes_all)[i] for i in mine]
     prec = PREC_FP32 if args.precision == "fp32" else PREC_REFINE
     free0 = torch.cuda.mem_get_info()[0]
     homs = [Homogenization(n, precision=prec, device=args.device) for n in sizes]
@@ -86,16 +134,29 @@ def main():
         run_pass(torch, homs, rhos, args.tol, batched)  # graph captures, first-touch
         times, upd, Cs, stats = [], [], None, None
         for _ in range(args.repeat):
+            if dist is not None:
+                dist.barrier()
             dt, tu, Cs, stats = run_pass(torch, homs, rhos, args.tol, batched)
+            dt, tu = max_over_ranks(dist, [dt, tu])  # the job's pass ends with its slowest rank
             times.append(dt)
             upd.append(tu)
         k = int(np.argmin(times))
+        Cs = gather_designs(dist, len(sizes_all), mine, [c for c in Cs])
+        stats = gather_designs(dist, len(sizes_all), mine, stats)
         res[arm] = {"s_per_pass": times[k], "s_update": upd[k], "s_all": times, "C": Cs, "stats": stats}
+    for hd in homs:
+        hd.close()
+    if dist is not None:
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    sizes = sizes_all
     seq, bat = res["sequential"], res["batched"]
     rel = [float(np.abs(bat["C"][i] - seq["C"][i]).max() / np.abs(seq["C"][i]).max()) for i in range(len(sizes))]
     rep = {
         "workload": "%d designs (%s), 6 load cases, relthres %g, %s" % (len(sizes), args.sizes, args.tol,
                                                                         args.precision),
+        "n_gpus": world,
         "designs_per_s_batched": len(sizes) / bat["s_per_pass"],
         "designs_per_s_sequential": len(sizes) / seq["s_per_pass"],
         "speedup": seq["s_per_pass"] / bat["s_per_pass"],
@@ -106,11 +167,9 @@ def main():
         "vcycles": [s["vcycles"] for s in bat["stats"]],
         "vcycles_equal": [s["vcycles"] for s in bat["stats"]] == [s["vcycles"] for s in seq["stats"]],
         "status": [s["status"] for s in bat["stats"]],
-        "device_mem_gb": round(mem_gb, 2),
+        "device_mem_gb_rank0": round(mem_gb, 2),
     }
     print(json.dumps(rep), flush=True)
-    for hd in homs:
-        hd.close()
 
 
 if __name__ == "__main__":
