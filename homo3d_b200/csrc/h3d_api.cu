@@ -144,6 +144,7 @@ struct h3d_handle {
     Level lv[MAXLV];
     double ked[576];
     KeMat ke;
+    KeMat64 ke64;
     RhsTab rhs;
     std::vector<float> qhost;
     int nsub = 0;
@@ -297,7 +298,7 @@ int enqueue_refine(h3d_handle *h, bool exact) {
     const Level &L0 = h->lv[0];
     launch_update64(L0, h->u64, L0.u, h->pin_state + NF, s);
     cudaMemsetAsync(L0.u, 0, sizeof(float) * field_floats(L0.P.nv), s);
-    launch_fine_residual64(L0, h->rho, h->ke, h->f0, h->u64, L0.f, exact, s);
+    launch_fine_residual64(L0, h->rho, h->ke, h->ke64, h->f0, h->u64, L0.f, exact, s);
     const int nb = norm_blocks(L0.P);
     launch_weighted_norm(L0.P, L0.f, h->partial, nb, s);
     launch_norm_finish(h->partial, nb, h->d_small, s);
@@ -740,7 +741,10 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
     }
     // element matrix and derived tables
     element_matrix(cfg->youngs_modulus, cfg->poisson_ratio, h->ked);
-    for (int i = 0; i < 576; i++) h->ke.k[i] = (float)h->ked[i];
+    for (int i = 0; i < 576; i++) {
+        h->ke.k[i] = (float)h->ked[i];
+        h->ke64.k[i] = h->ked[i];
+    }
     for (int c = 0; c < NCASE; c++)
         for (int a = 0; a < 24; a++) {
             double s = 0;

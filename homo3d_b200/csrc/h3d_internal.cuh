@@ -132,6 +132,7 @@ __device__ __forceinline__ int color_of_index(const Planes &P, long long v) {
 #endif
 
 struct KeMat { float k[576]; };        // element matrix, row-major, FP32
+struct KeMat64 { double k[576]; };     // the same in FP64 (exact refinement residual)
 struct RhsTab { float g[NCASE][24]; }; // Ke * chi0_c for the six unit strains
 
 struct Level {
@@ -201,7 +202,8 @@ void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, dou
 int fine_residual_blocks(const Level &L);
 void launch_rhs(const Level &L, const float *rho, const RhsTab &g, float *f, cudaStream_t s);
 // r = f - K u with u in FP64, the operator in difference form (refined precision)
-void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const float *f, const double *u64,
+void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const KeMat64 &ke64, const float *f,
+                            const double *u64,
                             float *r, bool exact, cudaStream_t s);
 // u64 += e + T over the level-0 vertices but the pinned origin
 void launch_update64(const Level &L, double *u64, const float *e, const double *T, cudaStream_t s);

@@ -135,6 +135,32 @@ struct VertexGeo {
 #pragma unroll
             for (int c = 0; c < 3; ++c) A[3 * r + c] = ke.k[(3 * an + r) * 24 + 3 * bn + c] * cs[(1 << r) ^ (1 << c)];
     }
+    // the coupling block in FP64 from an FP64 element matrix (the exact refinement
+    // residual): the same mirror sums with FP64 densities and products
+    __device__ __forceinline__ void block64(const KeMat64 &ke, int d, double A[9]) const {
+        const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
+        const int w0 = first_shared(d);
+        double cs[8];
+#pragma unroll
+        for (int m = 0; m < 8; ++m) cs[m] = 0.0;
+#pragma unroll
+        for (int w = 0; w < 8; ++w) {
+            const int bx = 1 - (w & 1) + dx, by = 1 - ((w >> 1) & 1) + dy, bz = 1 - (w >> 2) + dz;
+            if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
+            const int mir = w ^ w0;
+#pragma unroll
+            for (int m = 0; m < 8; ++m) {
+                if (m != 0 && m != 3 && m != 5 && m != 6) continue;
+                cs[m] += (__popc(mir & m) & 1) ? -(double)rw[w] : (double)rw[w];
+            }
+        }
+        const int an = 7 - w0;
+        const int bn = (1 - (w0 & 1) + dx) + 2 * (1 - ((w0 >> 1) & 1) + dy) + 4 * (1 - (w0 >> 2) + dz);
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) A[3 * r + c] = ke.k[(3 * an + r) * 24 + 3 * bn + c] * cs[(1 << r) ^ (1 << c)];
+    }
     // index of neighbour d in its colour plane set, and whether it is the pinned origin
     __device__ __forceinline__ unsigned nbr(const FineArgs &a, int d, int &Kn, bool &pinned) const {
         const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
@@ -322,7 +348,7 @@ __global__ void __launch_bounds__(FBS, 6) k_fine_residual(FineArgs a, const __gr
 // nonzero value only translates the solution.  EXACT accumulates the products in
 // FP64 too (the FP32-product form floors near 1e-6 of ||f||, independent of N).
 template <int K, bool EXACT>
-__device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const KeMat &ke,
+__device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const KeMat &ke, const KeMat64 &ke64,
                                                        const double *__restrict__ u64, long long p, int cb) {
     const long long me = (long long)K * a.P + p;
     if (K == 7 && p == 0) {
@@ -345,17 +371,30 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
         int Kn;
         bool pinned;
         const unsigned nid = g.nbr(a, d, Kn, pinned);
-        float A[9];
-        g.block(ke, d, A);
+        // EXACT: the block in FP64 (FP64 element matrix and densities, FP64
+        // products): no per-entry FP32-to-FP64 conversions, which run on the narrow
+        // conversion pipe; otherwise the FP32 block of the V-cycle operator
+        Acc A[9];
+        if (EXACT) {
+            double A64[9];
+            g.block64(ke64, d, A64);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) A[k] = (Acc)A64[k];
+        } else {
+            float A32[9];
+            g.block(ke, d, A32);
+#pragma unroll
+            for (int k = 0; k < 9; ++k) A[k] = (Acc)A32[k];
+        }
         const double *up = u64 + nid + (long long)(3 * cb) * a.nv;
 #pragma unroll
         for (int c = 0; c < CPT; ++c) {
             const Acc d0 = (Acc)(__ldg(up + (3 * c) * a.nv) - uv[3 * c]);
             const Acc d1 = (Acc)(__ldg(up + (3 * c + 1) * a.nv) - uv[3 * c + 1]);
             const Acc d2 = (Acc)(__ldg(up + (3 * c + 2) * a.nv) - uv[3 * c + 2]);
-            acc[3 * c + 0] = fma((Acc)A[0], d0, fma((Acc)A[1], d1, fma((Acc)A[2], d2, acc[3 * c + 0])));
-            acc[3 * c + 1] = fma((Acc)A[3], d0, fma((Acc)A[4], d1, fma((Acc)A[5], d2, acc[3 * c + 1])));
-            acc[3 * c + 2] = fma((Acc)A[6], d0, fma((Acc)A[7], d1, fma((Acc)A[8], d2, acc[3 * c + 2])));
+            acc[3 * c + 0] = fma(A[0], d0, fma(A[1], d1, fma(A[2], d2, acc[3 * c + 0])));
+            acc[3 * c + 1] = fma(A[3], d0, fma(A[4], d1, fma(A[5], d2, acc[3 * c + 1])));
+            acc[3 * c + 2] = fma(A[6], d0, fma(A[7], d1, fma(A[8], d2, acc[3 * c + 2])));
         }
     }
 #pragma unroll
@@ -367,20 +406,21 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
 
 template <bool EXACT>
 __global__ void __launch_bounds__(FBS, 4) k_fine_residual64(FineArgs a, const __grid_constant__ KeMat ke,
+                                                         const __grid_constant__ KeMat64 ke64,
                                                          const double *__restrict__ u64) {
     long long p;
     int cb;
     thread_task<CPT>(p, cb);
     if (p >= a.P) return;
     switch (blockIdx.y) {
-    case 0: fine_residual64_vertex<0, EXACT>(a, ke, u64, p, cb); break;
-    case 1: fine_residual64_vertex<1, EXACT>(a, ke, u64, p, cb); break;
-    case 2: fine_residual64_vertex<2, EXACT>(a, ke, u64, p, cb); break;
-    case 3: fine_residual64_vertex<3, EXACT>(a, ke, u64, p, cb); break;
-    case 4: fine_residual64_vertex<4, EXACT>(a, ke, u64, p, cb); break;
-    case 5: fine_residual64_vertex<5, EXACT>(a, ke, u64, p, cb); break;
-    case 6: fine_residual64_vertex<6, EXACT>(a, ke, u64, p, cb); break;
-    default: fine_residual64_vertex<7, EXACT>(a, ke, u64, p, cb); break;
+    case 0: fine_residual64_vertex<0, EXACT>(a, ke, ke64, u64, p, cb); break;
+    case 1: fine_residual64_vertex<1, EXACT>(a, ke, ke64, u64, p, cb); break;
+    case 2: fine_residual64_vertex<2, EXACT>(a, ke, ke64, u64, p, cb); break;
+    case 3: fine_residual64_vertex<3, EXACT>(a, ke, ke64, u64, p, cb); break;
+    case 4: fine_residual64_vertex<4, EXACT>(a, ke, ke64, u64, p, cb); break;
+    case 5: fine_residual64_vertex<5, EXACT>(a, ke, ke64, u64, p, cb); break;
+    case 6: fine_residual64_vertex<6, EXACT>(a, ke, ke64, u64, p, cb); break;
+    default: fine_residual64_vertex<7, EXACT>(a, ke, ke64, u64, p, cb); break;
     }
 }
 
@@ -468,13 +508,14 @@ void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, dou
     k_fine_residual<7><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
 }
 
-void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const float *f, const double *u64,
+void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const KeMat64 &ke64, const float *f,
+                            const double *u64,
                             float *r, bool exact, cudaStream_t s) {
     FineArgs a = make_args(L, rho);
     a.f = f;
     a.r = r;
-    if (exact) k_fine_residual64<true><<<dim3(task_blocks(a, CPT), 8), FBS, 0, s>>>(a, ke, u64);
-    else k_fine_residual64<false><<<dim3(task_blocks(a, CPT), 8), FBS, 0, s>>>(a, ke, u64);
+    if (exact) k_fine_residual64<true><<<dim3(task_blocks(a, CPT), 8), FBS, 0, s>>>(a, ke, ke64, u64);
+    else k_fine_residual64<false><<<dim3(task_blocks(a, CPT), 8), FBS, 0, s>>>(a, ke, ke64, u64);
 }
 
 void launch_rhs(const Level &L, const float *rho, const RhsTab &g, float *f, cudaStream_t s) {
