@@ -420,8 +420,8 @@ struct SolveRun {
 
     bool selected(int c) const { return ((mask >> c) & 1) != 0; }
     bool finished() const { return pending == P_DONE; }
-    long long n18() const { return (long long)NF * h->lv[0].P.nv; }      // FP64 planar field
-    long long nf32() const { return field_floats(h->lv[0].P.nv); }     // FP32 blocked field
+    long long n18() const { return field_floats(h->lv[0].P.nv); }      // elements of an FP64 field
+    long long nf32() const { return field_floats(h->lv[0].P.nv); }     // elements of an FP32 field
 
     int reset_solution() {
         if (refine) CK(cudaMemsetAsync(h->u64, 0, sizeof(double) * n18(), h->stream));
@@ -627,11 +627,10 @@ int factor_coarsest_check(h3d_handle *h) {
 int elastic_prepare(h3d_handle *h) {
     Level &L = h->lv[0];
     cudaStream_t s = h->stream;
-    const long long n18 = (long long)NF * L.P.nv;
     const int nb = norm_blocks(L.P);
     if (h->refine()) {
         launch_rhs(L, h->rho, h->rhs, h->f0, s);
-        CK(cudaMemcpyAsync(h->u64, h->chi, sizeof(double) * n18, cudaMemcpyDeviceToDevice, s));
+        CK(cudaMemcpyAsync(h->u64, h->chi, sizeof(double) * field_floats(L.P.nv), cudaMemcpyDeviceToDevice, s));
         launch_remove_mean64(L.P, h->u64, h->partial, nb, s);
     } else {
         launch_rhs(L, h->rho, h->rhs, L.f, s);
@@ -648,8 +647,8 @@ int elastic_prepare(h3d_handle *h) {
 int elastic_enqueue_energy(h3d_handle *h) {
     Level &L = h->lv[0];
     cudaStream_t s = h->stream;
-    const long long n18 = (long long)NF * L.P.nv;
-    if (h->refine()) CK(cudaMemcpyAsync(h->chi, h->u64, sizeof(double) * n18, cudaMemcpyDeviceToDevice, s));
+    if (h->refine())
+        CK(cudaMemcpyAsync(h->chi, h->u64, sizeof(double) * field_floats(L.P.nv), cudaMemcpyDeviceToDevice, s));
     else launch_convert_field(L.P.nv, L.u, h->chi, s);
     int nsm = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
@@ -731,11 +730,11 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
     }
     const long long nv0 = h->lv[0].P.nv;
     CK(cudaMalloc(&h->rho, sizeof(float) * nv0));
-    CK(cudaMalloc(&h->chi, sizeof(double) * NF * nv0));
-    CK(cudaMemset(h->chi, 0, sizeof(double) * NF * nv0));
+    CK(cudaMalloc(&h->chi, sizeof(double) * field_floats(nv0)));
+    CK(cudaMemset(h->chi, 0, sizeof(double) * field_floats(nv0)));
     if (h->refine()) {
-        CK(cudaMalloc(&h->u64, sizeof(double) * NF * nv0));
-        CK(cudaMemset(h->u64, 0, sizeof(double) * NF * nv0));
+        CK(cudaMalloc(&h->u64, sizeof(double) * field_floats(nv0)));
+        CK(cudaMemset(h->u64, 0, sizeof(double) * field_floats(nv0)));
         CK(cudaMalloc(&h->f0, sizeof(float) * field_floats(nv0)));
         CK(cudaMemset(h->f0, 0, sizeof(float) * field_floats(nv0)));
     }
@@ -1016,7 +1015,7 @@ int h3d_set_tuning(h3d_handle *h, int level, int gs_shape, int res_shape) {
 
 int h3d_reset_solutions(h3d_handle *h) {
     if (!h) return H3D_ERR_ARG;
-    CK(cudaMemsetAsync(h->chi, 0, sizeof(double) * NF * h->lv[0].P.nv, h->stream));
+    CK(cudaMemsetAsync(h->chi, 0, sizeof(double) * field_floats(h->lv[0].P.nv), h->stream));
     return H3D_OK;
 }
 

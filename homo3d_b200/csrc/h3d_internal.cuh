@@ -2,9 +2,8 @@
 //
 // Layout in HBM (every level):
 //   A vertex field holds the six load cases and three components as 18 planes
-//   (q = 3c + m for case c, component m).  FP32 fields interleave the planes in
-//   blocks of 128 vertices, value(q, v) = field[fidx(q, v)]; FP64 fields are
-//   planar, value(q, v) = field[q * nv + v].
+//   (q = 3c + m for case c, component m), interleaved in blocks of 128
+//   vertices: value(q, v) = field[fidx(q, v)] (FP32 and FP64 fields alike).
 //   Vertices are ordered by Gauss-Seidel colour, then lexicographically inside
 //   the colour: a vertex (x,y,z) has colour k = ((x+1)&1) | ((y+1)&1)<<1 |
 //   ((z+1)&1)<<2 (the reference's padded-position parity, grid.cu:143-200) and
@@ -28,12 +27,11 @@ constexpr int NCHUNK = 31;      // uint4 chunks per stencil (243 halves -> 248)
 constexpr int NCHUNK32 = 61;    // the same with FP32 entries (243 floats -> 244)
 constexpr float RHO_PENAL_MIN = 1e-9f;  // grid.h:425
 
-// FP32 vertex fields (u, f, r of every level): the 18 planes interleaved in
-// blocks of FVB vertices, value(plane q, vertex v) at fidx(q, v); the planes a
-// thread reads for one vertex are then immediate offsets from one address.  A
-// field holds field_floats(nv) floats (nv rounded up to a multiple of FVB).  The
-// FP64 fields (the refined solution, the stored solutions chi) stay planar:
-// value(q, v) at q * nv + v.
+// Vertex fields (u, f, r of every level in FP32; the refined solution and the
+// stored solutions chi in FP64): the 18 planes interleaved in blocks of FVB
+// vertices, value(plane q, vertex v) at fidx(q, v); the planes a thread reads for
+// one vertex are then immediate offsets from one address.  A field holds
+// field_floats(nv) elements (nv rounded up to a multiple of FVB).
 constexpr int FVB = 128;
 static_assert(FVB == 128, "fidx shifts by log2(FVB) = 7");
 __host__ __device__ inline long long fidx(int q, long long v) {
@@ -214,7 +212,7 @@ void launch_pin_deflate(const Level &L, const float *rho, const KeMat &ke, doubl
 void launch_pin_init(const Level &L, const double *sums, double *state, cudaStream_t s);
 // FP32 solutions: u += T (but the origin), f restored near the origin, T = 0
 void launch_pin_fold(const Level &L, const float *rho, const KeMat &ke, double *state, cudaStream_t s);
-// FP32 blocked field of nv vertices <-> FP64 planar field
+// FP32 field of nv vertices <-> FP64 field
 void launch_convert_field(long long nv, const float *src, double *dst, cudaStream_t s);
 void launch_convert_field(long long nv, const double *src, float *dst, cudaStream_t s);
 void launch_remove_mean64(const Planes &P, double *v, double *partial, int nblk, cudaStream_t s);

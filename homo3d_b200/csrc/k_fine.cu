@@ -357,10 +357,10 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
         return;
     }
     const VertexGeo<K> g(a, p);
-    const double *uvp = u64 + me + (long long)(3 * cb) * a.nv;
+    const double *uvp = u64 + fidx(3 * cb, me);
     double uv[3 * CPT];
 #pragma unroll
-    for (int q = 0; q < 3 * CPT; ++q) uv[q] = __ldg(uvp + q * a.nv);
+    for (int q = 0; q < 3 * CPT; ++q) uv[q] = __ldg(uvp + q * FVB);
     using Acc = typename std::conditional<EXACT, double, float>::type;
     Acc acc[3 * CPT];
 #pragma unroll
@@ -386,12 +386,12 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
 #pragma unroll
             for (int k = 0; k < 9; ++k) A[k] = (Acc)A32[k];
         }
-        const double *up = u64 + nid + (long long)(3 * cb) * a.nv;
+        const double *up = u64 + fidx(3 * cb, nid);  // planes 3cb.. of the neighbour, FVB apart
 #pragma unroll
         for (int c = 0; c < CPT; ++c) {
-            const Acc d0 = (Acc)(__ldg(up + (3 * c) * a.nv) - uv[3 * c]);
-            const Acc d1 = (Acc)(__ldg(up + (3 * c + 1) * a.nv) - uv[3 * c + 1]);
-            const Acc d2 = (Acc)(__ldg(up + (3 * c + 2) * a.nv) - uv[3 * c + 2]);
+            const Acc d0 = (Acc)(__ldg(up + (3 * c) * FVB) - uv[3 * c]);
+            const Acc d1 = (Acc)(__ldg(up + (3 * c + 1) * FVB) - uv[3 * c + 1]);
+            const Acc d2 = (Acc)(__ldg(up + (3 * c + 2) * FVB) - uv[3 * c + 2]);
             acc[3 * c + 0] = fma(A[0], d0, fma(A[1], d1, fma(A[2], d2, acc[3 * c + 0])));
             acc[3 * c + 1] = fma(A[3], d0, fma(A[4], d1, fma(A[5], d2, acc[3 * c + 1])));
             acc[3 * c + 2] = fma(A[6], d0, fma(A[7], d1, fma(A[8], d2, acc[3 * c + 2])));
@@ -532,7 +532,8 @@ __global__ void k_update64(long long nv, double *u, const float *__restrict__ e,
     if (i >= nv * NF) return;
     const long long v = i % nv, q = i / nv;
     if (v == pin) return;
-    u[i] += (double)e[fidx((int)q, v)] + T[q];
+    const long long o = fidx((int)q, v);
+    u[o] += (double)e[o] + T[q];
 }
 
 // ---- rigid-translation deflation of the pinned problem -------------------------
@@ -655,15 +656,21 @@ __global__ void k_pin_restore_f(FineArgs a, const __grid_constant__ KeMat ke, do
     for (int i = 0; i < NF; ++i) state[NF + i] = 0.0;
 }
 
-// FP32 blocked field <-> FP64 planar field (q * nv + v)
+// FP32 field <-> FP64 field (both blocked)
 __global__ void k_f32_to_f64(long long nv, const float *__restrict__ s, double *d) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < nv * NF) d[i] = (double)s[fidx((int)(i / nv), i % nv)];
+    if (i < nv * NF) {
+        const long long o = fidx((int)(i / nv), i % nv);
+        d[o] = (double)s[o];
+    }
 }
 
 __global__ void k_f64_to_f32(long long nv, const double *__restrict__ s, float *d) {
     const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < nv * NF) d[fidx((int)(i / nv), i % nv)] = (float)s[i];
+    if (i < nv * NF) {
+        const long long o = fidx((int)(i / nv), i % nv);
+        d[o] = (float)s[o];
+    }
 }
 
 void launch_update64(const Level &L, double *u64, const float *e, const double *T, cudaStream_t s) {
@@ -694,7 +701,7 @@ __global__ void __launch_bounds__(256) k_sum18_64(long long nv, const double *__
     for (int q = 0; q < NF; ++q) s[q] = 0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < nv; i += (long long)gridDim.x * blockDim.x)
 #pragma unroll
-        for (int q = 0; q < NF; ++q) s[q] += v[q * nv + i];
+        for (int q = 0; q < NF; ++q) s[q] += v[fidx(q, i)];
     block_reduce<NF>(s, partial, blockIdx.x);
 }
 
@@ -713,7 +720,7 @@ __global__ void k_sub_mean64(long long nv, double *v, const double *__restrict__
     if (i >= nv) return;
     const double inv = 1.0 / (double)nv;
 #pragma unroll
-    for (int q = 0; q < NF; ++q) v[q * nv + i] -= sum18[q] * inv;
+    for (int q = 0; q < NF; ++q) v[fidx(q, i)] -= sum18[q] * inv;
 }
 
 void launch_remove_mean64(const Planes &P, double *v, double *partial, int nblk, cudaStream_t s) {

@@ -191,11 +191,11 @@ __global__ void __launch_bounds__(TC_M) k_energy_tc(Planes P, const double *__re
             float U[TC_K];
 #pragma unroll
             for (int m = 0; m < 3; ++m) {
-                const double *cp = chi + (long long)(3 * j + m) * P.nv;
-                const double c0 = valid ? __ldg(cp + vtx[0]) : 0.0;
+                const double c0 = valid ? __ldg(chi + fidx(3 * j + m, vtx[0])) : 0.0;
 #pragma unroll
                 for (int a = 0; a < 8; ++a)
-                    U[3 * a + m] = valid ? tc_macro_disp(a, j, m) - (float)(__ldg(cp + vtx[a]) - c0) : 0.f;
+                    U[3 * a + m] = valid ? tc_macro_disp(a, j, m) - (float)(__ldg(chi + fidx(3 * j + m, vtx[a])) - c0)
+                                         : 0.f;
             }
 #pragma unroll
             for (int k4 = 0; k4 < TC_K / 4; ++k4) {

@@ -308,7 +308,7 @@ __global__ void k_wn_to_chi(Planes P, const float *__restrict__ y, int R, double
         float a = 0.f;
 #pragma unroll
         for (int t = 0; t < 8; ++t) a = fmaf(w[t], y[(long long)q * R3 + idx[t]], a);
-        chi[(long long)q * P.nv + v] = (double)N * (double)a;
+        chi[fidx(q, v)] = (double)N * (double)a;
     }
 }
 
