@@ -1096,6 +1096,12 @@ int h3d_batch_elastic_matrix(h3d_handle *const *hs, int n, double tol, double *C
         for (int i = 0; i < n; i++) {
             if (!live[i]) continue;
             h3d_handle *h = hs[i];
+            if (cudaSetDevice(h->device) != cudaSuccess) {  // the handles may sit on different GPUs
+                st[i] = fail(h, H3D_ERR_CUDA, "cudaSetDevice failed");
+                live[i] = 0;
+                nlive--;
+                continue;
+            }
             cudaError_t q = cudaStreamQuery(h->stream);
             if (q == cudaErrorNotReady) continue;
             progressed = true;
