@@ -117,6 +117,11 @@ def max_over_ranks(dist, value):
     return float(t.item())
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the eight colour
+# launches of one fine sweep, from an ncu capture of this bench's workload: every
+# colour launch reads the whole u field (it exceeds L2), 3.4x the algorithmic bytes
+SWEEP_TRAFFIC_BYTES = {256: 12_580_000_000}
+
 PRECISION_NAME = {0: "FP32 V-cycles on the correction of an FP64 solution (iterative refinement)",
                   1: "FP32 solution (the reference's scheme)"}
 
@@ -265,7 +270,9 @@ def gpu_arm(args):
                                 for c, r in zip(cycles, refs)),
             "roofline": {"kernel": "k_fine_gs (8 colour launches = one sweep)", "bound": "hbm",
                          "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
-                         "frac": round(achieved / peaks.get("hbm_gbs"), 4), "traffic": None,
+                         "frac": round(achieved / peaks.get("hbm_gbs"), 4),
+                         "traffic": SWEEP_TRAFFIC_BYTES.get(args.reso) if args.precision == 0 else None,
+                         "traffic_unit": "bytes of DRAM read + write per sweep (ncu capture)",
                          "sweep_ms": round(sweep_ms, 4), "fp32_tflops": round(flops_sweep / sweep_ms / 1e9, 2),
                          "peak_source": "measured" if "when" in peaks else "fallback"},
             "clocks": clk,
