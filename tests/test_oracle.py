@@ -1,5 +1,5 @@
 """CPU tests of the FP64 oracle: pins it to the reference's hard-coded tables and
-to analytic known answers before it is used to judge the CUDA library."""
+to analytic known answers before it is used to check the CUDA library."""
 import json
 import os
 
