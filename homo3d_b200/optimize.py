@@ -131,8 +131,13 @@ def main():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--relthres", type=float, default=1e-2)
     p.add_argument("--objective", choices=sorted(OBJECTIVES), default="bulk")
+    p.add_argument("--out-density", default="", help="write the final density in the binary voxel format")
     a = p.parse_args()
     rho, C, rec = optimize_bulk(a.reso, a.vol, a.iters, a.seed, a.relthres, objective=a.objective)
+    if a.out_density:
+        from .voxelio import write_density
+        n = round(rho.size ** (1 / 3))
+        write_density(a.out_density, rho, (n, n, n))
     print(json.dumps({"final_C": C.tolist(), "iterations": rec}))
 
 
