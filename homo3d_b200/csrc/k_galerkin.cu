@@ -158,61 +158,82 @@ __device__ __forceinline__ double hat_w(int ox, int oy, int oz, int r0, int r1, 
     return (double)((r0 - ox) * (r1 - oy) * (r2 - oz)) / (double)(r0 * r1 * r2);
 }
 
-// one thread per (coarse vertex offset vi in {-1,0,1}^3, neighbour d)
+// one CTA per (coarse vertex offset vi in {-1,0,1}^3, neighbour d); its threads
+// share the fine elements of the (2r)^3 box around the neighbour (one each for
+// ratio 2 and 4, a fixed strided set above that) and the contributions are summed
+// in a fixed tree order
+constexpr int PATCH_MAX_THREADS = 512;
 template <bool F32>
-__global__ void k_dirichlet_patch(Planes F, Planes C, int r0, int r1, int r2, const float *__restrict__ rho,
-                                  const double *__restrict__ ked, int pin_identity, uint4 *st) {
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= 27 * 27) return;
-    const int vi = t / 27, d = t % 27;
+__global__ void __launch_bounds__(PATCH_MAX_THREADS) k_dirichlet_patch(Planes F, Planes C, int r0, int r1, int r2,
+                                                                       const float *__restrict__ rho,
+                                                                       const double *__restrict__ ked, int pin_identity,
+                                                                       uint4 *st) {
+    __shared__ double red[PATCH_MAX_THREADS][9];
+    const int vi = blockIdx.x / 27, d = blockIdx.x % 27;
     const int vio[3] = {(vi % 3 - 1), (vi / 3 % 3 - 1), (vi / 9 - 1)};
     const int pi[3] = {vio[0] * r0, vio[1] * r1, vio[2] * r2};
     const int pj[3] = {pi[0] + (d % 3 - 1) * r0, pi[1] + (d / 3 % 3 - 1) * r1, pi[2] + (d / 9 - 1) * r2};
+    const int tid = threadIdx.x;
     double s[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    for (int ex = -r0; ex < r0; ex++)
-        for (int ey = -r1; ey < r1; ey++)
-            for (int ez = -r2; ez < r2; ez++) {
-                const int ep[3] = {pj[0] + ex, pj[1] + ey, pj[2] + ez};
-                const int eo[3] = {ep[0] - pi[0], ep[1] - pi[1], ep[2] - pi[2]};
-                if (eo[0] >= r0 || eo[0] < -r0 || eo[1] >= r1 || eo[1] < -r1 || eo[2] >= r2 || eo[2] < -r2) continue;
-                const long long fe =
-                    modp(ep[0], F.n[0]) + (long long)F.n[0] * (modp(ep[1], F.n[1]) + (long long)F.n[1] * modp(ep[2], F.n[2]));
-                const double rp = 1e-9 + (double)rho[fe];
-                for (int a = 0; a < 8; a++) {
-                    const int ap[3] = {ep[0] + (a & 1), ep[1] + ((a >> 1) & 1), ep[2] + (a >> 2)};
-                    const double wi = hat_w(ap[0] - pi[0], ap[1] - pi[1], ap[2] - pi[2], r0, r1, r2);
-                    if (wi == 0) continue;
-                    const bool ad = ap[0] == 0 && ap[1] == 0 && ap[2] == 0;
-                    for (int b = 0; b < 8; b++) {
-                        const int bp[3] = {ep[0] + (b & 1), ep[1] + ((b >> 1) & 1), ep[2] + (b >> 2)};
-                        const double wj = hat_w(bp[0] - pj[0], bp[1] - pj[1], bp[2] - pj[2], r0, r1, r2);
-                        if (wj == 0) continue;
-                        const bool bd = bp[0] == 0 && bp[1] == 0 && bp[2] == 0;
-                        if (ad || bd) {
-                            if (a == b && pin_identity)
-                                for (int i = 0; i < 3; i++) s[4 * i] += wi * wj;
-                        } else {
-                            for (int i = 0; i < 3; i++)
-                                for (int j = 0; j < 3; j++) s[3 * i + j] += wi * wj * rp * ked[(3 * a + i) * 24 + 3 * b + j];
-                        }
-                    }
+    for (int e = tid; e < 8 * r0 * r1 * r2; e += blockDim.x) {  // this thread's elements, in order
+    const int ex = e % (2 * r0) - r0, ey = (e / (2 * r0)) % (2 * r1) - r1, ez = e / (4 * r0 * r1) - r2;
+    const int ep[3] = {pj[0] + ex, pj[1] + ey, pj[2] + ez};
+    const int eo[3] = {ep[0] - pi[0], ep[1] - pi[1], ep[2] - pi[2]};
+    if (!(eo[0] >= r0 || eo[0] < -r0 || eo[1] >= r1 || eo[1] < -r1 || eo[2] >= r2 || eo[2] < -r2)) {
+        const long long fe =
+            modp(ep[0], F.n[0]) + (long long)F.n[0] * (modp(ep[1], F.n[1]) + (long long)F.n[1] * modp(ep[2], F.n[2]));
+        const double rp = 1e-9 + (double)rho[fe];
+        for (int a = 0; a < 8; a++) {
+            const int ap[3] = {ep[0] + (a & 1), ep[1] + ((a >> 1) & 1), ep[2] + (a >> 2)};
+            const double wi = hat_w(ap[0] - pi[0], ap[1] - pi[1], ap[2] - pi[2], r0, r1, r2);
+            if (wi == 0) continue;
+            const bool ad = ap[0] == 0 && ap[1] == 0 && ap[2] == 0;
+            for (int b = 0; b < 8; b++) {
+                const int bp[3] = {ep[0] + (b & 1), ep[1] + ((b >> 1) & 1), ep[2] + (b >> 2)};
+                const double wj = hat_w(bp[0] - pj[0], bp[1] - pj[1], bp[2] - pj[2], r0, r1, r2);
+                if (wj == 0) continue;
+                const bool bd = bp[0] == 0 && bp[1] == 0 && bp[2] == 0;
+                if (ad || bd) {
+                    if (a == b && pin_identity)
+                        for (int i = 0; i < 3; i++) s[4 * i] += wi * wj;
+                } else {
+                    for (int i = 0; i < 3; i++)
+                        for (int j = 0; j < 3; j++) s[3 * i + j] += wi * wj * rp * ked[(3 * a + i) * 24 + 3 * b + j];
                 }
             }
+        }
+    }
+    }
+#pragma unroll
+    for (int k = 0; k < 9; k++) red[tid][k] = s[k];
+    __syncthreads();
+    for (int half = blockDim.x / 2; half > 0; half /= 2) {  // blockDim.x is a power of two
+        if (tid < half)
+#pragma unroll
+            for (int k = 0; k < 9; k++) red[tid][k] += red[tid + half][k];
+        __syncthreads();
+    }
+    if (tid != 0) return;
+    double t[9];
+#pragma unroll
+    for (int k = 0; k < 9; k++) t[k] = red[0][k];
     if (d == 13)
         for (int i = 0; i < 3; i++)
-            if (fabs(s[4 * i]) < 1e-4) s[4 * i] = 1e-4;
+            if (fabs(t[4 * i]) < 1e-4) t[4 * i] = 1e-4;
     const long long v = vidx(C, modp(vio[0], C.n[0]), modp(vio[1], C.n[1]), modp(vio[2], C.n[2]));
-    for (int e = 0; e < 9; e++) StencilStore<F32>::putd(st, C.nv, v, 9 * d + e, s[e]);
+    for (int e = 0; e < 9; e++) StencilStore<F32>::putd(st, C.nv, v, 9 * d + e, t[e]);
 }
 
 void launch_dirichlet_patch(const Level &F, const Level &C, const float *rho, const double *ked, int pin_identity,
                             cudaStream_t s) {
+    int nt = 8 * C.ratio[0] * C.ratio[1] * C.ratio[2];  // (2r)^3 elements, a power of two
+    if (nt > PATCH_MAX_THREADS) nt = PATCH_MAX_THREADS;
     if (C.st32)
-        k_dirichlet_patch<true><<<(27 * 27 + 127) / 128, 128, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2],
-                                                                      rho, ked, pin_identity, C.st);
+        k_dirichlet_patch<true><<<27 * 27, nt, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], rho, ked,
+                                                       pin_identity, C.st);
     else
-        k_dirichlet_patch<false><<<(27 * 27 + 127) / 128, 128, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2],
-                                                                       rho, ked, pin_identity, C.st);
+        k_dirichlet_patch<false><<<27 * 27, nt, 0, s>>>(F.P, C.P, C.ratio[0], C.ratio[1], C.ratio[2], rho, ked,
+                                                        pin_identity, C.st);
 }
 
 // ---- deeper levels: R A P from the finer stencil -----------------------------------
