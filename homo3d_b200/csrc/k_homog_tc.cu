@@ -35,7 +35,7 @@ constexpr int TC_M = 128;             // elements per tile (= threads per CTA = 
 constexpr int TC_K = 24;              // element DOFs
 constexpr int TC_TILE_BYTES = TC_M * TC_K * 4;       // one 128 x 24 TF32 operand tile
 constexpr int TC_B_BYTES = TC_K * TC_K * 4;          // Ke as a 24 x 24 TF32 tile
-constexpr int TC_SMEM_USED = 2 * TC_TILE_BYTES + 2 * TC_B_BYTES + 64;
+constexpr int TC_SMEM_USED = 4 * TC_TILE_BYTES + 2 * TC_B_BYTES + 64;  // A hi/lo double-buffered, B hi/lo
 constexpr int TC_SMEM_REQUEST = 100 * 1024;          // > 227 KB / 3: at most two CTAs per SM
 constexpr int TC_TMEM_COLS = 256;                    // 6 x 24 FP32 accumulator columns, rounded up
 constexpr long long TC_WAIT_LIMIT = 1ll << 24;       // mbarrier polls before giving up
@@ -129,10 +129,10 @@ __global__ void __launch_bounds__(TC_M) k_energy_tc(Planes P, const double *__re
                                                     double *partial, TcDc dc, float *sens, int pitch, int *flag) {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     unsigned char *base = tc_smem + ((1024 - (smem_u32(tc_smem) & 1023)) & 1023);
-    unsigned char *Ahi = base, *Alo = base + TC_TILE_BYTES;
-    unsigned char *Bhi = base + 2 * TC_TILE_BYTES, *Blo = Bhi + TC_B_BYTES;
-    uint64_t *bar = reinterpret_cast<uint64_t *>(Blo + TC_B_BYTES);
-    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 1);
+    // A operand buffers b = 0, 1: hi at base + 2 b TILE, lo at base + (2 b + 1) TILE
+    unsigned char *Bhi = base + 4 * TC_TILE_BYTES, *Blo = Bhi + TC_B_BYTES;
+    uint64_t *bar = reinterpret_cast<uint64_t *>(Blo + TC_B_BYTES);  // one mbarrier per A buffer
+    uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
     const int tid = threadIdx.x, warp = tid >> 5;
 
     // Ke split into TF32 hi + lo, as the 24 x 24 B operand (B[n][k] = Ke[n][k])
@@ -144,6 +144,7 @@ __global__ void __launch_bounds__(TC_M) k_energy_tc(Planes P, const double *__re
     }
     if (tid == 0) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar)) : "memory");
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(bar + 1)) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     if (warp == 0) {
@@ -157,12 +158,12 @@ __global__ void __launch_bounds__(TC_M) k_energy_tc(Planes P, const double *__re
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = *tslot;
     const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
-    const uint32_t sAhi = smem_u32(Ahi), sAlo = smem_u32(Alo), sBhi = smem_u32(Bhi), sBlo = smem_u32(Blo);
+    const uint32_t sA = smem_u32(base), sBhi = smem_u32(Bhi), sBlo = smem_u32(Blo);
 
     double acc[21];
 #pragma unroll
     for (int t = 0; t < 21; ++t) acc[t] = 0;
-    uint32_t phase = 0;
+    uint32_t phase[2] = {0, 0};
     bool ok = true;
     const long long ntile = (P.nv + TC_M - 1) / TC_M;
     for (long long tile = blockIdx.x; tile < ntile && ok; tile += gridDim.x) {
@@ -183,12 +184,9 @@ __global__ void __launch_bounds__(TC_M) k_energy_tc(Planes P, const double *__re
             const int vz = (a >> 2) ? (z + 1 == P.n[2] ? 0 : z + 1) : z;
             vtx[a] = vidx(P, vx, vy, vz);
         }
-        float E[21];
-#pragma unroll
-        for (int j = 0; j < NCASE; ++j) {
-            if (!ok) continue;
-            // 1. gather U_j and store it as TF32 hi / lo operand rows
-            float U[TC_K];
+        // case j: U_j = chi0_j - chi_j over the element's 24 DOFs (FP64 chi relative
+        // to node 0), stored as TF32 hi / lo rows of A buffer j & 1
+        auto gather = [&](int j, float U[TC_K]) {
 #pragma unroll
             for (int m = 0; m < 3; ++m) {
                 const double c0 = valid ? __ldg(chi + fidx(3 * j + m, vtx[0])) : 0.0;
@@ -197,6 +195,7 @@ __global__ void __launch_bounds__(TC_M) k_energy_tc(Planes P, const double *__re
                     U[3 * a + m] = valid ? tc_macro_disp(a, j, m) - (float)(__ldg(chi + fidx(3 * j + m, vtx[a])) - c0)
                                          : 0.f;
             }
+            unsigned char *Ah = base + 2 * (j & 1) * TC_TILE_BYTES, *Al = Ah + TC_TILE_BYTES;
 #pragma unroll
             for (int k4 = 0; k4 < TC_K / 4; ++k4) {
                 float4 h, l;
@@ -204,52 +203,79 @@ __global__ void __launch_bounds__(TC_M) k_energy_tc(Planes P, const double *__re
                 h.y = tf32_hi(U[4 * k4 + 1]); l.y = U[4 * k4 + 1] - h.y;
                 h.z = tf32_hi(U[4 * k4 + 2]); l.z = U[4 * k4 + 2] - h.z;
                 h.w = tf32_hi(U[4 * k4 + 3]); l.w = U[4 * k4 + 3] - h.w;
-                *reinterpret_cast<float4 *>(Ahi + tc_off(tid, 4 * k4)) = h;
-                *reinterpret_cast<float4 *>(Alo + tc_off(tid, 4 * k4)) = l;
+                *reinterpret_cast<float4 *>(Ah + tc_off(tid, 4 * k4)) = h;
+                *reinterpret_cast<float4 *>(Al + tc_off(tid, 4 * k4)) = l;
             }
-            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-            __syncthreads();
-            // 2. KU_j = Ke U_j into TMEM columns 24j.. (lanes 0..127)
-            if (tid == 0) {
-                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t d = tmem + (uint32_t)(TC_K * j);
+        };
+        // KU_j = Ke U_j into TMEM columns 24j.. (lanes 0..127), committed to bar[j & 1]
+        auto issue = [&](int j) {
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t d = tmem + (uint32_t)(TC_K * j);
+            const uint32_t ahi = sA + (uint32_t)(2 * (j & 1) * TC_TILE_BYTES), alo = ahi + TC_TILE_BYTES;
 #pragma unroll
-                for (int s = 0; s < TC_K / 8; ++s) {
-                    const uint32_t ko = (uint32_t)(s * 256);  // two 16-byte K-chunks per K-step of 8
-                    tc_mma(d, tc_desc(sAhi + ko), tc_desc(sBhi + ko), s > 0 ? 1u : 0u);
-                    tc_mma(d, tc_desc(sAlo + ko), tc_desc(sBhi + ko), 1u);
-                    tc_mma(d, tc_desc(sAhi + ko), tc_desc(sBlo + ko), 1u);
-                }
-                tc_commit(bar);
+            for (int st = 0; st < TC_K / 8; ++st) {
+                const uint32_t ko = (uint32_t)(st * 256);  // two 16-byte K-chunks per K-step of 8
+                tc_mma(d, tc_desc(ahi + ko), tc_desc(sBhi + ko), st > 0 ? 1u : 0u);
+                tc_mma(d, tc_desc(alo + ko), tc_desc(sBhi + ko), 1u);
+                tc_mma(d, tc_desc(ahi + ko), tc_desc(sBlo + ko), 1u);
             }
-            const bool done = tc_wait(bar, phase);
-            phase ^= 1u;
+            tc_commit(bar + (j & 1));
+        };
+        // Pipeline: the gather of case j + 1 and its MMAs run while the MMAs of case
+        // j complete and case j's energies are read out of TMEM.  A buffer (j+1) & 1
+        // was last read by the MMAs of case j - 1, already waited for.
+        float E[21], Uc[TC_K], Un[TC_K];
+        gather(0, Uc);
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) issue(0);
+        int waited = 0, issued = 1;
+#pragma unroll
+        for (int j = 0; j < NCASE; ++j) {
+            if (!ok) continue;
+            if (j + 1 < NCASE) gather(j + 1, Un);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncthreads();  // A buffer (j+1) & 1 written; every thread past case j-1's TMEM reads
+            if (j + 1 < NCASE) {
+                if (tid == 0) issue(j + 1);
+                ++issued;
+            }
+            const bool done = tc_wait(bar + (j & 1), phase[j & 1]);
+            phase[j & 1] ^= 1u;
+            ++waited;
             if (__syncthreads_or(!done)) {  // uniform: every thread stops together
                 ok = false;
                 if (tid == 0) atomicExch(flag, 1);
                 continue;
             }
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            // 3. E_ij = U_j . KU_i for i <= j
+            // E_ij = U_j . KU_i for i <= j (three 8-column loads, one wait)
 #pragma unroll
             for (int i = 0; i <= j; ++i) {
-                float s = 0.f;
+                float ku[TC_K];
+                tc_ld8(lane_addr + (uint32_t)(TC_K * i), ku);
+                tc_ld8(lane_addr + (uint32_t)(TC_K * i + 8), ku + 8);
+                tc_ld8(lane_addr + (uint32_t)(TC_K * i + 16), ku + 16);
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                float sum = 0.f;
 #pragma unroll
-                for (int c8 = 0; c8 < TC_K / 8; ++c8) {
-                    float ku[8];
-                    tc_ld8(lane_addr + (uint32_t)(TC_K * i + 8 * c8), ku);
-                    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-                    for (int q = 0; q < 8; ++q) s = fmaf(U[8 * c8 + q], ku[q], s);
-                }
-                E[i * 6 - i * (i - 1) / 2 + (j - i)] = s;
+                for (int q = 0; q < TC_K; ++q) sum = fmaf(Uc[q], ku[q], sum);
+                E[i * 6 - i * (i - 1) / 2 + (j - i)] = sum;
             }
-            // the next case overwrites A and the next tile overwrites TMEM only after
-            // every thread is past its reads
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncthreads();
+#pragma unroll
+            for (int q = 0; q < TC_K; ++q) Uc[q] = Un[q];
         }
-        if (!ok) break;
+        // the next tile overwrites A and TMEM only after every thread is past its reads
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+        __syncthreads();
+        if (!ok) {  // a wait ran out: let the MMAs still in flight finish (bounded) before TMEM is freed
+            for (int k = waited; k < issued; ++k) {
+                (void)tc_wait(bar + (k & 1), phase[k & 1]);
+                phase[k & 1] ^= 1u;
+            }
+            break;
+        }
         if (valid) {
             if (SENS) {
                 float s = 0.f;
