@@ -62,12 +62,15 @@ __device__ __forceinline__ void load_block(const CoarseArgs &a, long long me, fl
 // threads of one vertex run in adjacent CTAs, so repeated stencil reads hit L2;
 // both shapes give the same result to the last bit.
 
-template <int K, bool SELF, bool F32, int C>
+// KC: the vertex colour, or -1 for the run-time colour kr (one code body for all
+// colours)
+template <int KC, bool SELF, bool F32, int C>
 __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, int i, int j, int l, int cb,
-                                             float acc[3 * C]) {
+                                             float acc[3 * C], int kr = KC) {
     static_assert(C % 2 == 0, "the load cases of a thread go in packed FP32x2 lane pairs");
     constexpr int NP = C / 2;
-    constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
+    const int K = KC >= 0 ? KC : kr;
+    const int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
     int ii[3], jj[3], ll[3];
     axis_nbrs_c(i, px, a.h[0], ii[0], ii[2]);
     axis_nbrs_c(j, py, a.h[1], jj[0], jj[2]);
@@ -160,13 +163,13 @@ __global__ void __launch_bounds__(128, CGS_MINB) k_coarse_gs(CoarseArgs a) {
     }
 }
 
-template <int K, bool F32, int CRES_CPT>
-__device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long p, int cb) {
+template <bool F32, int CRES_CPT>
+__device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long p, int cb, int K) {
     const long long me = (long long)K * a.P + p;
     int i, j, l;
     cplane_coords(a, p, i, j, l);
     float acc[3 * CRES_CPT];
-    coarse_apply<K, true, F32, CRES_CPT>(a, me, i, j, l, cb, acc);
+    coarse_apply<-1, true, F32, CRES_CPT>(a, me, i, j, l, cb, acc, K);
 #pragma unroll
     for (int q = 0; q < 3 * CRES_CPT; ++q) {
         const long long o = fidx(3 * cb + q, me);
@@ -174,13 +177,19 @@ __device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long
     }
 }
 
-template <int K, bool F32, int CRES_CPT, int CRES_MINB>
+// all eight colours in one launch, the colour in the low three bits of the block
+// index and a run-time value of one code body: the CTAs of one vertex block read
+// each other's neighbour rows while they are in L2, and a small level costs one
+// launch instead of eight
+template <bool F32, int CRES_CPT, int CRES_MINB>
 __global__ void __launch_bounds__(128, CRES_MINB) k_coarse_residual(CoarseArgs a) {
-    long long p;
-    int cb;
-    coarse_task<CRES_CPT>(p, cb);
+    constexpr int NG = NCASE / CRES_CPT;
+    const int K = (int)(blockIdx.x & 7u);
+    const unsigned bx = blockIdx.x >> 3;
+    const int cb = (int)(bx % NG) * CRES_CPT;
+    const long long p = (long long)(bx / NG) * blockDim.x + threadIdx.x;
     if (p >= a.P) return;
-    coarse_res_vertex<K, F32, CRES_CPT>(a, p, cb);
+    coarse_res_vertex<F32, CRES_CPT>(a, p, cb, K);
 }
 
 static CoarseArgs make_cargs(const Level &L) {
@@ -226,14 +235,7 @@ void launch_coarse_gs(const Level &L, float w, cudaStream_t s) {
 template <bool F32, int C, int MINB>
 static void coarse_residual_all(const CoarseArgs &a, cudaStream_t s) {
     const unsigned nb = (unsigned)((a.P + 127) / 128) * (NCASE / C);
-    k_coarse_residual<0, F32, C, MINB><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<1, F32, C, MINB><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<2, F32, C, MINB><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<3, F32, C, MINB><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<4, F32, C, MINB><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<5, F32, C, MINB><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<6, F32, C, MINB><<<nb, 128, 0, s>>>(a);
-    k_coarse_residual<7, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_residual<F32, C, MINB><<<nb * 8, 128, 0, s>>>(a);
 }
 
 void launch_coarse_residual(const Level &L, cudaStream_t s) {

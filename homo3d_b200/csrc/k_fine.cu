@@ -20,8 +20,9 @@
 // issue, 128 registers, 4 CTAs/SM); the residuals serve it by three threads with
 // two cases each in adjacent CTAs (fewer registers: the residual also writes r and
 // reduces the norms), where the densities and neighbour rows the three share hit
-// L1/L2.  The operator is applied in difference form,
-// sum_{d != 0} A_d (u_{v+d} - u_v), and the Gauss-Seidel step as u += D^-1 r with
+// L1/L2, and all eight colours of a residual go in one launch.  The operator is
+// applied in difference form, sum_{d != 0} A_d (u_{v+d} - u_v), and the
+// Gauss-Seidel step as u += D^-1 r with
 // the components in the reference's order: the same iteration in exact
 // arithmetic, and in FP32 it keeps rigid translations exact (see fine_apply).
 #include <type_traits>
@@ -30,7 +31,10 @@
 
 namespace h3d {
 
-constexpr int CPT = 2;            // load cases per thread of the residuals (three threads per vertex)
+constexpr int CPT = 2;            // load cases per thread of the FP32 residual (three threads per vertex)
+constexpr int RES_MINB = 6;       // its CTAs per SM
+constexpr int CPT64 = 2;          // load cases per thread of the FP64-solution residual
+constexpr int MINB64 = 4;         // its CTAs per SM
 constexpr int FBS = 128;          // threads per CTA
 
 struct FineArgs {
@@ -73,12 +77,13 @@ __host__ __device__ constexpr int first_shared(int d) {
 
 // geometry of one colour-K vertex: its element densities and the offsets of its
 // neighbours inside a colour plane (32-bit: a field plane holds < 2^31 vertices)
-template <int K>
+template <int KC>
 struct VertexGeo {
+    const int K;  // the colour: KC, or the run-time colour kr when KC < 0
     float rw[8];
     unsigned X[3], Y[3], Z[3];  // plane offsets of the neighbour rows: i, h0*j, h0*h1*l
-    __device__ __forceinline__ VertexGeo(const FineArgs &a, long long p) {
-        constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
+    __device__ __forceinline__ VertexGeo(const FineArgs &a, long long p, int kr = KC) : K(KC >= 0 ? KC : kr) {
+        const int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
         int i, j, l;
         plane_coords(a, p, i, j, l);
         const int x = 2 * i + px, y = 2 * j + py, z = 2 * l + pz;
@@ -275,22 +280,23 @@ __global__ void __launch_bounds__(FBS, MINB) k_fine_gs(FineArgs a, const __grid_
     }
 }
 
-template <int K>
+template <int KC>
 __device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const KeMat &ke, long long p, int cb,
-                                                     double nrm[CPT]) {
+                                                     double nrm[CPT], int kr = KC) {
+    const int K = KC >= 0 ? KC : kr;
     const long long me = (long long)K * a.P + p;
     if (K == 7 && p == 0) {
 #pragma unroll
         for (int q = 0; q < 3 * CPT; ++q) a.r[fidx(3 * cb + q, me)] = 0.f;
         return;
     }
-    const VertexGeo<K> g(a, p);
+    const VertexGeo<KC> g(a, p, K);
     float uv[3 * CPT];
 #pragma unroll
     for (int q = 0; q < 3 * CPT; ++q) uv[q] = __ldg(a.u + fidx(3 * cb + q, me));
     float acc[3 * CPT];
-    fine_apply<K, CPT>(a, ke, g, cb, uv, acc);
-    constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
+    fine_apply<KC, CPT>(a, ke, g, cb, uv, acc);
+    const int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
     int i, j, l;
     plane_coords(a, p, i, j, l);
     const double mult = (double)(axis_mult(2 * i + px, a.n[0]) * axis_mult(2 * j + py, a.n[1]) *
@@ -309,17 +315,35 @@ __device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const Ke
     }
 }
 
-// one colour per launch (the eight colour bodies in one kernel would not share
-// the instruction cache); the per-CTA norm partials of the CTA's two cases go to
-// row colour * gridDim.x + blockIdx.x, zeros for the other cases
-template <int K>
-__global__ void __launch_bounds__(FBS, 6) k_fine_residual(FineArgs a, const __grid_constant__ KeMat ke,
+// The residual has no order between the colours, so all eight run in one launch
+// with the colour in the low three bits of the block index: the eight CTAs of one
+// vertex block cover a 2x2x2 neighbourhood of the grid and read each other's rows
+// while they are in L2, where one launch per colour would stream the whole u
+// field from HBM once per colour.  The colour is a run-time value of one code
+// body (VertexGeo<-1>): eight compile-time colour bodies resident on an SM at
+// once thrash the instruction cache (2.5x slower at 256^3), while the run-time
+// colour costs a few integer operations per neighbour.  One thread per vertex
+// (six cases) is slower here too: 3.55 against 3.11 ms per 256^3 residual.  The
+// per-CTA norm partials of the CTA's two cases go to row colour * (CTAs per
+// colour) + CTA of the colour, zeros for the other cases, as with one launch per
+// colour, so the norms are summed in the same order.
+template <int C>
+__device__ __forceinline__ void colour_task(long long &p, int &cb, int &K, unsigned &bx) {
+    constexpr int NG = NCASE / C;
+    K = (int)(blockIdx.x & 7u);
+    bx = blockIdx.x >> 3;
+    cb = (int)(bx % NG) * C;
+    p = (long long)(bx / NG) * blockDim.x + threadIdx.x;
+}
+
+__global__ void __launch_bounds__(FBS, RES_MINB) k_fine_residual(FineArgs a, const __grid_constant__ KeMat ke,
                                                        double *partial) {
     long long p;
-    int cb;
-    thread_task<CPT>(p, cb);
-    double nrm[CPT] = {0, 0};
-    if (p < a.P) fine_residual_vertex<K>(a, ke, p, cb, nrm);
+    int cb, K;
+    unsigned bx;
+    colour_task<CPT>(p, cb, K, bx);
+    double nrm[CPT] = {};
+    if (p < a.P) fine_residual_vertex<-1>(a, ke, p, cb, nrm, K);
     if (!partial) return;
     __shared__ double sm[CPT][FBS / 32];
     const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
@@ -335,7 +359,7 @@ __global__ void __launch_bounds__(FBS, 6) k_fine_residual(FineArgs a, const __gr
         if (q >= cb && q < cb + CPT)
 #pragma unroll
             for (int w = 0; w < FBS / 32; ++w) v += sm[q - cb][w];
-        partial[((long long)K * gridDim.x + blockIdx.x) * NCASE + q] = v;
+        partial[((long long)K * (gridDim.x >> 3) + bx) * NCASE + q] = v;
     }
 }
 
@@ -347,24 +371,26 @@ __global__ void __launch_bounds__(FBS, 6) k_fine_residual(FineArgs a, const __gr
 // an ordinary neighbour: its value is held fixed by the correction sweeps, so a
 // nonzero value only translates the solution.  EXACT accumulates the products in
 // FP64 too (the FP32-product form floors near 1e-6 of ||f||, independent of N).
-template <int K, bool EXACT>
+template <int KC, bool EXACT>
 __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const KeMat &ke, const KeMat64 &ke64,
-                                                       const double *__restrict__ u64, long long p, int cb) {
+                                                       const double *__restrict__ u64, long long p, int cb,
+                                                       int kr = KC) {
+    const int K = KC >= 0 ? KC : kr;
     const long long me = (long long)K * a.P + p;
     if (K == 7 && p == 0) {
 #pragma unroll
-        for (int q = 0; q < 3 * CPT; ++q) a.r[fidx(3 * cb + q, me)] = 0.f;
+        for (int q = 0; q < 3 * CPT64; ++q) a.r[fidx(3 * cb + q, me)] = 0.f;
         return;
     }
-    const VertexGeo<K> g(a, p);
+    const VertexGeo<KC> g(a, p, K);
     const double *uvp = u64 + fidx(3 * cb, me);
-    double uv[3 * CPT];
+    double uv[3 * CPT64];
 #pragma unroll
-    for (int q = 0; q < 3 * CPT; ++q) uv[q] = __ldg(uvp + q * FVB);
+    for (int q = 0; q < 3 * CPT64; ++q) uv[q] = __ldg(uvp + q * FVB);
     using Acc = typename std::conditional<EXACT, double, float>::type;
-    Acc acc[3 * CPT];
+    Acc acc[3 * CPT64];
 #pragma unroll
-    for (int q = 0; q < 3 * CPT; ++q) acc[q] = 0;
+    for (int q = 0; q < 3 * CPT64; ++q) acc[q] = 0;
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         if (d == 13) continue;
@@ -388,7 +414,7 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
         }
         const double *up = u64 + fidx(3 * cb, nid);  // planes 3cb.. of the neighbour, FVB apart
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) {
+        for (int c = 0; c < CPT64; ++c) {
             const Acc d0 = (Acc)(__ldg(up + (3 * c) * FVB) - uv[3 * c]);
             const Acc d1 = (Acc)(__ldg(up + (3 * c + 1) * FVB) - uv[3 * c + 1]);
             const Acc d2 = (Acc)(__ldg(up + (3 * c + 2) * FVB) - uv[3 * c + 2]);
@@ -398,30 +424,22 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
         }
     }
 #pragma unroll
-    for (int q = 0; q < 3 * CPT; ++q) {
+    for (int q = 0; q < 3 * CPT64; ++q) {
         const long long o = fidx(3 * cb + q, me);
         a.r[o] = (float)((Acc)a.f[o] - acc[q]);
     }
 }
 
 template <bool EXACT>
-__global__ void __launch_bounds__(FBS, 4) k_fine_residual64(FineArgs a, const __grid_constant__ KeMat ke,
+__global__ void __launch_bounds__(FBS, MINB64) k_fine_residual64(FineArgs a, const __grid_constant__ KeMat ke,
                                                          const __grid_constant__ KeMat64 ke64,
                                                          const double *__restrict__ u64) {
     long long p;
-    int cb;
-    thread_task<CPT>(p, cb);
+    int cb, K;
+    unsigned bx;
+    colour_task<CPT64>(p, cb, K, bx);  // all colours in one launch, colour-minor
     if (p >= a.P) return;
-    switch (blockIdx.y) {
-    case 0: fine_residual64_vertex<0, EXACT>(a, ke, ke64, u64, p, cb); break;
-    case 1: fine_residual64_vertex<1, EXACT>(a, ke, ke64, u64, p, cb); break;
-    case 2: fine_residual64_vertex<2, EXACT>(a, ke, ke64, u64, p, cb); break;
-    case 3: fine_residual64_vertex<3, EXACT>(a, ke, ke64, u64, p, cb); break;
-    case 4: fine_residual64_vertex<4, EXACT>(a, ke, ke64, u64, p, cb); break;
-    case 5: fine_residual64_vertex<5, EXACT>(a, ke, ke64, u64, p, cb); break;
-    case 6: fine_residual64_vertex<6, EXACT>(a, ke, ke64, u64, p, cb); break;
-    default: fine_residual64_vertex<7, EXACT>(a, ke, ke64, u64, p, cb); break;
-    }
+    fine_residual64_vertex<-1, EXACT>(a, ke, ke64, u64, p, cb, K);
 }
 
 // f(case c) = sum_w (1e-9 + rho_w) * (Ke chi0_c)[rows of the vertex's local node in element w]
@@ -497,15 +515,7 @@ void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, dou
                           cudaStream_t s) {
     FineArgs a = make_args(L, rho);
     (void)nblk_norm;
-    const unsigned nb = task_blocks(a, CPT);
-    k_fine_residual<0><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
-    k_fine_residual<1><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
-    k_fine_residual<2><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
-    k_fine_residual<3><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
-    k_fine_residual<4><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
-    k_fine_residual<5><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
-    k_fine_residual<6><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
-    k_fine_residual<7><<<nb, FBS, 0, s>>>(a, ke, norm_partial);
+    k_fine_residual<<<task_blocks(a, CPT) * 8, FBS, 0, s>>>(a, ke, norm_partial);
 }
 
 void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const KeMat64 &ke64, const float *f,
@@ -514,8 +524,8 @@ void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, c
     FineArgs a = make_args(L, rho);
     a.f = f;
     a.r = r;
-    if (exact) k_fine_residual64<true><<<dim3(task_blocks(a, CPT), 8), FBS, 0, s>>>(a, ke, ke64, u64);
-    else k_fine_residual64<false><<<dim3(task_blocks(a, CPT), 8), FBS, 0, s>>>(a, ke, ke64, u64);
+    if (exact) k_fine_residual64<true><<<task_blocks(a, CPT64) * 8, FBS, 0, s>>>(a, ke, ke64, u64);
+    else k_fine_residual64<false><<<task_blocks(a, CPT64) * 8, FBS, 0, s>>>(a, ke, ke64, u64);
 }
 
 void launch_rhs(const Level &L, const float *rho, const RhsTab &g, float *f, cudaStream_t s) {
