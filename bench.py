@@ -128,11 +128,11 @@ PRECISION_NAME = {0: "FP32 V-cycles on the correction of an FP64 solution (itera
 
 def launches_per_step(nl, vcycles, reso, refine, refinements, coarsest_nv):
     """kernel launches of this library in one step, counted from the code paths
-    (equal to the ncu launch list of the 256^3 step: 1834)"""
+    (equal to the ncu launch list of the 256^3 step: 1414)"""
     nblk = -(-(reso ** 3 // 8) // 128) * 3 * 8                  # fine residual norm partials
     finish = 2 if nblk > 4096 else 1                            # one- or two-stage norm reduction
-    fine = 8 + 8 + finish + 8                                   # GS, residual (per colour), norms, GS
-    coarse = (nl - 2) * (8 + 8 + 8)                             # GS, residual, GS per colour
+    fine = 8 + 1 + finish + 8                                   # GS, residual (all colours), norms, GS
+    coarse = (nl - 2) * (8 + 1 + 8)                             # GS per colour, residual, GS per colour
     per_cycle = fine + coarse + 2 * (nl - 1) + 1 + 1            # restrict, prolong, coarsest apply, deflation
     per_refine = 1 + 1 + 2 + 3                                  # u64 += u, residual64, norms, deflation restart
     setup = 1 + 1 + 1 + (nl - 2) + 1 + 1 + 3 * coarsest_nv      # density, level 1, pin patch, deeper, assemble,

@@ -363,11 +363,20 @@ __global__ void __launch_bounds__(256) k_prolong2(Planes F, Planes C, FastDiv dn
         ci[id] = vidx(C, (id & 1) ? xp : x, ((id >> 1) & 1) ? yp : y, (id >> 2) ? zp : z);
     const long long cpl = F.nv / 8;
     const bool root = is_root && t == 0;
-#pragma unroll 1
+#pragma unroll 2
     for (int pl = 0; pl < NF; ++pl) {
-        float cv[8];
+        // the eight fine values are loaded before any is stored: the compiler
+        // cannot tell the eight colour planes apart, and read-add-write per vertex
+        // would wait on one DRAM round trip after another
+        float cv[8], fv[8];
 #pragma unroll
         for (int id = 0; id < 8; ++id) cv[id] = __ldg(&uc[fidx(pl, ci[id])]);
+#pragma unroll
+        for (int e = 0; e < 8; ++e) {
+            const int ex = e & 1, ey = (e >> 1) & 1, ez = e >> 2;
+            const int k = ((ex + 1) & 1) | (((ey + 1) & 1) << 1) | (((ez + 1) & 1) << 2);
+            fv[e] = uf[fidx(pl, k * cpl + t)];
+        }
 #pragma unroll
         for (int e = 0; e < 8; ++e) {
             if (e == 0 && root) continue;  // the pinned origin keeps its value
@@ -382,7 +391,7 @@ __global__ void __launch_bounds__(256) k_prolong2(Planes F, Planes C, FastDiv dn
             }
             // fine vertex (2x + ex, ...): colour of (ex, ey, ez), plane index t
             const int k = ((ex + 1) & 1) | (((ey + 1) & 1) << 1) | (((ez + 1) & 1) << 2);
-            uf[fidx(pl, k * cpl + t)] += acc;
+            uf[fidx(pl, k * cpl + t)] = fv[e] + acc;
         }
     }
 }
