@@ -536,13 +536,23 @@ void launch_rhs(const Level &L, const float *rho, const RhsTab &g, float *f, cud
 // ---- FP64 helpers of the refined mode ---------------------------------------------
 // u64 += e + T (T: the pending rigid translation of each of the 18 planes, see
 // k_pin_deflate); the pinned origin (colour 7, first vertex) keeps its value
-__global__ void k_update64(long long nv, double *u, const float *__restrict__ e, const double *__restrict__ T,
-                           long long pin) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i >= nv * NF) return;
-    const long long v = i % nv, q = i / nv;
-    if (v == pin) return;
-    const long long o = fidx((int)q, v);
+// Element-wise kernels over a blocked field run in storage order: one CTA of FVB
+// threads per (128-vertex block, plane) chunk c, plane q = c % 18, vertex
+// v = (c / 18) * FVB + thread (v >= nv in the padding of the last block).
+__device__ __forceinline__ void field_elem(long long &o, int &q, long long &v) {
+    const unsigned c = blockIdx.x;
+    q = (int)(c % NF);
+    v = (long long)(c / NF) * FVB + threadIdx.x;
+    o = (long long)c * FVB + threadIdx.x;
+}
+static unsigned field_chunks(long long nv) { return (unsigned)(field_floats(nv) / FVB); }
+
+__global__ void __launch_bounds__(FVB) k_update64(long long nv, double *u, const float *__restrict__ e,
+                                                 const double *__restrict__ T, long long pin) {
+    long long o, v;
+    int q;
+    field_elem(o, q, v);
+    if (v >= nv || v == pin) return;
     u[o] += (double)e[o] + T[q];
 }
 
@@ -667,25 +677,22 @@ __global__ void k_pin_restore_f(FineArgs a, const __grid_constant__ KeMat ke, do
 }
 
 // FP32 field <-> FP64 field (both blocked)
-__global__ void k_f32_to_f64(long long nv, const float *__restrict__ s, double *d) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < nv * NF) {
-        const long long o = fidx((int)(i / nv), i % nv);
-        d[o] = (double)s[o];
-    }
+__global__ void __launch_bounds__(FVB) k_f32_to_f64(long long nv, const float *__restrict__ s, double *d) {
+    long long o, v;
+    int q;
+    field_elem(o, q, v);
+    if (v < nv) d[o] = (double)s[o];
 }
 
-__global__ void k_f64_to_f32(long long nv, const double *__restrict__ s, float *d) {
-    const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (i < nv * NF) {
-        const long long o = fidx((int)(i / nv), i % nv);
-        d[o] = (float)s[o];
-    }
+__global__ void __launch_bounds__(FVB) k_f64_to_f32(long long nv, const double *__restrict__ s, float *d) {
+    long long o, v;
+    int q;
+    field_elem(o, q, v);
+    if (v < nv) d[o] = (float)s[o];
 }
 
 void launch_update64(const Level &L, double *u64, const float *e, const double *T, cudaStream_t s) {
-    const long long n = (long long)NF * L.P.nv;
-    k_update64<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(L.P.nv, u64, e, T, L.P.base[7]);
+    k_update64<<<field_chunks(L.P.nv), FVB, 0, s>>>(L.P.nv, u64, e, T, L.P.base[7]);
 }
 void launch_pin_deflate(const Level &L, const float *rho, const KeMat &ke, double *state, cudaStream_t s) {
     k_pin_deflate<<<1, PIN_THREADS, 0, s>>>(make_args(L, rho), ke, state);
@@ -698,10 +705,10 @@ void launch_pin_fold(const Level &L, const float *rho, const KeMat &ke, double *
     k_pin_restore_f<<<1, 32, 0, s>>>(make_args(L, rho), ke, state);
 }
 void launch_convert_field(long long nv, const float *src, double *dst, cudaStream_t s) {
-    k_f32_to_f64<<<(unsigned)((nv * NF + 255) / 256), 256, 0, s>>>(nv, src, dst);
+    k_f32_to_f64<<<field_chunks(nv), FVB, 0, s>>>(nv, src, dst);
 }
 void launch_convert_field(long long nv, const double *src, float *dst, cudaStream_t s) {
-    k_f64_to_f32<<<(unsigned)((nv * NF + 255) / 256), 256, 0, s>>>(nv, src, dst);
+    k_f64_to_f32<<<field_chunks(nv), FVB, 0, s>>>(nv, src, dst);
 }
 
 // mean of each of the 18 planes over unique vertices, removed in place (FP64)

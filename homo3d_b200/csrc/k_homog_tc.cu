@@ -221,24 +221,33 @@ __global__ void __launch_bounds__(TC_M) k_energy_tc(Planes P, const double *__re
             }
             tc_commit(bar + (j & 1));
         };
-        // Pipeline: the gather of case j + 1 and its MMAs run while the MMAs of case
-        // j complete and case j's energies are read out of TMEM.  A buffer (j+1) & 1
-        // was last read by the MMAs of case j - 1, already waited for.
+        // Pipeline (PIPE): the gather of case j + 1 and its MMAs run while the MMAs
+        // of case j complete and case j's energies are read out of TMEM.  A buffer
+        // (j+1) & 1 was last read by the MMAs of case j - 1, already waited for.
+        // Without PIPE, case j is gathered, multiplied and read out before case
+        // j + 1 starts.  Measured at 256^3: the pipeline makes the sensitivity form
+        // faster (6.9 against 7.7 ms per call) and the C form, which keeps 21 FP64
+        // sums per thread besides, 1.5 ms slower, so only the former uses it.
+        constexpr bool PIPE = SENS;
         float E[21], Uc[TC_K], Un[TC_K];
-        gather(0, Uc);
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (tid == 0) issue(0);
-        int waited = 0, issued = 1;
+        int waited = 0, issued = 0;
+        if (PIPE) {
+            gather(0, Uc);
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncthreads();
+            if (tid == 0) issue(0);
+            issued = 1;
+        }
 #pragma unroll
         for (int j = 0; j < NCASE; ++j) {
             if (!ok) continue;
-            if (j + 1 < NCASE) gather(j + 1, Un);
+            if (PIPE && j + 1 < NCASE) gather(j + 1, Un);
+            if (!PIPE) gather(j, Uc);
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
             asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            __syncthreads();  // A buffer (j+1) & 1 written; every thread past case j-1's TMEM reads
-            if (j + 1 < NCASE) {
-                if (tid == 0) issue(j + 1);
+            __syncthreads();  // the A buffer written; every thread past the previous case's TMEM reads
+            if (PIPE ? j + 1 < NCASE : true) {
+                if (tid == 0) issue(PIPE ? j + 1 : j);
                 ++issued;
             }
             const bool done = tc_wait(bar + (j & 1), phase[j & 1]);
@@ -263,8 +272,9 @@ __global__ void __launch_bounds__(TC_M) k_energy_tc(Planes P, const double *__re
                 for (int q = 0; q < TC_K; ++q) sum = fmaf(Uc[q], ku[q], sum);
                 E[i * 6 - i * (i - 1) / 2 + (j - i)] = sum;
             }
+            if (PIPE)
 #pragma unroll
-            for (int q = 0; q < TC_K; ++q) Uc[q] = Un[q];
+                for (int q = 0; q < TC_K; ++q) Uc[q] = Un[q];
         }
         // the next tile overwrites A and TMEM only after every thread is past its reads
         asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
