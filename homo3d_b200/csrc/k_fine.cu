@@ -115,56 +115,70 @@ struct VertexGeo {
     // an isotropic Ke is invariant under the mirrors up to the sign of the
     // components mirrored, so entry (r,c) = Ke[a_0][b_0](r,c) * sum_e +-rho_e with
     // the sign set by whether r and c lie on the mirrored axes: four signed
-    // density sums per block instead of 9 FMAs per shared element.
-    __device__ __forceinline__ void block(const KeMat &ke, int d, float A[9]) const {
+    // density sums per block (signed_sums) instead of 9 FMAs per shared element.
+    template <typename T>
+    __device__ __forceinline__ void block_t(const T *kk, int d, T A[9]) const {
         const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
         const int w0 = first_shared(d);
-        float cs[8];  // cs[m]: signed sum for the axis mask m = (1<<r) ^ (1<<c)
-#pragma unroll
-        for (int m = 0; m < 8; ++m) cs[m] = 0.f;
-#pragma unroll
-        for (int w = 0; w < 8; ++w) {
-            const int bx = 1 - (w & 1) + dx, by = 1 - ((w >> 1) & 1) + dy, bz = 1 - (w >> 2) + dz;
-            if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
-            const int mir = w ^ w0;
-#pragma unroll
-            for (int m = 0; m < 8; ++m) {
-                if (m != 0 && m != 3 && m != 5 && m != 6) continue;
-                cs[m] += (__popc(mir & m) & 1) ? -rw[w] : rw[w];
-            }
-        }
+        T cs[8];  // cs[m]: signed sum for the axis mask m = (1<<r) ^ (1<<c); m in {0, 3, 5, 6}
+        signed_sums<T>(dx, dy, dz, w0, cs);
         const int an = 7 - w0;
         const int bn = (1 - (w0 & 1) + dx) + 2 * (1 - ((w0 >> 1) & 1) + dy) + 4 * (1 - (w0 >> 2) + dz);
 #pragma unroll
         for (int r = 0; r < 3; ++r)
 #pragma unroll
-            for (int c = 0; c < 3; ++c) A[3 * r + c] = ke.k[(3 * an + r) * 24 + 3 * bn + c] * cs[(1 << r) ^ (1 << c)];
+            for (int c = 0; c < 3; ++c) A[3 * r + c] = kk[(3 * an + r) * 24 + 3 * bn + c] * cs[(1 << r) ^ (1 << c)];
     }
-    // the coupling block in FP64 from an FP64 element matrix (the exact refinement
-    // residual): the same mirror sums with FP64 densities and products
-    __device__ __forceinline__ void block64(const KeMat64 &ke, int d, double A[9]) const {
-        const int dx = d % 3 - 1, dy = d / 3 % 3 - 1, dz = d / 9 - 1;
-        const int w0 = first_shared(d);
-        double cs[8];
+    // The signed sums over the shared elements, folded one free axis at a time:
+    // element pairs along the first free axis (their sum and difference), then
+    // pairs of those along the next.  Along a free axis a the element with bit a
+    // set enters with a minus sign when a lies in the mask m, so the sign of an
+    // element is the parity of the mask axes on which it differs from w0.
+    // 0 / 2 / 8 / 16 additions for a corner / edge / face neighbour / the vertex
+    // itself, where the element-by-element sums took 4 / 8 / 16 / 32.
+    template <typename T>
+    __device__ __forceinline__ T rwv(int w) const { return (T)rw[w]; }
+    template <typename T>
+    __device__ __forceinline__ void signed_sums(int dx, int dy, int dz, int w0, T cs[8]) const {
+        int fa[3], nf = 0;  // the free axes (offset 0), ascending
+        if (dx == 0) fa[nf++] = 0;
+        if (dy == 0) fa[nf++] = 1;
+        if (dz == 0) fa[nf++] = 2;
 #pragma unroll
-        for (int m = 0; m < 8; ++m) cs[m] = 0.0;
+        for (int m = 0; m < 8; ++m) {
+            if (m != 0 && m != 3 && m != 5 && m != 6) { cs[m] = T(0); continue; }
+            if (nf == 0) {
+                cs[m] = rwv<T>(w0);
+            } else {
+                const int a = fa[0];
+                // level 1: pairs (w, w | a) for the 2^(nf-1) settings of the other free axes
+                T v[4];
 #pragma unroll
-        for (int w = 0; w < 8; ++w) {
-            const int bx = 1 - (w & 1) + dx, by = 1 - ((w >> 1) & 1) + dy, bz = 1 - (w >> 2) + dz;
-            if (bx < 0 || bx > 1 || by < 0 || by > 1 || bz < 0 || bz > 1) continue;
-            const int mir = w ^ w0;
-#pragma unroll
-            for (int m = 0; m < 8; ++m) {
-                if (m != 0 && m != 3 && m != 5 && m != 6) continue;
-                cs[m] += (__popc(mir & m) & 1) ? -(double)rw[w] : (double)rw[w];
+                for (int k = 0; k < 4; ++k) {
+                    if (k >= (1 << (nf - 1))) continue;
+                    int w = w0;
+                    if (nf > 1 && (k & 1)) w |= 1 << fa[1];
+                    if (nf > 2 && (k & 2)) w |= 1 << fa[2];
+                    v[k] = ((m >> a) & 1) ? rwv<T>(w) - rwv<T>(w | (1 << a)) : rwv<T>(w) + rwv<T>(w | (1 << a));
+                }
+                if (nf >= 2) {  // level 2: along fa[1]
+                    const bool mb = (m >> fa[1]) & 1;
+                    v[0] = mb ? v[0] - v[1] : v[0] + v[1];
+                    if (nf == 3) v[2] = mb ? v[2] - v[3] : v[2] + v[3];
+                }
+                if (nf == 3) {  // level 3: along fa[2]
+                    const bool mc = (m >> fa[2]) & 1;
+                    v[0] = mc ? v[0] - v[2] : v[0] + v[2];
+                }
+                cs[m] = v[0];
             }
         }
-        const int an = 7 - w0;
-        const int bn = (1 - (w0 & 1) + dx) + 2 * (1 - ((w0 >> 1) & 1) + dy) + 4 * (1 - (w0 >> 2) + dz);
-#pragma unroll
-        for (int r = 0; r < 3; ++r)
-#pragma unroll
-            for (int c = 0; c < 3; ++c) A[3 * r + c] = ke.k[(3 * an + r) * 24 + 3 * bn + c] * cs[(1 << r) ^ (1 << c)];
+    }
+    __device__ __forceinline__ void block(const KeMat &ke, int d, float A[9]) const { block_t<float>(ke.k, d, A); }
+    // the coupling block in FP64 from an FP64 element matrix (the exact refinement
+    // residual): the same signed sums with FP64 densities and products
+    __device__ __forceinline__ void block64(const KeMat64 &ke, int d, double A[9]) const {
+        block_t<double>(ke.k, d, A);
     }
     // index of neighbour d in its colour plane set, and whether it is the pinned origin
     __device__ __forceinline__ unsigned nbr(const FineArgs &a, int d, int &Kn, bool &pinned) const {
