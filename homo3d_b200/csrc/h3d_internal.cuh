@@ -194,6 +194,10 @@ struct StencilStore<true> {
 // ---- launch wrappers (kernels in the .cu files) --------------------------
 // fine level (k_fine.cu)
 void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, cudaStream_t s);
+// a colour sweep followed by the level-0 residual and its norm partials (the last
+// colour's launch computes its own vertices' residual)
+void launch_fine_gs_residual(const Level &L, const float *rho, const KeMat &ke, float w, double *norm_partial,
+                             cudaStream_t s);
 void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, double *norm_partial,
                           int nblk_norm, cudaStream_t s);
 // number of per-block norm partials launch_fine_residual writes

@@ -257,16 +257,21 @@ __device__ __forceinline__ void thread_task(long long &p, int &cb) {
     p = (long long)(blockIdx.x / NG) * blockDim.x + threadIdx.x;
 }
 
-template <int K, int C, int MINB>
-__global__ void __launch_bounds__(FBS, MINB) k_fine_gs(FineArgs a, const __grid_constant__ KeMat ke) {
-    long long p;
-    int cb;
-    thread_task<C>(p, cb);
-    if (p >= a.P) return;
+// one vertex of the colour sweep; RES (the last colour of a sweep) also writes
+// the residual of the updated vertex, whose neighbours (all of other colours) are
+// final: with acc = sum_d A_d (u_{v+d} - u_v) taken before the update and the
+// blocks of a row summing to zero, f - K u after u_v += e is (f - acc) - A_0 e,
+// e the change actually stored.  nrm[c] gathers the weighted squared residual.
+template <int K, int C, bool RES>
+__device__ __forceinline__ void fine_gs_vertex(const FineArgs &a, const KeMat &ke, long long p, int cb,
+                                               double nrm[C]) {
     const long long me = (long long)K * a.P + p;
     if (K == 7 && p == 0) {  // the pinned origin (grid.cu:445-447, 545)
 #pragma unroll
-        for (int q = 0; q < 3 * C; ++q) a.u[fidx(3 * cb + q, me)] = 0.f;
+        for (int q = 0; q < 3 * C; ++q) {
+            a.u[fidx(3 * cb + q, me)] = 0.f;
+            if (RES) a.r[fidx(3 * cb + q, me)] = 0.f;
+        }
         return;
     }
     const VertexGeo<K> g(a, p);
@@ -278,6 +283,13 @@ __global__ void __launch_bounds__(FBS, MINB) k_fine_gs(FineArgs a, const __grid_
     float ks[9];
     g.block(ke, 13, ks);
     const float w = a.w;
+    double mult = 0;
+    if (RES) {
+        constexpr int px = (K & 1) ^ 1, py = ((K >> 1) & 1) ^ 1, pz = ((K >> 2) & 1) ^ 1;
+        int i, j, l;
+        plane_coords(a, p, i, j, l);
+        mult = (double)(axis_mult(2 * i + px, a.n[0]) * axis_mult(2 * j + py, a.n[1]) * axis_mult(2 * l + pz, a.n[2]));
+    }
     // the reference's component-wise block Gauss-Seidel step (x, then y, then z,
     // each with the relaxed values of the earlier components) written as an
     // update of u by the residual r = f - K u
@@ -288,9 +300,59 @@ __global__ void __launch_bounds__(FBS, MINB) k_fine_gs(FineArgs a, const __grid_
         const float d0 = w * r0 / ks[0];
         const float d1 = w * (r1 - ks[3] * d0) / ks[4];
         const float d2 = w * (r2 - ks[6] * d0 - ks[7] * d1) / ks[8];
-        a.u[o] = uv[3 * c] + d0;
-        a.u[o + FVB] = uv[3 * c + 1] + d1;
-        a.u[o + 2 * FVB] = uv[3 * c + 2] + d2;
+        const float n0 = uv[3 * c] + d0, n1 = uv[3 * c + 1] + d1, n2 = uv[3 * c + 2] + d2;
+        a.u[o] = n0;
+        a.u[o + FVB] = n1;
+        a.u[o + 2 * FVB] = n2;
+        if (RES) {
+            const float e0 = n0 - uv[3 * c], e1 = n1 - uv[3 * c + 1], e2 = n2 - uv[3 * c + 2];
+            const float q0 = r0 - fmaf(ks[2], e2, fmaf(ks[1], e1, ks[0] * e0));
+            const float q1 = r1 - fmaf(ks[5], e2, fmaf(ks[4], e1, ks[3] * e0));
+            const float q2 = r2 - fmaf(ks[8], e2, fmaf(ks[7], e1, ks[6] * e0));
+            a.r[o] = q0;
+            a.r[o + FVB] = q1;
+            a.r[o + 2 * FVB] = q2;
+            nrm[c] += mult * ((double)q0 * q0 + (double)q1 * q1 + (double)q2 * q2);
+        }
+    }
+}
+
+// RES: the per-CTA norm partials go to the rows the residual of colour 7 would
+// write (row 7 * (CTAs per colour of the residual) + CTA of the colour, one row
+// per group of CPT cases, zeros for the other cases)
+template <int K, int C, int MINB, bool RES>
+__global__ void __launch_bounds__(FBS, MINB) k_fine_gs(FineArgs a, const __grid_constant__ KeMat ke,
+                                                    double *partial) {
+    long long p;
+    int cb;
+    thread_task<C>(p, cb);
+    double nrm[C];
+#pragma unroll
+    for (int c = 0; c < C; ++c) nrm[c] = 0;
+    if (!RES) {
+        if (p < a.P) fine_gs_vertex<K, C, false>(a, ke, p, cb, nrm);
+        return;
+    }
+    static_assert(!RES || (K == 7 && C % CPT == 0), "the fused residual is the last colour's");
+    if (p < a.P) fine_gs_vertex<K, C, RES>(a, ke, p, cb, nrm);
+    __shared__ double sm[C][FBS / 32];
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+#pragma unroll
+    for (int c = 0; c < C; ++c) {
+        const double v = warp_sum(nrm[c]);
+        if (lane == 0) sm[c][wid] = v;
+    }
+    __syncthreads();
+    constexpr int NG = NCASE / C, NGR = NCASE / CPT;  // case groups of this launch / of the residual
+    const long long pb = blockIdx.x / NG, npb = gridDim.x / NG;  // vertex block, vertex blocks
+    if (threadIdx.x < (C / CPT) * NCASE) {
+        const int gl = threadIdx.x / NCASE, q = threadIdx.x % NCASE;
+        const int g = cb / CPT + gl;  // the residual's case group of this row
+        double v = 0;
+        if (q >= g * CPT && q < (g + 1) * CPT)
+#pragma unroll
+            for (int w = 0; w < FBS / 32; ++w) v += sm[q - cb][w];
+        partial[((7 * npb + pb) * NGR + g) * NCASE + q] = v;
     }
 }
 
@@ -330,7 +392,8 @@ __device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const Ke
 }
 
 // The residual has no order between the colours, so all eight run in one launch
-// with the colour in the low three bits of the block index: the eight CTAs of one
+// with the colour the block index modulo the colour count (8, or 7 when the sweep
+// before it wrote colour 7's residual): the eight CTAs of one
 // vertex block cover a 2x2x2 neighbourhood of the grid and read each other's rows
 // while they are in L2, where one launch per colour would stream the whole u
 // field from HBM once per colour.  The colour is a run-time value of one code
@@ -342,20 +405,22 @@ __device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const Ke
 // colour) + CTA of the colour, zeros for the other cases, as with one launch per
 // colour, so the norms are summed in the same order.
 template <int C>
-__device__ __forceinline__ void colour_task(long long &p, int &cb, int &K, unsigned &bx) {
+__device__ __forceinline__ void colour_task(long long &p, int &cb, int &K, unsigned &bx, unsigned ncol = 8) {
     constexpr int NG = NCASE / C;
-    K = (int)(blockIdx.x & 7u);
-    bx = blockIdx.x >> 3;
+    K = (int)(blockIdx.x % ncol);
+    bx = blockIdx.x / ncol;
     cb = (int)(bx % NG) * C;
     p = (long long)(bx / NG) * blockDim.x + threadIdx.x;
 }
 
+template <unsigned NCOL>  // colours 0 .. NCOL-1 (8, or 7 after a sweep that did colour 7's)
 __global__ void __launch_bounds__(FBS, RES_MINB) k_fine_residual(FineArgs a, const __grid_constant__ KeMat ke,
                                                        double *partial) {
+    constexpr unsigned ncol = NCOL;
     long long p;
     int cb, K;
     unsigned bx;
-    colour_task<CPT>(p, cb, K, bx);
+    colour_task<CPT>(p, cb, K, bx, ncol);
     double nrm[CPT] = {};
     if (p < a.P) fine_residual_vertex<-1>(a, ke, p, cb, nrm, K);
     if (!partial) return;
@@ -373,7 +438,7 @@ __global__ void __launch_bounds__(FBS, RES_MINB) k_fine_residual(FineArgs a, con
         if (q >= cb && q < cb + CPT)
 #pragma unroll
             for (int w = 0; w < FBS / 32; ++w) v += sm[q - cb][w];
-        partial[((long long)K * (gridDim.x >> 3) + bx) * NCASE + q] = v;
+        partial[((long long)K * (gridDim.x / ncol) + bx) * NCASE + q] = v;
     }
 }
 
@@ -508,14 +573,14 @@ int fine_residual_blocks(const Level &L) { return (int)(((L.P.nv / 8 + FBS - 1) 
 template <int C, int MINB>
 static void fine_gs_sweep(const FineArgs &a, const KeMat &ke, cudaStream_t s) {
     const unsigned nb = task_blocks(a, C);
-    k_fine_gs<0, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<1, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<2, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<3, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<4, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<5, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<6, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
-    k_fine_gs<7, C, MINB><<<nb, FBS, 0, s>>>(a, ke);
+    k_fine_gs<0, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<1, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<2, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<3, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<4, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<5, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<6, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<7, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
 }
 
 void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, cudaStream_t s) {
@@ -525,11 +590,36 @@ void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, 
     else fine_gs_sweep<6, 4>(a, ke, s);
 }
 
+// a sweep followed by the residual (the down leg of a V-cycle): the last colour's
+// launch writes its own residual and norm partials, the residual launch covers
+// the other seven colours
+template <int C, int MINB>
+static void fine_gs_sweep_res(const FineArgs &a, const KeMat &ke, double *partial, cudaStream_t s) {
+    const unsigned nb = task_blocks(a, C);
+    k_fine_gs<0, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<1, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<2, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<3, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<4, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<5, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<6, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<7, C, MINB, true><<<nb, FBS, 0, s>>>(a, ke, partial);
+    k_fine_residual<7><<<task_blocks(a, CPT) * 7, FBS, 0, s>>>(a, ke, partial);
+}
+
+void launch_fine_gs_residual(const Level &L, const float *rho, const KeMat &ke, float w, double *norm_partial,
+                             cudaStream_t s) {
+    FineArgs a = make_args(L, rho);
+    a.w = w;
+    if (L.gs_shape == 1) fine_gs_sweep_res<2, 5>(a, ke, norm_partial, s);
+    else fine_gs_sweep_res<6, 4>(a, ke, norm_partial, s);
+}
+
 void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, double *norm_partial, int nblk_norm,
                           cudaStream_t s) {
     FineArgs a = make_args(L, rho);
     (void)nblk_norm;
-    k_fine_residual<<<task_blocks(a, CPT) * 8, FBS, 0, s>>>(a, ke, norm_partial);
+    k_fine_residual<8><<<task_blocks(a, CPT) * 8, FBS, 0, s>>>(a, ke, norm_partial);
 }
 
 void launch_fine_residual64(const Level &L, const float *rho, const KeMat &ke, const KeMat64 &ke64, const float *f,
