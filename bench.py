@@ -128,22 +128,26 @@ PRECISION_NAME = {0: "FP32 V-cycles on the correction of an FP64 solution (itera
 
 def launches_per_step(nl, vcycles, reso, refine, refinements, coarsest_nv):
     """kernel launches of this library in one step, counted from the code paths
-    (equal to the ncu launch list of the 256^3 step: 1414)"""
+    (equal to the ncu launch list of the 256^3 step); every step starts from zero
+    solutions, so the FP64 solution is cleared instead of copied and centred (no
+    kernel for 3) and the first refinement step sets f from f0 (1 kernel) instead
+    of u64 += u and the FP64 residual (2)"""
     nblk = -(-(reso ** 3 // 8) // 128) * 3 * 8                  # fine residual norm partials
     finish = 2 if nblk > 4096 else 1                            # one- or two-stage norm reduction
-    fine = 8 + 1 + finish + 8                                   # GS, residual (all colours), norms, GS
+    fine = 8 + 1 + finish + 8                                   # GS (last colour with its residual), residual, norms, GS
     coarse = (nl - 2) * (8 + 1 + 8)                             # GS per colour, residual, GS per colour
     per_cycle = fine + coarse + 2 * (nl - 1) + 1 + 1            # restrict, prolong, coarsest apply, deflation
     per_refine = 1 + 1 + 2 + 3                                  # u64 += u, residual64, norms, deflation restart
     setup = 1 + 1 + 1 + (nl - 2) + 1 + 1 + 3 * coarsest_nv      # density, level 1, pin patch, deeper, assemble,
     #                                                             first pivot, one launch per pivot column
     if refine:
-        pre = 1 + 3 + 3 + 2                                     # rhs, warm-start mean, balance, norms of f
+        pre = 1 + 3 + 2                                         # rhs, balance, norms of f
         post = 2                                                # C: energies, reduction
     else:
         pre = 1 + 1 + 3 + 3 + 2 + 3                             # rhs, convert, warm-start mean, balance, norms, deflation start
         post = 1 + 1 + 2                                        # pending shift into u, convert, C
-    return setup + pre + vcycles * per_cycle + refinements * per_refine + post
+    zero_start = -1 if refine and refinements > 0 else 0
+    return setup + pre + vcycles * per_cycle + refinements * per_refine + zero_start + post
 
 
 def make_density(args, rank):

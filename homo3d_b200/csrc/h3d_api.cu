@@ -174,6 +174,10 @@ struct h3d_handle {
     bool refine() const { return cfg.precision == H3D_PREC_REFINE; }
     bool have_density = false, have_stencils = false;
     bool tuned = false;  // launch shapes chosen (autotuner or h3d_set_tuning)
+    // chi_zero: the stored solutions chi are all zero (allocation, h3d_reset_solutions,
+    // no write since); u64_zero: the FP64 solution was set to zero by the last
+    // elastic_prepare and nothing has written it since (a solve's start reads it)
+    bool chi_zero = true, u64_zero = false;
     std::string err;
 };
 
@@ -306,6 +310,22 @@ int enqueue_refine(h3d_handle *h, bool exact) {
     return H3D_OK;
 }
 
+// the refinement step from a zero FP64 solution and correction (a solve's start
+// without a guess): u64 += 0 changes nothing and f0 - K 0 is f0 with the pinned
+// origin's entries 0, so level-0 f is set from f0 directly; the norms and the
+// deflation state are those enqueue_refine would compute, to the last bit
+int enqueue_zero_start(h3d_handle *h) {
+    cudaStream_t s = h->stream;
+    const Level &L0 = h->lv[0];
+    launch_rhs_at_zero(L0, h->f0, L0.f, s);
+    const int nb = norm_blocks(L0.P);
+    launch_weighted_norm(L0.P, L0.f, h->partial, nb, s);
+    launch_norm_finish(h->partial, nb, h->d_small, s);
+    cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, s);
+    enqueue_pin_init(h);
+    return H3D_OK;
+}
+
 // vgraph: one V-cycle (h3d_v_cycle); sgraph: the same with the deflation (solves);
 // rgraph / xgraph: the refinement step with FP32 / FP64 accumulation of the residual
 enum GraphKind { G_VCYCLE, G_SOLVE, G_REFINE, G_REFINE_EXACT };
@@ -411,6 +431,7 @@ struct SolveRun {
     int mask = 63, it = 0, nref = 0, status = H3D_OK, explode_left = 2, maxit = 200;
     double tol = 1e-2, theta = 1e-3;
     bool refine = false, exact = false, with_guess = false, fallback_tried = false, done_flag = false;
+    bool u64_zero = false;
     double fn[6] = {}, rel[6] = {1, 1, 1, 1, 1, 1}, base[6] = {1, 1, 1, 1, 1, 1};
     // largest selected stale estimate of each cycle since the last refinement
     std::vector<double> since_refine;
@@ -425,16 +446,25 @@ struct SolveRun {
     int reset_solution() {
         if (refine) CK(cudaMemsetAsync(h->u64, 0, sizeof(double) * n18(), h->stream));
         else CK(cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * nf32(), h->stream));
+        u64_zero = refine;
         return H3D_OK;
     }
+    // every start refinement runs with the correction u and the pending shift at
+    // 0; u64_zero: the FP64 solution too (reset, no V-cycle since)
     int launch_refine(Pending next) {
         nref++;
         since_refine.clear();
-        CK(cudaGraphLaunch(refine_step, h->stream));
+        if (next == P_START_REFINE && u64_zero) {
+            if (int e = enqueue_zero_start(h)) return e;
+            CKL();
+        } else {
+            CK(cudaGraphLaunch(refine_step, h->stream));
+        }
         pending = next;
         return H3D_OK;
     }
     int launch_cycle() {
+        u64_zero = false;
         if (it >= maxit) return finish(H3D_NOT_CONVERGED);
         CK(cudaGraphLaunch(h->sgraph, h->stream));
         pending = P_CYCLE;
@@ -464,6 +494,8 @@ struct SolveRun {
         tol = tolerance;
         with_guess = guess != 0;
         refine = h->refine();
+        u64_zero = refine && with_guess && h->u64_zero;  // a guess that is all zero
+        h->u64_zero = false;
         const Level &L0 = h->lv[0];
         if (!with_guess)
             if (int e = reset_solution()) return e;
@@ -629,8 +661,13 @@ int elastic_prepare(h3d_handle *h) {
     const int nb = norm_blocks(L.P);
     if (h->refine()) {
         launch_rhs(L, h->rho, h->rhs, h->f0, s);
-        CK(cudaMemcpyAsync(h->u64, h->chi, sizeof(double) * field_floats(L.P.nv), cudaMemcpyDeviceToDevice, s));
-        launch_remove_mean64(L.P, h->u64, h->partial, nb, s);
+        if (h->chi_zero) {  // the copy and its (zero) mean removal would leave zeros
+            CK(cudaMemsetAsync(h->u64, 0, sizeof(double) * field_floats(L.P.nv), s));
+        } else {
+            CK(cudaMemcpyAsync(h->u64, h->chi, sizeof(double) * field_floats(L.P.nv), cudaMemcpyDeviceToDevice, s));
+            launch_remove_mean64(L.P, h->u64, h->partial, nb, s);
+        }
+        h->u64_zero = h->chi_zero;
     } else {
         launch_rhs(L, h->rho, h->rhs, L.f, s);
         launch_convert_field(L.P.nv, h->chi, L.u, s);
@@ -649,6 +686,7 @@ int elastic_enqueue_energy(h3d_handle *h) {
     if (h->refine())
         CK(cudaMemcpyAsync(h->chi, h->u64, sizeof(double) * field_floats(L.P.nv), cudaMemcpyDeviceToDevice, s));
     else launch_convert_field(L.P.nv, L.u, h->chi, s);
+    h->chi_zero = false;
     int nsm = 0;
     CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
     const int eb = energy_tc_blocks(L.P, nsm);
@@ -1015,6 +1053,7 @@ int h3d_set_tuning(h3d_handle *h, int level, int gs_shape, int res_shape) {
 int h3d_reset_solutions(h3d_handle *h) {
     if (!h) return H3D_ERR_ARG;
     CK(cudaMemsetAsync(h->chi, 0, sizeof(double) * field_floats(h->lv[0].P.nv), h->stream));
+    h->chi_zero = true;
     return H3D_OK;
 }
 
@@ -1263,6 +1302,8 @@ int h3d_set_field(h3d_handle *h, int level, int field, const float *host) {
     if (field == H3D_FIELD_CHI || field == H3D_FIELD_SOLUTION) {
         double *dst = level != 0 ? nullptr : field == H3D_FIELD_CHI ? h->chi : h->u64;
         if (!dst) return fail(h, H3D_ERR_ARG, "no such FP64 field on this level / precision mode");
+        if (field == H3D_FIELD_CHI) h->chi_zero = false;
+        else h->u64_zero = false;
         if (int e = ensure_tmp(h, n18 + nf)) return e;
         CK(cudaMemcpyAsync(h->tmp, host, sizeof(float) * n18, cudaMemcpyHostToDevice, h->stream));
         launch_field_from_lex(L.P, h->tmp, h->tmp + n18, h->stream);
@@ -1296,6 +1337,7 @@ int h3d_warm_start_learned(h3d_handle *h, h3d_warmnet *net) {
     const float *y = nullptr;
     if (warmnet_forward_on(net, h->tmp, h->stream, &y) != H3D_OK) return fail(h, H3D_ERR_CUDA, "network forward failed");
     launch_warmnet_to_chi(L.P, y, R, h->chi, h->stream);
+    h->chi_zero = false;
     CKL();
     CK(cudaStreamSynchronize(h->stream));
     return H3D_OK;

@@ -214,6 +214,8 @@ void launch_update64(const Level &L, double *u64, const float *e, const double *
 void launch_pin_deflate(const Level &L, const float *rho, const KeMat &ke, double *state, cudaStream_t s);
 // state from the 18 plane sums of level-0 f: F = sums - f(origin), T = 0
 void launch_pin_init(const Level &L, const double *sums, double *state, cudaStream_t s);
+// f = f0 - K 0 on level 0 (f0 with the pinned origin's entries 0)
+void launch_rhs_at_zero(const Level &L, const float *f0, float *f, cudaStream_t s);
 // FP32 solutions: u += T (but the origin), f restored near the origin, T = 0
 void launch_pin_fold(const Level &L, const float *rho, const KeMat &ke, double *state, cudaStream_t s);
 // FP32 field of nv vertices <-> FP64 field

@@ -801,6 +801,18 @@ void launch_update64(const Level &L, double *u64, const float *e, const double *
 void launch_pin_deflate(const Level &L, const float *rho, const KeMat &ke, double *state, cudaStream_t s) {
     k_pin_deflate<<<1, PIN_THREADS, 0, s>>>(make_args(L, rho), ke, state);
 }
+// level-0 f of a zero FP64 solution: f0 - K 0 = f0 on every vertex but the pinned
+// origin, whose residual is 0 (what k_fine_residual64 computes for u64 = 0)
+__global__ void __launch_bounds__(FVB) k_rhs_at_zero(long long nv, const float *__restrict__ f0, float *f,
+                                                    long long pin) {
+    long long o, v;
+    int q;
+    field_elem(o, q, v);
+    if (v < nv) f[o] = v == pin ? 0.f : f0[o];
+}
+void launch_rhs_at_zero(const Level &L, const float *f0, float *f, cudaStream_t s) {
+    k_rhs_at_zero<<<field_chunks(L.P.nv), FVB, 0, s>>>(L.P.nv, f0, f, L.P.base[7]);
+}
 void launch_pin_init(const Level &L, const double *sums, double *state, cudaStream_t s) {
     k_pin_init<<<1, 32, 0, s>>>(sums, L.f, L.P.nv, L.P.base[7], state);
 }
