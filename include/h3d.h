@@ -167,7 +167,11 @@ H3D_API int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, 
 H3D_API int h3d_elastic_matrix(h3d_handle *h, double tol, double C[36], h3d_solve_stats *stats);
 /* sens = d obj / d rho_phys from dC = d obj / d C (float[36] row-major) */
 H3D_API int h3d_sensitivity(h3d_handle *h, const float dC[36], float *sens_dev, int pitchT);
-/* forget the stored solutions (warm start) */
+/* forget the stored solutions (warm start).  The next h3d_elastic_matrix then
+ * starts from zero without copying, centring or taking the FP64 residual of the
+ * zero solution (same results to the last bit, about 6 ms less at 256^3);
+ * writing the solutions through h3d_set_field, even with zeros, takes the full
+ * path */
 H3D_API int h3d_reset_solutions(h3d_handle *h);
 
 /* ---- autotuner (no reference counterpart) ----------------------------------
