@@ -263,13 +263,12 @@ int enqueue_vcycle(h3d_handle *h, float w, bool deflate = false) {
     const int nblk_r = fine_residual_blocks(h->lv[0]);
     for (int l = 0; l < h->nl; l++) {
         if (l > 0) {
-            if (l - 1 > 0) launch_coarse_residual(h->lv[l - 1], s);  // level 0's came with its sweep
             launch_restrict(h->lv[l - 1], h->lv[l], s);
             cudaMemsetAsync(h->lv[l].u, 0, sizeof(float) * field_floats(h->lv[l].P.nv), s);
         }
         if (l == h->nl - 1) launch_coarse_apply(h->lv[l], h->aug, h->cfg.coarse_mode == H3D_COARSE_PROJECT, s);
         else if (l == 0) launch_fine_gs_residual(h->lv[0], h->rho, h->ke, w, h->partial, s);
-        else launch_coarse_gs(h->lv[l], w, s);
+        else launch_coarse_gs_residual(h->lv[l], w, s);  // each level's residual comes with its sweep
     }
     for (int l = h->nl - 2; l >= 0; l--) {
         launch_prolong(h->lv[l], h->lv[l + 1], l == 0, s);

@@ -225,6 +225,9 @@ void launch_remove_mean64(const Planes &P, double *v, double *partial, int nblk,
 // coarse levels and transfers (k_coarse.cu)
 void launch_coarse_gs(const Level &L, float w, cudaStream_t s);
 void launch_coarse_residual(const Level &L, cudaStream_t s);
+// a coarse colour sweep followed by the level's residual (the last colour's launch
+// computes its own vertices' residual)
+void launch_coarse_gs_residual(const Level &L, float w, cudaStream_t s);
 void launch_restrict(const Level &F, const Level &C, cudaStream_t s);
 void launch_prolong(const Level &F, const Level &C, int is_root, cudaStream_t s);
 void launch_weighted_norm(const Planes &P, const float *v, double *partial, int nblk, cudaStream_t s);

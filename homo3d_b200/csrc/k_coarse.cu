@@ -136,7 +136,9 @@ __device__ __forceinline__ void coarse_task(long long &p, int &cb) {
     p = (long long)(blockIdx.x / NG) * blockDim.x + threadIdx.x;
 }
 
-template <int K, bool F32, int CGS_CPT, int CGS_MINB>
+// RES (the last colour of a sweep, whose neighbours are final) also writes the
+// residual of the updated vertex: r = f - acc - A_0 u with acc the neighbour sum
+template <int K, bool F32, int CGS_CPT, int CGS_MINB, bool RES = false>
 __global__ void __launch_bounds__(128, CGS_MINB) k_coarse_gs(CoarseArgs a) {
     long long p;
     int cb;
@@ -160,6 +162,12 @@ __global__ void __launch_bounds__(128, CGS_MINB) k_coarse_gs(CoarseArgs a) {
         u[0] = u0;
         u[FVB] = u1;
         u[2 * FVB] = u2;
+        if (RES) {
+            float *r = a.r + fidx(3 * (cb + c), me);
+#pragma unroll
+            for (int m = 0; m < 3; ++m)
+                r[m * FVB] = f[m * FVB] - acc[3 * c + m] - fmaf(ks[3 * m + 2], u2, fmaf(ks[3 * m + 1], u1, ks[3 * m] * u0));
+        }
     }
 }
 
@@ -177,15 +185,15 @@ __device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long
     }
 }
 
-// all eight colours in one launch, the colour in the low three bits of the block
-// index and a run-time value of one code body: the CTAs of one vertex block read
-// each other's neighbour rows while they are in L2, and a small level costs one
-// launch instead of eight
-template <bool F32, int CRES_CPT, int CRES_MINB>
+// all colours in one launch (eight, or seven after a sweep whose last colour wrote
+// its own residual), the colour the block index modulo NCOL and a run-time value
+// of one code body: the CTAs of one vertex block read each other's neighbour rows
+// while they are in L2, and a small level costs one launch instead of eight
+template <bool F32, int CRES_CPT, int CRES_MINB, unsigned NCOL>
 __global__ void __launch_bounds__(128, CRES_MINB) k_coarse_residual(CoarseArgs a) {
     constexpr int NG = NCASE / CRES_CPT;
-    const int K = (int)(blockIdx.x & 7u);
-    const unsigned bx = blockIdx.x >> 3;
+    const int K = (int)(blockIdx.x % NCOL);
+    const unsigned bx = blockIdx.x / NCOL;
     const int cb = (int)(bx % NG) * CRES_CPT;
     const long long p = (long long)(bx / NG) * blockDim.x + threadIdx.x;
     if (p >= a.P) return;
@@ -232,21 +240,51 @@ void launch_coarse_gs(const Level &L, float w, cudaStream_t s) {
     }
 }
 
-template <bool F32, int C, int MINB>
+template <bool F32, int C, int MINB, unsigned NCOL = 8>
 static void coarse_residual_all(const CoarseArgs &a, cudaStream_t s) {
     const unsigned nb = (unsigned)((a.P + 127) / 128) * (NCASE / C);
-    k_coarse_residual<F32, C, MINB><<<nb * 8, 128, 0, s>>>(a);
+    k_coarse_residual<F32, C, MINB, NCOL><<<nb * NCOL, 128, 0, s>>>(a);
 }
 
-void launch_coarse_residual(const Level &L, cudaStream_t s) {
-    CoarseArgs a = make_cargs(L);
+template <unsigned NCOL>
+static void coarse_residual_shape(const Level &L, const CoarseArgs &a, cudaStream_t s) {
     if (L.st32) {
-        if (L.res_shape == 1) coarse_residual_all<true, 6, 4>(a, s);
-        else coarse_residual_all<true, 2, 6>(a, s);
+        if (L.res_shape == 1) coarse_residual_all<true, 6, 4, NCOL>(a, s);
+        else coarse_residual_all<true, 2, 6, NCOL>(a, s);
     } else {
-        if (L.res_shape == 1) coarse_residual_all<false, 6, 4>(a, s);
-        else coarse_residual_all<false, 2, 6>(a, s);
+        if (L.res_shape == 1) coarse_residual_all<false, 6, 4, NCOL>(a, s);
+        else coarse_residual_all<false, 2, 6, NCOL>(a, s);
     }
+}
+
+void launch_coarse_residual(const Level &L, cudaStream_t s) { coarse_residual_shape<8>(L, make_cargs(L), s); }
+
+// a sweep followed by the level's residual: the last colour's launch writes its
+// own residual, the residual launch covers the other seven colours
+template <bool F32, int C, int MINB>
+static void coarse_gs_sweep_res(const CoarseArgs &a, cudaStream_t s) {
+    const unsigned nb = (unsigned)((a.P + 127) / 128) * (NCASE / C);
+    k_coarse_gs<0, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<1, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<2, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<3, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<4, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<5, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<6, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<7, F32, C, MINB, true><<<nb, 128, 0, s>>>(a);
+}
+
+void launch_coarse_gs_residual(const Level &L, float w, cudaStream_t s) {
+    CoarseArgs a = make_cargs(L);
+    a.w = w;
+    if (L.st32) {
+        if (L.gs_shape == 1) coarse_gs_sweep_res<true, 6, 4>(a, s);
+        else coarse_gs_sweep_res<true, 2, 6>(a, s);
+    } else {
+        if (L.gs_shape == 1) coarse_gs_sweep_res<false, 6, 4>(a, s);
+        else coarse_gs_sweep_res<false, 2, 6>(a, s);
+    }
+    coarse_residual_shape<7>(L, a, s);
 }
 
 // ---- transfers ---------------------------------------------------------------
