@@ -20,7 +20,8 @@
 // issue, 128 registers, 4 CTAs/SM); the residuals serve it by three threads with
 // two cases each in adjacent CTAs (fewer registers: the residual also writes r and
 // reduces the norms), where the densities and neighbour rows the three share hit
-// L1/L2, and all eight colours of a residual go in one launch.  The operator is
+// L1/L2, and all eight colours of a residual go in one launch (seven in a V-cycle,
+// where the sweep's last colour launch writes colour 7's residual).  The operator is
 // applied in difference form, sum_{d != 0} A_d (u_{v+d} - u_v), and the
 // Gauss-Seidel step as u += D^-1 r with
 // the components in the reference's order: the same iteration in exact
