@@ -1357,8 +1357,10 @@ int h3d_field_norms_static(h3d_handle *h, int field, double out[6]) {
     if (nb > STATIC_NORM_MAX_BLOCKS)
         return fail(h, H3D_ERR_ARG, "field needs more norm blocks than the static scratch holds (2048)");
     const double *tot = static_norm_totals(h->device);
-    if (!tot || launch_weighted_norm_static(h->device, L.P, v, nb, h->stream) != 0)
-        return fail(h, H3D_ERR_CUDA, "cudaGetSymbolAddress of the static norm scratch failed");
+    if (!tot) return fail(h, H3D_ERR_CUDA, "cudaGetSymbolAddress of the static norm scratch failed");
+    const int rc = launch_weighted_norm_static(h->device, L.P, v, nb, h->stream);
+    if (rc == -1) return fail(h, H3D_ERR_ARG, "norm block count outside 1..2048 for the static scratch");
+    if (rc != 0) return fail(h, H3D_ERR_CUDA, "cudaGetSymbolAddress of the static norm scratch failed");
     CKL();
     double sums[NCASE];
     CK(cudaMemcpyAsync(sums, tot, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, h->stream));

@@ -317,29 +317,33 @@ void launch_galerkin(const Level &F, const Level &C, cudaStream_t s) {
 }
 
 // ---- coarsest level ---------------------------------------------------------------
-// aug: [n][2n] row-major, left = K over unique DOFs (3*lexid + comp), right = I
+// aug: [n][2n] row-major, left = K over unique DOFs (3*lexid + comp), right = I.
+// One thread per row (vertex lex, component i) adds its 27 neighbour blocks in
+// neighbour order d = 0..26, so entries that several periodic images of one
+// neighbour fall on (grids of two or three cells per axis) are summed in a fixed
+// order and the coarsest inverse is the same from run to run.
 template <bool F32>
 __global__ void k_coarse_assemble(Planes C, const uint4 *__restrict__ st, double *aug, int n) {
     const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (t >= C.nv * 27) return;
-    const long long lex = t / 27;
-    const int d = (int)(t % 27);
+    if (t >= C.nv * 3) return;
+    const long long lex = t / 3;
+    const int i = (int)(t % 3);
     const int x = (int)(lex % C.n[0]);
     const int y = (int)((lex / C.n[0]) % C.n[1]), z = (int)(lex / ((long long)C.n[0] * C.n[1]));
     const long long v = vidx(C, x, y, z);
-    const int wx = wrap(x + d % 3 - 1, C.n[0]), wy = wrap(y + d / 3 % 3 - 1, C.n[1]), wz = wrap(z + d / 9 - 1, C.n[2]);
-    const long long w = wx + (long long)C.n[0] * (wy + (long long)C.n[1] * wz);
-    for (int i = 0; i < 3; i++)
-        for (int j = 0; j < 3; j++)
-            atomicAdd(&aug[(3 * lex + i) * (2LL * n) + 3 * w + j], (double)StencilStore<F32>::get(st, C.nv, v, 9 * d + 3 * i + j));
-    if (d == 0)
-        for (int i = 0; i < 3; i++) aug[(3 * lex + i) * (2LL * n) + n + 3 * lex + i] = 1.0;
+    double *row = aug + (3 * lex + i) * (2LL * n);
+    for (int d = 0; d < 27; d++) {
+        const int wx = wrap(x + d % 3 - 1, C.n[0]), wy = wrap(y + d / 3 % 3 - 1, C.n[1]), wz = wrap(z + d / 9 - 1, C.n[2]);
+        const long long w = wx + (long long)C.n[0] * (wy + (long long)C.n[1] * wz);
+        for (int j = 0; j < 3; j++) row[3 * w + j] += (double)StencilStore<F32>::get(st, C.nv, v, 9 * d + 3 * i + j);
+    }
+    row[n + 3 * lex + i] = 1.0;
 }
 
 void launch_coarse_assemble(const Level &C, double *aug, cudaStream_t s) {
     const int n = (int)(3 * C.P.nv);
     cudaMemsetAsync(aug, 0, sizeof(double) * (size_t)n * 2 * n, s);
-    const long long nt = C.P.nv * 27;
+    const long long nt = C.P.nv * 3;
     if (C.st32) k_coarse_assemble<true><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(C.P, C.st, aug, n);
     else k_coarse_assemble<false><<<(unsigned)((nt + 255) / 256), 256, 0, s>>>(C.P, C.st, aug, n);
 }

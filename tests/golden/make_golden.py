@@ -1,7 +1,7 @@
 """Regenerates the golden fixtures of this directory from the reference sources.
 
-Run in a checkout that has the reference (lavenklau/homo3d) at REFERENCE_ROOT
-(default /root/reference).  The fixtures are committed; tests never read the
+Run with the environment variable REFERENCE_ROOT set to a checkout of the
+reference (lavenklau/homo3d).  The fixtures are committed; tests never read the
 reference at run time.
 
   ke_lame72.json : the integer tables 72*K_lambda and 72*K_mu that the reference
@@ -13,7 +13,7 @@ import os
 import re
 import sys
 
-ROOT = os.environ.get("REFERENCE_ROOT", "/root/reference")
+ROOT = os.environ.get("REFERENCE_ROOT")
 
 
 def _table(src, name):
@@ -27,6 +27,8 @@ def _table(src, name):
 
 
 def main():
+    if not ROOT:
+        sys.exit("set REFERENCE_ROOT to a checkout of lavenklau/homo3d")
     path = os.path.join(ROOT, "homogenization", "templateMatrix.cpp")
     src = open(path).read()
     out = {
