@@ -9,8 +9,9 @@ a zero start to relthres 1e-5, and reduce the 6x6 homogenized tensor C.
 
 N > 1 runs under torchrun as independent replicas (one design per rank, no
 collective on the data path): value = total solves / max-over-ranks time.
---impl reference times the FP64 CPU restatement of the same V-cycle (the oracle)
-on the host cores, a bounded sample per step (see cpu_sample()).
+--impl reference times the FP64 CPU restatement of the same solve (the oracle) on
+all host cores at the full grid size: one V-cycle per step, the setup and the C
+reduction once (see reference_arm()).
 """
 import argparse
 import json
@@ -47,7 +48,8 @@ def parse():
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--profile", action="store_true",
                    help="only warm-up and timed steps (no e2e, setup or sweep side measurements), for ncu")
-    p.add_argument("--precision", type=int, default=0, help="0 refined (FP64 solution), 1 FP32")
+    p.add_argument("--precision", type=int, default=0,
+                   help="0 refined (FP64 solution), 1 FP32, 2 refined with the tensor-core level-0 residual")
     return p.parse_args()
 
 
@@ -123,10 +125,12 @@ def max_over_ranks(dist, value):
 SWEEP_TRAFFIC_BYTES = {256: 12_580_000_000}
 
 PRECISION_NAME = {0: "FP32 V-cycles on the correction of an FP64 solution (iterative refinement)",
-                  1: "FP32 solution (the reference's scheme)"}
+                  1: "FP32 solution (the reference's scheme)",
+                  2: "FP32 V-cycles on the correction of an FP64 solution (iterative refinement), level-0 "
+                     "residual on tcgen05 tensor cores (TF32 hi+lo operands, FP32 accumulation)"}
 
 
-def launches_per_step(nl, vcycles, reso, refine, refinements, coarsest_nv):
+def launches_per_step(nl, vcycles, reso, refine, refinements, coarsest_nv, mixed=False):
     """kernel launches of this library in one step, counted from the code paths
     (equal to the ncu launch list of the 256^3 step); every step starts from zero
     solutions, so the FP64 solution is cleared instead of copied and centred (no
@@ -135,6 +139,8 @@ def launches_per_step(nl, vcycles, reso, refine, refinements, coarsest_nv):
     nblk = -(-(reso ** 3 // 8) // 128) * 3 * 8                  # fine residual norm partials
     finish = 2 if nblk > 4096 else 1                            # one- or two-stage norm reduction
     fine = 8 + 1 + finish + 8                                   # GS (last colour with its residual), residual, norms, GS
+    if mixed:
+        fine = 8 + 1 + 1 + 8                                    # GS, tensor-core residual, norms, GS
     coarse = (nl - 2) * (8 + 1 + 8)                             # GS per colour, residual, GS per colour
     per_cycle = fine + coarse + 2 * (nl - 1) + 1 + 1            # restrict, prolong, coarsest apply, deflation
     per_refine = 1 + 1 + 2 + 3                                  # u64 += u, residual64, norms, deflation restart
@@ -225,6 +231,17 @@ def gpu_arm(args):
     torch.cuda.synchronize()
     e2e_ms = (time.perf_counter() - e0) * 1e3
     e2e_ms = max_over_ranks(dist, e2e_ms) / (args.steps * world)
+    if hd.last_stats["status"] != H.H3D_OK:
+        raise RuntimeError("end-to-end solve did not converge: %r" % (hd.last_stats,))
+    e2e_match = bool(np.abs(Ce - C).max() <= 1e-6 * np.abs(C).max())
+    if not e2e_match:
+        raise RuntimeError("end-to-end C differs from the device-timed C: %r vs %r" % (Ce, C))
+    # C against the FP64 oracle's committed solution of the same design
+    fx = oracle_fixture(args) if rank == 0 else None
+    c_err = None
+    if fx is not None:
+        Co = np.array(fx["C"]).reshape(6, 6)
+        c_err = float(np.abs(C - Co).max() / np.abs(Co).max())
 
     # setup alone, and the dominant kernel (fine-level Gauss-Seidel sweep) by itself
     s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -257,21 +274,17 @@ def gpu_arm(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(t_max / args.steps, 3),
             "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic: seeded trig-basis density, reflect6, vol %.2f, rho^3 (SIMP p=3)" % args.vol,
-            "config": {"workload": "6-case periodic homogenization solve, %d^3, E=10 nu=0.3, relthres %g, "
-                                   "zero start, MG V(1,1) with 8-colour GS and FP16 coarse stencils, %s" % (
-                                       args.reso, args.tol, PRECISION_NAME[args.precision]),
-                       "reso": args.reso, "load_cases": 6, "relthres": args.tol, "levels": hd.nlevels,
-                       "pin_mode": args.pin_mode, "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "inputs larger than L2 (fields %.1f GB)" % (3 * 18 * 4 * n3 / 1e9)},
+            "config": workload_config(args, hd.nlevels),
             "vcycles": vc, "vcycles_per_s": round(vc / (ms_per_solve * world) * 1e3, 2),
             "setup_ms": round(setup_ms, 3),
-            "C00": float(C[0, 0]), "C_e2e_match": bool(np.abs(Ce - C).max() <= 1e-6 * np.abs(C).max()),
+            "C00": float(C[0, 0]), "C_e2e_match": e2e_match,
+            "C_err_vs_oracle": c_err,
             "e2e": {"value": round(e2e_ms, 3), "unit": "ms", "h2d_bytes_per_step": int(rho_h.nbytes),
                     "d2h_bytes_per_step": 36 * 8},
             "refinements": refs[-1],
             "launch_shapes": hd.tuning(),
-            "gpu_launches": sum(launches_per_step(hd.nlevels, c, args.reso, args.precision == 0, r, coarsest_nv)
-                                for c, r in zip(cycles, refs)),
+            "gpu_launches": sum(launches_per_step(hd.nlevels, c, args.reso, args.precision != 1, r, coarsest_nv,
+                                                  args.precision == 2) for c, r in zip(cycles, refs)),
             "roofline": {"kernel": "k_fine_gs (8 colour launches = one sweep)", "bound": "hbm",
                          "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                          "frac": round(achieved / peaks.get("hbm_gbs"), 4),
@@ -287,67 +300,131 @@ def gpu_arm(args):
     return result
 
 
-def cpu_sample(args, vcycles=None, cycles_timed=1):
-    """FP64 CPU restatement of the same solve, bounded: hierarchy setup and
-    `cycles_timed` V-cycles at reso/2 (6 cases), scaled by 8 to reso^3 (all the
-    work is proportional to the vertex count), times the V-cycle count (the GPU's
-    when given, else the oracle's own count at 64^3)."""
-    import numpy as np
+FIXTURE = os.path.join(ROOT, "tests", "golden", "oracle_C.json")
+
+
+def workload_config(args, levels):
+    return {"workload": "6-case periodic homogenization solve, %d^3, E=10 nu=0.3, relthres %g, zero start, "
+                        "MG V(1,1) with 8-colour GS and FP16 coarse stencils, %s" % (
+                            args.reso, args.tol, PRECISION_NAME[args.precision]),
+            "reso": args.reso, "load_cases": 6, "relthres": args.tol, "vol": args.vol, "seed": args.seed,
+            "pin_mode": args.pin_mode, "levels": int(levels),
+            "parallelism": "replicas" if args.gpus > 1 else "single",
+            "l2": "inputs larger than L2 (level-0 fields %.1f GB)" % (3 * 18 * 4 * args.reso ** 3 / 1e9)}
+
+
+def oracle_fixture(args):
+    """the committed FP64-oracle record of this design (tests/golden/oracle_C.json),
+    or None"""
+    if not os.path.exists(FIXTURE):
+        return None
+    for c in json.load(open(FIXTURE))["cases"]:
+        if c["reso"] == args.reso and abs(c["vol"] - args.vol) < 1e-9 and c["seed"] == args.seed:
+            return c
+    return None
+
+
+def oracle_vcycles(args):
+    """(V-cycle count of the FP64 oracle's own solve of this design to relthres,
+    where it comes from)"""
+    fx = oracle_fixture(args)
+    if fx is not None and args.tol == 1e-5 and fx.get("vcycles_to_1e-5"):
+        return int(fx["vcycles_to_1e-5"]), "the oracle's own count for this design (tests/golden/oracle_C.json)"
     from oracle import oracle as O
     from homo3d_b200.density import synthetic_density
+    m0 = O.MG((64, 64, 64))
+    m0.set_density(synthetic_density(64, seed=args.seed, vol=args.vol).ravel() ** 3)
+    m0.update_stencils()
+    m0.rhs()
+    v, _ = m0.solve(args.tol, 200)
+    return int(v), "the oracle's own count for this design at 64^3"
 
+
+class OracleSolve:
+    """The FP64 CPU restatement of the solve (oracle/h3d_oracle.c, OpenMP on all
+    host cores) at the full grid size, timed piece by piece: hierarchy setup and
+    right-hand sides, single V-cycles, and the reduction of C."""
+
+    def __init__(self, args):
+        import numpy as np
+        from oracle import oracle as O
+        from homo3d_b200.density import synthetic_density
+        n = args.reso
+        self.m = O.MG((n, n, n))
+        self.m.set_density((synthetic_density(n, seed=args.seed, vol=args.vol).ravel() ** 3)
+                           .astype(np.float32).astype(np.float64))
+        self.timed = 0.0
+
+    def _t(self, fn):
+        t0 = time.perf_counter()
+        fn()
+        dt = time.perf_counter() - t0
+        self.timed += dt
+        return dt
+
+    def setup(self):
+        return self._t(lambda: (self.m.update_stencils(), self.m.rhs()))
+
+    def vcycle(self):
+        return self._t(lambda: self.m.vcycle(1.0))
+
+    def elastic(self):
+        return self._t(lambda: self.m.elastic_matrix())
+
+
+def cpu_sample(args, vcycles, vsource, cycles_timed=1):
+    """Bounded CPU sample of the same workload: the FP64 oracle's setup, one V-cycle
+    and the C reduction, each timed at the full grid size on all host cores; the
+    solve is the V-cycle time times a stated V-cycle count (cycle-count
+    extrapolated: the full oracle solve at 256^3 takes minutes)."""
     threads = os.cpu_count()
-    n = max(args.reso // 2, 16)
-    scale = (args.reso / n) ** 3
-    if vcycles is None:
-        m0 = O.MG((64, 64, 64))
-        m0.set_density(synthetic_density(64, seed=args.seed, vol=args.vol).ravel() ** 3)
-        m0.update_stencils()
-        m0.rhs()
-        vcycles, _ = m0.solve(args.tol, 200)
-        del m0
-    m = O.MG((n, n, n))
-    m.set_density(synthetic_density(n, seed=args.seed, vol=args.vol).ravel() ** 3)
-    t0 = time.perf_counter()
-    m.update_stencils()
-    m.rhs()
-    setup_s = time.perf_counter() - t0
-    t0 = time.perf_counter()
-    for _ in range(cycles_timed):
-        m.vcycle(1.0)
-    cyc_s = (time.perf_counter() - t0) / cycles_timed
-    t0 = time.perf_counter()
-    m.elastic_matrix()
-    c_s = time.perf_counter() - t0
-    ms = (setup_s + vcycles * cyc_s + c_s) * scale * 1e3
+    o = OracleSolve(args)
+    t_setup = o.setup()
+    t_cyc = [o.vcycle() for _ in range(cycles_timed)]
+    t_c = o.elastic()
+    cyc = statistics.median(t_cyc)
+    ms = (t_setup + vcycles * cyc + t_c) * 1e3
     return {"value": round(ms, 1), "unit": "ms", "cores": threads, "kind": "port",
-            "sample": "FP64 oracle, setup + %d V-cycle(s) + C at %d^3 scaled x%d to %d^3, x %d V-cycles"
-                      % (cycles_timed, n, int(scale), args.reso, vcycles),
-            "vcycles": int(vcycles), "ms_per_vcycle": round(cyc_s * scale * 1e3, 1),
-            "setup_ms": round(setup_s * scale * 1e3, 1)}
+            "sample": "FP64 oracle on %d host threads at %d^3: setup + %d V-cycle(s) + C timed, "
+                      "value = setup + %d x V-cycle + C (cycle-count extrapolated; %d V-cycles = %s)"
+                      % (threads, args.reso, cycles_timed, vcycles, vcycles, vsource),
+            "vcycles": int(vcycles), "ms_per_vcycle": round(cyc * 1e3, 1), "setup_ms": round(t_setup * 1e3, 1),
+            "C_ms": round(t_c * 1e3, 1), "timed_s": round(o.timed, 1)}
 
 
 def reference_arm(args):
+    """The reference's path on the host cores: the reference itself cannot be built
+    here (its hot path needs Eigen, glm, gflags and OpenVDB), so this times the FP64
+    CPU restatement of its solve (the oracle) on all host cores at the full grid
+    size.  Each step is one V-cycle; the hierarchy setup and the C reduction are
+    timed once; value = setup + V x (median V-cycle) + C, V the oracle's own
+    V-cycle count for this design (the same count the GPU line's cpu_baseline uses)."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return None
     os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
-    samples = []
-    cb = None
-    for i in range(min(args.warmup, 1) + args.steps):
-        cb = cpu_sample(args, vcycles=cb["vcycles"] if cb else None)
-        if i >= min(args.warmup, 1):
-            samples.append(cb["value"])
-    value = statistics.median(samples)
-    cb["value"] = value
+    vcycles, vsource = oracle_vcycles(args)
+    o = OracleSolve(args)
+    t_setup = o.setup()
+    for _ in range(min(args.warmup, 1)):
+        o.vcycle()
+    o.timed = t_setup
+    cyc = [o.vcycle() for _ in range(args.steps)]
+    t_c = o.elastic()
+    c_med = statistics.median(cyc)
+    value = round((t_setup + vcycles * c_med + t_c) * 1e3, 1)
+    threads = os.cpu_count()
+    cb = {"value": value, "unit": "ms", "cores": threads, "kind": "port",
+          "sample": "FP64 oracle on %d host threads at %d^3: setup once, %d timed V-cycles (one per step), "
+                    "C once; value = setup + %d x median V-cycle + C (cycle-count extrapolated; %d V-cycles = %s)"
+                    % (threads, args.reso, args.steps, vcycles, vcycles, vsource),
+          "vcycles": vcycles, "ms_per_vcycle": round(c_med * 1e3, 1), "setup_ms": round(t_setup * 1e3, 1),
+          "C_ms": round(t_c * 1e3, 1), "timed_s": round(o.timed, 1)}
     return {"metric": metric_name(args), "value": value, "unit": "ms", "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": value, "higher_is_better": False, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "impl": "reference",
             "data": "synthetic: seeded trig-basis density, reflect6, vol %.2f, rho^3 (SIMP p=3)" % args.vol,
-            "config": {"workload": "6-case periodic homogenization solve, %d^3, E=10 nu=0.3, relthres %g, "
-                                   "zero start, MG V(1,1) with 8-colour GS and FP16 coarse stencils, %s" % (
-                                       args.reso, args.tol, PRECISION_NAME[args.precision]),
-                       "reso": args.reso, "load_cases": 6, "relthres": args.tol},
+            "config": workload_config(args, o.m.nlevels),
             "cpu_baseline": cb,
             "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
@@ -359,7 +436,9 @@ def main():
     else:
         out = gpu_arm(args)
         if out is not None and not args.no_cpu_baseline and out["n_gpus"] == 1:
-            out["cpu_baseline"] = cpu_sample(args, vcycles=out["vcycles"])
+            os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+            vcycles, vsource = oracle_vcycles(args)
+            out["cpu_baseline"] = cpu_sample(args, vcycles, vsource)
     if out is not None:
         print(json.dumps(out), flush=True)
 

@@ -10,7 +10,7 @@ OUT_DIR = os.path.join(HERE, "lib")
 BUILD_DIR = os.path.join(HERE, "_build")
 LIB = os.path.join(OUT_DIR, "libh3d.so")
 
-SOURCES = ["k_fine.cu", "k_coarse.cu", "k_galerkin.cu", "k_homog_tc.cu", "k_design.cu", "k_mma.cu", "k_static_norm.cu", "k_warmnet.cu", "h3d_api.cu"]
+SOURCES = ["k_fine.cu", "k_fine_tc.cu", "k_coarse.cu", "k_galerkin.cu", "k_homog_tc.cu", "k_design.cu", "k_mma.cu", "k_static_norm.cu", "k_warmnet.cu", "h3d_api.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",

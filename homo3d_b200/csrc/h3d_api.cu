@@ -171,7 +171,11 @@ struct h3d_handle {
     cudaGraphExec_t fgraph = nullptr;   // coarsest assembly + Gauss-Jordan inverse (n + 1 launches)
     double *pin_state = nullptr;        // deflation: F[18], pending shift T[18], plane sums[18]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
-    bool refine() const { return cfg.precision == H3D_PREC_REFINE; }
+    bool refine() const { return cfg.precision != H3D_PREC_FP32; }
+    // the level-0 V-cycle residual on the tensor cores (k_fine_tc.cu)
+    bool mixed() const { return cfg.precision == H3D_PREC_MIXED; }
+    int num_sms = 0;
+    int *d_tcflag = nullptr;            // set by the tensor-core residual if an mbarrier wait timed out
     bool have_density = false, have_stencils = false;
     bool tuned = false;  // launch shapes chosen (autotuner or h3d_set_tuning)
     // chi_zero: the stored solutions chi are all zero (allocation, h3d_reset_solutions,
@@ -260,15 +264,22 @@ int destroy_graph(h3d_handle *h) {
 // cycle ends with the rigid-translation deflation (launch_pin_deflate).
 int enqueue_vcycle(h3d_handle *h, float w, bool deflate = false) {
     cudaStream_t s = h->stream;
-    const int nblk_r = fine_residual_blocks(h->lv[0]);
+    const int nblk_r = h->mixed() ? fine_residual_tc_blocks(h->lv[0].P, h->num_sms) : fine_residual_blocks(h->lv[0]);
     for (int l = 0; l < h->nl; l++) {
         if (l > 0) {
             launch_restrict(h->lv[l - 1], h->lv[l], s);
             cudaMemsetAsync(h->lv[l].u, 0, sizeof(float) * field_floats(h->lv[l].P.nv), s);
         }
-        if (l == h->nl - 1) launch_coarse_apply(h->lv[l], h->aug, h->cfg.coarse_mode == H3D_COARSE_PROJECT, s);
-        else if (l == 0) launch_fine_gs_residual(h->lv[0], h->rho, h->ke, w, h->partial, s);
-        else launch_coarse_gs_residual(h->lv[l], w, s);  // each level's residual comes with its sweep
+        if (l == h->nl - 1) {
+            launch_coarse_apply(h->lv[l], h->aug, h->cfg.coarse_mode == H3D_COARSE_PROJECT, s);
+        } else if (l == 0 && h->mixed()) {  // the sweep, then the residual on the tensor cores
+            launch_fine_gs(h->lv[0], h->rho, h->ke, w, s);
+            launch_fine_residual_tc(h->lv[0], h->rho, h->ke, h->partial, nblk_r, h->d_tcflag, s);
+        } else if (l == 0) {
+            launch_fine_gs_residual(h->lv[0], h->rho, h->ke, w, h->partial, s);
+        } else {
+            launch_coarse_gs_residual(h->lv[l], w, s);  // each level's residual comes with its sweep
+        }
     }
     for (int l = h->nl - 2; l >= 0; l--) {
         launch_prolong(h->lv[l], h->lv[l + 1], l == 0, s);
@@ -278,6 +289,7 @@ int enqueue_vcycle(h3d_handle *h, float w, bool deflate = false) {
     if (deflate) launch_pin_deflate(h->lv[0], h->rho, h->ke, h->pin_state, s);
     launch_norm_finish(h->partial, nblk_r, h->d_small, s);
     cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, s);
+    if (h->mixed()) cudaMemcpyAsync(&h->h_small[62], h->d_tcflag, sizeof(int), cudaMemcpyDeviceToHost, s);
     return H3D_OK;
 }
 
@@ -548,6 +560,8 @@ struct SolveRun {
         }
         case P_CYCLE: {
             it++;
+            if (h->mixed() && *reinterpret_cast<int *>(&h->h_small[62]))
+                return fail(h, H3D_ERR_CUDA, "tensor-core residual: mbarrier wait timed out");
             bool bad = false, done = true, trigger = true;
             double worst = 0;
             for (int c = 0; c < NCASE; c++) {
@@ -737,7 +751,7 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
         return fail(h, H3D_ERR_ARG, "invalid coarse_mode");
     if (cfg->pin_mode != H3D_PIN_IDENTITY && cfg->pin_mode != H3D_PIN_GALERKIN)
         return fail(h, H3D_ERR_ARG, "invalid pin_mode");
-    if (cfg->precision != H3D_PREC_REFINE && cfg->precision != H3D_PREC_FP32)
+    if (cfg->precision != H3D_PREC_REFINE && cfg->precision != H3D_PREC_FP32 && cfg->precision != H3D_PREC_MIXED)
         return fail(h, H3D_ERR_ARG, "invalid precision");
     if (cfg->stencil_precision != H3D_STENCIL_FP16 && cfg->stencil_precision != H3D_STENCIL_FP32)
         return fail(h, H3D_ERR_ARG, "invalid stencil_precision");
@@ -796,6 +810,11 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
     h->ndof = (int)(3 * C.P.nv);
     CK(cudaMalloc(&h->aug, sizeof(double) * gauss_jordan_doubles(h->ndof)));
     CK(cudaMalloc(&h->d_flag, sizeof(int)));
+    CK(cudaMalloc(&h->d_tcflag, sizeof(int)));
+    CK(cudaMemset(h->d_tcflag, 0, sizeof(int)));
+    CK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
+    if (h->mixed() && configure_fine_residual_tc() != 0)
+        return fail(h, H3D_ERR_CUDA, "tensor-core residual kernel could not be configured");
     // reduction scratch: residual partials, norms, C partials, means, OC
     size_t pn = ((size_t)fine_residual_blocks(h->lv[0]) + NORM_FINISH_CHUNKS) * NCASE;
     pn = std::max(pn, (size_t)4096 * 21);
@@ -837,7 +856,7 @@ int h3d_destroy(h3d_handle *h) {
     }
     cudaFree(h->rho); cudaFree(h->chi); cudaFree(h->u64); cudaFree(h->f0);
     cudaFree(h->q); cudaFree(h->d_ked); cudaFree(h->aug);
-    cudaFree(h->d_flag); cudaFree(h->partial); cudaFree(h->d_small); cudaFree(h->tmp); cudaFree(h->pin_state);
+    cudaFree(h->d_flag); cudaFree(h->d_tcflag); cudaFree(h->partial); cudaFree(h->d_small); cudaFree(h->tmp); cudaFree(h->pin_state);
     if (h->h_small) cudaFreeHost(h->h_small);
     if (h->ev0) cudaEventDestroy(h->ev0);
     if (h->ev1) cudaEventDestroy(h->ev1);
@@ -945,7 +964,13 @@ int h3d_update_residual(h3d_handle *h, int level) {
     if (int e = check_level(h, level)) return e;
     if (level == 0) {
         if (!h->have_density) return fail(h, H3D_ERR_STATE, "no density");
-        launch_fine_residual(h->lv[0], h->rho, h->ke, nullptr, 0, h->stream);
+        if (h->mixed()) {
+            CK(cudaSetDevice(h->device));
+            launch_fine_residual_tc(h->lv[0], h->rho, h->ke, nullptr, fine_residual_tc_blocks(h->lv[0].P, h->num_sms),
+                                    h->d_tcflag, h->stream);
+        } else {
+            launch_fine_residual(h->lv[0], h->rho, h->ke, nullptr, 0, h->stream);
+        }
     } else {
         if (!h->have_stencils) return fail(h, H3D_ERR_STATE, "no stencils");
         launch_coarse_residual(h->lv[level], h->stream);

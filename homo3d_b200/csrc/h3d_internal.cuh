@@ -252,6 +252,16 @@ void launch_coarse_assemble(const Level &C, double *aug, cudaStream_t s);
 size_t gauss_jordan_doubles(int n);
 void launch_gauss_jordan(double *aug, int n, int *flag, cudaStream_t s);
 void launch_coarse_apply(const Level &C, const double *aug, int project, cudaStream_t s);
+// level-0 residual on the tensor cores (k_fine_tc.cu): element products Ke U with
+// TF32 hi + lo operands and FP32 accumulation; a persistent grid of
+// fine_residual_tc_blocks CTAs writing one row of six norm partials each (partial
+// may be null); *flag is set if an mbarrier wait timed out.
+// configure_fine_residual_tc (once per device, before any launch or stream
+// capture) returns -1 when the kernel's shared memory cannot be granted
+int configure_fine_residual_tc();
+int fine_residual_tc_blocks(const Planes &P, int num_sms);
+int launch_fine_residual_tc(const Level &L, const float *rho, const KeMat &ke, double *partial, int nblk,
+                            int *flag, cudaStream_t s);
 // homogenized tensor and sensitivities on the tensor cores (k_homog_tc.cu):
 // a persistent grid of energy_tc_blocks CTAs; *flag is set if an mbarrier wait
 // timed out; the launchers return -1 when the kernel cannot be configured

@@ -1,10 +1,12 @@
 """OC design loops on the library's entry points: bulk-modulus maximisation (the
-loop of homo3d's optiBulk, homogenization/testAutoDiff.cu:282-331) and the
+loop of homo3d's optiBulk, homogenization/testAutoDiff.cu:282-331), shear-modulus
+maximisation (optiShear, homogenization/testAutoDiff.cu:334-381) and the
 negative-Poisson-ratio loop (example_opti_npr, Framework.cu:208-272).
 
 Per iteration: rho_phys = rho^3; update the hierarchy; six solves and C (warm
 start from the previous iteration); the objective, bulk
--(C00+C11+C22 + 2(C01+C02+C12))/3 or npr C01+C02+C12 - (C00+C11+C22) 0.8^iter;
+-(C00+C11+C22 + 2(C01+C02+C12))/3, shear -(C33+C44+C55)/3 or npr
+C01+C02+C12 - (C00+C11+C22) 0.8^iter;
 sensitivities wrt rho_phys, chain rule 3 rho^2; symmetrise; filter; OC update;
 symmetrise the density.  Every step runs on the handle's stream.
 
@@ -34,6 +36,18 @@ def bulk_objective(C):
     return -(C[0, 0] + C[1, 1] + C[2, 2] + 2 * (C[0, 1] + C[0, 2] + C[1, 2])) / 3.0
 
 
+def shear_objective(C):
+    """-(C33 + C44 + C55) / 3 (testAutoDiff.cu:343)"""
+    return -(C[3, 3] + C[4, 4] + C[5, 5]) / 3.0
+
+
+def shear_gradient():
+    dC = np.zeros((6, 6), np.float32)
+    for i in range(3, 6):
+        dC[i, i] = -1.0 / 3.0
+    return dC
+
+
 NPR_BETA = 0.8  # Framework.cu:241
 
 
@@ -51,6 +65,7 @@ def npr_gradient(it, beta=NPR_BETA):
 
 
 OBJECTIVES = {"bulk": (lambda C, it: bulk_objective(C), lambda it: bulk_gradient()),
+              "shear": (lambda C, it: shear_objective(C), lambda it: shear_gradient()),
               "npr": (npr_objective, npr_gradient)}
 
 
@@ -73,8 +88,8 @@ def optimize_bulk(reso, vol=0.3, iters=50, seed=0, relthres=1e-2, filter_radius=
                   sym="reflect6", finthres=5e-4, stop_on_converge=False, rho0=None, E=10.0, nu=0.3,
                   coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY, precision=PREC_REFINE, device=0,
                   on_solve=None, stencil=STENCIL_FP16, objective="bulk"):
-    """The OC loop of testAutoDiff.cu:282-331 (objective "bulk") or of
-    Framework.cu:208-272 ("npr"); on_solve(hom, rho_phys) is called after every
+    """The OC loop of testAutoDiff.cu:282-331 (objective "bulk"), of
+    testAutoDiff.cu:334-381 ("shear") or of Framework.cu:208-272 ("npr"); on_solve(hom, rho_phys) is called after every
     solve (e.g. to record training pairs)."""
     obj_fn, grad_fn = OBJECTIVES[objective]
     import torch

@@ -66,8 +66,12 @@ typedef enum {
                                    difference form whenever the stale residual has dropped
                                    by max(1e-3, 1e-5 N) or met the tolerance (iterative
                                    refinement) */
-    H3D_PREC_FP32 = 1           /* FP32 solution swept directly, as the reference does; its
+    H3D_PREC_FP32 = 1,          /* FP32 solution swept directly, as the reference does; its
                                    relative residual floors near 1e-6 * N */
+    H3D_PREC_MIXED = 2          /* H3D_PREC_REFINE with the level-0 residual of every V-cycle
+                                   formed element by element on the tensor cores: element
+                                   displacement differences and Ke as TF32 hi + lo parts,
+                                   FP32 accumulation (no reference counterpart) */
 } h3d_precision;
 
 /* storage of the Galerkin coarse-level stencils */

@@ -30,7 +30,7 @@ def oracle_loop(n, rho, iters, vol=0.3, objective="bulk"):
     return rho, objs
 
 
-@pytest.mark.parametrize("objective", ["bulk", "npr"])
+@pytest.mark.parametrize("objective", ["bulk", "shear", "npr"])
 def test_oc_loop_matches_oracle(torch_cuda, objective):
     n = 16
     rho0 = synthetic_density(n, seed=5, vol=0.3).ravel().astype(np.float32).astype(np.float64)
@@ -49,6 +49,13 @@ def test_oc_loop_improves_bulk_modulus(torch_cuda):
     assert objs[-1] < objs[0]  # obj = -bulk modulus decreases
     assert all(r["vcycles"] >= 1 for r in rec)
     assert rec[-1]["vcycles"] <= rec[0]["vcycles"]  # warm start pays off
+
+
+def test_shear_loop_raises_shear_modulus(torch_cuda):
+    rho, C, rec = optimize_bulk(32, iters=8, seed=3, relthres=1e-2, objective="shear")
+    objs = [r["obj"] for r in rec]
+    assert objs[-1] < objs[0]  # obj = -shear modulus decreases
+    assert abs(rho.astype(np.float64).mean() - 0.3) < 2e-4
 
 
 def test_npr_loop_lowers_poisson_coupling(torch_cuda):
