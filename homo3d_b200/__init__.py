@@ -63,6 +63,13 @@ class SolveStats(ctypes.Structure):
                 "solve_ms": self.solve_ms, "refinements": self.refinements}
 
 
+class DesignParams(ctypes.Structure):
+    """h3d_design_params: the update after a solve (h3d_design_step)"""
+    _fields_ = [("penal", ctypes.c_float), ("sym", ctypes.c_int), ("filter_radius", ctypes.c_float),
+                ("filter_periodic", ctypes.c_int), ("volratio", ctypes.c_float), ("min_rho", ctypes.c_float),
+                ("step_limit", ctypes.c_float), ("damp", ctypes.c_float)]
+
+
 _lib = None
 _vp, _ip, _dp, _fp = ctypes.c_void_p, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_double), \
     ctypes.POINTER(ctypes.c_float)
@@ -104,6 +111,7 @@ _SIGS = {
                       ctypes.c_float],
     "h3d_oc_filter": [_vp, _vp, _vp, _ip, ctypes.c_int, ctypes.c_float, ctypes.c_int],
     "h3d_symmetrize": [_vp, _vp, _ip, ctypes.c_int],
+    "h3d_design_step": [_vp, _fp, _vp, _vp, ctypes.POINTER(DesignParams)],
     "h3d_get_field": [_vp, ctypes.c_int, ctypes.c_int, _fp],
     "h3d_set_field": [_vp, ctypes.c_int, ctypes.c_int, _fp],
     "h3d_mma_create": [ctypes.c_int, ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -368,6 +376,16 @@ class Homogenization(_Handle):
 
     def set_tuning(self, level, gs_shape, res_shape=0):
         self.check(lib().h3d_set_tuning(self._h, int(level), int(gs_shape), int(res_shape)))
+
+    def design_step(self, dC, rho, sens, volratio, penal=3.0, sym="reflect6", filter_radius=2.0, periodic=False,
+                    min_rho=1e-3, step_limit=0.05, damp=0.5):
+        """One OC design update after a solve, as one captured graph on the device
+        (h3d_design_step): sens = dObj/drho from dC through rho^penal, symmetrised,
+        filtered; rho updated by OC and symmetrised.  rho, sens: CUDA tensors."""
+        d = np.ascontiguousarray(dC, dtype=np.float32).reshape(36)
+        prm = DesignParams(float(penal), SYMMETRY[sym] if sym else -1, float(filter_radius), int(periodic),
+                           float(volratio), float(min_rho), float(step_limit), float(damp))
+        self.check(lib().h3d_design_step(self._h, d.ctypes.data_as(_fp), _ptr(rho), _ptr(sens), ctypes.byref(prm)))
 
     def warm_start_learned(self, net):
         """stored solutions from a WarmNet's prediction for the current density"""

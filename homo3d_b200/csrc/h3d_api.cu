@@ -169,6 +169,10 @@ struct h3d_handle {
     cudaGraphExec_t xgraph = nullptr;   // the same with the FP64-accumulated residual
     cudaGraphExec_t sgraph = nullptr;   // a solve's V-cycle: vgraph + rigid-translation deflation
     cudaGraphExec_t fgraph = nullptr;   // coarsest assembly + Gauss-Jordan inverse (n + 1 launches)
+    cudaGraphExec_t dgraph = nullptr;   // design step (h3d_design_step)
+    float *d_dcw = nullptr, *h_dcw = nullptr;  // sensitivity weights: device copy, pinned host source
+    h3d_design_params dkey{};           // parameters and buffers the design graph was captured for
+    const float *dkey_rho = nullptr, *dkey_sens = nullptr;
     double *pin_state = nullptr;        // deflation: F[18], pending shift T[18], plane sums[18]
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool refine() const { return cfg.precision != H3D_PREC_FP32; }
@@ -254,6 +258,7 @@ int destroy_graph(h3d_handle *h) {
     if (h->xgraph) { cudaGraphExecDestroy(h->xgraph); h->xgraph = nullptr; }
     if (h->sgraph) { cudaGraphExecDestroy(h->sgraph); h->sgraph = nullptr; }
     if (h->fgraph) { cudaGraphExecDestroy(h->fgraph); h->fgraph = nullptr; }
+    if (h->dgraph) { cudaGraphExecDestroy(h->dgraph); h->dgraph = nullptr; }
     return H3D_OK;
 }
 
@@ -856,6 +861,8 @@ int h3d_destroy(h3d_handle *h) {
     }
     cudaFree(h->rho); cudaFree(h->chi); cudaFree(h->u64); cudaFree(h->f0);
     cudaFree(h->q); cudaFree(h->d_ked); cudaFree(h->aug);
+    cudaFree(h->d_dcw);
+    if (h->h_dcw) cudaFreeHost(h->h_dcw);
     cudaFree(h->d_flag); cudaFree(h->d_tcflag); cudaFree(h->partial); cudaFree(h->d_small); cudaFree(h->tmp); cudaFree(h->pin_state);
     if (h->h_small) cudaFreeHost(h->h_small);
     if (h->ev0) cudaEventDestroy(h->ev0);
@@ -1272,6 +1279,65 @@ int h3d_symmetrize(h3d_handle *h, float *field_dev, const int reso[3], int sym) 
     CK(cudaSetDevice(h->device));
     launch_symmetrize(reso, field_dev, sym, h->stream);
     CKL();
+    return H3D_OK;
+}
+
+int h3d_design_step(h3d_handle *h, const float dC[36], float *rho_dev, float *sens_dev, const h3d_design_params *prm) {
+    if (!h || !dC || !rho_dev || !sens_dev || !prm) return H3D_ERR_ARG;
+    const Planes &P = h->lv[0].P;
+    const int *n = P.n;
+    if (prm->sym < -1 || prm->sym > 2) return fail(h, H3D_ERR_ARG, "sym must be -1, 0, 1 or 2");
+    if (prm->sym > 0 && (n[0] != n[1] || n[1] != n[2]))
+        return fail(h, H3D_ERR_ARG, "reflect6 and rotate3 need a cubic grid");
+    if (!(prm->volratio > 0 && prm->volratio <= 1)) return fail(h, H3D_ERR_ARG, "volratio outside (0, 1]");
+    CK(cudaSetDevice(h->device));
+    const long long ne = (long long)n[0] * n[1] * n[2];
+    if (int e = ensure_tmp(h, (size_t)ne)) return e;
+    if (!h->d_dcw) CK(cudaMalloc(&h->d_dcw, sizeof(float) * 32));
+    if (!h->h_dcw) CK(cudaMallocHost(&h->h_dcw, sizeof(float) * 32));
+    if (h->dgraph && (h->dkey_rho != rho_dev || h->dkey_sens != sens_dev ||
+                      std::memcmp(&h->dkey, prm, sizeof(h3d_design_params)) != 0)) {
+        cudaGraphExecDestroy(h->dgraph);
+        h->dgraph = nullptr;
+    }
+    if (!h->dgraph) {
+        if (configure_energy_tc() != 0) return fail(h, H3D_ERR_CUDA, "tensor-core energy kernel could not be configured");
+        int nsm = 0;
+        CK(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, h->device));
+        cudaStream_t s = h->stream;
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+        cudaMemcpyAsync(h->d_dcw, h->h_dcw, sizeof(float) * 21, cudaMemcpyHostToDevice, s);
+        cudaMemsetAsync(h->d_flag, 0, sizeof(int), s);
+        cudaMemsetAsync(sens_dev, 0, sizeof(float) * ne, s);
+        launch_sensitivity_tc_dev(P, h->chi, h->ke, h->d_dcw, sens_dev, n[0], energy_tc_blocks(P, nsm), h->d_flag, s);
+        launch_penalize(ne, rho_dev, sens_dev, prm->penal, 1, s);
+        if (prm->sym >= 0) launch_symmetrize(n, sens_dev, prm->sym, s);
+        if (prm->filter_radius > 0) {
+            cudaMemsetAsync(h->tmp, 0, sizeof(float) * ne, s);
+            launch_filter(n, n[0], sens_dev, rho_dev, h->tmp, prm->filter_radius, prm->filter_periodic, s);
+            cudaMemcpyAsync(sens_dev, h->tmp, sizeof(float) * ne, cudaMemcpyDeviceToDevice, s);
+        }
+        launch_oc(sens_dev, rho_dev, h->tmp, ne, prm->volratio, prm->min_rho, prm->step_limit, prm->damp, h->partial,
+                  s);
+        if (prm->sym >= 0) launch_symmetrize(n, rho_dev, prm->sym, s);
+        cudaMemcpyAsync(&h->h_small[63], h->d_flag, sizeof(int), cudaMemcpyDeviceToHost, s);
+        CK(cudaStreamEndCapture(s, &g));
+        cudaError_t e = cudaGraphInstantiate(&h->dgraph, g, 0);
+        cudaGraphDestroy(g);
+        if (e != cudaSuccess) {
+            h->dgraph = nullptr;
+            return fail(h, H3D_ERR_CUDA, std::string("graph: ") + cudaGetErrorString(e));
+        }
+        h->dkey = *prm;
+        h->dkey_rho = rho_dev;
+        h->dkey_sens = sens_dev;
+    }
+    sensitivity_weights(P, dC, h->h_dcw);
+    CK(cudaGraphLaunch(h->dgraph, h->stream));
+    CK(cudaStreamSynchronize(h->stream));
+    if (*reinterpret_cast<int *>(&h->h_small[63]))
+        return fail(h, H3D_ERR_CUDA, "tensor-core energy kernel: mbarrier wait timed out");
     return H3D_OK;
 }
 

@@ -271,6 +271,13 @@ int launch_elastic_tc(const Planes &P, const double *chi, const float *rho, cons
 int launch_sensitivity_tc(const Planes &P, const double *chi, const KeMat &ke, const float *dc36, float *sens,
                           int pitch, int nblk, int *flag, cudaStream_t s);
 void launch_elastic_finish(const double *partial, int nblk, double *out21, cudaStream_t s);
+// the same sensitivity with its 21 weights (sensitivity_weights) read from device
+// memory at run time, for captured graphs; configure_energy_tc first (outside any
+// capture), -1 if the kernels cannot be configured
+void sensitivity_weights(const Planes &P, const float *dc36, float w21[21]);
+int configure_energy_tc();
+void launch_sensitivity_tc_dev(const Planes &P, const double *chi, const KeMat &ke, const float *dcw, float *sens,
+                               int pitch, int nblk, int *flag, cudaStream_t s);
 // design (k_design.cu)
 void launch_density_in(const int n[3], const float *src, int pitch, float *dst, cudaStream_t s);
 void launch_penalize(long long n, const float *rho, float *out, float p, int backward, cudaStream_t s);

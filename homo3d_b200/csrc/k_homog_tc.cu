@@ -123,10 +123,12 @@ struct TcDc { float w[21]; };  // (dC_ij + [i!=j] dC_ji) / |Y| for the 21 pairs
 
 // SENS = false: per-block FP64 partial sums of (1e-9 + rho_e) E_ij (21 values);
 // SENS = true: sens[x + (y + z*ny)*pitch] = sum_t dc_t E_t per element
+// dcw (SENS only, may be null): the 21 weights read from device memory instead of dc
 template <bool SENS>
 __global__ void __launch_bounds__(TC_M) k_energy_tc(Planes P, const double *__restrict__ chi,
                                                     const float *__restrict__ rho, const __grid_constant__ KeMat ke,
-                                                    double *partial, TcDc dc, float *sens, int pitch, int *flag) {
+                                                    double *partial, TcDc dc, const float *dcw, float *sens, int pitch,
+                                                    int *flag) {
     extern __shared__ __align__(1024) unsigned char tc_smem[];
     unsigned char *base = tc_smem + ((1024 - (smem_u32(tc_smem) & 1023)) & 1023);
     // A operand buffers b = 0, 1: hi at base + 2 b TILE, lo at base + (2 b + 1) TILE
@@ -134,6 +136,8 @@ __global__ void __launch_bounds__(TC_M) k_energy_tc(Planes P, const double *__re
     uint64_t *bar = reinterpret_cast<uint64_t *>(Blo + TC_B_BYTES);  // one mbarrier per A buffer
     uint32_t *tslot = reinterpret_cast<uint32_t *>(bar + 2);
     const int tid = threadIdx.x, warp = tid >> 5;
+    __shared__ float dcs[21];
+    if (SENS && tid < 21) dcs[tid] = dcw ? dcw[tid] : dc.w[tid];
 
     // Ke split into TF32 hi + lo, as the 24 x 24 B operand (B[n][k] = Ke[n][k])
     for (int q = tid; q < TC_K * TC_K; q += TC_M) {
@@ -290,7 +294,7 @@ __global__ void __launch_bounds__(TC_M) k_energy_tc(Planes P, const double *__re
             if (SENS) {
                 float s = 0.f;
 #pragma unroll
-                for (int t = 0; t < 21; ++t) s = fmaf(E[t], dc.w[t], s);
+                for (int t = 0; t < 21; ++t) s = fmaf(E[t], dcs[t], s);
                 sens[x + ((long long)y + (long long)z * P.n[1]) * pitch] = s;
             } else {
                 const double rp = (double)(RHO_PENAL_MIN + rho[e]);
@@ -339,7 +343,7 @@ int launch_elastic_tc(const Planes &P, const double *chi, const float *rho, cons
                       int nblk, int *flag, cudaStream_t s) {
     if (!tc_configured((const void *)k_energy_tc<false>)) return -1;
     TcDc dc{};
-    k_energy_tc<false><<<nblk, TC_M, TC_SMEM_REQUEST, s>>>(P, chi, rho, ke, partial, dc, nullptr, 0, flag);
+    k_energy_tc<false><<<nblk, TC_M, TC_SMEM_REQUEST, s>>>(P, chi, rho, ke, partial, dc, nullptr, nullptr, 0, flag);
     return 0;
 }
 
@@ -354,8 +358,30 @@ int launch_sensitivity_tc(const Planes &P, const double *chi, const KeMat &ke, c
             const double w = dc36[i * 6 + j] + (i != j ? dc36[j * 6 + i] : 0.f);
             dc.w[t] = (float)(w / vol);
         }
-    k_energy_tc<true><<<nblk, TC_M, TC_SMEM_REQUEST, s>>>(P, chi, nullptr, ke, nullptr, dc, sens, pitch, flag);
+    k_energy_tc<true><<<nblk, TC_M, TC_SMEM_REQUEST, s>>>(P, chi, nullptr, ke, nullptr, dc, nullptr, sens, pitch,
+                                                           flag);
     return 0;
+}
+
+// the 21 weights (dC_ij + [i != j] dC_ji) / |Y| of the sensitivity for dC[36]
+void sensitivity_weights(const Planes &P, const float *dc36, float w21[21]) {
+    const double vol = (double)P.nv;
+    int t = 0;
+    for (int i = 0; i < 6; i++)
+        for (int j = i; j < 6; j++, t++) {
+            const double w = dc36[i * 6 + j] + (i != j ? dc36[j * 6 + i] : 0.f);
+            w21[t] = (float)(w / vol);
+        }
+}
+
+int configure_energy_tc() {
+    return tc_configured((const void *)k_energy_tc<false>) && tc_configured((const void *)k_energy_tc<true>) ? 0 : -1;
+}
+
+void launch_sensitivity_tc_dev(const Planes &P, const double *chi, const KeMat &ke, const float *dcw, float *sens,
+                               int pitch, int nblk, int *flag, cudaStream_t s) {
+    TcDc dc{};
+    k_energy_tc<true><<<nblk, TC_M, TC_SMEM_REQUEST, s>>>(P, chi, nullptr, ke, nullptr, dc, dcw, sens, pitch, flag);
 }
 
 }  // namespace h3d

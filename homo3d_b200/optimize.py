@@ -87,9 +87,12 @@ class ConvergeChecker:
 def optimize_bulk(reso, vol=0.3, iters=50, seed=0, relthres=1e-2, filter_radius=2.0, step=0.05, damp=0.5,
                   sym="reflect6", finthres=5e-4, stop_on_converge=False, rho0=None, E=10.0, nu=0.3,
                   coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY, precision=PREC_REFINE, device=0,
-                  on_solve=None, stencil=STENCIL_FP16, objective="bulk"):
+                  on_solve=None, stencil=STENCIL_FP16, objective="bulk", device_step=True):
     """The OC loop of testAutoDiff.cu:282-331 (objective "bulk"), of
-    testAutoDiff.cu:334-381 ("shear") or of Framework.cu:208-272 ("npr"); on_solve(hom, rho_phys) is called after every
+    testAutoDiff.cu:334-381 ("shear") or of Framework.cu:208-272 ("npr");
+    device_step runs the update after each solve (sensitivity, SIMP backward,
+    symmetry, filter, OC, symmetry) as one captured graph (h3d_design_step),
+    otherwise as separate entry-point calls; on_solve(hom, rho_phys) is called after every
     solve (e.g. to record training pairs)."""
     obj_fn, grad_fn = OBJECTIVES[objective]
     import torch
@@ -118,13 +121,16 @@ def optimize_bulk(reso, vol=0.3, iters=50, seed=0, relthres=1e-2, filter_radius=
         if on_solve is not None:
             on_solve(hom, rhop)
         obj = float(obj_fn(C, it))
-        hom.Sensitivity(grad_fn(it), sens)
-        hom.penalize_backward(rho, sens, 3.0)
         done = checker.is_converge(it, obj)
-        symmetrize(hom, sens, n, sym)
-        oc.filterSens(sens, rho, n[0], n, filter_radius)
-        oc.update(sens, rho, vol)
-        symmetrize(hom, rho, n, sym)
+        if device_step:
+            hom.design_step(grad_fn(it), rho, sens, vol, 3.0, sym, filter_radius, False, 1e-3, step, damp)
+        else:
+            hom.Sensitivity(grad_fn(it), sens)
+            hom.penalize_backward(rho, sens, 3.0)
+            symmetrize(hom, sens, n, sym)
+            oc.filterSens(sens, rho, n[0], n, filter_radius)
+            oc.update(sens, rho, vol)
+            symmetrize(hom, rho, n, sym)
         e1.record(stream)
         e1.synchronize()
         records.append({"iter": it, "obj": obj, "vcycles": st["vcycles"], "solve_ms": st["solve_ms"],

@@ -219,6 +219,31 @@ H3D_API int h3d_oc_filter(h3d_handle *h, float *sens_dev, const float *rho_dev, 
 /* sym: 0 reflect3, 1 reflect6, 2 rotate3; lexicographic, pitch nx */
 H3D_API int h3d_symmetrize(h3d_handle *h, float *field_dev, const int reso[3], int sym);
 
+/* ---- one design update after a solve, on the device (testAutoDiff.cu:298-327,
+ * the body of optiBulk / optiShear / optiNpr after objective.eval()) ---------------
+ * sens = dObj/drho_phys from dC (as h3d_sensitivity), times p rho^(p-1) (the SIMP
+ * backward, homoExpression.h:89-119 through rho.pow(p)); symmetrised
+ * (symmetrizeField, Framework.cuh:222-236); filtered (OCOptimizer::filterSens,
+ * OCOptimizer.cu:134-152) unless filter_radius <= 0; the OC update of rho
+ * (OCOptimizer::update, OCOptimizer.cu:38-67); rho symmetrised.  rho_dev and
+ * sens_dev are the caller's lexicographic density and sensitivity (pitch nx).  The
+ * sequence is captured once per (rho, sens, parameters) as a CUDA graph on the
+ * handle's stream and replayed; dC is read from host memory when it runs, so no
+ * step waits on the host.  The call returns after the graph has run (the energy
+ * kernel's wait flag is checked then). */
+typedef struct {
+    float penal;                /* SIMP exponent p of rho_phys = rho^p */
+    int sym;                    /* 0 reflect3, 1 reflect6, 2 rotate3, -1 none */
+    float filter_radius;        /* cone filter radius; <= 0: no filter */
+    int filter_periodic;        /* periodic filter window */
+    float volratio;             /* target volume fraction */
+    float min_rho;              /* lower density bound (0.001 in the reference) */
+    float step_limit;           /* OC move limit */
+    float damp;                 /* OC damping exponent */
+} h3d_design_params;
+H3D_API int h3d_design_step(h3d_handle *h, const float dC[36], float *rho_dev, float *sens_dev,
+                            const h3d_design_params *prm);
+
 /* ---- MMA optimiser (MMAOptimizer, mmaOptimizer.h:12-36, mmaOpt.cu:429-1062) -
  * Method of moving asymptotes with m constraints g_i(x) <= 0 (1 <= m <= 4) on n
  * design variables; FP64 state on the device, float design and gradients at the

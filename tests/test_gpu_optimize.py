@@ -69,3 +69,26 @@ def test_npr_loop_lowers_poisson_coupling(torch_cuda):
     rho, C, rec = optimize_bulk(n, iters=10, rho0=rho0, relthres=1e-2, objective="npr")
     ratio = lambda c: (c[0, 1] + c[0, 2] + c[1, 2]) / (c[0, 0] + c[1, 1] + c[2, 2])
     assert ratio(C) < ratio(C0)  # the coupling falls relative to the diagonal
+
+
+@pytest.mark.parametrize("objective", ["bulk", "npr"])
+def test_device_design_step_equals_separate_calls(torch_cuda, objective):
+    """the captured design-step graph (h3d_design_step) runs the same kernels in the
+    same order as the separate entry points: the same densities to the last bit
+    (npr changes dC every iteration: the graph reads it at run time)"""
+    n = 16
+    rho0 = synthetic_density(n, seed=7, vol=0.3).ravel()
+    a = optimize_bulk(n, iters=4, rho0=rho0, relthres=1e-6, objective=objective, device_step=True)
+    b = optimize_bulk(n, iters=4, rho0=rho0, relthres=1e-6, objective=objective, device_step=False)
+    assert np.array_equal(a[0], b[0])
+    assert [r["obj"] for r in a[2]] == [r["obj"] for r in b[2]]
+
+
+def test_design_step_rejects_bad_arguments(torch_cuda):
+    torch = torch_cuda
+    hd = H.Homogenization(8)
+    rho = torch.full((8 ** 3,), 0.3, device="cuda")
+    sens = torch.zeros_like(rho)
+    with pytest.raises(H.H3DError):
+        hd.design_step(np.zeros((6, 6)), rho, sens, 1.5)
+    hd.close()
