@@ -46,6 +46,9 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--pin-mode", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="solve", choices=["solve", "mma"],
+                   help="solve: the homogenization step (default); mma: one MMA design update")
+    p.add_argument("--mma-m", type=int, default=1, help="constraints of the mma workload")
     p.add_argument("--profile", action="store_true",
                    help="only warm-up and timed steps (no e2e, setup or sweep side measurements), for ncu")
     p.add_argument("--precision", type=int, default=0,
@@ -429,8 +432,72 @@ def reference_arm(args):
             "e2e": {"value": value, "unit": "ms", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
 
 
+def mma_problem(n, m, seed=0):
+    """a separable design problem of n variables and m linear constraints: objective
+    gradient -w / x^2 (compliance-like), constraints A x - 0.3 sum(A) <= 0"""
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    w = rng.uniform(0.2, 1.0, n)
+    A = rng.uniform(0.5, 1.5, (m, n)) / n
+    return w, A
+
+
+def mma_arm(args):
+    """--workload mma: ms per MMA design update (MMAOptimizer::update,
+    mmaOpt.cu:1021-1062) with reso^3 design variables and --mma-m constraints,
+    through the library (h3d_mma_update, wall clock with the device synchronised:
+    the update runs its Newton steps under host control), beside the FP64 oracle's
+    MMA on the host (cpu_baseline, one update)."""
+    import numpy as np
+    import torch
+
+    import homo3d_b200 as H
+    n, m = args.reso ** 3, args.mma_m
+    w, A = mma_problem(n, m)
+    x0 = np.full(n, 0.3, np.float32)
+    df = (-w / 0.3 ** 2).astype(np.float32)
+    g = (A @ x0.astype(np.float64) - 0.3 * A.sum(axis=1)).astype(np.float32)
+    dev = torch.device("cuda", 0)
+    dft, gt = torch.tensor(df, device=dev), torch.tensor(g, device=dev)
+    dgt = [torch.tensor(A[i].astype(np.float32), device=dev) for i in range(m)]
+    times = []
+    for rep in range(args.warmup + args.steps):
+        mma = H.MMAOptimizer(m, n)
+        mma.setBound(0.001, 1.0)
+        x = torch.tensor(x0, device=dev)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        mma.update(0, x, dft, gt, dgt)
+        torch.cuda.synchronize()
+        if rep >= args.warmup:
+            times.append((time.perf_counter() - t0) * 1e3)
+        steps = mma.newton_steps
+        mma.close()
+    ms = statistics.median(times)
+    out = {"metric": "ms per MMA design update, %d^3 design variables, %d constraint(s)" % (args.reso, m),
+           "value": round(ms, 3), "unit": "ms", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+           "ms_per_step": round(ms, 3), "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+           "dtype": "f64", "data": "synthetic separable problem (objective gradient -w/x^2, linear constraints)",
+           "config": {"workload": "MMA update", "n": n, "m": m}, "newton_steps": steps,
+           "ms_all": [round(t, 3) for t in times]}
+    if not args.no_cpu_baseline:
+        from oracle import oracle as O
+        ora = O.MMA(m, n)
+        ora.set_bound(0.001, 1.0)
+        t0 = time.perf_counter()
+        ora.update(0, x0.astype(np.float64), df.astype(np.float64), g.astype(np.float64), A)
+        cs = time.perf_counter() - t0
+        out["cpu_baseline"] = {"value": round(cs * 1e3, 1), "unit": "ms", "cores": 1, "kind": "port",
+                               "sample": "FP64 oracle MMA (oracle/mma_oracle.c), one update of the same problem",
+                               "newton_steps": int(ora.newton)}
+    return out
+
+
 def main():
     args = parse()
+    if args.workload == "mma":
+        print(json.dumps(mma_arm(args)), flush=True)
+        return
     if args.impl == "reference":
         out = reference_arm(args)
     else:

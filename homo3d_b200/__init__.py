@@ -112,6 +112,8 @@ _SIGS = {
     "h3d_oc_filter": [_vp, _vp, _vp, _ip, ctypes.c_int, ctypes.c_float, ctypes.c_int],
     "h3d_symmetrize": [_vp, _vp, _ip, ctypes.c_int],
     "h3d_design_step": [_vp, _fp, _vp, _vp, ctypes.POINTER(DesignParams)],
+    "h3d_init_density_trig": [_vp, _vp, _ip, ctypes.c_int, _fp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
+                              ctypes.c_int],
     "h3d_get_field": [_vp, ctypes.c_int, ctypes.c_int, _fp],
     "h3d_set_field": [_vp, ctypes.c_int, ctypes.c_int, _fp],
     "h3d_mma_create": [ctypes.c_int, ctypes.c_int64, ctypes.c_double, ctypes.c_double, ctypes.c_double,
@@ -386,6 +388,19 @@ class Homogenization(_Handle):
         prm = DesignParams(float(penal), SYMMETRY[sym] if sym else -1, float(filter_radius), int(periodic),
                            float(volratio), float(min_rho), float(step_limit), float(damp))
         self.check(lib().h3d_design_step(self._h, d.ctypes.data_as(_fp), _ptr(rho), _ptr(sens), ctypes.byref(prm)))
+
+    def init_density_trig(self, rho, n_period=10, vol=0.3, sym="reflect6", centered=False, coeff=None, seed=0):
+        """the reference's trig-basis initial density (randTri, Framework.cuh:238-310)
+        into the CUDA tensor rho (the handle's grid); coefficients drawn uniformly in
+        [-1, 1) from SplitMix64(seed) unless given"""
+        from .density import trig_init_coefficients
+        if coeff is None:
+            coeff = trig_init_coefficients(n_period, seed, centered)
+        c = np.ascontiguousarray(coeff, dtype=np.float32)
+        self.check(lib().h3d_init_density_trig(self._h, _ptr(rho), _i3(self.dims[0]), int(n_period),
+                                               c.ctypes.data_as(_fp), c.size, int(centered), float(vol),
+                                               SYMMETRY[sym] if sym else -1))
+        return c
 
     def warm_start_learned(self, net):
         """stored solutions from a WarmNet's prediction for the current density"""

@@ -1282,6 +1282,50 @@ int h3d_symmetrize(h3d_handle *h, float *field_dev, const int reso[3], int sym) 
     return H3D_OK;
 }
 
+int h3d_init_density_trig(h3d_handle *h, float *rho_dev, const int reso[3], int n_period, const float *coeff,
+                          int ncoeff, int centered, float volratio, int sym) {
+    if (!h || !rho_dev || !reso || !coeff) return H3D_ERR_ARG;
+    if (n_period < 1 || n_period > 50) return fail(h, H3D_ERR_ARG, "n_period outside 1..50");
+    const int nbasis = 6 * n_period + 36 * n_period * n_period;
+    if (ncoeff != nbasis + (centered ? 4 : 0))
+        return fail(h, H3D_ERR_ARG, "coefficient count must be 6 P + 36 P^2 (+ 4 when centred)");
+    if (!(volratio > 0 && volratio <= 1)) return fail(h, H3D_ERR_ARG, "volratio outside (0, 1]");
+    if (sym < -1 || sym > 2) return fail(h, H3D_ERR_ARG, "sym must be -1, 0, 1 or 2");
+    if (sym > 0 && (reso[0] != reso[1] || reso[1] != reso[2]))
+        return fail(h, H3D_ERR_ARG, "reflect6 and rotate3 need a cubic grid");
+    for (int d = 0; d < 3; d++)
+        if (reso[d] < 2) return fail(h, H3D_ERR_ARG, "each axis needs at least two cells");
+    // rotation of the unit quaternion (w, x, y, z) of the four extra coefficients
+    float rot[9] = {1, 0, 0, 0, 1, 0, 0, 0, 1};
+    if (centered) {
+        double q[4] = {coeff[nbasis], coeff[nbasis + 1], coeff[nbasis + 2], coeff[nbasis + 3]};
+        const double qn = std::sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2] + q[3] * q[3]);
+        if (!(qn > 0)) return fail(h, H3D_ERR_ARG, "zero quaternion");
+        for (double &v : q) v /= qn;
+        const double w = q[0], x = q[1], y = q[2], z = q[3];
+        const double R[9] = {1 - 2 * (y * y + z * z), 2 * (x * y - w * z),     2 * (x * z + w * y),
+                             2 * (x * y + w * z),     1 - 2 * (x * x + z * z), 2 * (y * z - w * x),
+                             2 * (x * z - w * y),     2 * (y * z + w * x),     1 - 2 * (x * x + y * y)};
+        for (int i = 0; i < 9; i++) rot[i] = (float)R[i];
+    }
+    CK(cudaSetDevice(h->device));
+    float *dcoeff = nullptr;
+    CK(cudaMalloc(&dcoeff, sizeof(float) * ncoeff));
+    cudaError_t e = cudaMemcpyAsync(dcoeff, coeff, sizeof(float) * ncoeff, cudaMemcpyHostToDevice, h->stream);
+    int rc = H3D_OK;
+    if (e != cudaSuccess) rc = fail(h, H3D_ERR_CUDA, cudaGetErrorString(e));
+    else if (launch_trig_init(reso, n_period, dcoeff, centered, rot, volratio, sym, rho_dev, h->partial, h->stream) != 0)
+        rc = fail(h, H3D_ERR_CUDA, "trig-basis kernel could not be configured");
+    e = cudaStreamSynchronize(h->stream);
+    cudaFree(dcoeff);
+    if (rc == H3D_OK && e != cudaSuccess) rc = fail(h, H3D_ERR_CUDA, cudaGetErrorString(e));
+    if (rc == H3D_OK) {
+        e = cudaGetLastError();
+        if (e != cudaSuccess) rc = fail(h, H3D_ERR_CUDA, std::string("launch: ") + cudaGetErrorString(e));
+    }
+    return rc;
+}
+
 int h3d_design_step(h3d_handle *h, const float dC[36], float *rho_dev, float *sens_dev, const h3d_design_params *prm) {
     if (!h || !dC || !rho_dev || !sens_dev || !prm) return H3D_ERR_ARG;
     const Planes &P = h->lv[0].P;

@@ -286,6 +286,11 @@ void launch_oc(const float *sens, float *rho, float *rho_new, long long n, float
 void launch_filter(const int n[3], int pitch, const float *sens, const float *rho, float *out, float radius,
                    int periodic, cudaStream_t s);
 void launch_symmetrize(const int n[3], float *v, int sym, cudaStream_t s);
+// the reference's trig-basis initial density (randTri): basis sum with P periods,
+// symmetrised (sym >= 0), level-set mapped to volume vol; scratch holds 4 + 1184
+// doubles; -1 if the kernel's shared memory (6 P x 64 floats) cannot be granted
+int launch_trig_init(const int n[3], int P, const float *coeff_dev, int centered, const float rot[9], float vol, int sym,
+                     float *rho, double *scratch, cudaStream_t s);
 // weighted norms with file-scope device scratch (k_static_norm.cu), on the
 // current device: the launcher returns -1 when nblk exceeds STATIC_NORM_MAX_BLOCKS
 // and -2 when the array's address cannot be looked up; the totals pointer is the

@@ -284,4 +284,140 @@ void launch_symmetrize(const int n[3], float *v, int sym, cudaStream_t s) {
     }
 }
 
+// ---- the reference's trig-basis initial density -----------------------------------
+// randTribase_sincos_kernel (Framework.cuh:106-222) and randTri (Framework.cuh:238-310):
+// at voxel (x, y, z) with p = (x, y, z) / (dim - 1) (centred: p - 1/2 rotated by the
+// unit quaternion of the four coefficients after the basis ones), with
+// c[a][i] = cos(2 pi (i+1) p_a), s[a][i] = sin(2 pi (i+1) p_a), i < P:
+//   first order,  6P terms:   coeff[i] c[i%3][i/3] for i < 3P, then
+//                             coeff[i] s[j%3][j/3] with j = i - 3P;
+//   second order, 36P^2 terms: coeff[6P + 6P j + k] v(j) v(k), j, k < 6P, where
+//                             v(j) = c[j/P][j%P] for j < 3P, s[j/P-3][j%P] otherwise.
+// One thread per voxel; its 6P basis values v(j) in shared memory (P <= 50).  The
+// sum runs in FP64 and is rounded to FP32 (the reference sums eight FP32 partials of
+// a warp-strided split).
+struct TrigArgs {
+    int n[3];
+    int P;
+    int centered;
+    float rot[9];  // row-major rotation of the centred position
+};
+
+constexpr int TRIG_BS = 64;
+
+__global__ void __launch_bounds__(TRIG_BS) k_trig_basis(TrigArgs a, const float *__restrict__ coeff, float *out) {
+    extern __shared__ float tv[];  // [6P][TRIG_BS]
+    const long long ne = (long long)a.n[0] * a.n[1] * a.n[2];
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const int P = a.P, t = threadIdx.x;
+    float p[3] = {0.f, 0.f, 0.f};
+    if (e < ne) {
+        const int x = (int)(e % a.n[0]);
+        const long long tt = e / a.n[0];
+        const int y = (int)(tt % a.n[1]), z = (int)(tt / a.n[1]);
+        p[0] = (float)x / (float)(a.n[0] - 1);
+        p[1] = (float)y / (float)(a.n[1] - 1);
+        p[2] = (float)z / (float)(a.n[2] - 1);
+        if (a.centered) {
+            const float q[3] = {p[0] - 0.5f, p[1] - 0.5f, p[2] - 0.5f};
+            for (int r = 0; r < 3; ++r) p[r] = a.rot[3 * r] * q[0] + a.rot[3 * r + 1] * q[1] + a.rot[3 * r + 2] * q[2];
+        }
+    }
+    constexpr float pi2 = 3.1415926f * 2;  // the reference's constant (Framework.cuh:113)
+    for (int j = 0; j < 3 * P; ++j) {
+        const int ax = j / P, i = j % P;
+        tv[j * TRIG_BS + t] = cosf(pi2 * (i + 1) * p[ax]);
+        tv[(3 * P + j) * TRIG_BS + t] = sinf(pi2 * (i + 1) * p[ax]);
+    }
+    if (e >= ne) return;
+    double sum = 0;
+    for (int i = 0; i < 6 * P; ++i) {  // first order: component fastest
+        const int j = i < 3 * P ? i : i - 3 * P;
+        const int v = (j % 3) * P + j / 3 + (i < 3 * P ? 0 : 3 * P);
+        sum += (double)coeff[i] * (double)tv[v * TRIG_BS + t];
+    }
+    const float *c2 = coeff + 6 * P;
+    for (int j = 0; j < 6 * P; ++j) {
+        const double vj = (double)tv[j * TRIG_BS + t];
+        double inner = 0;
+        for (int k = 0; k < 6 * P; ++k) inner += (double)c2[6 * P * j + k] * (double)tv[k * TRIG_BS + t];
+        sum += vj * inner;
+    }
+    out[e] = (float)sum;
+}
+
+// level-set volume search of randTri: x = m + (M - m) / (1 + exp(-15 (v - t))),
+// M = min(1.5 vol, 1), m = 0.001; t bisected on [-37 P^2, 37 P^2] for at most 60
+// steps until the mean is within 1e-3 (relative) of vol.
+// state: [0] t_l, [1] t_u, [2] done, [3] t, [4 ..] block partial sums
+__device__ __forceinline__ float trig_level_map(float v, float t, float M) {
+    const float sgm = 1.f / (1 + expf(-15.f * (v - t)));
+    return sgm * (M - 0.001f) + 0.001f;
+}
+
+__global__ void k_level_init(double *st, float P) {
+    if (threadIdx.x == 0) {
+        const float tu = P * P * 37;
+        st[0] = -tu;
+        st[1] = tu;
+        st[2] = 0.0;
+        st[3] = 0.0;
+    }
+}
+
+__global__ void __launch_bounds__(OC_BS) k_level_step(const float *__restrict__ v, long long n, float M, double *st) {
+    if (st[2] != 0.0) return;
+    const float t = ((float)st[1] + (float)st[0]) / 2;
+    double s = 0;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        s += trig_level_map(v[i], t, M);
+    double ss[1] = {s};
+    block_reduce<1>(ss, st + 4, blockIdx.x);
+}
+
+__global__ void k_level_decide(double *st, int nb, long long n, float vol) {
+    if (threadIdx.x != 0 || st[2] != 0.0) return;
+    double s = 0;
+    for (int b = 0; b < nb; b++) s += st[4 + b];
+    const float mean = (float)(s / (double)n);
+    const float t = ((float)st[1] + (float)st[0]) / 2;
+    st[3] = t;
+    if (fabsf(mean - vol) / vol < 1e-3f) {
+        st[2] = 1.0;
+        return;
+    }
+    if (mean > vol) st[0] = t;
+    if (mean < vol) st[1] = t;
+}
+
+__global__ void k_level_apply(float *v, long long n, float M, const double *st) {
+    const float t = (float)st[3];
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        v[i] = trig_level_map(v[i], t, M);
+}
+
+int launch_trig_init(const int n[3], int P, const float *coeff_dev, int centered, const float rot[9], float vol, int sym,
+                     float *rho, double *scratch, cudaStream_t s) {
+    TrigArgs a;
+    for (int d = 0; d < 3; ++d) a.n[d] = n[d];
+    a.P = P;
+    a.centered = centered;
+    for (int i = 0; i < 9; ++i) a.rot[i] = rot[i];
+    const long long ne = (long long)n[0] * n[1] * n[2];
+    const size_t smem = sizeof(float) * 6 * P * TRIG_BS;
+    if (cudaFuncSetAttribute((const void *)k_trig_basis, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+        cudaSuccess)
+        return -1;
+    k_trig_basis<<<(unsigned)((ne + TRIG_BS - 1) / TRIG_BS), TRIG_BS, smem, s>>>(a, coeff_dev, rho);
+    if (sym >= 0) launch_symmetrize(n, rho, sym, s);
+    const float M = fminf(vol * 1.5f, 1.f);
+    k_level_init<<<1, 32, 0, s>>>(scratch, (float)P);
+    for (int it = 0; it < 60; ++it) {
+        k_level_step<<<OC_NB, OC_BS, 0, s>>>(rho, ne, M, scratch);
+        k_level_decide<<<1, 32, 0, s>>>(scratch, OC_NB, ne, vol);
+    }
+    k_level_apply<<<OC_NB, OC_BS, 0, s>>>(rho, ne, M, scratch);
+    return 0;
+}
+
 }  // namespace h3d

@@ -30,6 +30,15 @@ class SplitMix64:
         return (self.next_u64() >> 11) * (1.0 / (1 << 53))
 
 
+def trig_init_coefficients(n_period, seed=0, centered=False):
+    """coefficients of the reference's randTri initialiser (Framework.cuh:238-310):
+    6 P + 36 P^2 (+ 4 for the centred form) values uniform in [-1, 1), drawn here from
+    SplitMix64(seed) in place of the reference's clock-seeded curand generator"""
+    rng = SplitMix64(seed)
+    nb = 6 * n_period + 36 * n_period * n_period + (4 if centered else 0)
+    return np.array([2.0 * rng.uniform() - 1.0 for _ in range(nb)], np.float32)
+
+
 def trig_coefficients(seed):
     rng = SplitMix64(seed)
     a = np.zeros((3, 3, 3))

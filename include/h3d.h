@@ -219,6 +219,18 @@ H3D_API int h3d_oc_filter(h3d_handle *h, float *sens_dev, const float *rho_dev, 
 /* sym: 0 reflect3, 1 reflect6, 2 rotate3; lexicographic, pitch nx */
 H3D_API int h3d_symmetrize(h3d_handle *h, float *field_dev, const int reso[3], int sym);
 
+/* ---- the reference's trig-basis initial density (Framework.cuh:106-310 randTri with
+ * randTribase_sincos_kernel; -init random / randcenter) -------------------------
+ * rho_dev[x + nx (y + ny z)] = the basis sum of n_period periods per axis with the
+ * caller's coefficients (6 P + 36 P^2 of them, the reference draws them uniformly
+ * in [-1, 1) from a clock-seeded generator; centered = 1 takes four more, a
+ * quaternion rotating the centred position), symmetrised (sym as h3d_symmetrize,
+ * -1 none), then mapped through the level set m + (M - m) sigmoid(15 (v - t)),
+ * M = min(1.5 volratio, 1), m = 0.001, with t bisected until the mean volume is
+ * within 1e-3 of volratio.  1 <= n_period <= 50. */
+H3D_API int h3d_init_density_trig(h3d_handle *h, float *rho_dev, const int reso[3], int n_period, const float *coeff,
+                                  int ncoeff, int centered, float volratio, int sym);
+
 /* ---- one design update after a solve, on the device (testAutoDiff.cu:298-327,
  * the body of optiBulk / optiShear / optiNpr after objective.eval()) ---------------
  * sens = dObj/drho_phys from dC (as h3d_sensitivity), times p rho^(p-1) (the SIMP
