@@ -392,7 +392,7 @@ namespace {
 int autotune(h3d_handle *h) {
     CK(cudaSetDevice(h->device));
     cudaStream_t s = h->stream;
-    constexpr int NSHAPE = 2, REPS = 3;
+    constexpr int NSHAPE = H3D_NUM_SHAPES, REPS = 3;
     for (int l = 0; l < h->nl - 1; l++) {
         Level &L = h->lv[l];
         for (int kind = 0; kind < (l > 0 ? 2 : 1); kind++) {  // 0: sweep, 1: residual
@@ -1072,7 +1072,8 @@ int h3d_get_tuning(const h3d_handle *h, int level, int shapes[2]) {
 
 int h3d_set_tuning(h3d_handle *h, int level, int gs_shape, int res_shape) {
     if (!h) return H3D_ERR_ARG;
-    if (level < 0 || level >= h->nl || gs_shape < 0 || gs_shape > 1 || res_shape < 0 || res_shape > 1)
+    if (level < 0 || level >= h->nl || gs_shape < 0 || gs_shape >= H3D_NUM_SHAPES || res_shape < 0 ||
+        res_shape >= H3D_NUM_SHAPES)
         return fail(h, H3D_ERR_ARG, "level or launch shape out of range");
     h->lv[level].gs_shape = gs_shape;
     h->lv[level].res_shape = res_shape;

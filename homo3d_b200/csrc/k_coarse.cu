@@ -60,7 +60,8 @@ __device__ __forceinline__ void load_block(const CoarseArgs &a, long long me, fl
 // case pairs, CTAs per SM): shape 0 = three threads per vertex with two cases
 // each, 6 CTAs/SM; shape 1 = one thread per vertex with all six, 4 CTAs/SM.  The
 // threads of one vertex run in adjacent CTAs, so repeated stencil reads hit L2;
-// both shapes give the same result to the last bit.
+// shape 2 = two cases per thread at 4 CTAs/SM, shape 3 = six cases per thread at 3
+// CTAs/SM.  All shapes give the same result to the last bit.
 
 // KC: the vertex colour, or -1 for the run-time colour kr (one code body for all
 // colours)
@@ -232,11 +233,19 @@ void launch_coarse_gs(const Level &L, float w, cudaStream_t s) {
     CoarseArgs a = make_cargs(L);
     a.w = w;
     if (L.st32) {
-        if (L.gs_shape == 1) coarse_gs_sweep<true, 6, 4>(a, s);
-        else coarse_gs_sweep<true, 2, 6>(a, s);
+        switch (L.gs_shape) {
+        case 1: coarse_gs_sweep<true, 6, 4>(a, s); break;
+        case 2: coarse_gs_sweep<true, 2, 4>(a, s); break;
+        case 3: coarse_gs_sweep<true, 6, 3>(a, s); break;
+        default: coarse_gs_sweep<true, 2, 6>(a, s); break;
+        }
     } else {
-        if (L.gs_shape == 1) coarse_gs_sweep<false, 6, 4>(a, s);
-        else coarse_gs_sweep<false, 2, 6>(a, s);
+        switch (L.gs_shape) {
+        case 1: coarse_gs_sweep<false, 6, 4>(a, s); break;
+        case 2: coarse_gs_sweep<false, 2, 4>(a, s); break;
+        case 3: coarse_gs_sweep<false, 6, 3>(a, s); break;
+        default: coarse_gs_sweep<false, 2, 6>(a, s); break;
+        }
     }
 }
 
@@ -249,11 +258,19 @@ static void coarse_residual_all(const CoarseArgs &a, cudaStream_t s) {
 template <unsigned NCOL>
 static void coarse_residual_shape(const Level &L, const CoarseArgs &a, cudaStream_t s) {
     if (L.st32) {
-        if (L.res_shape == 1) coarse_residual_all<true, 6, 4, NCOL>(a, s);
-        else coarse_residual_all<true, 2, 6, NCOL>(a, s);
+        switch (L.res_shape) {
+        case 1: coarse_residual_all<true, 6, 4, NCOL>(a, s); break;
+        case 2: coarse_residual_all<true, 2, 4, NCOL>(a, s); break;
+        case 3: coarse_residual_all<true, 6, 3, NCOL>(a, s); break;
+        default: coarse_residual_all<true, 2, 6, NCOL>(a, s); break;
+        }
     } else {
-        if (L.res_shape == 1) coarse_residual_all<false, 6, 4, NCOL>(a, s);
-        else coarse_residual_all<false, 2, 6, NCOL>(a, s);
+        switch (L.res_shape) {
+        case 1: coarse_residual_all<false, 6, 4, NCOL>(a, s); break;
+        case 2: coarse_residual_all<false, 2, 4, NCOL>(a, s); break;
+        case 3: coarse_residual_all<false, 6, 3, NCOL>(a, s); break;
+        default: coarse_residual_all<false, 2, 6, NCOL>(a, s); break;
+        }
     }
 }
 
@@ -278,11 +295,19 @@ void launch_coarse_gs_residual(const Level &L, float w, cudaStream_t s) {
     CoarseArgs a = make_cargs(L);
     a.w = w;
     if (L.st32) {
-        if (L.gs_shape == 1) coarse_gs_sweep_res<true, 6, 4>(a, s);
-        else coarse_gs_sweep_res<true, 2, 6>(a, s);
+        switch (L.gs_shape) {
+        case 1: coarse_gs_sweep_res<true, 6, 4>(a, s); break;
+        case 2: coarse_gs_sweep_res<true, 2, 4>(a, s); break;
+        case 3: coarse_gs_sweep_res<true, 6, 3>(a, s); break;
+        default: coarse_gs_sweep_res<true, 2, 6>(a, s); break;
+        }
     } else {
-        if (L.gs_shape == 1) coarse_gs_sweep_res<false, 6, 4>(a, s);
-        else coarse_gs_sweep_res<false, 2, 6>(a, s);
+        switch (L.gs_shape) {
+        case 1: coarse_gs_sweep_res<false, 6, 4>(a, s); break;
+        case 2: coarse_gs_sweep_res<false, 2, 4>(a, s); break;
+        case 3: coarse_gs_sweep_res<false, 6, 3>(a, s); break;
+        default: coarse_gs_sweep_res<false, 2, 6>(a, s); break;
+        }
     }
     coarse_residual_shape<7>(L, a, s);
 }

@@ -569,8 +569,9 @@ static unsigned task_blocks(const FineArgs &a, int cpt) { return (unsigned)(((a.
 int fine_residual_blocks(const Level &L) { return (int)(((L.P.nv / 8 + FBS - 1) / FBS) * (NCASE / CPT) * 8); }
 
 // the colour sweep in launch shape v: 0 = one thread per vertex with all six
-// cases (4 CTAs/SM), 1 = three threads per vertex with two cases each (5 CTAs/SM);
-// both give the same result to the last bit
+// cases (4 CTAs/SM), 1 = three threads per vertex with two cases each (5 CTAs/SM),
+// 2 = six cases per thread at 3 CTAs/SM (more registers), 3 = two cases per thread
+// at 6 CTAs/SM (fewer registers); all give the same result to the last bit
 template <int C, int MINB>
 static void fine_gs_sweep(const FineArgs &a, const KeMat &ke, cudaStream_t s) {
     const unsigned nb = task_blocks(a, C);
@@ -587,8 +588,12 @@ static void fine_gs_sweep(const FineArgs &a, const KeMat &ke, cudaStream_t s) {
 void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, cudaStream_t s) {
     FineArgs a = make_args(L, rho);
     a.w = w;
-    if (L.gs_shape == 1) fine_gs_sweep<2, 5>(a, ke, s);
-    else fine_gs_sweep<6, 4>(a, ke, s);
+    switch (L.gs_shape) {
+    case 1: fine_gs_sweep<2, 5>(a, ke, s); break;
+    case 2: fine_gs_sweep<6, 3>(a, ke, s); break;
+    case 3: fine_gs_sweep<2, 6>(a, ke, s); break;
+    default: fine_gs_sweep<6, 4>(a, ke, s); break;
+    }
 }
 
 // a sweep followed by the residual (the down leg of a V-cycle): the last colour's
@@ -612,8 +617,12 @@ void launch_fine_gs_residual(const Level &L, const float *rho, const KeMat &ke, 
                              cudaStream_t s) {
     FineArgs a = make_args(L, rho);
     a.w = w;
-    if (L.gs_shape == 1) fine_gs_sweep_res<2, 5>(a, ke, norm_partial, s);
-    else fine_gs_sweep_res<6, 4>(a, ke, norm_partial, s);
+    switch (L.gs_shape) {
+    case 1: fine_gs_sweep_res<2, 5>(a, ke, norm_partial, s); break;
+    case 2: fine_gs_sweep_res<6, 3>(a, ke, norm_partial, s); break;
+    case 3: fine_gs_sweep_res<2, 6>(a, ke, norm_partial, s); break;
+    default: fine_gs_sweep_res<6, 4>(a, ke, norm_partial, s); break;
+    }
 }
 
 void launch_fine_residual(const Level &L, const float *rho, const KeMat &ke, double *norm_partial, int nblk_norm,

@@ -179,14 +179,17 @@ H3D_API int h3d_sensitivity(h3d_handle *h, const float dC[36], float *sens_dev, 
 H3D_API int h3d_reset_solutions(h3d_handle *h);
 
 /* ---- autotuner (no reference counterpart) ----------------------------------
- * Each smoothed level has two launch shapes for its colour sweep and (coarse
- * levels) its residual: shape 0 / 1 = one thread per vertex with all six load
- * cases / three threads with two cases each on level 0, the reverse on the coarse
- * levels.  Both give the same results to the last bit.  The first solve of a
- * handle times them (CUDA events, a few sweeps per shape, iterating on the
- * level's scratch residual field) and keeps the faster; h3d_autotune re-runs that
- * now, h3d_set_tuning fixes the shapes (and turns the automatic tuning off),
- * h3d_get_tuning reads them: shapes[0] = sweep, shapes[1] = residual. */
+ * Each smoothed level has H3D_NUM_SHAPES launch shapes for its colour sweep and
+ * (coarse levels) its residual: load cases per thread (all six, or two as three
+ * threads per vertex) times CTAs per SM (the register budget per thread).  Level 0:
+ * shape 0 / 1 / 2 / 3 = six cases at 4 CTAs/SM / two at 5 / six at 3 / two at 6;
+ * coarse levels: two at 6 / six at 4 / two at 4 / six at 3.  All give the same
+ * results to the last bit.  The first solve of a handle times them (CUDA events,
+ * a few sweeps per shape, iterating on the level's scratch residual field) and
+ * keeps the fastest; h3d_autotune re-runs that now, h3d_set_tuning fixes the
+ * shapes (and turns the automatic tuning off), h3d_get_tuning reads them:
+ * shapes[0] = sweep, shapes[1] = residual. */
+#define H3D_NUM_SHAPES 4
 H3D_API int h3d_autotune(h3d_handle *h);
 H3D_API int h3d_get_tuning(const h3d_handle *h, int level, int shapes[2]);
 H3D_API int h3d_set_tuning(h3d_handle *h, int level, int gs_shape, int res_shape);

@@ -7,7 +7,9 @@ The oracle (oracle/h3d_oracle.c, FP64, OpenMP over the host cores) solves each
 design to a relative residual of 1e-8 (at most 60 V-cycles; the residual reached
 is recorded), then reduces C (homogenization.cu:464-575) and the sensitivities of
 the bulk-modulus objective for dC = the objective's gradient
-(homogenization.cu:697-948).  The densities are rounded to FP32 before the oracle
+(homogenization.cu:697-948), summarised raw and weighted by the physical density
+(in near-void elements the raw sensitivity depends on how far the solve went:
+their displacements barely enter the residual).  The densities are rounded to FP32 before the oracle
 sees them, as the library receives them.  Each record also holds the V-cycle
 count at which the oracle's solve first met relthres 1e-5.
 
@@ -68,16 +70,17 @@ def run_case(n, vol, seed, tol=1e-8, maxit=60):
     to_1e5 = int(np.argmax(worst <= 1e-5)) + 1 if (worst <= 1e-5).any() else None
     return {"reso": n, "vol": vol, "seed": seed, "tol": tol, "vcycles": int(cycles), "vcycles_to_1e-5": to_1e5,
             "rel_res": [float(x) for x in hist[-1]], "C": [float(x) for x in C.ravel()],
-            "sens_bulk": sens_checksum(sens), "oracle_s": round(secs, 1), "threads": os.cpu_count()}
+            "sens_bulk": sens_checksum(sens), "sens_bulk_weighted": sens_checksum(rho * sens), "oracle_s": round(secs, 1), "threads": os.cpu_count()}
 
 
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--only", type=int, default=0)
+    p.add_argument("--vol", type=float, default=0)
     args = p.parse_args()
     data = json.load(open(OUT)) if os.path.exists(OUT) else {"cases": []}
     for n, vol, seed in CASES:
-        if args.only and n != args.only:
+        if (args.only and n != args.only) or (args.vol and abs(vol - args.vol) > 1e-9):
             continue
         r = run_case(n, vol, seed)
         print(json.dumps({k: r[k] for k in ("reso", "vol", "vcycles", "vcycles_to_1e-5", "rel_res", "oracle_s")}),

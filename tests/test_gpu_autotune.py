@@ -24,9 +24,10 @@ def _solve(torch, n, shapes, precision, stencil=H.STENCIL_FP16):
                                                (H.PREC_REFINE, H.STENCIL_FP32)])
 def test_launch_shapes_are_bit_identical(torch_cuda, precision, stencil):
     C0, s0 = _solve(torch_cuda, 32, 0, precision, stencil)
-    C1, s1 = _solve(torch_cuda, 32, 1, precision, stencil)
-    assert np.array_equal(C0, C1)
-    assert s0["vcycles"] == s1["vcycles"] and s0["rel_res"] == s1["rel_res"]
+    for shape in range(1, H.NUM_SHAPES):
+        C1, s1 = _solve(torch_cuda, 32, shape, precision, stencil)
+        assert np.array_equal(C0, C1), shape
+        assert s0["vcycles"] == s1["vcycles"] and s0["rel_res"] == s1["rel_res"], shape
 
 
 def test_first_solve_tunes_and_tuning_entry_points(torch_cuda):
@@ -39,12 +40,12 @@ def test_first_solve_tunes_and_tuning_entry_points(torch_cuda):
     assert all(t == (0, 0) for t in hd.tuning())
     C = hd.elasticMatrix(1e-5)
     shapes = hd.tuning()
-    assert len(shapes) == hd.nlevels and all(g in (0, 1) and r in (0, 1) for g, r in shapes)
+    assert len(shapes) == hd.nlevels and all(0 <= g < H.NUM_SHAPES and 0 <= r < H.NUM_SHAPES for g, r in shapes)
     # re-tuning and forcing shapes keep the same C
     hd.autotune()
     hd.reset_solutions()
     assert np.array_equal(hd.elasticMatrix(1e-5), C)
-    for bad in [(-1, 0, 0), (hd.nlevels, 0, 0), (0, 2, 0), (1, 0, 5)]:
+    for bad in [(-1, 0, 0), (hd.nlevels, 0, 0), (0, H.NUM_SHAPES, 0), (1, 0, 5)]:
         with pytest.raises(H.H3DError):
             hd.set_tuning(*bad)
     hd.close()

@@ -58,12 +58,19 @@ def solve_and_check(torch, n, vol, precision=H.PREC_REFINE):
         assert err <= 1e-4, (n, vol, err)
         sens = torch.zeros(n ** 3, dtype=torch.float32, device="cuda")
         hd.Sensitivity(bulk_dC(), sens)
-        s, s2, octs = checksum(sens.cpu().numpy(), n)
-        ref = fx["sens_bulk"]
-        assert abs(s - ref["sum"]) <= 1e-4 * abs(ref["sum"])
-        assert abs(s2 - ref["sumsq"]) <= 1e-4 * abs(ref["sumsq"])
-        ro = np.array(ref["octants"])
-        assert np.abs(octs - ro).max() <= 1e-4 * np.abs(ro).max()
+        sh = sens.cpu().numpy()
+        # weighted by the physical density everywhere; raw where no element is
+        # near-void (at volume 0.1 the raw sensitivity of the void phase depends on
+        # how far the solve went: its displacements barely enter the residual)
+        checks = [(rho.astype(np.float64) * sh, fx["sens_bulk_weighted"])]
+        if vol >= 0.3:
+            checks.append((sh, fx["sens_bulk"]))
+        for field, ref in checks:
+            s, s2, octs = checksum(field, n)
+            assert abs(s - ref["sum"]) <= 1e-4 * abs(ref["sum"])
+            assert abs(s2 - ref["sumsq"]) <= 1e-4 * abs(ref["sumsq"])
+            ro = np.array(ref["octants"])
+            assert np.abs(octs - ro).max() <= 1e-4 * np.abs(ro).max()
         return st
     finally:
         hd.close()
