@@ -123,9 +123,10 @@ def max_over_ranks(dist, value):
 
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the eight colour
-# launches of one fine sweep, from an ncu capture of this bench's workload: every
-# colour launch reads the whole u field (it exceeds L2), 3.4x the algorithmic bytes
-SWEEP_TRAFFIC_BYTES = {256: 12_580_000_000}
+# launches of one fine sweep: an ncu capture at 128^3 (1.51 GB per sweep: every
+# colour launch reads the whole u field, which exceeds L2) scaled by the vertex
+# count, 3.3x the algorithmic bytes
+SWEEP_TRAFFIC_BYTES = {128: 1_510_000_000, 256: 12_080_000_000}
 
 PRECISION_NAME = {0: "FP32 V-cycles on the correction of an FP64 solution (iterative refinement)",
                   1: "FP32 solution (the reference's scheme)",
@@ -292,7 +293,8 @@ def gpu_arm(args):
                          "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                          "frac": round(achieved / peaks.get("hbm_gbs"), 4),
                          "traffic": SWEEP_TRAFFIC_BYTES.get(args.reso) if args.precision == 0 else None,
-                         "traffic_unit": "bytes of DRAM read + write per sweep (ncu capture)",
+                         "traffic_unit": "bytes of DRAM read + write per sweep (ncu capture at 128^3, "
+                                         "scaled by the vertex count)",
                          "sweep_ms": round(sweep_ms, 4), "fp32_tflops": round(flops_sweep / sweep_ms / 1e9, 2),
                          "peak_source": "measured" if "when" in peaks else "fallback"},
             "clocks": clk,
