@@ -46,6 +46,7 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--pin-mode", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--no-north-star", action="store_true", help="skip the mixed-precision arm of the same step")
     p.add_argument("--workload", default="solve", choices=["solve", "mma"],
                    help="solve: the homogenization step (default); mma: one MMA design update")
     p.add_argument("--mma-m", type=int, default=1, help="constraints of the mma workload")
@@ -300,9 +301,56 @@ def gpu_arm(args):
             "clocks": clk,
         }
     hd.close()
+    if rank == 0 and world == 1 and args.precision == 0 and not args.no_north_star:
+        result["north_star"] = north_star(args, rho_d, ms_per_solve, vc, c_err, fx)
     if dist is not None:
         dist.destroy_process_group()
     return result
+
+
+def north_star(args, rho_d, plain_ms, plain_vc, plain_err, fx):
+    """The precision arms of the same step on the same design, device-timed like the
+    headline value: the plain arm (the headline: refined FP32 V-cycles, SIMT
+    operator) against the mixed arm (the level-0 V-cycle residual on the tensor
+    cores, H3D_PREC_MIXED).  The learned warm start is not in the step: its trained
+    network saves no V-cycles on fresh designs (the solver's fallback rejects its
+    prediction), so it would only add its forward pass."""
+    import numpy as np
+    import torch
+
+    import homo3d_b200 as H
+    hm = H.Homogenization(args.reso, pin_mode=args.pin_mode, precision=H.PREC_MIXED)
+    stream = torch.cuda.ExternalStream(hm.stream)
+
+    def step():
+        hm.update(rho_d)
+        hm.reset_solutions()
+        return hm.elasticMatrix(args.tol)
+
+    for _ in range(max(1, min(args.warmup, 2))):
+        step()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    cyc = []
+    for _ in range(args.steps):
+        C = step()
+        cyc.append(hm.last_stats["vcycles"])
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    st = hm.last_stats
+    hm.close()
+    mixed_ms = ev0.elapsed_time(ev1) / args.steps
+    err = None
+    if fx is not None:
+        Co = np.array(fx["C"]).reshape(6, 6)
+        err = float(np.abs(C - Co).max() / np.abs(Co).max())
+    return {"plain_ms": round(plain_ms, 3), "mixed_ms": round(mixed_ms, 3),
+            "ratio_mixed_over_plain": round(mixed_ms / plain_ms, 4), "target_ratio": 0.5,
+            "plain_vcycles": plain_vc, "mixed_vcycles": int(round(sum(cyc) / len(cyc))),
+            "mixed_status": st["status"], "plain_C_err": plain_err, "mixed_C_err": err,
+            "learned": "not in the step (saves no V-cycles on fresh designs)",
+            "plain": PRECISION_NAME[0], "mixed": PRECISION_NAME[2]}
 
 
 FIXTURE = os.path.join(ROOT, "tests", "golden", "oracle_C.json")

@@ -113,6 +113,7 @@ _SIGS = {
     "h3d_oc_filter": [_vp, _vp, _vp, _ip, ctypes.c_int, ctypes.c_float, ctypes.c_int],
     "h3d_symmetrize": [_vp, _vp, _ip, ctypes.c_int],
     "h3d_design_step": [_vp, _fp, _vp, _vp, ctypes.POINTER(DesignParams)],
+    "h3d_conv_radial": [_vp, _vp, _vp, _ip, ctypes.c_float, ctypes.c_int, ctypes.c_int],
     "h3d_init_density_trig": [_vp, _vp, _ip, ctypes.c_int, _fp, ctypes.c_int, ctypes.c_int, ctypes.c_float,
                               ctypes.c_int],
     "h3d_get_field": [_vp, ctypes.c_int, ctypes.c_int, _fp],
@@ -402,6 +403,12 @@ class Homogenization(_Handle):
                                                c.ctypes.data_as(_fp), c.size, int(centered), float(vol),
                                                SYMMETRY[sym] if sym else -1))
         return c
+
+    def conv_radial(self, x, out, radius, periodic=False, adjoint=False):
+        """out = rho.conv(radial_convker_t<Spline4>(radius)) of the reference's
+        expression layer (or its transpose), on the handle's grid; CUDA tensors"""
+        self.check(lib().h3d_conv_radial(self._h, _ptr(x), _ptr(out), _i3(self.dims[0]), float(radius),
+                                         int(periodic), int(adjoint)))
 
     def warm_start_learned(self, net):
         """stored solutions from a WarmNet's prediction for the current density"""

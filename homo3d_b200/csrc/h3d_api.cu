@@ -1327,6 +1327,24 @@ int h3d_init_density_trig(h3d_handle *h, float *rho_dev, const int reso[3], int 
     return rc;
 }
 
+int h3d_conv_radial(h3d_handle *h, const float *in_dev, float *out_dev, const int reso[3], float radius, int periodic,
+                    int adjoint) {
+    if (!h || !in_dev || !out_dev || !reso) return H3D_ERR_ARG;
+    if (in_dev == out_dev) return fail(h, H3D_ERR_ARG, "input and output must not overlap");
+    if (!(radius > 0) || radius > 32) return fail(h, H3D_ERR_ARG, "radius outside (0, 32]");
+    for (int d = 0; d < 3; d++)
+        if (reso[d] < 1) return fail(h, H3D_ERR_ARG, "empty grid");
+    const int hw = (int)(radius + 0.5f);
+    if (periodic && (reso[0] <= 2 * hw || reso[1] <= 2 * hw || reso[2] <= 2 * hw))
+        return fail(h, H3D_ERR_ARG, "periodic window wider than the grid");
+    CK(cudaSetDevice(h->device));
+    const size_t ne = (size_t)reso[0] * reso[1] * reso[2];
+    if (int e = ensure_tmp(h, ne)) return e;
+    launch_conv_radial(reso, in_dev, out_dev, h->tmp, radius, periodic, adjoint, h->stream);
+    CKL();
+    return H3D_OK;
+}
+
 int h3d_design_step(h3d_handle *h, const float dC[36], float *rho_dev, float *sens_dev, const h3d_design_params *prm) {
     if (!h || !dC || !rho_dev || !sens_dev || !prm) return H3D_ERR_ARG;
     const Planes &P = h->lv[0].P;

@@ -286,6 +286,11 @@ void launch_oc(const float *sens, float *rho, float *rho_new, long long n, float
 void launch_filter(const int n[3], int pitch, const float *sens, const float *rho, float *out, float radius,
                    int periodic, cudaStream_t s);
 void launch_symmetrize(const int n[3], float *v, int sym, cudaStream_t s);
+// radial Spline4 convolution of the expression layer (k_design.cu): forward out =
+// conv(in) with ws = the in-grid weight sums, or adjoint out = conv^T(in) (ws is
+// recomputed); ws holds nx ny nz floats
+void launch_conv_radial(const int n[3], const float *in, float *out, float *ws, float radius, int periodic,
+                        int adjoint, cudaStream_t s);
 // the reference's trig-basis initial density (randTri): basis sum with P periods,
 // symmetrised (sym >= 0), level-set mapped to volume vol; scratch holds 4 + 1184
 // doubles; -1 if the kernel's shared memory (6 P x 64 floats) cannot be granted

@@ -420,4 +420,59 @@ int launch_trig_init(const int n[3], int P, const float *coeff_dev, int centered
     return 0;
 }
 
+// ---- radial convolution of the expression layer ---------------------------------
+// rho.conv(radial_convker_t<Spline4>(r)) (TensorExpression.h:946-1131,
+// TensorExpression.cuh:288-369): window offsets |o_a| <= (int)(r + 0.5), weight
+// w(o) = 1 - 6 q + 8 q^1.5 - 3 q^2 for q = |o|^2 / r^2 < 1 (0 otherwise); out(p) =
+// sum_o w(o) in(p + o) / ws(p) over the offsets inside the grid (periodic: all,
+// wrapped), ws(p) the sum of those weights.  The adjoint (the backward of the
+// expression) is g_in(p) = sum_o w(o) g_out(p - o) / ws(p - o).
+__device__ __forceinline__ float spline4_weight(int ox, int oy, int oz, float r) {
+    const float q = (float)(ox * ox + oy * oy + oz * oz) / (r * r);
+    const float rq = sqrtf(q);
+    return q < 1.f ? 1.f - 6.f * q + 8.f * q * rq - 3.f * q * q : 0.f;
+}
+
+// mode 0: out = conv(in), ws = weight sums; mode 1: ws only; mode 2: out = adjoint(in) with ws
+__global__ void __launch_bounds__(256) k_conv_radial(int n0, int n1, int n2, const float *__restrict__ in, float *out,
+                                                     float *ws, float r, int hw, int periodic, int mode) {
+    const long long e = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    const long long ne = (long long)n0 * n1 * n2;
+    if (e >= ne) return;
+    const int x = (int)(e % n0);
+    const long long t = e / n0;
+    const int y = (int)(t % n1), z = (int)(t / n1);
+    float sum = 0.f, wsum = 0.f;
+    for (int oz = -hw; oz <= hw; ++oz)
+        for (int oy = -hw; oy <= hw; ++oy)
+            for (int ox = -hw; ox <= hw; ++ox) {
+                const float w = spline4_weight(ox, oy, oz, r);
+                // forward reads p + o, the adjoint p - o
+                int px = mode == 2 ? x - ox : x + ox, py = mode == 2 ? y - oy : y + oy, pz = mode == 2 ? z - oz : z + oz;
+                const bool inside = px >= 0 && px < n0 && py >= 0 && py < n1 && pz >= 0 && pz < n2;
+                if (!inside && !periodic) continue;
+                if (!inside) { px = (px + n0) % n0; py = (py + n1) % n1; pz = (pz + n2) % n2; }
+                const long long q = px + (long long)n0 * (py + (long long)n1 * pz);
+                wsum += w;
+                if (mode == 0) sum += w * in[q];
+                else if (mode == 2) sum += w * in[q] / ws[q];
+            }
+    if (mode == 0) { out[e] = sum / wsum; ws[e] = wsum; }
+    else if (mode == 1) ws[e] = wsum;
+    else out[e] = sum;
+}
+
+void launch_conv_radial(const int n[3], const float *in, float *out, float *ws, float radius, int periodic,
+                        int adjoint, cudaStream_t s) {
+    const int hw = (int)(radius + 0.5f);
+    const long long ne = (long long)n[0] * n[1] * n[2];
+    const unsigned nb = (unsigned)((ne + 255) / 256);
+    if (!adjoint) {
+        k_conv_radial<<<nb, 256, 0, s>>>(n[0], n[1], n[2], in, out, ws, radius, hw, periodic, 0);
+    } else {
+        k_conv_radial<<<nb, 256, 0, s>>>(n[0], n[1], n[2], in, out, ws, radius, hw, periodic, 1);
+        k_conv_radial<<<nb, 256, 0, s>>>(n[0], n[1], n[2], in, out, ws, radius, hw, periodic, 2);
+    }
+}
+
 }  // namespace h3d

@@ -144,6 +144,84 @@ def optimize_bulk(reso, vol=0.3, iters=50, seed=0, relthres=1e-2, filter_radius=
     return out, C, records
 
 
+SGM_K, SGM_C = 30.0, 0.5            # .sgm() defaults (TensorExpression.h:555)
+ANI_SCALE, VOL_SCALE = 1000.0, 1000.0  # Framework.cu:314, 320
+
+
+def shear_isotropy_terms(C):
+    """(objective, dC of it, anisotropy constraint (2S/D - 1)^2 ANI_SCALE, its dC) of
+    example_opti_shear_isotropy (Framework.cu:303-318): S = C33 + C44 + C55,
+    D = C00 + C11 + C22 - C01 - C02 - C12 (upper entries, as Ch(0,1) records them)"""
+    S = C[3, 3] + C[4, 4] + C[5, 5]
+    D = C[0, 0] + C[1, 1] + C[2, 2] - C[0, 1] - C[0, 2] - C[1, 2]
+    q = 2 * S / D - 1
+    con = q * q * ANI_SCALE
+    dS, dD = ANI_SCALE * 2 * q * 2 / D, ANI_SCALE * 2 * q * (-2 * S / (D * D))
+    dC = np.zeros((6, 6), np.float32)
+    for i in range(3):
+        dC[3 + i, 3 + i] = dS
+        dC[i, i] = dD
+    dC[0, 1] = dC[0, 2] = dC[1, 2] = -dD
+    return -S / 3.0, shear_gradient(), con, dC
+
+
+def optimize_shear_isotropy(reso, vol=0.3, iters=20, seed=0, relthres=1e-2, filter_radius=2.0, sym="reflect6",
+                            rho0=None, E=10.0, nu=0.3, device=0, precision=PREC_REFINE):
+    """example_opti_shear_isotropy (Framework.cu:274-351): maximise the shear modulus
+    -(C33 + C44 + C55) / 3 by MMA (2 constraints; a0 = 1, a = 0, c = 1000, d = 1,
+    bounds [0.001, 1]) with the physical density rho_phys = sgm(conv(rho))^3 (radial
+    Spline4 convolution of radius filter_radius, sigmoid 1 / (1 + exp(-30 (v - 0.5)))):
+    g0 = (mean sgm(conv(rho)) - vol) 1000 with the unscaled, unsymmetrised gradient of
+    the mean, g1 = (anisotropy) 1000 - 0.1 with the gradient of the anisotropy
+    (symmetrised); the objective gradient symmetrised.  The scalings are the
+    reference's."""
+    import torch
+
+    from . import MMAOptimizer
+    hom = Homogenization(reso, E, nu, COARSE_EXACT, PIN_IDENTITY, precision, device)
+    n = hom.dims[0]
+    ne = n[0] * n[1] * n[2]
+    dev = torch.device("cuda", device)
+    if rho0 is None:
+        rho0 = synthetic_density(n[0], seed=seed, vol=vol).ravel()
+    rho = torch.tensor(np.asarray(rho0, dtype=np.float32).ravel(), device=dev)
+    z, tmp, grad_obj, grad_ani, grad_vol = (torch.empty_like(rho) for _ in range(5))
+    sens = torch.empty_like(rho)
+    mma = MMAOptimizer(2, ne, 1.0, 0.0, 1000.0, 1.0, device=device)
+    mma.setBound(0.001, 1.0)
+    stream = torch.cuda.ExternalStream(hom.stream, device=dev)
+    records = []
+    for it in range(iters):
+        with torch.cuda.stream(stream):
+            hom.conv_radial(rho, z, filter_radius)
+            y = torch.sigmoid(SGM_K * (z - SGM_C))
+            rhop = y ** 3
+            dphys = 3 * y * y * SGM_K * y * (1 - y)           # d rho_phys / d z
+        hom.update(rhop)
+        C = hom.elasticMatrix(relthres)
+        obj, dC_obj, con, dC_con = shear_isotropy_terms(C)
+        for dC, out in ((dC_obj, grad_obj), (dC_con, grad_ani)):
+            hom.Sensitivity(dC, sens)
+            with torch.cuda.stream(stream):
+                torch.mul(sens, dphys, out=tmp)
+            hom.conv_radial(tmp, out, filter_radius, adjoint=True)
+            symmetrize(hom, out, n, sym)
+        with torch.cuda.stream(stream):
+            volr = float(y.double().mean())
+            torch.mul(SGM_K * y * (1 - y), 1.0 / ne, out=tmp)
+        hom.conv_radial(tmp, grad_vol, filter_radius, adjoint=True)
+        hom.sync()
+        gval = torch.tensor([(volr - vol) * VOL_SCALE, con * ANI_SCALE - 0.1], dtype=torch.float32, device=dev)
+        mma.update(it, rho, grad_obj, gval, [grad_vol, grad_ani])
+        records.append({"iter": it, "obj": float(obj), "anisotropy": float(con), "vol": volr,
+                        "zener": float(np.sqrt(con / ANI_SCALE) + 1), "vcycles": hom.last_stats["vcycles"],
+                        "newton": mma.newton_steps})
+    out = rho.cpu().numpy()
+    mma.close()
+    hom.close()
+    return out, C, records
+
+
 def main():
     p = argparse.ArgumentParser()
     p.add_argument("--reso", type=int, default=128)

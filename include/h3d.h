@@ -234,6 +234,16 @@ H3D_API int h3d_symmetrize(h3d_handle *h, float *field_dev, const int reso[3], i
 H3D_API int h3d_init_density_trig(h3d_handle *h, float *rho_dev, const int reso[3], int n_period, const float *coeff,
                                   int ncoeff, int centered, float volratio, int sym);
 
+/* ---- radial convolution of the expression layer (AutoDiff/TensorExpression.h:946-1131,
+ * rho.conv(radial_convker_t<float, Spline4>(radius)), TensorExpression.cuh:288-369) ---
+ * out[p] = sum_o w(o) in[p + o] / sum_o w(o) over the window offsets |o_a| <=
+ * (int)(radius + 0.5) that stay inside the grid (periodic = 1: all of them,
+ * wrapped), w(o) = 1 - 6 q + 8 q^1.5 - 3 q^2 for q = |o|^2 / radius^2 < 1; with
+ * adjoint = 1 the transpose of that map (the expression's backward).  in and out
+ * are lexicographic device arrays of nx ny nz floats and must not overlap. */
+H3D_API int h3d_conv_radial(h3d_handle *h, const float *in_dev, float *out_dev, const int reso[3], float radius,
+                            int periodic, int adjoint);
+
 /* ---- one design update after a solve, on the device (testAutoDiff.cu:298-327,
  * the body of optiBulk / optiShear / optiNpr after objective.eval()) ---------------
  * sens = dObj/drho_phys from dC (as h3d_sensitivity), times p rho^(p-1) (the SIMP

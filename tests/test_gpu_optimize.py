@@ -92,3 +92,70 @@ def test_design_step_rejects_bad_arguments(torch_cuda):
     with pytest.raises(H.H3DError):
         hd.design_step(np.zeros((6, 6)), rho, sens, 1.5)
     hd.close()
+
+
+@pytest.mark.parametrize("periodic", [False, True])
+def test_conv_radial_and_adjoint_match_restatement(torch_cuda, periodic):
+    from oracle import expr_oracle as X
+    torch = torch_cuda
+    n, r = 16, 2.0
+    hd = H.Homogenization(n)
+    a = np.random.default_rng(3).uniform(0, 1, (n, n, n))
+    t = torch.tensor(a.ravel(), dtype=torch.float32, device="cuda")
+    out = torch.empty_like(t)
+    hd.conv_radial(t, out, r, periodic)
+    ref, _ = X.conv(a, r, periodic)
+    assert np.abs(out.cpu().numpy() - ref.ravel()).max() < 1e-6
+    hd.conv_radial(t, out, r, periodic, adjoint=True)
+    ref = X.conv_adjoint(a, r, periodic)
+    assert np.abs(out.cpu().numpy() - ref.ravel()).max() < 1e-5 * np.abs(ref).max()
+    # the adjoint is the transpose: <conv a, b> = <a, conv^T b>
+    b = np.random.default_rng(4).uniform(-1, 1, (n, n, n))
+    lhs = (X.conv(a, r, periodic)[0] * b).sum()
+    rhs = (a * X.conv_adjoint(b, r, periodic)).sum()
+    assert abs(lhs - rhs) < 1e-9 * abs(lhs)
+    hd.close()
+
+
+def oracle_shear_isotropy(n, rho, iters, vol=0.3, r=2.0):
+    """example_opti_shear_isotropy (Framework.cu:274-351) on the FP64 oracle pieces"""
+    from homo3d_b200.optimize import SGM_C, SGM_K, ANI_SCALE, VOL_SCALE, shear_isotropy_terms
+    from oracle import expr_oracle as X
+    ne = n ** 3
+    mma = O.MMA(2, ne, 1.0, 0.0, 1000.0, 1.0)
+    mma.set_bound(0.001, 1.0)
+    objs = []
+    for it in range(iters):
+        z = X.conv(rho.reshape(n, n, n), r)[0].ravel()
+        y = 1.0 / (1.0 + np.exp(-SGM_K * (z - SGM_C)))
+        rhop = (y ** 3).astype(np.float32).astype(np.float64)
+        m = O.MG((n, n, n))
+        m.set_density(rhop)
+        m.update_stencils()
+        m.rhs()
+        m.solve(1e-10, 400)
+        C = m.elastic_matrix()
+        obj, dC_obj, con, dC_con = shear_isotropy_terms(C)
+        objs.append(obj)
+        dphys = 3 * y * y * SGM_K * y * (1 - y)
+        grads = []
+        for dC in (dC_obj, dC_con):
+            s = m.sensitivity(dC.astype(np.float64)) * dphys
+            g = X.conv_adjoint(s.reshape(n, n, n), r).ravel()
+            grads.append(O.symmetrize_f32((n, n, n), g, "reflect6").astype(np.float64))
+        gvol = X.conv_adjoint((SGM_K * y * (1 - y) / ne).reshape(n, n, n), r).ravel()
+        gval = np.array([(y.mean() - vol) * VOL_SCALE, con * ANI_SCALE - 0.1])
+        rho = mma.update(it, rho, grads[0], gval, np.stack([gvol, grads[1]]))
+    return rho, objs
+
+
+def test_shear_isotropy_mma_loop_matches_oracle(torch_cuda):
+    from homo3d_b200.optimize import optimize_shear_isotropy
+    n = 16
+    rho0 = synthetic_density(n, seed=9, vol=0.3).ravel().astype(np.float32).astype(np.float64)
+    rho, C, rec = optimize_shear_isotropy(n, iters=3, rho0=rho0, relthres=1e-8)
+    ref_rho, ref_objs = oracle_shear_isotropy(n, rho0.copy(), 3)
+    objs = [r["obj"] for r in rec]
+    for a, b in zip(objs, ref_objs):
+        assert abs(a - b) / abs(b) < 1e-4, (objs, ref_objs)
+    assert np.abs(rho - ref_rho).max() < 2e-3
