@@ -61,9 +61,7 @@ __device__ __forceinline__ void load_block(const CoarseArgs &a, long long me, fl
 // each, 6 CTAs/SM; shape 1 = one thread per vertex with all six, 4 CTAs/SM.  The
 // threads of one vertex run in adjacent CTAs, so repeated stencil reads hit L2;
 // shape 2 = two cases per thread at 4 CTAs/SM, shape 3 = six cases per thread at 3
-// CTAs/SM, shapes 4 / 5 = shapes 0 / 1 with the odd colours' vertex blocks in
-// reverse order (the residual, one launch, runs shapes 4 / 5 as 0 / 1).  All shapes
-// give the same result to the last bit.
+// CTAs/SM.  All shapes give the same result to the last bit.
 
 // KC: the vertex colour, or -1 for the run-time colour kr (one code body for all
 // colours)
@@ -133,21 +131,19 @@ __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, 
 // thread -> (vertex p, first load case cb) for C cases per thread: the NCASE / C
 // CTAs of a case group cover the same 128 vertices with different load cases
 template <int C>
-__device__ __forceinline__ void coarse_task(long long &p, int &cb, bool rev = false) {
+__device__ __forceinline__ void coarse_task(long long &p, int &cb) {
     constexpr int NG = NCASE / C;
     cb = (int)(blockIdx.x % NG) * C;
-    const long long vb = rev ? (long long)(gridDim.x / NG) - 1 - (long long)(blockIdx.x / NG) : blockIdx.x / NG;
-    p = vb * blockDim.x + threadIdx.x;
+    p = (long long)(blockIdx.x / NG) * blockDim.x + threadIdx.x;
 }
 
 // RES (the last colour of a sweep, whose neighbours are final) also writes the
 // residual of the updated vertex: r = f - acc - A_0 u with acc the neighbour sum
-// ALT: odd colours take their vertex blocks in reverse order (see k_fine_gs)
-template <int K, bool F32, int CGS_CPT, int CGS_MINB, bool RES = false, bool ALT = false>
+template <int K, bool F32, int CGS_CPT, int CGS_MINB, bool RES = false>
 __global__ void __launch_bounds__(128, CGS_MINB) k_coarse_gs(CoarseArgs a) {
     long long p;
     int cb;
-    coarse_task<CGS_CPT>(p, cb, ALT && (K & 1));
+    coarse_task<CGS_CPT>(p, cb);
     if (p >= a.P) return;
     const long long me = (long long)K * a.P + p;
     int i, j, l;
@@ -220,17 +216,17 @@ static CoarseArgs make_cargs(const Level &L) {
     return a;
 }
 
-template <bool F32, int C, int MINB, bool ALT = false>
+template <bool F32, int C, int MINB>
 static void coarse_gs_sweep(const CoarseArgs &a, cudaStream_t s) {
     const unsigned nb = (unsigned)((a.P + 127) / 128) * (NCASE / C);
-    k_coarse_gs<0, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<1, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<2, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<3, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<4, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<5, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<6, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<7, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<0, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<1, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<2, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<3, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<4, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<5, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<6, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<7, F32, C, MINB><<<nb, 128, 0, s>>>(a);
 }
 
 void launch_coarse_gs(const Level &L, float w, cudaStream_t s) {
@@ -241,8 +237,6 @@ void launch_coarse_gs(const Level &L, float w, cudaStream_t s) {
         case 1: coarse_gs_sweep<true, 6, 4>(a, s); break;
         case 2: coarse_gs_sweep<true, 2, 4>(a, s); break;
         case 3: coarse_gs_sweep<true, 6, 3>(a, s); break;
-        case 4: coarse_gs_sweep<true, 2, 6, true>(a, s); break;
-        case 5: coarse_gs_sweep<true, 6, 4, true>(a, s); break;
         default: coarse_gs_sweep<true, 2, 6>(a, s); break;
         }
     } else {
@@ -250,8 +244,6 @@ void launch_coarse_gs(const Level &L, float w, cudaStream_t s) {
         case 1: coarse_gs_sweep<false, 6, 4>(a, s); break;
         case 2: coarse_gs_sweep<false, 2, 4>(a, s); break;
         case 3: coarse_gs_sweep<false, 6, 3>(a, s); break;
-        case 4: coarse_gs_sweep<false, 2, 6, true>(a, s); break;
-        case 5: coarse_gs_sweep<false, 6, 4, true>(a, s); break;
         default: coarse_gs_sweep<false, 2, 6>(a, s); break;
         }
     }
@@ -267,16 +259,14 @@ template <unsigned NCOL>
 static void coarse_residual_shape(const Level &L, const CoarseArgs &a, cudaStream_t s) {
     if (L.st32) {
         switch (L.res_shape) {
-        case 1:
-        case 5: coarse_residual_all<true, 6, 4, NCOL>(a, s); break;
+        case 1: coarse_residual_all<true, 6, 4, NCOL>(a, s); break;
         case 2: coarse_residual_all<true, 2, 4, NCOL>(a, s); break;
         case 3: coarse_residual_all<true, 6, 3, NCOL>(a, s); break;
         default: coarse_residual_all<true, 2, 6, NCOL>(a, s); break;
         }
     } else {
         switch (L.res_shape) {
-        case 1:
-        case 5: coarse_residual_all<false, 6, 4, NCOL>(a, s); break;
+        case 1: coarse_residual_all<false, 6, 4, NCOL>(a, s); break;
         case 2: coarse_residual_all<false, 2, 4, NCOL>(a, s); break;
         case 3: coarse_residual_all<false, 6, 3, NCOL>(a, s); break;
         default: coarse_residual_all<false, 2, 6, NCOL>(a, s); break;
@@ -288,17 +278,17 @@ void launch_coarse_residual(const Level &L, cudaStream_t s) { coarse_residual_sh
 
 // a sweep followed by the level's residual: the last colour's launch writes its
 // own residual, the residual launch covers the other seven colours
-template <bool F32, int C, int MINB, bool ALT = false>
+template <bool F32, int C, int MINB>
 static void coarse_gs_sweep_res(const CoarseArgs &a, cudaStream_t s) {
     const unsigned nb = (unsigned)((a.P + 127) / 128) * (NCASE / C);
-    k_coarse_gs<0, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<1, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<2, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<3, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<4, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<5, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<6, F32, C, MINB, false, ALT><<<nb, 128, 0, s>>>(a);
-    k_coarse_gs<7, F32, C, MINB, true, ALT><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<0, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<1, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<2, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<3, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<4, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<5, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<6, F32, C, MINB><<<nb, 128, 0, s>>>(a);
+    k_coarse_gs<7, F32, C, MINB, true><<<nb, 128, 0, s>>>(a);
 }
 
 void launch_coarse_gs_residual(const Level &L, float w, cudaStream_t s) {
@@ -309,8 +299,6 @@ void launch_coarse_gs_residual(const Level &L, float w, cudaStream_t s) {
         case 1: coarse_gs_sweep_res<true, 6, 4>(a, s); break;
         case 2: coarse_gs_sweep_res<true, 2, 4>(a, s); break;
         case 3: coarse_gs_sweep_res<true, 6, 3>(a, s); break;
-        case 4: coarse_gs_sweep_res<true, 2, 6, true>(a, s); break;
-        case 5: coarse_gs_sweep_res<true, 6, 4, true>(a, s); break;
         default: coarse_gs_sweep_res<true, 2, 6>(a, s); break;
         }
     } else {
@@ -318,8 +306,6 @@ void launch_coarse_gs_residual(const Level &L, float w, cudaStream_t s) {
         case 1: coarse_gs_sweep_res<false, 6, 4>(a, s); break;
         case 2: coarse_gs_sweep_res<false, 2, 4>(a, s); break;
         case 3: coarse_gs_sweep_res<false, 6, 3>(a, s); break;
-        case 4: coarse_gs_sweep_res<false, 2, 6, true>(a, s); break;
-        case 5: coarse_gs_sweep_res<false, 6, 4, true>(a, s); break;
         default: coarse_gs_sweep_res<false, 2, 6>(a, s); break;
         }
     }

@@ -251,13 +251,11 @@ __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, c
 // thread -> (vertex p in the colour plane, first case cb) for C cases per thread;
 // the NCASE / C case groups of a vertex block are adjacent CTAs
 // vertex block are adjacent CTAs
-// REV: the vertex blocks in reverse order (the last block first)
 template <int C>
-__device__ __forceinline__ void thread_task(long long &p, int &cb, bool rev = false) {
+__device__ __forceinline__ void thread_task(long long &p, int &cb) {
     constexpr int NG = NCASE / C;
     cb = (int)(blockIdx.x % NG) * C;
-    const long long vb = rev ? (long long)(gridDim.x / NG) - 1 - (long long)(blockIdx.x / NG) : blockIdx.x / NG;
-    p = vb * blockDim.x + threadIdx.x;
+    p = (long long)(blockIdx.x / NG) * blockDim.x + threadIdx.x;
 }
 
 // one vertex of the colour sweep; RES (the last colour of a sweep) also writes
@@ -323,16 +321,12 @@ __device__ __forceinline__ void fine_gs_vertex(const FineArgs &a, const KeMat &k
 // RES: the per-CTA norm partials go to the rows the residual of colour 7 would
 // write (row 7 * (CTAs per colour of the residual) + CTA of the colour, one row
 // per group of CPT cases, zeros for the other cases)
-// ALT: the odd colours run their vertex blocks in reverse order, so each colour
-// launch starts where the previous one ended and finds that part of u in L2 (the
-// order inside a colour does not change the result)
-template <int K, int C, int MINB, bool RES, bool ALT = false>
+template <int K, int C, int MINB, bool RES>
 __global__ void __launch_bounds__(FBS, MINB) k_fine_gs(FineArgs a, const __grid_constant__ KeMat ke,
                                                     double *partial) {
-    constexpr bool REV = ALT && (K & 1);
     long long p;
     int cb;
-    thread_task<C>(p, cb, REV);
+    thread_task<C>(p, cb);
     double nrm[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) nrm[c] = 0;
@@ -351,8 +345,7 @@ __global__ void __launch_bounds__(FBS, MINB) k_fine_gs(FineArgs a, const __grid_
     }
     __syncthreads();
     constexpr int NG = NCASE / C, NGR = NCASE / CPT;  // case groups of this launch / of the residual
-    const long long npb = gridDim.x / NG;  // vertex blocks
-    const long long pb = REV ? npb - 1 - (long long)(blockIdx.x / NG) : blockIdx.x / NG;  // this vertex block
+    const long long pb = blockIdx.x / NG, npb = gridDim.x / NG;  // vertex block, vertex blocks
     if (threadIdx.x < (C / CPT) * NCASE) {
         const int gl = threadIdx.x / NCASE, q = threadIdx.x % NCASE;
         const int g = cb / CPT + gl;  // the residual's case group of this row
@@ -578,19 +571,18 @@ int fine_residual_blocks(const Level &L) { return (int)(((L.P.nv / 8 + FBS - 1) 
 // the colour sweep in launch shape v: 0 = one thread per vertex with all six
 // cases (4 CTAs/SM), 1 = three threads per vertex with two cases each (5 CTAs/SM),
 // 2 = six cases per thread at 3 CTAs/SM (more registers), 3 = two cases per thread
-// at 6 CTAs/SM (fewer registers), 4 / 5 = shapes 0 / 1 with the odd colours' vertex
-// blocks in reverse order; all give the same result to the last bit
-template <int C, int MINB, bool ALT = false>
+// at 6 CTAs/SM (fewer registers); all give the same result to the last bit
+template <int C, int MINB>
 static void fine_gs_sweep(const FineArgs &a, const KeMat &ke, cudaStream_t s) {
     const unsigned nb = task_blocks(a, C);
-    k_fine_gs<0, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<1, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<2, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<3, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<4, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<5, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<6, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<7, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<0, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<1, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<2, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<3, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<4, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<5, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<6, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<7, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
 }
 
 void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, cudaStream_t s) {
@@ -600,8 +592,6 @@ void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, 
     case 1: fine_gs_sweep<2, 5>(a, ke, s); break;
     case 2: fine_gs_sweep<6, 3>(a, ke, s); break;
     case 3: fine_gs_sweep<2, 6>(a, ke, s); break;
-    case 4: fine_gs_sweep<6, 4, true>(a, ke, s); break;
-    case 5: fine_gs_sweep<2, 5, true>(a, ke, s); break;
     default: fine_gs_sweep<6, 4>(a, ke, s); break;
     }
 }
@@ -609,17 +599,17 @@ void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, 
 // a sweep followed by the residual (the down leg of a V-cycle): the last colour's
 // launch writes its own residual and norm partials, the residual launch covers
 // the other seven colours
-template <int C, int MINB, bool ALT = false>
+template <int C, int MINB>
 static void fine_gs_sweep_res(const FineArgs &a, const KeMat &ke, double *partial, cudaStream_t s) {
     const unsigned nb = task_blocks(a, C);
-    k_fine_gs<0, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<1, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<2, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<3, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<4, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<5, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<6, C, MINB, false, ALT><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<7, C, MINB, true, ALT><<<nb, FBS, 0, s>>>(a, ke, partial);
+    k_fine_gs<0, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<1, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<2, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<3, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<4, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<5, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<6, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
+    k_fine_gs<7, C, MINB, true><<<nb, FBS, 0, s>>>(a, ke, partial);
     k_fine_residual<7><<<task_blocks(a, CPT) * 7, FBS, 0, s>>>(a, ke, partial);
 }
 
@@ -631,8 +621,6 @@ void launch_fine_gs_residual(const Level &L, const float *rho, const KeMat &ke, 
     case 1: fine_gs_sweep_res<2, 5>(a, ke, norm_partial, s); break;
     case 2: fine_gs_sweep_res<6, 3>(a, ke, norm_partial, s); break;
     case 3: fine_gs_sweep_res<2, 6>(a, ke, norm_partial, s); break;
-    case 4: fine_gs_sweep_res<6, 4, true>(a, ke, norm_partial, s); break;
-    case 5: fine_gs_sweep_res<2, 5, true>(a, ke, norm_partial, s); break;
     default: fine_gs_sweep_res<6, 4>(a, ke, norm_partial, s); break;
     }
 }

@@ -183,15 +183,13 @@ H3D_API int h3d_reset_solutions(h3d_handle *h);
  * (coarse levels) its residual: load cases per thread (all six, or two as three
  * threads per vertex) times CTAs per SM (the register budget per thread).  Level 0:
  * shape 0 / 1 / 2 / 3 = six cases at 4 CTAs/SM / two at 5 / six at 3 / two at 6;
- * coarse levels: two at 6 / six at 4 / two at 4 / six at 3; shapes 4 / 5 = shapes
- * 0 / 1 with the odd colours' vertex blocks in reverse order, so a colour launch
- * starts on the part of the field the previous one left in L2.  All give the same
+ * coarse levels: two at 6 / six at 4 / two at 4 / six at 3.  All give the same
  * results to the last bit.  The first solve of a handle times them (CUDA events,
  * a few sweeps per shape, iterating on the level's scratch residual field) and
  * keeps the fastest; h3d_autotune re-runs that now, h3d_set_tuning fixes the
  * shapes (and turns the automatic tuning off), h3d_get_tuning reads them:
  * shapes[0] = sweep, shapes[1] = residual. */
-#define H3D_NUM_SHAPES 6
+#define H3D_NUM_SHAPES 4
 H3D_API int h3d_autotune(h3d_handle *h);
 H3D_API int h3d_get_tuning(const h3d_handle *h, int level, int shapes[2]);
 H3D_API int h3d_set_tuning(h3d_handle *h, int level, int gs_shape, int res_shape);
