@@ -103,6 +103,7 @@ _SIGS = {
     "h3d_autotune": [_vp],
     "h3d_get_tuning": [_vp, ctypes.c_int, _ip],
     "h3d_set_tuning": [_vp, ctypes.c_int, ctypes.c_int, ctypes.c_int],
+    "h3d_set_vcycle_bottom": [_vp, ctypes.c_int64],
     "h3d_batch_update_density": [ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.c_int],
     "h3d_batch_elastic_matrix": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_double, _dp,
                                  ctypes.POINTER(SolveStats), _ip],
@@ -377,6 +378,10 @@ class Homogenization(_Handle):
             self.check(lib().h3d_get_tuning(self._h, l, sh))
             out.append((sh[0], sh[1]))
         return out
+
+    def set_vcycle_bottom(self, max_level_vertices):
+        """levels of at most this many vertices run in one cooperative launch (0: off)"""
+        self.check(lib().h3d_set_vcycle_bottom(self._h, int(max_level_vertices)))
 
     def set_tuning(self, level, gs_shape, res_shape=0):
         self.check(lib().h3d_set_tuning(self._h, int(level), int(gs_shape), int(res_shape)))

@@ -180,6 +180,11 @@ struct h3d_handle {
     bool mixed() const { return cfg.precision == H3D_PREC_MIXED; }
     int num_sms = 0;
     int *d_tcflag = nullptr;            // set by the tensor-core residual if an mbarrier wait timed out
+    // cooperative bottom of the V-cycle: levels of at most bottom_nv vertices (0: off,
+    // the default: its grid barriers cost more than the graph's launch boundaries)
+    long long bottom_nv = 0;
+    unsigned *d_bar = nullptr;          // its grid-barrier state
+    int *d_botflag = nullptr;           // set if one of its barrier waits ran out
     bool have_density = false, have_stencils = false;
     bool tuned = false;  // launch shapes chosen (autotuner or h3d_set_tuning)
     // chi_zero: the stored solutions chi are all zero (allocation, h3d_reset_solutions,
@@ -267,10 +272,33 @@ int destroy_graph(h3d_handle *h) {
 // stopping test of MG.cpp:130-139 reads).  The refined solve runs the same cycle on
 // the FP32 correction u, with level-0 f holding f0 - K u64.  Inside a solve the
 // cycle ends with the rigid-translation deflation (launch_pin_deflate).
+// the first level of the cooperative bottom (k_vcycle_bottom), or -1: the
+// largest level of at most bottom_nv vertices, with a smoothed level below it
+int bottom_first(const h3d_handle *h, float w) {
+    if (h->bottom_nv <= 0 || w != 1.f) return -1;
+    int first = -1;
+    for (int l = h->nl - 2; l >= 1; l--)
+        if (h->lv[l].P.nv <= h->bottom_nv) first = l;
+    if (first < 0 || !vcycle_bottom_fits(h->lv, first, h->nl)) return -1;
+    return first;
+}
+
 int enqueue_vcycle(h3d_handle *h, float w, bool deflate = false) {
     cudaStream_t s = h->stream;
     const int nblk_r = h->mixed() ? fine_residual_tc_blocks(h->lv[0].P, h->num_sms) : fine_residual_blocks(h->lv[0]);
+    int bfirst = bottom_first(h, w);
+    int bblk = 0;
+    if (bfirst >= 0) {
+        bblk = vcycle_bottom_blocks(h->num_sms, h->ndof, h->lv[bfirst].st32);
+        if (bblk <= 0) bfirst = -1;
+    }
     for (int l = 0; l < h->nl; l++) {
+        if (l == bfirst) {  // restriction into `bfirst`, down to the coarsest solve and back up
+            if (launch_vcycle_bottom(h->lv, bfirst, h->nl, h->aug, h->cfg.coarse_mode == H3D_COARSE_PROJECT, h->d_bar,
+                                     h->d_botflag, bblk, s) != 0)
+                return fail(h, H3D_ERR_CUDA, "cooperative V-cycle bottom could not be launched");
+            break;
+        }
         if (l > 0) {
             launch_restrict(h->lv[l - 1], h->lv[l], s);
             cudaMemsetAsync(h->lv[l].u, 0, sizeof(float) * field_floats(h->lv[l].P.nv), s);
@@ -286,7 +314,7 @@ int enqueue_vcycle(h3d_handle *h, float w, bool deflate = false) {
             launch_coarse_gs_residual(h->lv[l], w, s);  // each level's residual comes with its sweep
         }
     }
-    for (int l = h->nl - 2; l >= 0; l--) {
+    for (int l = (bfirst >= 0 ? bfirst : h->nl - 1) - 1; l >= 0; l--) {
         launch_prolong(h->lv[l], h->lv[l + 1], l == 0, s);
         if (l == 0) launch_fine_gs(h->lv[0], h->rho, h->ke, w, s);
         else launch_coarse_gs(h->lv[l], w, s);
@@ -295,6 +323,7 @@ int enqueue_vcycle(h3d_handle *h, float w, bool deflate = false) {
     launch_norm_finish(h->partial, nblk_r, h->d_small, s);
     cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, s);
     if (h->mixed()) cudaMemcpyAsync(&h->h_small[62], h->d_tcflag, sizeof(int), cudaMemcpyDeviceToHost, s);
+    if (bfirst >= 0) cudaMemcpyAsync(&h->h_small[61], h->d_botflag, sizeof(int), cudaMemcpyDeviceToHost, s);
     return H3D_OK;
 }
 
@@ -539,6 +568,8 @@ struct SolveRun {
         theta = std::max(1e-3, 1e-5 * nmax);
         CK(cudaEventRecord(h->ev0, h->stream));
         CK(cudaMemsetAsync(h->pin_state + NF, 0, sizeof(double) * NF, h->stream));  // no pending shift
+        CK(cudaMemsetAsync(h->d_botflag, 0, sizeof(int), h->stream));
+        h->h_small[61] = 0.0;
         if (refine) {
             CK(cudaMemsetAsync(L0.u, 0, sizeof(float) * nf32(), h->stream));
             return launch_refine(P_START_REFINE);
@@ -567,6 +598,8 @@ struct SolveRun {
             it++;
             if (h->mixed() && *reinterpret_cast<int *>(&h->h_small[62]))
                 return fail(h, H3D_ERR_CUDA, "tensor-core residual: mbarrier wait timed out");
+            if (*reinterpret_cast<int *>(&h->h_small[61]))
+                return fail(h, H3D_ERR_CUDA, "cooperative V-cycle bottom: a grid barrier wait timed out");
             bool bad = false, done = true, trigger = true;
             double worst = 0;
             for (int c = 0; c < NCASE; c++) {
@@ -817,6 +850,10 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
     CK(cudaMalloc(&h->d_flag, sizeof(int)));
     CK(cudaMalloc(&h->d_tcflag, sizeof(int)));
     CK(cudaMemset(h->d_tcflag, 0, sizeof(int)));
+    CK(cudaMalloc(&h->d_bar, 2 * sizeof(unsigned)));
+    CK(cudaMemset(h->d_bar, 0, 2 * sizeof(unsigned)));
+    CK(cudaMalloc(&h->d_botflag, sizeof(int)));
+    CK(cudaMemset(h->d_botflag, 0, sizeof(int)));
     CK(cudaDeviceGetAttribute(&h->num_sms, cudaDevAttrMultiProcessorCount, h->device));
     if (h->mixed() && configure_fine_residual_tc() != 0)
         return fail(h, H3D_ERR_CUDA, "tensor-core residual kernel could not be configured");
@@ -829,6 +866,7 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
     CK(cudaMalloc(&h->partial, sizeof(double) * pn));
     CK(cudaMalloc(&h->d_small, sizeof(double) * 64));
     CK(cudaMallocHost(&h->h_small, sizeof(double) * 64));
+    std::memset(h->h_small, 0, sizeof(double) * 64);
     CK(cudaMalloc(&h->pin_state, sizeof(double) * 3 * NF));
     CK(cudaMemset(h->pin_state, 0, sizeof(double) * 3 * NF));
     CK(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
@@ -862,6 +900,8 @@ int h3d_destroy(h3d_handle *h) {
     cudaFree(h->rho); cudaFree(h->chi); cudaFree(h->u64); cudaFree(h->f0);
     cudaFree(h->q); cudaFree(h->d_ked); cudaFree(h->aug);
     cudaFree(h->d_dcw);
+    cudaFree(h->d_bar);
+    cudaFree(h->d_botflag);
     if (h->h_dcw) cudaFreeHost(h->h_dcw);
     cudaFree(h->d_flag); cudaFree(h->d_tcflag); cudaFree(h->partial); cudaFree(h->d_small); cudaFree(h->tmp); cudaFree(h->pin_state);
     if (h->h_small) cudaFreeHost(h->h_small);
@@ -1079,6 +1119,13 @@ int h3d_set_tuning(h3d_handle *h, int level, int gs_shape, int res_shape) {
     h->lv[level].res_shape = res_shape;
     destroy_graph(h);
     h->tuned = true;
+    return H3D_OK;
+}
+
+int h3d_set_vcycle_bottom(h3d_handle *h, int64_t max_level_vertices) {
+    if (!h || max_level_vertices < 0) return H3D_ERR_ARG;
+    h->bottom_nv = max_level_vertices;
+    destroy_graph(h);
     return H3D_OK;
 }
 

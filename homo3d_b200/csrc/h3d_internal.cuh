@@ -252,6 +252,14 @@ void launch_coarse_assemble(const Level &C, double *aug, cudaStream_t s);
 size_t gauss_jordan_doubles(int n);
 void launch_gauss_jordan(double *aug, int n, int *flag, cudaStream_t s);
 void launch_coarse_apply(const Level &C, const double *aug, int project, cudaStream_t s);
+// the V-cycle from the restriction into level `first` to the post-smoothing of
+// that level in one cooperative launch of nblk CTAs (k_coarse.cu); bar: two
+// unsigned of barrier state, *flag set if a grid barrier's wait ran out; -1 if the
+// levels do not fit (vcycle_bottom_fits), -2 if the launch failed
+int launch_vcycle_bottom(const Level *lv, int first, int nl, const double *aug, int project, unsigned *bar, int *flag,
+                         int nblk, cudaStream_t s);
+int vcycle_bottom_blocks(int num_sms, int ndof, bool f32);
+bool vcycle_bottom_fits(const Level *lv, int first, int nl);
 // level-0 residual on the tensor cores (k_fine_tc.cu): element products Ke U with
 // TF32 hi + lo operands and FP32 accumulation; a persistent grid of
 // fine_residual_tc_blocks CTAs writing one row of six norm partials each (partial

@@ -65,7 +65,9 @@ __device__ __forceinline__ void load_block(const CoarseArgs &a, long long me, fl
 
 // KC: the vertex colour, or -1 for the run-time colour kr (one code body for all
 // colours)
-template <int KC, bool SELF, bool F32, int C>
+// CG: neighbour values through L2 only (ld.global.cg), for kernels that read values
+// other CTAs wrote earlier in the same launch
+template <int KC, bool SELF, bool F32, int C, bool CG = false>
 __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, int i, int j, int l, int cb,
                                              float acc[3 * C], int kr = KC) {
     static_assert(C % 2 == 0, "the load cases of a thread go in packed FP32x2 lane pairs");
@@ -110,7 +112,9 @@ __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, 
         for (int jp = 0; jp < NP; ++jp) {
             float2 uu[3];
 #pragma unroll
-            for (int m = 0; m < 3; ++m) uu[m] = make_float2(up[(6 * jp + m) * FVB], up[(6 * jp + 3 + m) * FVB]);
+            for (int m = 0; m < 3; ++m)
+                uu[m] = CG ? make_float2(__ldcg(up + (6 * jp + m) * FVB), __ldcg(up + (6 * jp + 3 + m) * FVB))
+                           : make_float2(up[(6 * jp + m) * FVB], up[(6 * jp + 3 + m) * FVB]);
 #pragma unroll
             for (int r = 0; r < 3; ++r)
                 acc2[3 * jp + r] = __ffma2_rn(make_float2(s[3 * r], s[3 * r]), uu[0],
@@ -629,6 +633,341 @@ void launch_stencil_to_lex(const Level &L, float *dst_lex, cudaStream_t s) {
 }
 void launch_stencil_from_lex(const Level &L, const float *src_lex, cudaStream_t s) {
     k_stencil_lex<<<(unsigned)((L.P.nv + 127) / 128), 128, 0, s>>>(L.P, nullptr, nullptr, src_lex, L.st, L.st32);
+}
+
+// ---- the bottom of the V-cycle in one cooperative launch -------------------------
+// The small levels cost a launch per colour (about 6 us each inside a graph,
+// whatever the level's size).  k_vcycle_bottom runs the V-cycle's steps from the
+// restriction into level `first` down to the coarsest solve and back up to the
+// post-smoothing of level `first` as phases of one cooperative launch, separated by
+// grid-wide barriers: per smoothed level on the way down, restriction (and the
+// cleared correction), eight colours (the last with its residual), the residual of
+// the other seven colours; at the bottom the restriction and the dense coarsest
+// solve; per level on the way up, prolongation and eight colours.  Each phase runs
+// the arithmetic of the separate kernels in the same order (two load cases per
+// thread, ratio-2 transfers), so the results are the same to the last bit.  Values
+// that other CTAs wrote earlier in the launch are read through L2 (ld.global.cg).
+// The barrier is a counter and a generation number in global memory; a wait that
+// runs out (it cannot, with all CTAs resident, but it is bounded) sets *flag and
+// the CTA leaves the kernel, whose later waits then run out too.
+constexpr int BOT_MAXLV = 8;
+constexpr int BOT_T = 128;
+constexpr long long BOT_WAIT_LIMIT = 1ll << 24;  // polls of the generation (L2 round trips)
+
+struct BottomArgs {
+    CoarseArgs lv[BOT_MAXLV + 1];  // lv[0]: the level above `first` (its residual, its u after the cycle)
+    Planes P[BOT_MAXLV + 1];
+    int nlv;                       // levels from `first` to the coarsest
+    int project;                   // coarsest: remove the mean first
+    int ndof;                      // coarsest unknowns
+    const double *aug;             // coarsest [K | K^-1]
+    unsigned *bar;                 // [0] arrivals, [1] generation
+    int *flag;
+};
+
+__device__ __forceinline__ bool bottom_sync(unsigned *bar, int *flag) {
+    __shared__ int gone;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        gone = 0;
+        volatile unsigned *gen = bar + 1;
+        const unsigned g = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long it = 0;
+            while (*gen == g) {
+                if (++it > BOT_WAIT_LIMIT) {
+                    gone = 1;
+                    atomicExch(flag, 1);
+                    break;
+                }
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return gone == 0;
+}
+
+// restriction (ratio 2) of F's residual into C's right-hand side, C's correction cleared
+__device__ void bottom_restrict(const CoarseArgs &Fa, const Planes &F, const CoarseArgs &Ca, const Planes &C) {
+    const long long total = C.nv * NCASE;
+    for (long long t = blockIdx.x * (long long)BOT_T + threadIdx.x; t < total; t += (long long)gridDim.x * BOT_T) {
+        const int c = (int)(t / C.nv);
+        const long long v = t - (long long)c * C.nv;
+        const int x = (int)(v % C.n[0]), y = (int)((v / C.n[0]) % C.n[1]), z = (int)(v / ((long long)C.n[0] * C.n[1]));
+        const int xm = x == 0 ? C.n[0] - 1 : x - 1, ym = y == 0 ? C.n[1] - 1 : y - 1, zm = z == 0 ? C.n[2] - 1 : z - 1;
+        const long long cpl = F.nv / 8;
+        float a0 = 0.f, a1 = 0.f, a2 = 0.f;
+#pragma unroll
+        for (int ox = -1; ox <= 1; ox++)
+#pragma unroll
+            for (int oy = -1; oy <= 1; oy++)
+#pragma unroll
+                for (int oz = -1; oz <= 1; oz++) {
+                    const float w = (float)((2 - abs(ox)) * (2 - abs(oy)) * (2 - abs(oz))) / 8.f;
+                    const int k = ((ox + 1) & 1) | (((oy + 1) & 1) << 1) | (((oz + 1) & 1) << 2);
+                    const long long fi = k * cpl + (ox < 0 ? xm : x) +
+                                         (long long)C.n[0] * ((oy < 0 ? ym : y) + (long long)C.n[1] * (oz < 0 ? zm : z));
+                    const float *src = Fa.r + fidx(3 * c, fi);
+                    a0 = fmaf(__ldcg(&src[0]), w, a0);
+                    a1 = fmaf(__ldcg(&src[FVB]), w, a1);
+                    a2 = fmaf(__ldcg(&src[2 * FVB]), w, a2);
+                }
+        float *dst = const_cast<float *>(Ca.f) + fidx(3 * c, vidx(C, x, y, z));
+        dst[0] = a0;
+        dst[FVB] = a1;
+        dst[2 * FVB] = a2;
+    }
+    const long long nu = field_floats(C.nv);
+    for (long long t = blockIdx.x * (long long)BOT_T + threadIdx.x; t < nu; t += (long long)gridDim.x * BOT_T)
+        Ca.u[t] = 0.f;
+}
+
+// trilinear prolongation (ratio 2) of C's correction into F's
+__device__ void bottom_prolong(const CoarseArgs &Fa, const Planes &F, const CoarseArgs &Ca, const Planes &C) {
+    for (long long t = blockIdx.x * (long long)BOT_T + threadIdx.x; t < C.nv; t += (long long)gridDim.x * BOT_T) {
+        const int x = (int)(t % C.n[0]), y = (int)((t / C.n[0]) % C.n[1]), z = (int)(t / ((long long)C.n[0] * C.n[1]));
+        const int xp = x + 1 == C.n[0] ? 0 : x + 1, yp = y + 1 == C.n[1] ? 0 : y + 1, zp = z + 1 == C.n[2] ? 0 : z + 1;
+        long long ci[8];
+#pragma unroll
+        for (int id = 0; id < 8; ++id)
+            ci[id] = vidx(C, (id & 1) ? xp : x, ((id >> 1) & 1) ? yp : y, (id >> 2) ? zp : z);
+        const long long cpl = F.nv / 8;
+        for (int pl = 0; pl < NF; ++pl) {
+            float cv[8], fv[8];
+#pragma unroll
+            for (int id = 0; id < 8; ++id) cv[id] = __ldcg(&Ca.u[fidx(pl, ci[id])]);
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int ex = e & 1, ey = (e >> 1) & 1, ez = e >> 2;
+                const int k = ((ex + 1) & 1) | (((ey + 1) & 1) << 1) | (((ez + 1) & 1) << 2);
+                fv[e] = __ldcg(&Fa.u[fidx(pl, k * cpl + t)]);
+            }
+#pragma unroll
+            for (int e = 0; e < 8; ++e) {
+                const int ex = e & 1, ey = (e >> 1) & 1, ez = e >> 2;
+                float acc = 0.f;
+#pragma unroll
+                for (int id = 0; id < 8; ++id) {
+                    const int ox = id & 1, oy = (id >> 1) & 1, oz = id >> 2;
+                    const float w =
+                        (float)((2 - abs(ox * 2 - ex)) * (2 - abs(oy * 2 - ey)) * (2 - abs(oz * 2 - ez))) / 8.f;
+                    if (w == 0.f) continue;
+                    acc = fmaf(cv[id], w, acc);
+                }
+                const int k = ((ex + 1) & 1) | (((ey + 1) & 1) << 1) | (((ez + 1) & 1) << 2);
+                Fa.u[fidx(pl, k * cpl + t)] = fv[e] + acc;
+            }
+        }
+    }
+}
+
+// one colour K of the sweep (two load cases per thread); RES: also the residual
+template <bool F32, int K, bool RES>
+__device__ void bottom_gs_k(const CoarseArgs &a) {
+    constexpr int C = 2, NG = NCASE / C;
+    constexpr bool res = RES;
+    const long long nvb = (a.P + BOT_T - 1) / BOT_T * NG;
+    for (long long b = blockIdx.x; b < nvb; b += gridDim.x) {
+        const int cb = (int)(b % NG) * C;
+        const long long p = (b / NG) * BOT_T + threadIdx.x;
+        if (p >= a.P) continue;
+        const long long me = (long long)K * a.P + p;
+        int i, j, l;
+        cplane_coords(a, p, i, j, l);
+        float acc[3 * C], ks[9];
+        coarse_apply<K, false, F32, C, true>(a, me, i, j, l, cb, acc);
+        load_block<13, F32>(a, me, ks);
+        const float w = a.w;
+#pragma unroll
+        for (int c = 0; c < C; ++c) {
+            float *u = a.u + fidx(3 * (cb + c), me);
+            const float *f = a.f + fidx(3 * (cb + c), me);
+            const float f0 = __ldcg(f), f1 = __ldcg(f + FVB), f2 = __ldcg(f + 2 * FVB);
+            float u0 = __ldcg(u), u1 = __ldcg(u + FVB), u2 = __ldcg(u + 2 * FVB);
+            u0 = w * (f0 - acc[3 * c] - ks[1] * u1 - ks[2] * u2) / ks[0] + (1.f - w) * u0;
+            u1 = w * (f1 - acc[3 * c + 1] - ks[3] * u0 - ks[5] * u2) / ks[4] + (1.f - w) * u1;
+            u2 = w * (f2 - acc[3 * c + 2] - ks[6] * u0 - ks[7] * u1) / ks[8] + (1.f - w) * u2;
+            u[0] = u0;
+            u[FVB] = u1;
+            u[2 * FVB] = u2;
+            if (res) {
+                float *r = a.r + fidx(3 * (cb + c), me);
+                const float ff[3] = {f0, f1, f2};
+#pragma unroll
+                for (int m = 0; m < 3; ++m)
+                    r[m * FVB] = ff[m] - acc[3 * c + m] - fmaf(ks[3 * m + 2], u2, fmaf(ks[3 * m + 1], u1, ks[3 * m] * u0));
+            }
+        }
+    }
+}
+
+template <bool F32>
+__device__ void bottom_gs(const CoarseArgs &a, int K, bool res) {
+    switch (K) {
+    case 0: bottom_gs_k<F32, 0, false>(a); break;
+    case 1: bottom_gs_k<F32, 1, false>(a); break;
+    case 2: bottom_gs_k<F32, 2, false>(a); break;
+    case 3: bottom_gs_k<F32, 3, false>(a); break;
+    case 4: bottom_gs_k<F32, 4, false>(a); break;
+    case 5: bottom_gs_k<F32, 5, false>(a); break;
+    case 6: bottom_gs_k<F32, 6, false>(a); break;
+    default:
+        if (res) bottom_gs_k<F32, 7, true>(a);
+        else bottom_gs_k<F32, 7, false>(a);
+        break;
+    }
+}
+
+// the residual of colours 0..6 (colour 7's came with its sweep)
+template <bool F32>
+__device__ void bottom_residual(const CoarseArgs &a) {
+    constexpr int C = 2, NG = NCASE / C, NCOL = 7;
+    const long long nvb = (a.P + BOT_T - 1) / BOT_T * NG * NCOL;
+    for (long long b = blockIdx.x; b < nvb; b += gridDim.x) {
+        const int K = (int)(b % NCOL);
+        const long long bx = b / NCOL;
+        const int cb = (int)(bx % NG) * C;
+        const long long p = (bx / NG) * BOT_T + threadIdx.x;
+        if (p >= a.P) continue;
+        const long long me = (long long)K * a.P + p;
+        int i, j, l;
+        cplane_coords(a, p, i, j, l);
+        float acc[3 * C];
+        coarse_apply<-1, true, F32, C, true>(a, me, i, j, l, cb, acc, K);
+#pragma unroll
+        for (int q = 0; q < 3 * C; ++q) {
+            const long long o = fidx(3 * cb + q, me);
+            a.r[o] = __ldcg(a.f + o) - acc[q];
+        }
+    }
+}
+
+// the dense coarsest solve, one CTA per load case (the arithmetic of k_coarse_apply)
+__device__ void bottom_coarsest(const BottomArgs &A, double *b) {
+    const CoarseArgs &a = A.lv[A.nlv];
+    const Planes &C = A.P[A.nlv];
+    const int n = A.ndof;
+    __shared__ double mean[3];
+    for (int c = blockIdx.x; c < NCASE; c += gridDim.x) {
+        for (int i = threadIdx.x; i < n; i += BOT_T) {
+            const long long lex = i / 3;
+            const int comp = i % 3;
+            const int x = (int)(lex % C.n[0]), y = (int)((lex / C.n[0]) % C.n[1]),
+                      z = (int)(lex / ((long long)C.n[0] * C.n[1]));
+            b[i] = __ldcg(a.f + fidx(3 * c + comp, vidx(C, x, y, z)));
+        }
+        __syncthreads();
+        if (threadIdx.x < 3) {
+            double sum = 0;
+            if (A.project)
+                for (int i = threadIdx.x; i < n; i += 3) sum += b[i];
+            mean[threadIdx.x] = sum / (double)(n / 3);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += BOT_T) b[i] -= mean[i % 3];
+        __syncthreads();
+        for (int i = threadIdx.x; i < n; i += BOT_T) {
+            const double *row = A.aug + (long long)i * 2 * n + n;
+            double sum = 0;
+            for (int j = 0; j < n; j++) sum = fma(row[j], b[j], sum);
+            const long long lex = i / 3;
+            const int comp = i % 3;
+            const int x = (int)(lex % C.n[0]), y = (int)((lex / C.n[0]) % C.n[1]),
+                      z = (int)(lex / ((long long)C.n[0] * C.n[1]));
+            a.u[fidx(3 * c + comp, vidx(C, x, y, z))] = (float)sum;
+        }
+        __syncthreads();
+    }
+}
+
+template <bool F32>
+__global__ void __launch_bounds__(BOT_T) k_vcycle_bottom(const __grid_constant__ BottomArgs A) {
+    extern __shared__ double bot_b[];
+    const int L = A.nlv;  // lv[1..L-1] smoothed, lv[L] the coarsest
+    for (int l = 1; l < L; ++l) {
+        bottom_restrict(A.lv[l - 1], A.P[l - 1], A.lv[l], A.P[l]);
+        if (!bottom_sync(A.bar, A.flag)) return;
+        for (int K = 0; K < 8; ++K) {
+            bottom_gs<F32>(A.lv[l], K, K == 7);
+            if (!bottom_sync(A.bar, A.flag)) return;
+        }
+        bottom_residual<F32>(A.lv[l]);
+        if (!bottom_sync(A.bar, A.flag)) return;
+    }
+    bottom_restrict(A.lv[L - 1], A.P[L - 1], A.lv[L], A.P[L]);
+    if (!bottom_sync(A.bar, A.flag)) return;
+    bottom_coarsest(A, bot_b);
+    if (!bottom_sync(A.bar, A.flag)) return;
+    for (int l = L - 1; l >= 1; --l) {
+        bottom_prolong(A.lv[l], A.P[l], A.lv[l + 1], A.P[l + 1]);
+        if (!bottom_sync(A.bar, A.flag)) return;
+        for (int K = 0; K < 8; ++K) {
+            bottom_gs<F32>(A.lv[l], K, false);
+            if (l > 1 || K < 7)
+                if (!bottom_sync(A.bar, A.flag)) return;
+        }
+    }
+}
+
+// first: the first level of the bottom; levels first-1 .. nl-1 are passed
+int launch_vcycle_bottom(const Level *lv, int first, int nl, const double *aug, int project, unsigned *bar, int *flag,
+                         int nblk, cudaStream_t s) {
+    BottomArgs A;
+    A.nlv = nl - first;
+    if (A.nlv < 1 || A.nlv > BOT_MAXLV || first < 1) return -1;
+    for (int i = 0; i <= A.nlv; ++i) {
+        A.lv[i] = make_cargs(lv[first - 1 + i]);
+        A.P[i] = lv[first - 1 + i].P;
+    }
+    A.project = project;
+    A.ndof = (int)(3 * lv[nl - 1].P.nv);
+    A.aug = aug;
+    A.bar = bar;
+    A.flag = flag;
+    const bool f32 = lv[first].st32;
+    cudaLaunchConfig_t cfg = {};
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeCooperative;
+    attr[0].val.cooperative = 1;
+    cfg.gridDim = dim3((unsigned)nblk);
+    cfg.blockDim = dim3(BOT_T);
+    cfg.dynamicSmemBytes = sizeof(double) * (size_t)A.ndof;
+    cfg.stream = s;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), s);
+    const cudaError_t e = f32 ? cudaLaunchKernelEx(&cfg, k_vcycle_bottom<true>, A)
+                              : cudaLaunchKernelEx(&cfg, k_vcycle_bottom<false>, A);
+    return e == cudaSuccess ? 0 : -2;
+}
+
+// CTAs of the cooperative grid: all resident at once (blocks per SM from the
+// occupancy query, at most four)
+int vcycle_bottom_blocks(int num_sms, int ndof, bool f32) {
+    int per = 0;
+    const cudaError_t e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per, f32 ? (const void *)k_vcycle_bottom<true> : (const void *)k_vcycle_bottom<false>, BOT_T,
+        sizeof(double) * (size_t)ndof);
+    if (e != cudaSuccess || per < 1) return 0;
+    return num_sms;  // one CTA per SM: the fewest arrivals per barrier
+}
+
+// whether levels first..nl-2 can run in the bottom kernel: even smoothed levels,
+// ratio 2 everywhere below `first - 1`, at most BOT_MAXLV levels
+bool vcycle_bottom_fits(const Level *lv, int first, int nl) {
+    if (first < 1 || nl - first < 1 || nl - first > BOT_MAXLV) return false;
+    for (int l = first; l < nl; ++l) {
+        if (lv[l].ratio[0] != 2 || lv[l].ratio[1] != 2 || lv[l].ratio[2] != 2) return false;
+        if (!lv[l - 1].P.even) return false;
+        if (l < nl - 1 && !lv[l].P.even) return false;
+    }
+    return true;
 }
 
 }  // namespace h3d

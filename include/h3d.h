@@ -191,6 +191,16 @@ H3D_API int h3d_reset_solutions(h3d_handle *h);
  * shapes[0] = sweep, shapes[1] = residual. */
 #define H3D_NUM_SHAPES 4
 H3D_API int h3d_autotune(h3d_handle *h);
+/* The V-cycle's levels of at most max_level_vertices vertices (0, the default: none)
+ * run from the restriction into the largest of them to its post-smoothing in one
+ * cooperative kernel launch (no reference counterpart; the reference launches every
+ * colour and transfer of every level): per level and colour a phase separated by a
+ * grid-wide barrier, the same arithmetic as the separate launches, the same results
+ * to the last bit.  Levels with other than ratio-2 coarsening below it fall back to
+ * separate launches.  Off by default: on B200 a grid barrier costs about as much
+ * as a kernel boundary inside the captured V-cycle graph, and the bottom measured
+ * slower (256^3: 12.70 against 12.41 ms per V-cycle with levels up to 32^3). */
+H3D_API int h3d_set_vcycle_bottom(h3d_handle *h, int64_t max_level_vertices);
 H3D_API int h3d_get_tuning(const h3d_handle *h, int level, int shapes[2]);
 H3D_API int h3d_set_tuning(h3d_handle *h, int level, int gs_shape, int res_shape);
 
