@@ -53,7 +53,8 @@ def parse():
     p.add_argument("--profile", action="store_true",
                    help="only warm-up and timed steps (no e2e, setup or sweep side measurements), for ncu")
     p.add_argument("--precision", type=int, default=0,
-                   help="0 refined (FP64 solution), 1 FP32, 2 refined with the tensor-core level-0 residual")
+                   help="0 refined (FP64 solution), 1 FP32, 2 refined with an FP32-accumulated refinement "
+                        "residual, 3 as 2 with the tensor-core level-0 residual")
     return p.parse_args()
 
 
@@ -131,8 +132,11 @@ SWEEP_TRAFFIC_BYTES = {128: 1_510_000_000, 256: 12_080_000_000}
 
 PRECISION_NAME = {0: "FP32 V-cycles on the correction of an FP64 solution (iterative refinement)",
                   1: "FP32 solution (the reference's scheme)",
-                  2: "FP32 V-cycles on the correction of an FP64 solution (iterative refinement), level-0 "
-                     "residual on tcgen05 tensor cores (TF32 hi+lo operands, FP32 accumulation)"}
+                  2: "FP32 V-cycles on the correction of an FP64 solution (iterative refinement) with the "
+                     "refinement residual accumulated in FP32",
+                  3: "FP32 V-cycles on the correction of an FP64 solution (iterative refinement) with the "
+                     "refinement residual accumulated in FP32 and the level-0 V-cycle residual on tcgen05 "
+                     "tensor cores (TF32 hi+lo operands, FP32 accumulation)"}
 
 
 def launches_per_step(nl, vcycles, reso, refine, refinements, coarsest_nv, mixed=False):
@@ -289,7 +293,7 @@ def gpu_arm(args):
             "refinements": refs[-1],
             "launch_shapes": hd.tuning(),
             "gpu_launches": sum(launches_per_step(hd.nlevels, c, args.reso, args.precision != 1, r, coarsest_nv,
-                                                  args.precision == 2) for c, r in zip(cycles, refs)),
+                                                  args.precision == 3) for c, r in zip(cycles, refs)),
             "roofline": {"kernel": "k_fine_gs (8 colour launches = one sweep)", "bound": "hbm",
                          "achieved": round(achieved, 1), "peak": peaks.get("hbm_gbs"), "unit": "GB/s",
                          "frac": round(achieved / peaks.get("hbm_gbs"), 4),
@@ -311,46 +315,52 @@ def gpu_arm(args):
 def north_star(args, rho_d, plain_ms, plain_vc, plain_err, fx):
     """The precision arms of the same step on the same design, device-timed like the
     headline value: the plain arm (the headline: refined FP32 V-cycles, SIMT
-    operator) against the mixed arm (the level-0 V-cycle residual on the tensor
-    cores, H3D_PREC_MIXED).  The learned warm start is not in the step: its trained
-    network saves no V-cycles on fresh designs (the solver's fallback rejects its
-    prediction), so it would only add its forward pass."""
+    operator, FP64-accumulated refinement residual) against the mixed arms
+    (H3D_PREC_MIXED: the refinement residual accumulated in FP32; H3D_PREC_MIXED_TC:
+    besides, the level-0 V-cycle residual on the tensor cores).  The learned warm
+    start is not in the step: its trained network saves no V-cycles on fresh
+    designs (the solver's fallback rejects its prediction), so it would only add
+    its forward pass."""
     import numpy as np
     import torch
 
     import homo3d_b200 as H
-    hm = H.Homogenization(args.reso, pin_mode=args.pin_mode, precision=H.PREC_MIXED)
-    stream = torch.cuda.ExternalStream(hm.stream)
 
-    def step():
-        hm.update(rho_d)
-        hm.reset_solutions()
-        return hm.elasticMatrix(args.tol)
+    def arm(precision):
+        hm = H.Homogenization(args.reso, pin_mode=args.pin_mode, precision=precision)
+        stream = torch.cuda.ExternalStream(hm.stream)
 
-    for _ in range(max(1, min(args.warmup, 2))):
-        step()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    torch.cuda.synchronize()
-    ev0.record(stream)
-    cyc = []
-    for _ in range(args.steps):
-        C = step()
-        cyc.append(hm.last_stats["vcycles"])
-    ev1.record(stream)
-    torch.cuda.synchronize()
-    st = hm.last_stats
-    hm.close()
-    mixed_ms = ev0.elapsed_time(ev1) / args.steps
-    err = None
-    if fx is not None:
-        Co = np.array(fx["C"]).reshape(6, 6)
-        err = float(np.abs(C - Co).max() / np.abs(Co).max())
-    return {"plain_ms": round(plain_ms, 3), "mixed_ms": round(mixed_ms, 3),
-            "ratio_mixed_over_plain": round(mixed_ms / plain_ms, 4), "target_ratio": 0.5,
-            "plain_vcycles": plain_vc, "mixed_vcycles": int(round(sum(cyc) / len(cyc))),
-            "mixed_status": st["status"], "plain_C_err": plain_err, "mixed_C_err": err,
-            "learned": "not in the step (saves no V-cycles on fresh designs)",
-            "plain": PRECISION_NAME[0], "mixed": PRECISION_NAME[2]}
+        def step():
+            hm.update(rho_d)
+            hm.reset_solutions()
+            return hm.elasticMatrix(args.tol)
+
+        for _ in range(max(1, min(args.warmup, 2))):
+            step()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        cyc = []
+        for _ in range(args.steps):
+            C = step()
+            cyc.append(hm.last_stats["vcycles"])
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        st = hm.last_stats
+        hm.close()
+        err = None
+        if fx is not None:
+            Co = np.array(fx["C"]).reshape(6, 6)
+            err = float(np.abs(C - Co).max() / np.abs(Co).max())
+        ms = ev0.elapsed_time(ev1) / args.steps
+        return {"ms": round(ms, 3), "ratio_over_plain": round(ms / plain_ms, 4),
+                "vcycles": int(round(sum(cyc) / len(cyc))), "refinements": st["refinements"],
+                "status": st["status"], "C_err": err, "scheme": PRECISION_NAME[precision]}
+
+    mixed, mixed_tc = arm(H.PREC_MIXED), arm(H.PREC_MIXED_TC)
+    return {"plain_ms": round(plain_ms, 3), "plain_vcycles": plain_vc, "plain_C_err": plain_err,
+            "target_ratio": 0.5, "mixed": mixed, "mixed_tc": mixed_tc,
+            "learned": "not in the step (saves no V-cycles on fresh designs)", "plain": PRECISION_NAME[0]}
 
 
 FIXTURE = os.path.join(ROOT, "tests", "golden", "oracle_C.json")

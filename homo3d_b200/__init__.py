@@ -34,7 +34,7 @@ H3D_OK, H3D_ERR_ARG, H3D_ERR_CUDA, H3D_ERR_NOMEM, H3D_NOT_CONVERGED, H3D_DIVERGE
 FIELD_U, FIELD_F, FIELD_R, FIELD_STENCIL, FIELD_CHI, FIELD_SOLUTION = range(6)
 COARSE_EXACT, COARSE_PROJECT = 0, 1
 PIN_IDENTITY, PIN_GALERKIN = 0, 1
-PREC_REFINE, PREC_FP32, PREC_MIXED = 0, 1, 2
+PREC_REFINE, PREC_FP32, PREC_MIXED, PREC_MIXED_TC = 0, 1, 2, 3
 NUM_SHAPES = 4  # launch shapes per kernel family the autotuner searches (H3D_NUM_SHAPES)
 STENCIL_FP16, STENCIL_FP32 = 0, 1
 SYMMETRY = {"reflect3": 0, "reflect6": 1, "rotate3": 2}

@@ -177,7 +177,9 @@ struct h3d_handle {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
     bool refine() const { return cfg.precision != H3D_PREC_FP32; }
     // the level-0 V-cycle residual on the tensor cores (k_fine_tc.cu)
-    bool mixed() const { return cfg.precision == H3D_PREC_MIXED; }
+    bool mixed() const { return cfg.precision == H3D_PREC_MIXED_TC; }
+    // the refinement residual accumulated in FP32 down to relthres 2e-6
+    bool fp32_refine() const { return cfg.precision == H3D_PREC_MIXED || cfg.precision == H3D_PREC_MIXED_TC; }
     int num_sms = 0;
     int *d_tcflag = nullptr;            // set by the tensor-core residual if an mbarrier wait timed out
     // cooperative bottom of the V-cycle: levels of at most bottom_nv vertices (0: off,
@@ -559,7 +561,7 @@ struct SolveRun {
         if (int e = build_graph(h, G_SOLVE)) return e;
         // below ~1e-4 the FP32 products of the difference-form residual would floor
         // the iteration, so tight targets take the FP64-accumulating residual
-        exact = refine && tol < 1e-4;
+        exact = refine && tol < (h->fp32_refine() ? 2e-6 : 1e-4);
         if (refine)
             if (int e = build_graph(h, exact ? G_REFINE_EXACT : G_REFINE)) return e;
         refine_step = exact ? h->xgraph : h->rgraph;
@@ -789,7 +791,8 @@ static int create_impl(h3d_handle *h, const h3d_config *cfg) {
         return fail(h, H3D_ERR_ARG, "invalid coarse_mode");
     if (cfg->pin_mode != H3D_PIN_IDENTITY && cfg->pin_mode != H3D_PIN_GALERKIN)
         return fail(h, H3D_ERR_ARG, "invalid pin_mode");
-    if (cfg->precision != H3D_PREC_REFINE && cfg->precision != H3D_PREC_FP32 && cfg->precision != H3D_PREC_MIXED)
+    if (cfg->precision != H3D_PREC_REFINE && cfg->precision != H3D_PREC_FP32 && cfg->precision != H3D_PREC_MIXED &&
+        cfg->precision != H3D_PREC_MIXED_TC)
         return fail(h, H3D_ERR_ARG, "invalid precision");
     if (cfg->stencil_precision != H3D_STENCIL_FP16 && cfg->stencil_precision != H3D_STENCIL_FP32)
         return fail(h, H3D_ERR_ARG, "invalid stencil_precision");

@@ -68,7 +68,12 @@ typedef enum {
                                    refinement) */
     H3D_PREC_FP32 = 1,          /* FP32 solution swept directly, as the reference does; its
                                    relative residual floors near 1e-6 * N */
-    H3D_PREC_MIXED = 2          /* H3D_PREC_REFINE with the level-0 residual of every V-cycle
+    H3D_PREC_MIXED = 2,         /* H3D_PREC_REFINE with the refinement residual accumulated
+                                   in FP32 (FP64 differences, FP32 products and sums) down
+                                   to relthres 2e-6, below which it accumulates in FP64;
+                                   that residual's floor is ~1e-6 of ||f|| at any grid
+                                   size (no reference counterpart) */
+    H3D_PREC_MIXED_TC = 3       /* H3D_PREC_MIXED with the level-0 residual of every V-cycle
                                    formed element by element on the tensor cores: element
                                    displacement differences and Ke as TF32 hi + lo parts,
                                    FP32 accumulation (no reference counterpart) */

@@ -76,14 +76,14 @@ def solve_and_check(torch, n, vol, precision=H.PREC_REFINE):
         hd.close()
 
 
-@pytest.mark.parametrize("precision", [H.PREC_REFINE, H.PREC_MIXED])
+@pytest.mark.parametrize("precision", [H.PREC_REFINE, H.PREC_MIXED, H.PREC_MIXED_TC])
 def test_benchmark_design_256_matches_oracle(torch_cuda, precision):
     st = solve_and_check(torch_cuda, 256, 0.3, precision)
     assert st["vcycles"] <= 12
 
 
 @pytest.mark.parametrize("vol", [0.1, 0.3, 0.5])
-@pytest.mark.parametrize("precision", [H.PREC_REFINE, H.PREC_MIXED])
+@pytest.mark.parametrize("precision", [H.PREC_REFINE, H.PREC_MIXED, H.PREC_MIXED_TC])
 def test_128_designs_match_oracle(torch_cuda, vol, precision):
     solve_and_check(torch_cuda, 128, vol, precision)
 

@@ -1,4 +1,4 @@
-"""The level-0 residual on the tensor cores (precision H3D_PREC_MIXED, k_fine_tc.cu)
+"""The level-0 residual on the tensor cores (precision H3D_PREC_MIXED_TC, k_fine_tc.cu)
 against the FP64 oracle (update_residual_otf_kernel_1, grid.cu:1277-1461), and the
 mixed-precision solve against the refined one and the oracle.
 
@@ -23,7 +23,7 @@ pytestmark = pytest.mark.gpu
 def test_tc_residual_matches_oracle(torch_cuda, n, scale):
     """random fields of widely different magnitudes; 12 and 28 leave partial 8^3
     bricks (every grid of 32 or more cells per axis is a multiple of 8)"""
-    hd, m, _ = make_pair(torch_cuda, n=n, seed=3, precision=H.PREC_MIXED)
+    hd, m, _ = make_pair(torch_cuda, n=n, seed=3, precision=H.PREC_MIXED_TC)
     nv = n ** 3
     u0, f0 = random_field(nv, 3, scale), random_field(nv, 4, scale)
     u0[0] = 0
@@ -41,7 +41,7 @@ def test_tc_residual_matches_oracle(torch_cuda, n, scale):
 
 def test_tc_residual_is_deterministic(torch_cuda):
     n = 32
-    hd, _, _ = make_pair(torch_cuda, n=n, seed=4, precision=H.PREC_MIXED)
+    hd, _, _ = make_pair(torch_cuda, n=n, seed=4, precision=H.PREC_MIXED_TC)
     nv = n ** 3
     hd.grid.set(H.FIELD_U, to_lib_field(random_field(nv, 8)))
     hd.grid.set(H.FIELD_F, to_lib_field(random_field(nv, 9)))
@@ -55,7 +55,7 @@ def test_tc_residual_is_deterministic(torch_cuda):
 
 def test_mixed_vcycle_matches_oracle(torch_cuda):
     n = 32
-    hd, m, _ = make_pair(torch_cuda, n=n, seed=5, precision=H.PREC_MIXED)
+    hd, m, _ = make_pair(torch_cuda, n=n, seed=5, precision=H.PREC_MIXED_TC)
     copy_stencils_to_oracle(hd, m)
     hd.grid.enforce_unit_macro_strain()
     m.rhs()
@@ -73,12 +73,12 @@ def test_mixed_solve_matches_refined_and_oracle(torch_cuda, n, seed, vol):
     rho = smooth_density(n, seed=seed, vol=vol)
     t = torch_cuda.tensor(rho, dtype=torch_cuda.float32, device="cuda")
     out = {}
-    for prec in (H.PREC_REFINE, H.PREC_MIXED):
+    for prec in (H.PREC_REFINE, H.PREC_MIXED_TC):
         hd = H.Homogenization(n, precision=prec)
         hd.update(t)
         out[prec] = (hd.elasticMatrix(1e-5), hd.last_stats)
         hd.close()
-    (Cr, sr), (Cm, sm) = out[H.PREC_REFINE], out[H.PREC_MIXED]
+    (Cr, sr), (Cm, sm) = out[H.PREC_REFINE], out[H.PREC_MIXED_TC]
     assert sm["status"] == H.H3D_OK and max(sm["rel_res"]) <= 1e-5
     assert sm["vcycles"] <= sr["vcycles"] + 1, (sm, sr)
     Cref = oracle_C(n, rho).elastic_matrix()
