@@ -200,12 +200,14 @@ struct VertexGeo {
 template <int K, int C>
 __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, const VertexGeo<K> &g, int cb,
                                            const float uv[3 * C], float acc[3 * C]) {
-    static_assert(C % 2 == 0, "the load cases of a thread go in packed FP32x2 lane pairs");
     constexpr int NP = C / 2;  // case pairs per thread
+    constexpr int NS = C % 2;  // an odd last case, on scalar lanes
     // lane pair (case cb+2j, case cb+2j+1) of each component: Blackwell's packed
     // FP32x2 add and FMA do both cases in one instruction with the rounding of the
-    // scalar forms, so the sums are the same as the scalar per-case loop
-    float2 acc2[3 * NP], nuv2[3 * NP];
+    // scalar forms, so the sums are the same as the scalar per-case loop (the odd
+    // case runs the scalar forms in the same order)
+    float2 acc2[3 * NP + 1], nuv2[3 * NP + 1];
+    float acc1[3 * NS + 1], nuv1[3 * NS + 1];
 #pragma unroll
     for (int j = 0; j < NP; ++j)
 #pragma unroll
@@ -213,6 +215,11 @@ __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, c
             acc2[3 * j + m] = make_float2(0.f, 0.f);
             nuv2[3 * j + m] = make_float2(-uv[6 * j + m], -uv[6 * j + 3 + m]);
         }
+#pragma unroll
+    for (int m = 0; m < 3 * NS; ++m) {
+        acc1[m] = 0.f;
+        nuv1[m] = -uv[6 * NP + m];
+    }
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         if (d == 13) continue;
@@ -238,6 +245,14 @@ __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, c
                                                         __ffma2_rn(make_float2(A[3 * r + 2], A[3 * r + 2]), dd[2],
                                                                    acc2[3 * j + r])));
         }
+        if (NS) {
+            float dd[3];
+#pragma unroll
+            for (int m = 0; m < 3; ++m) dd[m] = __fadd_rn(pinned ? 0.f : __ldg(up + (6 * NP + m) * FVB), nuv1[m]);
+#pragma unroll
+            for (int r = 0; r < 3; ++r)
+                acc1[r] = __fmaf_rn(A[3 * r], dd[0], __fmaf_rn(A[3 * r + 1], dd[1], __fmaf_rn(A[3 * r + 2], dd[2], acc1[r])));
+        }
     }
 #pragma unroll
     for (int j = 0; j < NP; ++j)
@@ -246,6 +261,8 @@ __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, c
             acc[6 * j + m] = acc2[3 * j + m].x;
             acc[6 * j + 3 + m] = acc2[3 * j + m].y;
         }
+#pragma unroll
+    for (int m = 0; m < 3 * NS; ++m) acc[6 * NP + m] = acc1[m];
 }
 
 // thread -> (vertex p in the colour plane, first case cb) for C cases per thread;
@@ -570,8 +587,9 @@ int fine_residual_blocks(const Level &L) { return (int)(((L.P.nv / 8 + FBS - 1) 
 
 // the colour sweep in launch shape v: 0 = one thread per vertex with all six
 // cases (4 CTAs/SM), 1 = three threads per vertex with two cases each (5 CTAs/SM),
-// 2 = six cases per thread at 3 CTAs/SM (more registers), 3 = two cases per thread
-// at 6 CTAs/SM (fewer registers); all give the same result to the last bit
+// 2 = three cases per thread (two threads per vertex, one case pair and one scalar
+// case) at 5 CTAs/SM, 3 = two cases per thread at 6 CTAs/SM (fewer registers);
+// all give the same result to the last bit
 template <int C, int MINB>
 static void fine_gs_sweep(const FineArgs &a, const KeMat &ke, cudaStream_t s) {
     const unsigned nb = task_blocks(a, C);
@@ -590,7 +608,7 @@ void launch_fine_gs(const Level &L, const float *rho, const KeMat &ke, float w, 
     a.w = w;
     switch (L.gs_shape) {
     case 1: fine_gs_sweep<2, 5>(a, ke, s); break;
-    case 2: fine_gs_sweep<6, 3>(a, ke, s); break;
+    case 2: fine_gs_sweep<3, 5>(a, ke, s); break;
     case 3: fine_gs_sweep<2, 6>(a, ke, s); break;
     default: fine_gs_sweep<6, 4>(a, ke, s); break;
     }
@@ -609,7 +627,10 @@ static void fine_gs_sweep_res(const FineArgs &a, const KeMat &ke, double *partia
     k_fine_gs<4, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
     k_fine_gs<5, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
     k_fine_gs<6, C, MINB, false><<<nb, FBS, 0, s>>>(a, ke, nullptr);
-    k_fine_gs<7, C, MINB, true><<<nb, FBS, 0, s>>>(a, ke, partial);
+    // the last colour writes its residual with the norm partials of the residual's
+    // case pairs: an odd case count per thread takes the six-case kernel for it
+    constexpr int CR = (C % CPT == 0) ? C : 6, MR = (C % CPT == 0) ? MINB : 4;
+    k_fine_gs<7, CR, MR, true><<<task_blocks(a, CR), FBS, 0, s>>>(a, ke, partial);
     k_fine_residual<7><<<task_blocks(a, CPT) * 7, FBS, 0, s>>>(a, ke, partial);
 }
 
@@ -619,7 +640,7 @@ void launch_fine_gs_residual(const Level &L, const float *rho, const KeMat &ke, 
     a.w = w;
     switch (L.gs_shape) {
     case 1: fine_gs_sweep_res<2, 5>(a, ke, norm_partial, s); break;
-    case 2: fine_gs_sweep_res<6, 3>(a, ke, norm_partial, s); break;
+    case 2: fine_gs_sweep_res<3, 5>(a, ke, norm_partial, s); break;
     case 3: fine_gs_sweep_res<2, 6>(a, ke, norm_partial, s); break;
     default: fine_gs_sweep_res<6, 4>(a, ke, norm_partial, s); break;
     }
