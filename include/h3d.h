@@ -187,7 +187,7 @@ H3D_API int h3d_reset_solutions(h3d_handle *h);
  * Each smoothed level has H3D_NUM_SHAPES launch shapes for its colour sweep and
  * (coarse levels) its residual: load cases per thread (all six, or two as three
  * threads per vertex) times CTAs per SM (the register budget per thread).  Level 0:
- * shape 0 / 1 / 2 / 3 = six cases at 4 CTAs/SM / two at 5 / six at 3 / two at 6;
+ * shape 0 / 1 / 2 / 3 = six cases at 4 CTAs/SM / two at 5 / three at 5 / two at 6;
  * coarse levels: two at 6 / six at 4 / two at 4 / six at 3.  All give the same
  * results to the last bit.  The first solve of a handle times them (CUDA events,
  * a few sweeps per shape, iterating on the level's scratch residual field) and
