@@ -42,7 +42,9 @@ def test_training_fits_solver_pairs_and_the_hook_starts_the_solve(torch_cuda):
     rows = WN.compare_starts(net, n, seeds=[100, 101], relthres=1e-5)
     for r in rows:
         assert abs(r["learned_C00"] - r["zero_C00"]) <= 1e-5 * abs(r["zero_C00"])
-        assert r["learned_vcycles"] <= r["zero_vcycles"] + 1
+        # the solver drops a starting guess whose residual exceeds a zero start's,
+        # so a learned start never costs V-cycles
+        assert r["learned_vcycles"] <= r["zero_vcycles"]
 
 
 def test_bad_guess_falls_back_to_zero_start(torch_cuda):
@@ -58,3 +60,40 @@ def test_bad_guess_falls_back_to_zero_start(torch_cuda):
     hd.grid.set(H.FIELD_CHI, wild)
     hd.elasticMatrix(1e-5)
     assert hd.last_stats["vcycles"] == k0
+
+
+@pytest.mark.parametrize("n", [64, 128])
+def test_coarse_resolution_start_cannot_save_vcycles(torch_cuda, n):
+    """The bound on any warm start predicted at a coarser resolution: the converged
+    solution itself, averaged over 2^3 vertex blocks (half resolution) and
+    interpolated back trilinearly, starts the relthres-1e-5 solve no better than
+    zero (its interpolation error leaves a residual above ||f||), and the same
+    solution with 1 %% random noise neither; only the full-resolution solution
+    itself saves V-cycles.  A learned network at the solve's resolution would have
+    to be accurate to well under 1 %% per vertex to pay."""
+    torch = torch_cuda
+    rho = smooth_density(n, seed=0).astype(np.float32)
+    hd = H.Homogenization(n)
+    hd.update(torch.tensor(rho, device="cuda"))
+    hd.elasticMatrix(1e-9)
+    chi = hd.grid.get(H.FIELD_CHI)
+    hd.reset_solutions()
+    hd.elasticMatrix(1e-5)
+    zero = hd.last_stats["vcycles"]
+    c = torch.tensor(chi.reshape(6, n, n, n, 3).astype(np.float64))
+    R = n // 2
+    cm = c.reshape(6, R, 2, R, 2, R, 2, 3).mean(dim=(2, 4, 6)).permute(0, 4, 1, 2, 3)
+    big = torch.cat([cm, cm[:, :, :1]], 2)
+    big = torch.cat([big, big[:, :, :, :1]], 3)
+    big = torch.cat([big, big[:, :, :, :, :1]], 4)
+    up = torch.nn.functional.interpolate(big, size=(n + 2,) * 3, mode="trilinear", align_corners=True)[:, :, :n, :n, :n]
+    guess = up.permute(0, 2, 3, 4, 1).numpy().reshape(6, n ** 3, 3).astype(np.float32)
+    noisy = (chi * (1 + 0.01 * np.random.default_rng(0).standard_normal(chi.shape))).astype(np.float32)
+    counts = {}
+    for name, g in (("half", guess), ("noisy", noisy), ("exact", chi)):
+        hd.grid.set(H.FIELD_CHI, g)
+        hd.elasticMatrix(1e-5)
+        counts[name] = hd.last_stats["vcycles"]
+    hd.close()
+    assert counts["half"] >= zero and counts["noisy"] >= zero, (zero, counts)
+    assert counts["exact"] < zero, (zero, counts)
