@@ -68,9 +68,9 @@ def test_coarse_resolution_start_cannot_save_vcycles(torch_cuda, n):
     solution itself, sampled at the even vertices (half resolution) and
     interpolated back trilinearly, starts the relthres-1e-5 solve no better than
     zero (its interpolation error leaves a residual above ||f||), and the same
-    solution with 1 %% random noise neither; only the full-resolution solution
+    solution with 1 % random noise neither; only the full-resolution solution
     itself saves V-cycles.  A learned network at the solve's resolution would have
-    to be accurate to well under 1 %% per vertex to pay."""
+    to be accurate to well under 1 % per vertex to pay."""
     torch = torch_cuda
     rho = smooth_density(n, seed=0).astype(np.float32)
     hd = H.Homogenization(n)
