@@ -23,7 +23,7 @@ import os
 import numpy as np
 
 __all__ = ["Homogenization", "MG", "Grid", "OCOptimizer", "MMAOptimizer", "WarmNet", "H3DError", "symmetrize", "lib",
-           "LIB_PATH", "batch_update", "batch_elasticMatrix",
+           "LIB_PATH", "batch_update", "batch_elasticMatrix", "Lockstep",
            "reference_resolution"]
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
@@ -107,6 +107,9 @@ _SIGS = {
     "h3d_batch_update_density": [ctypes.POINTER(_vp), ctypes.POINTER(_vp), ctypes.c_int],
     "h3d_batch_elastic_matrix": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_double, _dp,
                                  ctypes.POINTER(SolveStats), _ip],
+    "h3d_lockstep_create": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)],
+    "h3d_lockstep_elastic_matrix": [_vp, ctypes.c_double, _dp, ctypes.POINTER(SolveStats), _ip],
+    "h3d_lockstep_destroy": [_vp],
     "h3d_penalize": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float],
     "h3d_penalize_backward": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float],
     "h3d_oc_update": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
@@ -157,11 +160,16 @@ def lib():
         L.h3d_mma_last_error.restype = ctypes.c_char_p
         L.h3d_warmnet_last_error.argtypes = [_vp]
         L.h3d_warmnet_last_error.restype = ctypes.c_char_p
+        L.h3d_lockstep_last_error.argtypes = [_vp]
+        L.h3d_lockstep_last_error.restype = ctypes.c_char_p
         _lib = L
     return _lib
 
 
-def _ptr(x):
+def _ptr(x, need=0, what="buffer"):
+    """device address of a CUDA tensor (or an int address, taken as is); need > 0:
+    the float32 elements the library will read or write through it (the C-ABI
+    cannot check a buffer's size, so a short tensor is refused here)"""
     if x is None:
         return None
     if isinstance(x, int):
@@ -171,6 +179,11 @@ def _ptr(x):
             raise ValueError("expected a CUDA tensor")
         if not x.is_contiguous():
             raise ValueError("expected a contiguous tensor")
+        if need:
+            if x.element_size() != 4 or not x.is_floating_point():
+                raise ValueError("%s: expected a float32 tensor" % what)
+            if x.numel() < need:
+                raise ValueError("%s holds %d values; %d are needed" % (what, x.numel(), need))
         # the handle's stream does not wait on torch's: finish the tensor's producers first
         import torch
         torch.cuda.current_stream(x.device).synchronize()
@@ -180,6 +193,14 @@ def _ptr(x):
 
 def _i3(v):
     return (ctypes.c_int * 3)(*[int(a) for a in v])
+
+
+def _extent(dims, pitch=-1):
+    """elements a lexicographic cell field of dims spans with row pitch `pitch`
+    (the x extent when negative): the last cell's index + 1"""
+    n0, n1, n2 = (int(a) for a in dims)
+    p = n0 if pitch is None or int(pitch) < 0 else int(pitch)
+    return (n0 - 1) + p * ((n1 - 1) + n1 * (n2 - 1)) + 1
 
 
 def reference_resolution(reso):
@@ -345,8 +366,10 @@ class Homogenization(_Handle):
         return ke.reshape(24, 24)
 
     def update(self, rho_phys, pitchT=-1):
-        """rho_phys: CUDA tensor of the physical (penalised) density, lexicographic."""
-        self.check(lib().h3d_update_density(self._h, _ptr(rho_phys), int(pitchT)))
+        """rho_phys: CUDA tensor of the physical (penalised) density, lexicographic on
+        the handle's grid (dims[0]: the reference's rounding of the requested size)."""
+        need = _extent(self.dims[0], pitchT)
+        self.check(lib().h3d_update_density(self._h, _ptr(rho_phys, need, "density"), int(pitchT)))
 
     def elasticMatrix(self, tol=1e-2):
         C = np.zeros(36)
@@ -359,7 +382,8 @@ class Homogenization(_Handle):
 
     def Sensitivity(self, dC, sens, pitchT=-1):
         d = np.ascontiguousarray(dC, dtype=np.float32).reshape(36)
-        self.check(lib().h3d_sensitivity(self._h, d.ctypes.data_as(_fp), _ptr(sens), int(pitchT)))
+        self.check(lib().h3d_sensitivity(self._h, d.ctypes.data_as(_fp),
+                                         _ptr(sens, _extent(self.dims[0], pitchT), "sensitivity"), int(pitchT)))
         self.sync()  # the caller's buffer is read on other streams
 
     def reset_solutions(self):
@@ -394,7 +418,9 @@ class Homogenization(_Handle):
         d = np.ascontiguousarray(dC, dtype=np.float32).reshape(36)
         prm = DesignParams(float(penal), SYMMETRY[sym] if sym else -1, float(filter_radius), int(periodic),
                            float(volratio), float(min_rho), float(step_limit), float(damp))
-        self.check(lib().h3d_design_step(self._h, d.ctypes.data_as(_fp), _ptr(rho), _ptr(sens), ctypes.byref(prm)))
+        ne = _extent(self.dims[0])
+        self.check(lib().h3d_design_step(self._h, d.ctypes.data_as(_fp), _ptr(rho, ne, "rho"),
+                                         _ptr(sens, ne, "sensitivity"), ctypes.byref(prm)))
 
     def init_density_trig(self, rho, n_period=10, vol=0.3, sym="reflect6", centered=False, coeff=None, seed=0):
         """the reference's trig-basis initial density (randTri, Framework.cuh:238-310)
@@ -404,7 +430,8 @@ class Homogenization(_Handle):
         if coeff is None:
             coeff = trig_init_coefficients(n_period, seed, centered)
         c = np.ascontiguousarray(coeff, dtype=np.float32)
-        self.check(lib().h3d_init_density_trig(self._h, _ptr(rho), _i3(self.dims[0]), int(n_period),
+        self.check(lib().h3d_init_density_trig(self._h, _ptr(rho, _extent(self.dims[0]), "rho"), _i3(self.dims[0]),
+                                               int(n_period),
                                                c.ctypes.data_as(_fp), c.size, int(centered), float(vol),
                                                SYMMETRY[sym] if sym else -1))
         return c
@@ -412,7 +439,9 @@ class Homogenization(_Handle):
     def conv_radial(self, x, out, radius, periodic=False, adjoint=False):
         """out = rho.conv(radial_convker_t<Spline4>(radius)) of the reference's
         expression layer (or its transpose), on the handle's grid; CUDA tensors"""
-        self.check(lib().h3d_conv_radial(self._h, _ptr(x), _ptr(out), _i3(self.dims[0]), float(radius),
+        ne = _extent(self.dims[0])
+        self.check(lib().h3d_conv_radial(self._h, _ptr(x, ne, "input"), _ptr(out, ne, "output"), _i3(self.dims[0]),
+                                         float(radius),
                                          int(periodic), int(adjoint)))
 
     def warm_start_learned(self, net):
@@ -421,11 +450,13 @@ class Homogenization(_Handle):
 
     def penalize(self, rho, rho_phys, p=3.0):
         """rho_phys = rho^p on the handle's stream (the reference's rho.pow(3))."""
-        self.check(lib().h3d_penalize(self._h, _ptr(rho), _ptr(rho_phys), rho.numel(), float(p)))
+        self.check(lib().h3d_penalize(self._h, _ptr(rho, rho.numel(), "rho"), _ptr(rho_phys, rho.numel(), "rho_phys"),
+                                      rho.numel(), float(p)))
 
     def penalize_backward(self, rho, grad, p=3.0):
         """grad *= p rho^(p-1)."""
-        self.check(lib().h3d_penalize_backward(self._h, _ptr(rho), _ptr(grad), rho.numel(), float(p)))
+        self.check(lib().h3d_penalize_backward(self._h, _ptr(rho, rho.numel(), "rho"),
+                                               _ptr(grad, rho.numel(), "gradient"), rho.numel(), float(p)))
         self.sync()
 
     def field_norms(self, field):
@@ -455,13 +486,16 @@ class OCOptimizer:
 
     def update(self, sens, rho, volratio):
         hd = self._handle()
-        hd.check(lib().h3d_oc_update(hd._h, _ptr(sens), _ptr(rho), self.ne, volratio, self.minRho,
+        hd.check(lib().h3d_oc_update(hd._h, _ptr(sens, self.ne, "sensitivity"), _ptr(rho, self.ne, "rho"), self.ne,
+                                     volratio, self.minRho,
                                      self.step_limit, self.damp))
         hd.sync()
 
     def filterSens(self, sens, rho, pitchT, reso, radius=2.0, periodic=False):
         hd = self._handle()
-        hd.check(lib().h3d_oc_filter(hd._h, _ptr(sens), _ptr(rho), _i3(reso), int(pitchT), radius, int(periodic)))
+        ne = _extent(reso, pitchT)
+        hd.check(lib().h3d_oc_filter(hd._h, _ptr(sens, ne, "sensitivity"), _ptr(rho, ne, "rho"), _i3(reso),
+                                     int(pitchT), radius, int(periodic)))
         hd.sync()
 
 
@@ -493,7 +527,7 @@ class MMAOptimizer:
 
     def setBound(self, xmin, xmax):
         if hasattr(xmin, "data_ptr"):
-            self.check(lib().h3d_mma_set_bounds(self._h, _ptr(xmin), _ptr(xmax)))
+            self.check(lib().h3d_mma_set_bounds(self._h, _ptr(xmin, self.n, "xmin"), _ptr(xmax, self.n, "xmax")))
         else:
             self.check(lib().h3d_mma_set_bounds_scalar(self._h, float(xmin), float(xmax)))
 
@@ -501,10 +535,10 @@ class MMAOptimizer:
         """x is replaced in place by the new design; dgdx is a sequence of m tensors"""
         if len(dgdx) != self.m:
             raise ValueError("dgdx needs one gradient per constraint")
-        ptrs = (ctypes.c_void_p * self.m)(*[_ptr(g).value for g in dgdx])
+        ptrs = (ctypes.c_void_p * self.m)(*[_ptr(g, self.n, "constraint gradient").value for g in dgdx])
         steps = ctypes.c_int(0)
-        self.check(lib().h3d_mma_update(self._h, int(itn), _ptr(x), _ptr(dfdx), _ptr(gval), ptrs,
-                                        ctypes.byref(steps)))
+        self.check(lib().h3d_mma_update(self._h, int(itn), _ptr(x, self.n, "design"), _ptr(dfdx, self.n, "gradient"),
+                                        _ptr(gval, self.m, "constraint values"), ptrs, ctypes.byref(steps)))
         self.newton_steps = steps.value
 
 
@@ -557,17 +591,21 @@ class WarmNet:
         import torch
         b = x.shape[0]
         y = torch.empty((b, self.NOUT, self.reso ** 3), dtype=torch.float32, device=x.device)
-        self.check(lib().h3d_warmnet_forward(self._h, _ptr(x), b, _ptr(y)))
+        self.check(lib().h3d_warmnet_forward(self._h, _ptr(x, b * self.reso ** 3, "input"), b, _ptr(y)))
         return y
 
     def gradients(self, x, t):
         loss = ctypes.c_double()
-        self.check(lib().h3d_warmnet_gradients(self._h, _ptr(x), _ptr(t), x.shape[0], ctypes.byref(loss)))
+        b = x.shape[0]
+        self.check(lib().h3d_warmnet_gradients(self._h, _ptr(x, b * self.reso ** 3, "input"),
+                                               _ptr(t, b * self.NOUT * self.reso ** 3, "target"), b, ctypes.byref(loss)))
         return loss.value
 
     def train_step(self, x, t, lr=1e-3):
         loss = ctypes.c_double()
-        self.check(lib().h3d_warmnet_train_step(self._h, _ptr(x), _ptr(t), x.shape[0], float(lr),
+        b = x.shape[0]
+        self.check(lib().h3d_warmnet_train_step(self._h, _ptr(x, b * self.reso ** 3, "input"),
+                                                _ptr(t, b * self.NOUT * self.reso ** 3, "target"), b, float(lr),
                                                 ctypes.byref(loss)))
         return loss.value
 
@@ -588,7 +626,8 @@ def batch_update(homs, rho_phys):
     concurrently; rho_phys: one contiguous CUDA tensor per design."""
     if len(homs) != len(rho_phys):
         raise ValueError("one density per design")
-    ptrs = (_vp * len(homs))(*[_ptr(r).value for r in rho_phys])
+    ptrs = (_vp * len(homs))(*[_ptr(r, _extent(h.dims[0]), "density of design %d" % i).value
+                               for i, (h, r) in enumerate(zip(homs, rho_phys))])
     code = lib().h3d_batch_update_density(_handle_array(homs), ptrs, len(homs))
     if code != H3D_OK:
         for h in homs:
@@ -619,7 +658,52 @@ def batch_elasticMatrix(homs, tol=1e-2):
     return C.reshape(n, 6, 6)
 
 
+class Lockstep:
+    """Designs solved in lockstep: one launch per V-cycle step over all of them and
+    one captured graph per batch V-cycle (h3d_lockstep_*).  The handles must be
+    H3D_PREC_FP32 designs on one GPU with the same material, stencil precision and
+    coarse mode (resolutions below 512); close the batch before its handles."""
+
+    def __init__(self, homs):
+        self.homs = list(homs)
+        b = _vp()
+        code = lib().h3d_lockstep_create(_handle_array(self.homs), len(self.homs), ctypes.byref(b))
+        if code != H3D_OK:
+            msg = lib().h3d_last_error(self.homs[0]._h).decode() if self.homs else ""
+            raise H3DError(code, msg or "h3d_lockstep_create failed")
+        self._b = b
+
+    def elasticMatrix(self, tol=1e-2):
+        """batch_elasticMatrix over the batch's designs; returns the [n, 6, 6] C and
+        sets each design's last_stats"""
+        n = len(self.homs)
+        C = np.zeros((n, 36))
+        st = (SolveStats * n)()
+        status = np.full(n, -1, dtype=np.int32)
+        code = lib().h3d_lockstep_elastic_matrix(self._b, float(tol), C.ctypes.data_as(_dp), st,
+                                                 status.ctypes.data_as(_ip))
+        if code not in (H3D_OK, H3D_NOT_CONVERGED) and (status == -1).any():
+            raise H3DError(code, lib().h3d_lockstep_last_error(self._b).decode())
+        for i, h in enumerate(self.homs):
+            h.last_stats = st[i].as_dict()
+        for i, h in enumerate(self.homs):
+            if status[i] not in (H3D_OK, H3D_NOT_CONVERGED):
+                raise H3DError(int(status[i]), "design %d: %s" % (i, lib().h3d_last_error(h._h).decode()))
+        return C.reshape(n, 6, 6)
+
+    def close(self):
+        if getattr(self, "_b", None):
+            lib().h3d_lockstep_destroy(self._b)
+            self._b = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
 def symmetrize(handle, field, reso, sym="reflect6"):
     """Orbit-average a lexicographic CUDA field in place (TensorExpression.h:425-445)."""
-    handle.check(lib().h3d_symmetrize(handle._h, _ptr(field), _i3(reso), SYMMETRY[sym]))
+    handle.check(lib().h3d_symmetrize(handle._h, _ptr(field, _extent(reso), "field"), _i3(reso), SYMMETRY[sym]))
     handle.sync()

@@ -331,13 +331,14 @@ int enqueue_vcycle(h3d_handle *h, float w, bool deflate = false) {
 
 // deflation state from the current level-0 f: F = sum of f over the vertices but
 // the origin, pending shift T = 0
-void enqueue_pin_init(h3d_handle *h) {
+void enqueue_pin_init(h3d_handle *h, cudaStream_t s) {
     const Level &L0 = h->lv[0];
     const int nb = norm_blocks(L0.P);
-    launch_mean_partial(L0.P, L0.f, h->partial, nb, h->stream);
-    launch_sum18_finish(h->partial, nb, h->pin_state + 2 * NF, h->stream);
-    launch_pin_init(L0, h->pin_state + 2 * NF, h->pin_state, h->stream);
+    launch_mean_partial(L0.P, L0.f, h->partial, nb, s);
+    launch_sum18_finish(h->partial, nb, h->pin_state + 2 * NF, s);
+    launch_pin_init(L0, h->pin_state + 2 * NF, h->pin_state, s);
 }
+void enqueue_pin_init(h3d_handle *h) { enqueue_pin_init(h, h->stream); }
 
 // the refinement step of the refined solve: fold the correction into the FP64
 // solution (u64 += u + T, u = 0), recompute level-0 f = f0 - K u64 from it, read
@@ -565,7 +566,23 @@ struct SolveRun {
         if (refine)
             if (int e = build_graph(h, exact ? G_REFINE_EXACT : G_REFINE)) return e;
         refine_step = exact ? h->xgraph : h->rgraph;
-        if (int e = weighted_norms(h, L0.P, refine ? h->f0 : L0.f, fn)) return e;
+        {  // the reference norms, read by start() once the stream has drained
+            const float *rhs = refine ? h->f0 : L0.f;
+            const int nb = norm_blocks(L0.P);
+            launch_weighted_norm(L0.P, rhs, h->partial, nb, h->stream);
+            launch_norm_finish(h->partial, nb, h->d_small, h->stream);
+            CKL();
+            CK(cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, h->stream));
+        }
+        return H3D_OK;
+    }
+
+    // the first step, after begin(): a batch begins every design before it starts
+    // any, so the designs' preparations overlap
+    int start() {
+        CK(cudaStreamSynchronize(h->stream));
+        for (int c = 0; c < NCASE; c++) fn[c] = std::sqrt(h->h_small[c]);
+        const Level &L0 = h->lv[0];
         const int nmax = std::max(L0.P.n[0], std::max(L0.P.n[1], L0.P.n[2]));
         theta = std::max(1e-3, 1e-5 * nmax);
         CK(cudaEventRecord(h->ev0, h->stream));
@@ -1093,6 +1110,7 @@ int h3d_v_cycle(h3d_handle *h, float w, int pre, int post) {
 int h3d_solve(h3d_handle *h, int case_mask, double tol, int with_guess, h3d_solve_stats *stats) {
     SolveRun run;
     if (int e = run.begin(h, case_mask, tol, with_guess)) return e;
+    if (int e = run.start()) return e;
     while (!run.finished()) {
         CK(cudaStreamSynchronize(h->stream));
         if (int e = run.advance()) return e;
@@ -1205,6 +1223,14 @@ int h3d_batch_elastic_matrix(h3d_handle *const *hs, int n, double tol, double *C
             if (int e = elastic_prepare(h)) return e;
             return runs[i].begin(h, 63, tol, 1);
         }();
+    }
+    for (int i = 0; i < n; i++) {
+        if (st[i] != H3D_OK) continue;
+        h3d_handle *h = hs[i];
+        st[i] = [&]() -> int {
+            CK(cudaSetDevice(h->device));
+            return runs[i].start();
+        }();
         live[i] = st[i] == H3D_OK;
     }
     // advance whichever design's step has completed; each design's V-cycles and
@@ -1261,6 +1287,368 @@ int h3d_batch_elastic_matrix(h3d_handle *const *hs, int n, double tol, double *C
     }
     return first;
 }
+
+}  // extern "C"
+
+// ---- lockstep batches -------------------------------------------------------
+// The V-cycle of enqueue_vcycle for all designs at once: level index l runs, for
+// the designs that have it, the restriction into l (clearing l's solution), then
+// the down leg's sweep and residual, or the coarsest solve where l is a design's
+// last level; the up leg prolongs and sweeps; then the deflation and the norms.
+// Each design sees its own launches' operations in its own order.
+struct h3d_lockstep {
+    std::vector<h3d_handle *> hs;
+    int n = 0, device = 0, lmax = 0, project = 0;
+    bool f32 = false;
+    KeMat ke;
+    BatchTab fine, norm;
+    BatchTab coarse[MAXLV], xfer[MAXLV], coarsest[MAXLV];
+    cudaStream_t stream = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    cudaEvent_t ev0 = nullptr;
+    int *d_active = nullptr, *h_active = nullptr;
+    double *d_norms = nullptr, *h_norms = nullptr;
+    std::string err;
+};
+
+namespace {
+
+int lfail(h3d_lockstep *b, int code, const std::string &msg) {
+    if (b) b->err = msg;
+    return code;
+}
+
+#define LCK(call)                                                                                    \
+    do {                                                                                             \
+        cudaError_t e_ = (call);                                                                     \
+        if (e_ != cudaSuccess)                                                                       \
+            return lfail(b, e_ == cudaErrorMemoryAllocation ? H3D_ERR_NOMEM : H3D_ERR_CUDA,          \
+                         std::string(#call) + ": " + cudaGetErrorString(e_));                        \
+    } while (0)
+
+void lockstep_free(h3d_lockstep *b) {
+    if (b->device >= 0) cudaSetDevice(b->device);
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    batch_tab_free(b->fine);
+    batch_tab_free(b->norm);
+    for (int l = 0; l < MAXLV; l++) {
+        batch_tab_free(b->coarse[l]);
+        batch_tab_free(b->xfer[l]);
+        batch_tab_free(b->coarsest[l]);
+    }
+    if (b->d_active) cudaFree(b->d_active);
+    if (b->h_active) cudaFreeHost(b->h_active);
+    if (b->d_norms) cudaFree(b->d_norms);
+    if (b->h_norms) cudaFreeHost(b->h_norms);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->stream) cudaStreamDestroy(b->stream);
+}
+
+// the batch V-cycle on b->stream (captured once)
+void lockstep_enqueue(h3d_lockstep *b) {
+    cudaStream_t s = b->stream;
+    cudaMemcpyAsync(b->d_active, b->h_active, sizeof(int) * b->n, cudaMemcpyHostToDevice, s);
+    launch_fine_sweep_batch(b->fine, b->ke, b->d_active, true, s);
+    for (int l = 1; l < b->lmax; l++) {
+        if (b->xfer[l].n) launch_restrict_batch(b->xfer[l], b->d_active, s);
+        if (b->coarse[l].n) launch_coarse_sweep_batch(b->coarse[l], b->f32, b->d_active, true, s);
+        if (b->coarsest[l].n) launch_coarse_apply_batch(b->coarsest[l], b->d_active, b->project, s);
+    }
+    for (int l = b->lmax - 2; l >= 0; l--) {
+        if (!b->xfer[l + 1].n) continue;
+        launch_prolong_batch(b->xfer[l + 1], b->d_active, l == 0, s);
+        if (l == 0) launch_fine_sweep_batch(b->fine, b->ke, b->d_active, false, s);
+        else launch_coarse_sweep_batch(b->coarse[l], b->f32, b->d_active, false, s);
+    }
+    launch_pin_deflate_batch(b->fine, b->ke, b->d_active, s);
+    launch_norm_finish_batch(b->norm, b->d_active, b->d_norms, s);
+    cudaMemcpyAsync(b->h_norms, b->d_norms, sizeof(double) * NCASE * b->n, cudaMemcpyDeviceToHost, s);
+}
+
+int lockstep_build(h3d_lockstep *b) {
+    const int n = b->n;
+    std::vector<const Level *> a, c;
+    std::vector<const float *> rho;
+    std::vector<double *> part, state;
+    std::vector<const double *> aug;
+    std::vector<int> des, nblk;
+    auto tab_rc = [&](int rc, const char *what) -> int {
+        if (rc == 0) return H3D_OK;
+        return lfail(b, rc == -2 ? H3D_ERR_NOMEM : H3D_ERR_ARG, std::string("lockstep table: ") + what);
+    };
+    for (int i = 0; i < n; i++) {
+        h3d_handle *h = b->hs[i];
+        a.push_back(&h->lv[0]);
+        rho.push_back(h->rho);
+        part.push_back(h->partial);
+        state.push_back(h->pin_state);
+        des.push_back(i);
+        nblk.push_back(fine_residual_blocks(h->lv[0]));
+    }
+    if (int e = tab_rc(fine_batch_create(a.data(), rho.data(), part.data(), state.data(), des.data(), n, &b->fine),
+                       "level 0"))
+        return e;
+    if (int e = tab_rc(norm_batch_create(part.data(), nblk.data(), des.data(), n, &b->norm), "norms")) return e;
+    for (int l = 1; l < b->lmax; l++) {
+        std::vector<const Level *> F, Cl, S, Z;
+        std::vector<int> dx, ds, dz;
+        std::vector<const double *> az;
+        for (int i = 0; i < n; i++) {
+            h3d_handle *h = b->hs[i];
+            if (l >= h->nl) continue;
+            F.push_back(&h->lv[l - 1]);
+            Cl.push_back(&h->lv[l]);
+            dx.push_back(i);
+            if (l < h->nl - 1) {
+                S.push_back(&h->lv[l]);
+                ds.push_back(i);
+            } else {
+                Z.push_back(&h->lv[l]);
+                az.push_back(h->aug);
+                dz.push_back(i);
+            }
+        }
+        if (!F.empty())
+            if (int e = tab_rc(transfer_batch_create(F.data(), Cl.data(), dx.data(), (int)F.size(), &b->xfer[l]),
+                               "transfers"))
+                return e;
+        if (!S.empty())
+            if (int e = tab_rc(coarse_batch_create(S.data(), ds.data(), (int)S.size(), &b->coarse[l]), "coarse level"))
+                return e;
+        if (!Z.empty())
+            if (int e = tab_rc(coarsest_batch_create(Z.data(), az.data(), dz.data(), (int)Z.size(), &b->coarsest[l]),
+                               "coarsest level"))
+                return e;
+    }
+    LCK(cudaMalloc(&b->d_active, sizeof(int) * n));
+    LCK(cudaMallocHost(&b->h_active, sizeof(int) * n));
+    LCK(cudaMalloc(&b->d_norms, sizeof(double) * NCASE * n));
+    LCK(cudaMallocHost(&b->h_norms, sizeof(double) * NCASE * n));
+    LCK(cudaMemset(b->d_norms, 0, sizeof(double) * NCASE * n));
+    std::memset(b->h_norms, 0, sizeof(double) * NCASE * n);
+    for (int i = 0; i < n; i++) b->h_active[i] = 1;
+    LCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    LCK(cudaEventCreate(&b->ev0));
+    cudaGraph_t g = nullptr;
+    LCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    lockstep_enqueue(b);
+    LCK(cudaStreamEndCapture(b->stream, &g));
+    const cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e != cudaSuccess) {
+        b->graph = nullptr;
+        return lfail(b, H3D_ERR_CUDA, std::string("lockstep graph: ") + cudaGetErrorString(e));
+    }
+    return H3D_OK;
+}
+
+// one design of a lockstep solve: SolveRun's FP32 branch with the stale residual
+// norms of each cycle read from the batch's host mirror, its other launches on
+// the batch stream
+struct LockRun {
+    h3d_handle *h = nullptr;
+    int it = 0, status = H3D_OK, explode_left = 2, maxit = 200;
+    double tol = 1e-2, theta = 1e-3;
+    double fn[6] = {}, rel[6] = {1, 1, 1, 1, 1, 1};
+    bool live = false;
+
+    // before the first batch cycle, on the design's stream: balanced right-hand
+    // side, reference norms (to the host mirror), deflation state (SolveRun::begin
+    // with a guess, FP32 mode); read_begin takes the norms once the stream drained
+    int begin(h3d_handle *hh, double tolerance) {
+        h = hh;
+        tol = tolerance;
+        const Level &L0 = h->lv[0];
+        const int nb = norm_blocks(L0.P);
+        launch_mean_partial(L0.P, L0.f, h->partial, nb, h->stream);
+        launch_remove_mean(L0.P, L0.f, h->partial, nb, h->stream);
+        launch_weighted_norm(L0.P, L0.f, h->partial, nb, h->stream);
+        launch_norm_finish(h->partial, nb, h->d_small, h->stream);
+        CKL();
+        CK(cudaMemcpyAsync(h->h_small, h->d_small, sizeof(double) * NCASE, cudaMemcpyDeviceToHost, h->stream));
+        CK(cudaMemsetAsync(h->pin_state + NF, 0, sizeof(double) * NF, h->stream));
+        enqueue_pin_init(h);
+        CKL();
+        return H3D_OK;
+    }
+    void read_begin() {
+        for (int c = 0; c < NCASE; c++) fn[c] = std::sqrt(h->h_small[c]);
+        const Level &L0 = h->lv[0];
+        const int nmax = std::max(L0.P.n[0], std::max(L0.P.n[1], L0.P.n[2]));
+        theta = std::max(1e-3, 1e-5 * nmax);
+        live = true;
+    }
+    int finish(int st, cudaStream_t s) {
+        status = st;
+        launch_pin_fold(h->lv[0], h->rho, h->ke, h->pin_state, s);
+        CK(cudaEventRecord(h->ev1, s));
+        live = false;
+        return H3D_OK;
+    }
+    // after a batch cycle; norms: this design's six stale residual norms squared
+    int advance(const double *norms, cudaStream_t s) {
+        it++;
+        bool bad = false, done = true;
+        for (int c = 0; c < NCASE; c++) {
+            rel[c] = std::sqrt(norms[c]) / (fn[c] + 1e-10);
+            if (!(rel[c] <= 10.0)) bad = true;
+            if (!(rel[c] <= tol)) done = false;
+        }
+        if (bad) {  // MG.cpp:140-182: restart from zero once, then give up
+            if (--explode_left <= 0) return finish(H3D_DIVERGED, s);
+            launch_pin_fold(h->lv[0], h->rho, h->ke, h->pin_state, s);  // restores f
+            CK(cudaMemsetAsync(h->lv[0].u, 0, sizeof(float) * field_floats(h->lv[0].P.nv), s));
+            CK(cudaMemsetAsync(h->pin_state + NF, 0, sizeof(double) * NF, s));
+            enqueue_pin_init(h, s);
+            CKL();
+        } else if (done) {
+            return finish(H3D_OK, s);
+        }
+        if (it >= maxit) return finish(H3D_NOT_CONVERGED, s);
+        return H3D_OK;
+    }
+};
+
+}  // namespace
+
+extern "C" {
+
+int h3d_lockstep_create(h3d_handle *const *hs, int n, h3d_lockstep **out) {
+    if (!out) return H3D_ERR_ARG;
+    *out = nullptr;
+    if (!hs || n < 1 || n > H3D_LOCKSTEP_MAX) return H3D_ERR_ARG;
+    for (int i = 0; i < n; i++)
+        if (!hs[i]) return H3D_ERR_ARG;
+    if (int e = distinct_handles(hs, n)) return e;
+    h3d_handle *h0 = hs[0];
+    for (int i = 0; i < n; i++) {
+        h3d_handle *h = hs[i];
+        if (h->device != h0->device) return fail(h0, H3D_ERR_ARG, "lockstep: handles on different devices");
+        if (h->cfg.precision != H3D_PREC_FP32) return fail(h0, H3D_ERR_ARG, "lockstep: needs H3D_PREC_FP32 handles");
+        if (std::memcmp(h->ke.k, h0->ke.k, sizeof(h->ke.k)) != 0)
+            return fail(h0, H3D_ERR_ARG, "lockstep: handles with different materials");
+        if (h->cfg.stencil_precision != h0->cfg.stencil_precision || h->cfg.coarse_mode != h0->cfg.coarse_mode)
+            return fail(h0, H3D_ERR_ARG, "lockstep: different stencil precision or coarse mode");
+        for (int l = 1; l < h->nl; l++)
+            if (h->lv[l].ratio[0] != 2 || h->lv[l].ratio[1] != 2 || h->lv[l].ratio[2] != 2 || !h->lv[l - 1].P.even)
+                return fail(h0, H3D_ERR_ARG, "lockstep: needs ratio-2 coarsening of even levels");
+    }
+    h3d_lockstep *b = new (std::nothrow) h3d_lockstep();
+    if (!b) return H3D_ERR_NOMEM;
+    b->hs.assign(hs, hs + n);
+    b->n = n;
+    b->device = h0->device;
+    b->ke = h0->ke;
+    b->f32 = h0->cfg.stencil_precision == H3D_STENCIL_FP32;
+    b->project = h0->cfg.coarse_mode == H3D_COARSE_PROJECT;
+    for (int i = 0; i < n; i++) b->lmax = std::max(b->lmax, hs[i]->nl);
+    if (cudaSetDevice(b->device) != cudaSuccess) {
+        delete b;
+        return fail(h0, H3D_ERR_CUDA, "cudaSetDevice failed");
+    }
+    if (int e = lockstep_build(b)) {
+        fail(h0, e, b->err);
+        lockstep_free(b);
+        delete b;
+        return e;
+    }
+    *out = b;
+    return H3D_OK;
+}
+
+int h3d_lockstep_destroy(h3d_lockstep *b) {
+    if (!b) return H3D_ERR_ARG;
+    lockstep_free(b);
+    delete b;
+    return H3D_OK;
+}
+
+const char *h3d_lockstep_last_error(const h3d_lockstep *b) { return b ? b->err.c_str() : "null lockstep batch"; }
+
+int h3d_lockstep_elastic_matrix(h3d_lockstep *b, double tol, double *C, h3d_solve_stats *stats, int *status) {
+    if (!b || !C) return H3D_ERR_ARG;
+    LCK(cudaSetDevice(b->device));
+    const int n = b->n;
+    std::vector<LockRun> runs(n);
+    std::vector<int> st(n, H3D_OK);
+    for (int i = 0; i < n; i++) {
+        h3d_handle *h = b->hs[i];
+        if (!h->have_stencils) {
+            st[i] = fail(h, H3D_ERR_STATE, "no stencils");
+            continue;
+        }
+        st[i] = elastic_prepare(h);
+        if (st[i] == H3D_OK) st[i] = runs[i].begin(h, tol);
+    }
+    // the designs' own streams hold their preparation: drain them before the
+    // batch stream takes over
+    for (int i = 0; i < n; i++) {
+        if (cudaStreamSynchronize(b->hs[i]->stream) != cudaSuccess && st[i] == H3D_OK)
+            st[i] = fail(b->hs[i], H3D_ERR_CUDA, "stream synchronisation failed");
+        if (st[i] == H3D_OK) runs[i].read_begin();
+        else runs[i].live = false;
+    }
+    LCK(cudaEventRecord(b->ev0, b->stream));
+    for (int i = 0; i < n; i++)
+        if (runs[i].live) LCK(cudaEventRecord(b->hs[i]->ev0, b->stream));
+    for (;;) {
+        int nlive = 0;
+        for (int i = 0; i < n; i++) {
+            b->h_active[i] = runs[i].live ? 1 : 0;
+            nlive += b->h_active[i];
+        }
+        if (!nlive) break;
+        LCK(cudaGraphLaunch(b->graph, b->stream));
+        LCK(cudaStreamSynchronize(b->stream));
+        for (int i = 0; i < n; i++) {
+            if (!b->h_active[i]) continue;
+            const int e = runs[i].advance(b->h_norms + NCASE * i, b->stream);
+            if (e != H3D_OK) {
+                st[i] = e;
+                runs[i].live = false;
+            }
+        }
+    }
+    LCK(cudaStreamSynchronize(b->stream));
+    for (int i = 0; i < n; i++) {
+        h3d_handle *h = b->hs[i];
+        if (st[i] != H3D_OK) continue;
+        if (stats) {
+            h3d_solve_stats &s1 = stats[i];
+            s1.vcycles = runs[i].it;
+            s1.refinements = 0;
+            s1.status = runs[i].status;
+            for (int c = 0; c < NCASE; c++) s1.rel_res[c] = runs[i].rel[c];
+            float ms = 0;
+            cudaEventElapsedTime(&ms, h->ev0, h->ev1);
+            s1.solve_ms = ms;
+        }
+        st[i] = runs[i].status;
+        if (st[i] != H3D_OK && st[i] != H3D_NOT_CONVERGED) {
+            fail(h, st[i], "multigrid diverged");
+            continue;
+        }
+        if (int e = elastic_enqueue_energy(h)) st[i] = e;
+    }
+    int first = H3D_OK;
+    for (int i = 0; i < n; i++) {
+        h3d_handle *h = b->hs[i];
+        if (st[i] == H3D_OK || st[i] == H3D_NOT_CONVERGED) {
+            if (cudaStreamSynchronize(h->stream) != cudaSuccess) st[i] = fail(h, H3D_ERR_CUDA, "stream synchronisation failed");
+            else if (int e = elastic_read(h, C + 36 * (size_t)i)) st[i] = e;
+        }
+        if (status) status[i] = st[i];
+        if (st[i] != H3D_OK && first == H3D_OK) {
+            first = st[i];
+            b->err = h->err;
+        }
+    }
+    return first;
+}
+
+}  // extern "C"
+
+extern "C" {
 
 int h3d_sensitivity(h3d_handle *h, const float dC[36], float *sens_dev, int pitchT) {
     if (!h || !dC || !sens_dev) return H3D_ERR_ARG;

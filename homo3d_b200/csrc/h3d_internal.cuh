@@ -129,6 +129,50 @@ __device__ __forceinline__ int color_of_index(const Planes &P, long long v) {
 }
 #endif
 
+// ---- lockstep batches of designs (h3d_batch_*): one launch per step over a level
+// of several designs.  Design slot i of a batched launch owns its CTAs
+// [start[i], start[i+1]); tables live in device memory, built once per batch.
+constexpr int BATCH_MAX = 64;  // designs per batch
+struct BatchSlices {
+    int n;
+    unsigned start[BATCH_MAX + 1];
+};
+#ifdef __CUDACC__
+// the slot whose slice holds CTA b (the last slot starting at or before b, so
+// empty slices are skipped)
+__device__ __forceinline__ int batch_slice(const BatchSlices &s, unsigned b) {
+    int lo = 0, hi = __ldg(&s.n) - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(&s.start[mid]) <= b) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+// a design's launch arguments copied to shared memory by the CTA (argument structs
+// with default member initialisers cannot be __shared__ objects themselves); every
+// thread of the CTA must call it
+template <typename T>
+__device__ __forceinline__ const T &stage_args(const T &src, unsigned *buf) {
+    static_assert(sizeof(T) % 4 == 0, "copied as 32-bit words");
+    const unsigned *w = reinterpret_cast<const unsigned *>(&src);
+    for (int i = threadIdx.x; i < (int)(sizeof(T) / 4); i += blockDim.x) buf[i] = __ldg(w + i);
+    __syncthreads();
+    return *reinterpret_cast<const T *>(buf);
+}
+#endif
+// host view of one device table: its address, slot count and launch sizes
+struct BatchTab {
+    void *dev = nullptr;
+    int n = 0;
+    unsigned grid[4] = {0, 0, 0, 0};
+    size_t smem = 0;
+};
+inline void batch_tab_free(BatchTab &t) {
+    if (t.dev) cudaFree(t.dev);
+    t = BatchTab();
+}
+
 struct KeMat { float k[576]; };        // element matrix, row-major, FP32
 struct KeMat64 { double k[576]; };     // the same in FP64 (exact refinement residual)
 struct RhsTab { float g[NCASE][24]; }; // Ke * chi0_c for the six unit strains
@@ -320,6 +364,32 @@ int warmnet_device(const h3d_warmnet *n);
 int warmnet_forward_on(h3d_warmnet *n, const float *x, cudaStream_t s, const float **y);
 void launch_warmnet_density_pool(const float *rho, int N, int R, float *out, cudaStream_t s);
 void launch_warmnet_to_chi(const Planes &P, const float *y, int R, double *chi, cudaStream_t s);
+// lockstep batches (k_fine.cu, k_coarse.cu, k_galerkin.cu).  The create functions
+// copy a table to the device (not inside a stream capture) and return 0, -1 for a
+// slot count outside 1..BATCH_MAX, -2 if the device table cannot be allocated.
+// design[i]: slot i's index in the `active` flags the launches read.
+// level 0 of each design: the sweep (shape 0), the seven-colour residual and the
+// deflation (state: the design's deflation state)
+int fine_batch_create(const Level *const *lv0, const float *const *rho, double *const *partial,
+                      double *const *state, const int *design, int n, BatchTab *out);
+void launch_fine_sweep_batch(const BatchTab &t, const KeMat &ke, const int *active, bool residual, cudaStream_t s);
+void launch_pin_deflate_batch(const BatchTab &t, const KeMat &ke, const int *active, cudaStream_t s);
+// one coarse level of each design (all with the same stencil precision): the
+// sweep (shape 0), with residual the down leg's sweep and residual
+int coarse_batch_create(const Level *const *lv, const int *design, int n, BatchTab *out);
+void launch_coarse_sweep_batch(const BatchTab &t, bool f32, const int *active, bool residual, cudaStream_t s);
+// ratio-2 transfers between levels F[i] (even) and C[i]: restriction of F.r into
+// C.f with C.u cleared, prolongation of C.u into F.u (is_root: F is level 0)
+int transfer_batch_create(const Level *const *F, const Level *const *C, const int *design, int n, BatchTab *out);
+void launch_restrict_batch(const BatchTab &t, const int *active, cudaStream_t s);
+void launch_prolong_batch(const BatchTab &t, const int *active, int is_root, cudaStream_t s);
+// the per-case norms of each design from its nblk[i] partials into out + 6 * design[i]
+// (the same two-stage order as launch_norm_finish above NORM_FINISH_DIRECT blocks)
+int norm_batch_create(double *const *partial, const int *nblk, const int *design, int n, BatchTab *out);
+void launch_norm_finish_batch(const BatchTab &t, const int *active, double *out, cudaStream_t s);
+// the coarsest solve of each design (aug[i]: its [K | K^-1])
+int coarsest_batch_create(const Level *const *lv, const double *const *aug, const int *design, int n, BatchTab *out);
+void launch_coarse_apply_batch(const BatchTab &t, const int *active, int project, cudaStream_t s);
 // field conversion (k_coarse.cu)
 void launch_field_to_lex(const Planes &P, const float *src, float *dst_lex, cudaStream_t s);
 void launch_field_from_lex(const Planes &P, const float *src_lex, float *dst, cudaStream_t s);

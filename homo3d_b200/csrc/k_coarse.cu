@@ -135,19 +135,21 @@ __device__ __forceinline__ void coarse_apply(const CoarseArgs &a, long long me, 
 // thread -> (vertex p, first load case cb) for C cases per thread: the NCASE / C
 // CTAs of a case group cover the same 128 vertices with different load cases
 template <int C>
-__device__ __forceinline__ void coarse_task(long long &p, int &cb) {
+__device__ __forceinline__ void coarse_task(long long &p, int &cb, unsigned bid) {
     constexpr int NG = NCASE / C;
-    cb = (int)(blockIdx.x % NG) * C;
-    p = (long long)(blockIdx.x / NG) * blockDim.x + threadIdx.x;
+    cb = (int)(bid % NG) * C;
+    p = (long long)(bid / NG) * blockDim.x + threadIdx.x;
 }
 
 // RES (the last colour of a sweep, whose neighbours are final) also writes the
-// residual of the updated vertex: r = f - acc - A_0 u with acc the neighbour sum
-template <int K, bool F32, int CGS_CPT, int CGS_MINB, bool RES = false>
-__global__ void __launch_bounds__(128, CGS_MINB) k_coarse_gs(CoarseArgs a) {
+// residual of the updated vertex: r = f - acc - A_0 u with acc the neighbour sum.
+// bid: the CTA's index in the design's launch (blockIdx.x, or its slice of a
+// batched launch)
+template <int K, bool F32, int CGS_CPT, bool RES>
+__device__ __forceinline__ void coarse_gs_block(const CoarseArgs &a, unsigned bid) {
     long long p;
     int cb;
-    coarse_task<CGS_CPT>(p, cb);
+    coarse_task<CGS_CPT>(p, cb, bid);
     if (p >= a.P) return;
     const long long me = (long long)K * a.P + p;
     int i, j, l;
@@ -176,6 +178,11 @@ __global__ void __launch_bounds__(128, CGS_MINB) k_coarse_gs(CoarseArgs a) {
     }
 }
 
+template <int K, bool F32, int CGS_CPT, int CGS_MINB, bool RES = false>
+__global__ void __launch_bounds__(128, CGS_MINB) k_coarse_gs(CoarseArgs a) {
+    coarse_gs_block<K, F32, CGS_CPT, RES>(a, blockIdx.x);
+}
+
 template <bool F32, int CRES_CPT>
 __device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long p, int cb, int K) {
     const long long me = (long long)K * a.P + p;
@@ -194,15 +201,20 @@ __device__ __forceinline__ void coarse_res_vertex(const CoarseArgs &a, long long
 // its own residual), the colour the block index modulo NCOL and a run-time value
 // of one code body: the CTAs of one vertex block read each other's neighbour rows
 // while they are in L2, and a small level costs one launch instead of eight
-template <bool F32, int CRES_CPT, int CRES_MINB, unsigned NCOL>
-__global__ void __launch_bounds__(128, CRES_MINB) k_coarse_residual(CoarseArgs a) {
+template <bool F32, int CRES_CPT, unsigned NCOL>
+__device__ __forceinline__ void coarse_residual_block(const CoarseArgs &a, unsigned bid) {
     constexpr int NG = NCASE / CRES_CPT;
-    const int K = (int)(blockIdx.x % NCOL);
-    const unsigned bx = blockIdx.x / NCOL;
+    const int K = (int)(bid % NCOL);
+    const unsigned bx = bid / NCOL;
     const int cb = (int)(bx % NG) * CRES_CPT;
     const long long p = (long long)(bx / NG) * blockDim.x + threadIdx.x;
     if (p >= a.P) return;
     coarse_res_vertex<F32, CRES_CPT>(a, p, cb, K);
+}
+
+template <bool F32, int CRES_CPT, int CRES_MINB, unsigned NCOL>
+__global__ void __launch_bounds__(128, CRES_MINB) k_coarse_residual(CoarseArgs a) {
+    coarse_residual_block<F32, CRES_CPT, NCOL>(a, blockIdx.x);
 }
 
 static CoarseArgs make_cargs(const Level &L) {
@@ -383,11 +395,11 @@ __global__ void __launch_bounds__(256) k_prolong(Planes F, Planes C, int r0, int
 // of each colour plane.  Fine vertex 2X + o has the colour of o's parities and, in
 // that colour's plane, the coordinates X - [o < 0] (wrapped) per axis; the sums
 // run in the general kernel's order, so the results are identical.
-__global__ void __launch_bounds__(256) k_restrict2(Planes F, Planes C, FastDiv dn0, FastDiv dn1,
-                                                   const float *__restrict__ rf, float *fc) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+// thread t of case c; uc (or nullptr): the coarse solution, cleared at the vertex
+__device__ __forceinline__ void restrict2_thread(const Planes &F, const Planes &C, const FastDiv &dn0,
+                                                 const FastDiv &dn1, const float *__restrict__ rf, float *fc,
+                                                 float *uc, long long t, int c) {
     if (t >= C.nv) return;
-    const int c = blockIdx.y;
     const unsigned q = (unsigned)t, tq = dn0.div(q), zq = dn1.div(tq);
     const int x = (int)(q - tq * (unsigned)C.n[0]), y = (int)(tq - zq * (unsigned)C.n[1]), z = (int)zq;
     const int xm = x == 0 ? C.n[0] - 1 : x - 1, ym = y == 0 ? C.n[1] - 1 : y - 1, zm = z == 0 ? C.n[2] - 1 : z - 1;
@@ -408,18 +420,30 @@ __global__ void __launch_bounds__(256) k_restrict2(Planes F, Planes C, FastDiv d
                 a1 = fmaf(__ldg(&src[FVB]), w, a1);
                 a2 = fmaf(__ldg(&src[2 * FVB]), w, a2);
             }
-    float *dst = fc + fidx(3 * c, vidx(C, x, y, z));
+    const long long cv = vidx(C, x, y, z);
+    float *dst = fc + fidx(3 * c, cv);
     dst[0] = a0;
     dst[FVB] = a1;
     dst[2 * FVB] = a2;
+    if (uc) {
+        float *z0 = uc + fidx(3 * c, cv);
+        z0[0] = 0.f;
+        z0[FVB] = 0.f;
+        z0[2 * FVB] = 0.f;
+    }
+}
+
+__global__ void __launch_bounds__(256) k_restrict2(Planes F, Planes C, FastDiv dn0, FastDiv dn1,
+                                                   const float *__restrict__ rf, float *fc) {
+    restrict2_thread(F, C, dn0, dn1, rf, fc, nullptr, blockIdx.x * (long long)blockDim.x + threadIdx.x, blockIdx.y);
 }
 
 // Ratio 2: one thread per coarse cell X; its eight fine vertices 2X + e take
 // their corrections from the cell's eight corners, read once per plane.  Fine
 // vertex 2X + e sits at index X (lexicographic) of colour plane k(e).
-__global__ void __launch_bounds__(256) k_prolong2(Planes F, Planes C, FastDiv dn0, FastDiv dn1, int is_root,
-                                                  const float *__restrict__ uc, float *uf) {
-    const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+__device__ __forceinline__ void prolong2_thread(const Planes &F, const Planes &C, const FastDiv &dn0,
+                                                const FastDiv &dn1, int is_root, const float *__restrict__ uc,
+                                                float *uf, long long t) {
     if (t >= C.nv) return;
     const unsigned q = (unsigned)t, tq = dn0.div(q), zq = dn1.div(tq);
     const int x = (int)(q - tq * (unsigned)C.n[0]), y = (int)(tq - zq * (unsigned)C.n[1]), z = (int)zq;
@@ -461,6 +485,11 @@ __global__ void __launch_bounds__(256) k_prolong2(Planes F, Planes C, FastDiv dn
             uf[fidx(pl, k * cpl + t)] = fv[e] + acc;
         }
     }
+}
+
+__global__ void __launch_bounds__(256) k_prolong2(Planes F, Planes C, FastDiv dn0, FastDiv dn1, int is_root,
+                                                  const float *__restrict__ uc, float *uf) {
+    prolong2_thread(F, C, dn0, dn1, is_root, uc, uf, blockIdx.x * (long long)blockDim.x + threadIdx.x);
 }
 
 static bool ratio2(const Level &C) { return C.ratio[0] == 2 && C.ratio[1] == 2 && C.ratio[2] == 2; }
@@ -518,7 +547,7 @@ void launch_weighted_norm(const Planes &P, const float *v, double *partial, int 
 }
 
 template <int N>
-__global__ void __launch_bounds__(256) k_finish(const double *__restrict__ partial, int nblk, double *out) {
+__device__ __forceinline__ void finish_block(const double *__restrict__ partial, int nblk, double *out) {
     double s[N];
 #pragma unroll
     for (int c = 0; c < N; ++c) s[c] = 0;
@@ -528,19 +557,30 @@ __global__ void __launch_bounds__(256) k_finish(const double *__restrict__ parti
     block_reduce<N>(s, out, 0);
 }
 
+template <int N>
+__global__ void __launch_bounds__(256) k_finish(const double *__restrict__ partial, int nblk, double *out) {
+    finish_block<N>(partial, nblk, out);
+}
+
 // first stage of a long reduction: CTA g sums the partials of blocks
 // [g*per, (g+1)*per) into out[g*N + c]
 template <int N>
-__global__ void __launch_bounds__(256) k_finish_chunks(const double *__restrict__ partial, int nblk, int per,
-                                                       double *out) {
-    const int b0 = blockIdx.x * per, b1 = min(nblk, b0 + per);
+__device__ __forceinline__ void finish_chunk_block(const double *__restrict__ partial, int nblk, int per,
+                                                   double *out, int g) {
+    const int b0 = g * per, b1 = min(nblk, b0 + per);
     double s[N];
 #pragma unroll
     for (int c = 0; c < N; ++c) s[c] = 0;
     for (int b = b0 + threadIdx.x; b < b1; b += blockDim.x)
 #pragma unroll
         for (int c = 0; c < N; ++c) s[c] += partial[(long long)b * N + c];
-    block_reduce<N>(s, out, blockIdx.x);
+    block_reduce<N>(s, out, g);
+}
+
+template <int N>
+__global__ void __launch_bounds__(256) k_finish_chunks(const double *__restrict__ partial, int nblk, int per,
+                                                       double *out) {
+    finish_chunk_block<N>(partial, nblk, per, out, blockIdx.x);
 }
 
 void launch_norm_finish(const double *partial, int nblk, double *out6, cudaStream_t s) {
@@ -968,6 +1008,226 @@ bool vcycle_bottom_fits(const Level *lv, int first, int nl) {
         if (l < nl - 1 && !lv[l].P.even) return false;
     }
     return true;
+}
+
+// ---- lockstep batches: a level (or a transfer) of several designs per launch ----
+// Each design's CTAs run the body of its own launch with the CTA index inside its
+// slice (BatchSlices), on its arguments staged in shared memory, so the results
+// are those of the design's own launches to the last bit; designs whose flag in
+// `active` is 0 return at once.  Sweeps and residuals in launch shape 0 (two cases
+// per thread, 6 CTAs/SM).
+constexpr int BATCH_CPT = 2, BATCH_MINB = 6;
+
+struct CoarseEnt {
+    CoarseArgs a;
+    int design;
+};
+struct CoarseBatchTab {
+    BatchSlices gs;   // CTAs of one colour of the sweep
+    BatchSlices res;  // CTAs of the seven-colour residual
+    CoarseEnt e[BATCH_MAX];
+};
+
+template <int K, bool F32, bool RES>
+__global__ void __launch_bounds__(128, BATCH_MINB) k_coarse_gs_batch(const CoarseBatchTab *__restrict__ t,
+                                                                   const int *__restrict__ active) {
+    __shared__ __align__(16) unsigned buf[sizeof(CoarseArgs) / 4];
+    const int i = batch_slice(t->gs, blockIdx.x);
+    const CoarseEnt &en = t->e[i];
+    if (!__ldg(&active[en.design])) return;
+    const CoarseArgs &a = stage_args(en.a, buf);
+    coarse_gs_block<K, F32, BATCH_CPT, RES>(a, blockIdx.x - __ldg(&t->gs.start[i]));
+}
+
+template <bool F32>
+__global__ void __launch_bounds__(128, BATCH_MINB) k_coarse_residual_batch(const CoarseBatchTab *__restrict__ t,
+                                                                         const int *__restrict__ active) {
+    __shared__ __align__(16) unsigned buf[sizeof(CoarseArgs) / 4];
+    const int i = batch_slice(t->res, blockIdx.x);
+    const CoarseEnt &en = t->e[i];
+    if (!__ldg(&active[en.design])) return;
+    const CoarseArgs &a = stage_args(en.a, buf);
+    coarse_residual_block<F32, BATCH_CPT, 7>(a, blockIdx.x - __ldg(&t->res.start[i]));
+}
+
+template <typename Tab>
+static int upload_tab(const Tab &t, int n, BatchTab *out) {
+    void *d = nullptr;
+    if (cudaMalloc(&d, sizeof(Tab)) != cudaSuccess) return -2;
+    if (cudaMemcpy(d, &t, sizeof(Tab), cudaMemcpyHostToDevice) != cudaSuccess) {
+        cudaFree(d);
+        return -2;
+    }
+    out->dev = d;
+    out->n = n;
+    return 0;
+}
+
+int coarse_batch_create(const Level *const *lv, const int *design, int n, BatchTab *out) {
+    if (n < 1 || n > BATCH_MAX) return -1;
+    CoarseBatchTab *t = new CoarseBatchTab();
+    t->gs.n = t->res.n = n;
+    t->gs.start[0] = t->res.start[0] = 0;
+    for (int i = 0; i < n; i++) {
+        t->e[i].a = make_cargs(*lv[i]);
+        t->e[i].design = design[i];
+        const unsigned nb = (unsigned)((t->e[i].a.P + 127) / 128) * (NCASE / BATCH_CPT);
+        t->gs.start[i + 1] = t->gs.start[i] + nb;
+        t->res.start[i + 1] = t->res.start[i] + nb * 7;
+    }
+    const int rc = upload_tab(*t, n, out);
+    if (rc == 0) {
+        out->grid[0] = t->gs.start[n];
+        out->grid[1] = t->res.start[n];
+    }
+    delete t;
+    return rc;
+}
+
+template <bool F32>
+static void coarse_sweep_batch(const BatchTab &t, const int *active, bool residual, cudaStream_t s) {
+    const CoarseBatchTab *d = static_cast<const CoarseBatchTab *>(t.dev);
+    const unsigned g = t.grid[0];
+    k_coarse_gs_batch<0, F32, false><<<g, 128, 0, s>>>(d, active);
+    k_coarse_gs_batch<1, F32, false><<<g, 128, 0, s>>>(d, active);
+    k_coarse_gs_batch<2, F32, false><<<g, 128, 0, s>>>(d, active);
+    k_coarse_gs_batch<3, F32, false><<<g, 128, 0, s>>>(d, active);
+    k_coarse_gs_batch<4, F32, false><<<g, 128, 0, s>>>(d, active);
+    k_coarse_gs_batch<5, F32, false><<<g, 128, 0, s>>>(d, active);
+    k_coarse_gs_batch<6, F32, false><<<g, 128, 0, s>>>(d, active);
+    if (residual) {
+        k_coarse_gs_batch<7, F32, true><<<g, 128, 0, s>>>(d, active);
+        k_coarse_residual_batch<F32><<<t.grid[1], 128, 0, s>>>(d, active);
+    } else {
+        k_coarse_gs_batch<7, F32, false><<<g, 128, 0, s>>>(d, active);
+    }
+}
+
+void launch_coarse_sweep_batch(const BatchTab &t, bool f32, const int *active, bool residual, cudaStream_t s) {
+    if (f32) coarse_sweep_batch<true>(t, active, residual, s);
+    else coarse_sweep_batch<false>(t, active, residual, s);
+}
+
+// ratio-2 transfers: one slice of ceil(C.nv / 256) CTAs per design for both
+struct TransferEnt {
+    Planes F, C;
+    FastDiv dn0, dn1;   // division by C.n[0], C.n[1]
+    const float *rf;    // F.r
+    float *fc, *uc;     // C.f, C.u
+    float *uf;          // F.u
+    int design;
+    int pad;
+};
+struct TransferBatchTab {
+    BatchSlices sl;
+    TransferEnt e[BATCH_MAX];
+};
+
+__global__ void __launch_bounds__(256) k_restrict_batch(const TransferBatchTab *__restrict__ t,
+                                                        const int *__restrict__ active) {
+    __shared__ __align__(16) unsigned buf[sizeof(TransferEnt) / 4];
+    const int i = batch_slice(t->sl, blockIdx.x);
+    if (!__ldg(&active[t->e[i].design])) return;
+    const TransferEnt &e = stage_args(t->e[i], buf);
+    const long long tt = (long long)(blockIdx.x - __ldg(&t->sl.start[i])) * blockDim.x + threadIdx.x;
+    restrict2_thread(e.F, e.C, e.dn0, e.dn1, e.rf, e.fc, e.uc, tt, blockIdx.y);
+}
+
+__global__ void __launch_bounds__(256) k_prolong_batch(const TransferBatchTab *__restrict__ t,
+                                                       const int *__restrict__ active, int is_root) {
+    __shared__ __align__(16) unsigned buf[sizeof(TransferEnt) / 4];
+    const int i = batch_slice(t->sl, blockIdx.x);
+    if (!__ldg(&active[t->e[i].design])) return;
+    const TransferEnt &e = stage_args(t->e[i], buf);
+    const long long tt = (long long)(blockIdx.x - __ldg(&t->sl.start[i])) * blockDim.x + threadIdx.x;
+    prolong2_thread(e.F, e.C, e.dn0, e.dn1, is_root, e.uc, e.uf, tt);
+}
+
+int transfer_batch_create(const Level *const *F, const Level *const *C, const int *design, int n, BatchTab *out) {
+    if (n < 1 || n > BATCH_MAX) return -1;
+    TransferBatchTab *t = new TransferBatchTab();
+    t->sl.n = n;
+    t->sl.start[0] = 0;
+    for (int i = 0; i < n; i++) {
+        TransferEnt &e = t->e[i];
+        e.F = F[i]->P;
+        e.C = C[i]->P;
+        e.dn0 = FastDiv((unsigned)C[i]->P.n[0]);
+        e.dn1 = FastDiv((unsigned)C[i]->P.n[1]);
+        e.rf = F[i]->r;
+        e.fc = C[i]->f;
+        e.uc = C[i]->u;
+        e.uf = F[i]->u;
+        e.design = design[i];
+        t->sl.start[i + 1] = t->sl.start[i] + (unsigned)((C[i]->P.nv + 255) / 256);
+    }
+    const int rc = upload_tab(*t, n, out);
+    if (rc == 0) out->grid[0] = t->sl.start[n];
+    delete t;
+    return rc;
+}
+
+void launch_restrict_batch(const BatchTab &t, const int *active, cudaStream_t s) {
+    k_restrict_batch<<<dim3(t.grid[0], NCASE), 256, 0, s>>>(static_cast<const TransferBatchTab *>(t.dev), active);
+}
+
+void launch_prolong_batch(const BatchTab &t, const int *active, int is_root, cudaStream_t s) {
+    k_prolong_batch<<<t.grid[0], 256, 0, s>>>(static_cast<const TransferBatchTab *>(t.dev), active, is_root);
+}
+
+// per-case norms: the first stage (NORM_FINISH_CHUNKS CTAs) for designs above
+// NORM_FINISH_DIRECT partials, then one CTA per design
+struct NormEnt {
+    const double *partial;
+    double *mid;  // the first stage's sums behind the partials (two-stage designs)
+    int nblk, per, two, design;
+};
+struct NormBatchTab {
+    BatchSlices chunks;  // first-stage CTAs (none for one-stage designs)
+    NormEnt e[BATCH_MAX];
+};
+
+__global__ void __launch_bounds__(256) k_finish_chunks_batch(const NormBatchTab *__restrict__ t,
+                                                             const int *__restrict__ active) {
+    const int i = batch_slice(t->chunks, blockIdx.x);
+    const NormEnt &e = t->e[i];
+    if (!__ldg(&active[e.design])) return;
+    finish_chunk_block<NCASE>(e.partial, e.nblk, e.per, e.mid, (int)(blockIdx.x - __ldg(&t->chunks.start[i])));
+}
+
+__global__ void __launch_bounds__(256) k_finish_batch(const NormBatchTab *__restrict__ t, const int *__restrict__ active,
+                                                      double *out) {
+    const NormEnt &e = t->e[blockIdx.x];
+    if (!__ldg(&active[e.design])) return;
+    if (e.two) finish_block<NCASE>(e.mid, NORM_FINISH_CHUNKS, out + (long long)NCASE * e.design);
+    else finish_block<NCASE>(e.partial, e.nblk, out + (long long)NCASE * e.design);
+}
+
+int norm_batch_create(double *const *partial, const int *nblk, const int *design, int n, BatchTab *out) {
+    if (n < 1 || n > BATCH_MAX) return -1;
+    NormBatchTab *t = new NormBatchTab();
+    t->chunks.n = n;
+    t->chunks.start[0] = 0;
+    for (int i = 0; i < n; i++) {
+        NormEnt &e = t->e[i];
+        e.partial = partial[i];
+        e.nblk = nblk[i];
+        e.two = nblk[i] > NORM_FINISH_DIRECT;
+        e.per = (nblk[i] + NORM_FINISH_CHUNKS - 1) / NORM_FINISH_CHUNKS;
+        e.mid = partial[i] + (long long)nblk[i] * NCASE;
+        e.design = design[i];
+        t->chunks.start[i + 1] = t->chunks.start[i] + (e.two ? NORM_FINISH_CHUNKS : 0);
+    }
+    const int rc = upload_tab(*t, n, out);
+    if (rc == 0) out->grid[0] = t->chunks.start[n];
+    delete t;
+    return rc;
+}
+
+void launch_norm_finish_batch(const BatchTab &t, const int *active, double *out, cudaStream_t s) {
+    const NormBatchTab *d = static_cast<const NormBatchTab *>(t.dev);
+    if (t.grid[0] > 0) k_finish_chunks_batch<<<t.grid[0], 256, 0, s>>>(d, active);
+    k_finish_batch<<<t.n, 256, 0, s>>>(d, active, out);
 }
 
 }  // namespace h3d

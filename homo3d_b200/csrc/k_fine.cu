@@ -269,10 +269,10 @@ __device__ __forceinline__ void fine_apply(const FineArgs &a, const KeMat &ke, c
 // the NCASE / C case groups of a vertex block are adjacent CTAs
 // vertex block are adjacent CTAs
 template <int C>
-__device__ __forceinline__ void thread_task(long long &p, int &cb) {
+__device__ __forceinline__ void thread_task(long long &p, int &cb, unsigned bid) {
     constexpr int NG = NCASE / C;
-    cb = (int)(blockIdx.x % NG) * C;
-    p = (long long)(blockIdx.x / NG) * blockDim.x + threadIdx.x;
+    cb = (int)(bid % NG) * C;
+    p = (long long)(bid / NG) * blockDim.x + threadIdx.x;
 }
 
 // one vertex of the colour sweep; RES (the last colour of a sweep) also writes
@@ -337,13 +337,15 @@ __device__ __forceinline__ void fine_gs_vertex(const FineArgs &a, const KeMat &k
 
 // RES: the per-CTA norm partials go to the rows the residual of colour 7 would
 // write (row 7 * (CTAs per colour of the residual) + CTA of the colour, one row
-// per group of CPT cases, zeros for the other cases)
-template <int K, int C, int MINB, bool RES>
-__global__ void __launch_bounds__(FBS, MINB) k_fine_gs(FineArgs a, const __grid_constant__ KeMat ke,
-                                                    double *partial) {
+// per group of CPT cases, zeros for the other cases).  bid / nblk: the CTA's index
+// and the CTA count of the design's launch (blockIdx.x / gridDim.x, or the slice
+// of a batched launch, k_fine_gs_batch)
+template <int K, int C, bool RES>
+__device__ __forceinline__ void fine_gs_block(const FineArgs &a, const KeMat &ke, double *partial, unsigned bid,
+                                              unsigned nblk) {
     long long p;
     int cb;
-    thread_task<C>(p, cb);
+    thread_task<C>(p, cb, bid);
     double nrm[C];
 #pragma unroll
     for (int c = 0; c < C; ++c) nrm[c] = 0;
@@ -362,7 +364,7 @@ __global__ void __launch_bounds__(FBS, MINB) k_fine_gs(FineArgs a, const __grid_
     }
     __syncthreads();
     constexpr int NG = NCASE / C, NGR = NCASE / CPT;  // case groups of this launch / of the residual
-    const long long pb = blockIdx.x / NG, npb = gridDim.x / NG;  // vertex block, vertex blocks
+    const long long pb = bid / NG, npb = nblk / NG;  // vertex block, vertex blocks
     if (threadIdx.x < (C / CPT) * NCASE) {
         const int gl = threadIdx.x / NCASE, q = threadIdx.x % NCASE;
         const int g = cb / CPT + gl;  // the residual's case group of this row
@@ -372,6 +374,12 @@ __global__ void __launch_bounds__(FBS, MINB) k_fine_gs(FineArgs a, const __grid_
             for (int w = 0; w < FBS / 32; ++w) v += sm[q - cb][w];
         partial[((7 * npb + pb) * NGR + g) * NCASE + q] = v;
     }
+}
+
+template <int K, int C, int MINB, bool RES>
+__global__ void __launch_bounds__(FBS, MINB) k_fine_gs(FineArgs a, const __grid_constant__ KeMat ke,
+                                                    double *partial) {
+    fine_gs_block<K, C, RES>(a, ke, partial, blockIdx.x, gridDim.x);
 }
 
 template <int KC>
@@ -423,22 +431,23 @@ __device__ __forceinline__ void fine_residual_vertex(const FineArgs &a, const Ke
 // colour) + CTA of the colour, zeros for the other cases, as with one launch per
 // colour, so the norms are summed in the same order.
 template <int C>
-__device__ __forceinline__ void colour_task(long long &p, int &cb, int &K, unsigned &bx, unsigned ncol = 8) {
+__device__ __forceinline__ void colour_task(long long &p, int &cb, int &K, unsigned &bx, unsigned bid,
+                                            unsigned ncol = 8) {
     constexpr int NG = NCASE / C;
-    K = (int)(blockIdx.x % ncol);
-    bx = blockIdx.x / ncol;
+    K = (int)(bid % ncol);
+    bx = bid / ncol;
     cb = (int)(bx % NG) * C;
     p = (long long)(bx / NG) * blockDim.x + threadIdx.x;
 }
 
 template <unsigned NCOL>  // colours 0 .. NCOL-1 (8, or 7 after a sweep that did colour 7's)
-__global__ void __launch_bounds__(FBS, RES_MINB) k_fine_residual(FineArgs a, const __grid_constant__ KeMat ke,
-                                                       double *partial) {
+__device__ __forceinline__ void fine_residual_block(const FineArgs &a, const KeMat &ke, double *partial, unsigned bid,
+                                                    unsigned nblk) {
     constexpr unsigned ncol = NCOL;
     long long p;
     int cb, K;
     unsigned bx;
-    colour_task<CPT>(p, cb, K, bx, ncol);
+    colour_task<CPT>(p, cb, K, bx, bid, ncol);
     double nrm[CPT] = {};
     if (p < a.P) fine_residual_vertex<-1>(a, ke, p, cb, nrm, K);
     if (!partial) return;
@@ -456,8 +465,14 @@ __global__ void __launch_bounds__(FBS, RES_MINB) k_fine_residual(FineArgs a, con
         if (q >= cb && q < cb + CPT)
 #pragma unroll
             for (int w = 0; w < FBS / 32; ++w) v += sm[q - cb][w];
-        partial[((long long)K * (gridDim.x / ncol) + bx) * NCASE + q] = v;
+        partial[((long long)K * (nblk / ncol) + bx) * NCASE + q] = v;
     }
+}
+
+template <unsigned NCOL>
+__global__ void __launch_bounds__(FBS, RES_MINB) k_fine_residual(FineArgs a, const __grid_constant__ KeMat ke,
+                                                       double *partial) {
+    fine_residual_block<NCOL>(a, ke, partial, blockIdx.x, gridDim.x);
 }
 
 // ---- refined precision: residual of an FP64 solution ----------------------------
@@ -534,7 +549,7 @@ __global__ void __launch_bounds__(FBS, MINB64) k_fine_residual64(FineArgs a, con
     long long p;
     int cb, K;
     unsigned bx;
-    colour_task<CPT64>(p, cb, K, bx);  // all colours in one launch, colour-minor
+    colour_task<CPT64>(p, cb, K, bx, blockIdx.x);  // all colours in one launch, colour-minor
     if (p >= a.P) return;
     fine_residual64_vertex<-1, EXACT>(a, ke, ke64, u64, p, cb, K);
 }
@@ -709,8 +724,7 @@ __global__ void __launch_bounds__(FVB) k_update64(long long nv, double *u, const
 // or n + 1 past the origin's own d = 13) and cr = 3c + r; the products of each
 // neighbour are summed over d in ascending order by one thread per (c, r).
 constexpr int PIN_THREADS = 26 * NF;
-__global__ void __launch_bounds__(PIN_THREADS) k_pin_deflate(FineArgs a, const __grid_constant__ KeMat ke,
-                                                              double *state) {
+__device__ __forceinline__ void pin_deflate_block(const FineArgs &a, const KeMat &ke, double *state) {
     __shared__ double qpart[26][NF];
     __shared__ double al[NF];
     __shared__ double Ms[9];
@@ -768,6 +782,11 @@ __global__ void __launch_bounds__(PIN_THREADS) k_pin_deflate(FineArgs a, const _
     const double t = (double)A[r] * al[3 * c] + (double)A[3 + r] * al[3 * c + 1] + (double)A[6 + r] * al[3 * c + 2];
     float *fp = const_cast<float *>(a.f) + fidx(3 * c + r, nid);
     *fp = (float)((double)*fp + t);
+}
+
+__global__ void __launch_bounds__(PIN_THREADS) k_pin_deflate(FineArgs a, const __grid_constant__ KeMat ke,
+                                                              double *state) {
+    pin_deflate_block(a, ke, state);
 }
 
 // state: F = (plane sums of f) - f at the origin, T = 0
@@ -856,6 +875,112 @@ void launch_convert_field(long long nv, const float *src, double *dst, cudaStrea
 }
 void launch_convert_field(long long nv, const double *src, float *dst, cudaStream_t s) {
     k_f64_to_f32<<<field_chunks(nv), FVB, 0, s>>>(nv, src, dst);
+}
+
+// ---- lockstep batches: the level 0 of several designs in one launch per step ----
+// Each design owns a slice of the launch's CTAs (BatchSlices) and runs the same
+// per-CTA body as its own launch would, with its CTA index inside the slice, so
+// every design's fields and norm partials are those of its own launches, to the
+// last bit.  A CTA copies its design's arguments to shared memory once; a design
+// whose flag in `active` is 0 (converged) returns at once.  The sweep runs in
+// launch shape 0 (six cases per thread, 4 CTAs/SM).
+struct FineEnt {
+    FineArgs a;
+    double *partial;  // the design's norm partials
+    double *state;    // its deflation state
+    int design;       // its index in the active flags
+};
+struct FineBatchTab {
+    BatchSlices gs;   // CTAs of one colour of the sweep
+    BatchSlices res;  // CTAs of the seven-colour residual
+    FineEnt e[BATCH_MAX];
+};
+
+template <int K, bool RES>
+__global__ void __launch_bounds__(FBS, 4) k_fine_gs_batch(const FineBatchTab *__restrict__ t,
+                                                        const int *__restrict__ active,
+                                                        const __grid_constant__ KeMat ke) {
+    __shared__ __align__(16) unsigned buf[(sizeof(FineArgs) + 3) / 4];
+    const int i = batch_slice(t->gs, blockIdx.x);
+    const FineEnt &en = t->e[i];
+    if (!__ldg(&active[en.design])) return;
+    const FineArgs &a = stage_args(en.a, buf);
+    const unsigned b0 = __ldg(&t->gs.start[i]), b1 = __ldg(&t->gs.start[i + 1]);
+    fine_gs_block<K, 6, RES>(a, ke, en.partial, blockIdx.x - b0, b1 - b0);
+}
+
+__global__ void __launch_bounds__(FBS, RES_MINB) k_fine_residual_batch(const FineBatchTab *__restrict__ t,
+                                                                      const int *__restrict__ active,
+                                                                      const __grid_constant__ KeMat ke) {
+    __shared__ __align__(16) unsigned buf[(sizeof(FineArgs) + 3) / 4];
+    const int i = batch_slice(t->res, blockIdx.x);
+    const FineEnt &en = t->e[i];
+    if (!__ldg(&active[en.design])) return;
+    const FineArgs &a = stage_args(en.a, buf);
+    const unsigned b0 = __ldg(&t->res.start[i]), b1 = __ldg(&t->res.start[i + 1]);
+    fine_residual_block<7>(a, ke, en.partial, blockIdx.x - b0, b1 - b0);
+}
+
+// one CTA per design
+__global__ void __launch_bounds__(PIN_THREADS) k_pin_deflate_batch(const FineBatchTab *__restrict__ t,
+                                                                    const int *__restrict__ active,
+                                                                    const __grid_constant__ KeMat ke) {
+    __shared__ __align__(16) unsigned buf[(sizeof(FineArgs) + 3) / 4];
+    const FineEnt &en = t->e[blockIdx.x];
+    if (!__ldg(&active[en.design])) return;
+    const FineArgs &a = stage_args(en.a, buf);
+    pin_deflate_block(a, ke, en.state);
+}
+
+int fine_batch_create(const Level *const *lv0, const float *const *rho, double *const *partial,
+                      double *const *state, const int *design, int n, BatchTab *out) {
+    if (n < 1 || n > BATCH_MAX) return -1;
+    FineBatchTab *t = new FineBatchTab();
+    t->gs.n = t->res.n = n;
+    t->gs.start[0] = t->res.start[0] = 0;
+    for (int i = 0; i < n; i++) {
+        t->e[i].a = make_args(*lv0[i], rho[i]);
+        t->e[i].partial = partial[i];
+        t->e[i].state = state[i];
+        t->e[i].design = design[i];
+        t->gs.start[i + 1] = t->gs.start[i] + task_blocks(t->e[i].a, 6);
+        t->res.start[i + 1] = t->res.start[i] + task_blocks(t->e[i].a, CPT) * 7;
+    }
+    void *d = nullptr;
+    int rc = cudaMalloc(&d, sizeof(FineBatchTab)) == cudaSuccess ? 0 : -2;
+    if (rc == 0 && cudaMemcpy(d, t, sizeof(FineBatchTab), cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
+    if (rc == 0) {
+        out->dev = d;
+        out->n = n;
+        out->grid[0] = t->gs.start[n];
+        out->grid[1] = t->res.start[n];
+    } else if (d) {
+        cudaFree(d);
+    }
+    delete t;
+    return rc;
+}
+
+void launch_fine_sweep_batch(const BatchTab &t, const KeMat &ke, const int *active, bool residual, cudaStream_t s) {
+    const FineBatchTab *d = static_cast<const FineBatchTab *>(t.dev);
+    const unsigned g = t.grid[0];
+    k_fine_gs_batch<0, false><<<g, FBS, 0, s>>>(d, active, ke);
+    k_fine_gs_batch<1, false><<<g, FBS, 0, s>>>(d, active, ke);
+    k_fine_gs_batch<2, false><<<g, FBS, 0, s>>>(d, active, ke);
+    k_fine_gs_batch<3, false><<<g, FBS, 0, s>>>(d, active, ke);
+    k_fine_gs_batch<4, false><<<g, FBS, 0, s>>>(d, active, ke);
+    k_fine_gs_batch<5, false><<<g, FBS, 0, s>>>(d, active, ke);
+    k_fine_gs_batch<6, false><<<g, FBS, 0, s>>>(d, active, ke);
+    if (residual) {
+        k_fine_gs_batch<7, true><<<g, FBS, 0, s>>>(d, active, ke);
+        k_fine_residual_batch<<<t.grid[1], FBS, 0, s>>>(d, active, ke);
+    } else {
+        k_fine_gs_batch<7, false><<<g, FBS, 0, s>>>(d, active, ke);
+    }
+}
+
+void launch_pin_deflate_batch(const BatchTab &t, const KeMat &ke, const int *active, cudaStream_t s) {
+    k_pin_deflate_batch<<<t.n, PIN_THREADS, 0, s>>>(static_cast<const FineBatchTab *>(t.dev), active, ke);
 }
 
 // mean of each of the 18 planes over unique vertices, removed in place (FP64)

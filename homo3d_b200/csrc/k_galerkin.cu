@@ -452,12 +452,11 @@ void launch_gauss_jordan(double *aug, int n, int *flag, cudaStream_t s) {
     }
 }
 
-// one block per load case: b (optionally minus its mean per component), x = K^-1 b
-__global__ void __launch_bounds__(256) k_coarse_apply(Planes C, const double *__restrict__ aug, int n, int project,
-                                                      const float *__restrict__ f, float *u) {
-    extern __shared__ double b[];
+// one block per load case c: b (optionally minus its mean per component), x = K^-1 b;
+// b: n doubles of shared memory
+__device__ __forceinline__ void coarse_apply_block(const Planes &C, const double *__restrict__ aug, int n, int project,
+                                                   const float *__restrict__ f, float *u, int c, double *b) {
     __shared__ double mean[3];
-    const int c = blockIdx.x;
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
         const long long lex = i / 3;
         const int comp = i % 3;
@@ -485,9 +484,78 @@ __global__ void __launch_bounds__(256) k_coarse_apply(Planes C, const double *__
     }
 }
 
+__global__ void __launch_bounds__(256) k_coarse_apply(Planes C, const double *__restrict__ aug, int n, int project,
+                                                      const float *__restrict__ f, float *u) {
+    extern __shared__ double b[];
+    coarse_apply_block(C, aug, n, project, f, u, blockIdx.x, b);
+}
+
 void launch_coarse_apply(const Level &C, const double *aug, int project, cudaStream_t s) {
     const int n = (int)(3 * C.P.nv);
     k_coarse_apply<<<NCASE, 256, (size_t)n * sizeof(double), s>>>(C.P, aug, n, project, C.f, C.u);
+}
+
+// lockstep batches: the coarsest solves of several designs in one launch, six
+// CTAs (one per load case) per design, each the CTA of the design's own launch
+struct CoarsestEnt {
+    Planes C;
+    const double *aug;
+    const float *f;
+    float *u;
+    int n, design;
+};
+struct CoarsestBatchTab {
+    int n;
+    CoarsestEnt e[BATCH_MAX];
+};
+
+__global__ void __launch_bounds__(256) k_coarse_apply_batch(const CoarsestBatchTab *__restrict__ t,
+                                                            const int *__restrict__ active, int project) {
+    extern __shared__ double b[];
+    __shared__ __align__(16) unsigned buf[sizeof(CoarsestEnt) / 4];
+    const int i = blockIdx.x / NCASE, c = blockIdx.x % NCASE;
+    if (!__ldg(&active[t->e[i].design])) return;
+    const CoarsestEnt &e = stage_args(t->e[i], buf);
+    coarse_apply_block(e.C, e.aug, e.n, project, e.f, e.u, c, b);
+}
+
+int coarsest_batch_create(const Level *const *lv, const double *const *aug, const int *design, int n, BatchTab *out) {
+    if (n < 1 || n > BATCH_MAX) return -1;
+    CoarsestBatchTab *t = new CoarsestBatchTab();
+    t->n = n;
+    int nmax = 0;
+    for (int i = 0; i < n; i++) {
+        CoarsestEnt &e = t->e[i];
+        e.C = lv[i]->P;
+        e.aug = aug[i];
+        e.f = lv[i]->f;
+        e.u = lv[i]->u;
+        e.n = (int)(3 * lv[i]->P.nv);
+        e.design = design[i];
+        nmax = e.n > nmax ? e.n : nmax;
+    }
+    void *d = nullptr;
+    int rc = cudaMalloc(&d, sizeof(CoarsestBatchTab)) == cudaSuccess ? 0 : -2;
+    if (rc == 0 && cudaMemcpy(d, t, sizeof(CoarsestBatchTab), cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
+    if (rc == 0 && nmax * sizeof(double) > 48 * 1024 &&
+        cudaFuncSetAttribute(k_coarse_apply_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)(nmax * sizeof(double))) != cudaSuccess)
+        rc = -2;
+    if (rc == 0) {
+        out->dev = d;
+        out->n = n;
+        out->grid[0] = (unsigned)(n * NCASE);
+        out->smem = (size_t)nmax * sizeof(double);
+    } else if (d) {
+        cudaFree(d);
+    }
+    delete t;
+    return rc;
+}
+
+void launch_coarse_apply_batch(const BatchTab &t, const int *active, int project, cudaStream_t s) {
+    k_coarse_apply_batch<<<t.grid[0], 256, t.smem, s>>>(static_cast<const CoarsestBatchTab *>(t.dev), active,
+                                                         project);
 }
 
 }  // namespace h3d

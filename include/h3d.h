@@ -222,6 +222,26 @@ H3D_API int h3d_batch_update_density(h3d_handle *const *hs, const float *const *
  * in resolution and precision mode.  Returns the first non-OK status. */
 H3D_API int h3d_batch_elastic_matrix(h3d_handle *const *hs, int n, double tol, double *C,
                                      h3d_solve_stats *stats, int *status);
+/* Lockstep batches: the designs step through their V-cycles together.  Every
+ * step of a batch V-cycle (a colour of a level's sweep, a residual, a transfer,
+ * the coarsest solves, the deflation, the norms) is one launch over all designs
+ * of that level, each design owning a slice of its CTAs; the batch V-cycle is one
+ * captured CUDA graph, and the host decides once per cycle which designs are still
+ * running (a converged design's CTAs return at once).  Requirements: 1 to
+ * H3D_LOCKSTEP_MAX distinct H3D_PREC_FP32 handles on one device with the same
+ * material, stencil precision and coarse mode, and ratio-2 coarsening on every
+ * level (resolutions below 512); otherwise H3D_ERR_ARG.  The batch holds the
+ * handles' buffer addresses: destroy it before any of its handles.
+ * h3d_lockstep_elastic_matrix is h3d_batch_elastic_matrix over the batch's
+ * handles, with the same C, statistics and status as h3d_elastic_matrix on each
+ * handle to the last bit (solve_ms: from the batch's start to the design's end). */
+#define H3D_LOCKSTEP_MAX 64
+typedef struct h3d_lockstep h3d_lockstep;
+H3D_API int h3d_lockstep_create(h3d_handle *const *hs, int n, h3d_lockstep **out);
+H3D_API int h3d_lockstep_elastic_matrix(h3d_lockstep *b, double tol, double *C, h3d_solve_stats *stats,
+                                        int *status);
+H3D_API int h3d_lockstep_destroy(h3d_lockstep *b);
+H3D_API const char *h3d_lockstep_last_error(const h3d_lockstep *b);
 
 /* ---- SIMP penalisation, the expression rho.pow(p) (TensorExpression.h:517-531) */
 /* rho_phys = rho^p */

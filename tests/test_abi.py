@@ -38,7 +38,8 @@ def test_library_exports_every_declared_symbol():
 
 
 def test_binding_signatures_cover_the_header():
-    bound = set(H._SIGS) | {"h3d_last_error", "h3d_stream", "h3d_mma_last_error", "h3d_warmnet_last_error"}
+    bound = set(H._SIGS) | {"h3d_last_error", "h3d_stream", "h3d_mma_last_error", "h3d_warmnet_last_error",
+                            "h3d_lockstep_last_error"}
     assert bound == set(declared_symbols())
 
 
@@ -56,6 +57,11 @@ def test_cpp_shim_compiles_and_links(tmp_path):
     r = subprocess.run(["g++", "-std=c++17", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(out),
                         "-L", os.path.dirname(H.LIB_PATH), "-lh3d"], capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_buffer_extent_rule():
+    assert H._extent((4, 5, 6)) == 120
+    assert H._extent((4, 5, 6), 8) == 3 + 8 * (4 + 5 * 5) + 1
 
 
 def test_reference_resolution_rule():
