@@ -47,8 +47,9 @@ def parse():
     p.add_argument("--pin-mode", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
     p.add_argument("--no-north-star", action="store_true", help="skip the mixed-precision arm of the same step")
-    p.add_argument("--workload", default="solve", choices=["solve", "mma"],
-                   help="solve: the homogenization step (default); mma: one MMA design update")
+    p.add_argument("--workload", default="solve", choices=["solve", "mma", "batch"],
+                   help="solve: the homogenization step (default); mma: one MMA design update; "
+                        "batch: designs/s of 24 designs of 64^3-128^3 solved together")
     p.add_argument("--mma-m", type=int, default=1, help="constraints of the mma workload")
     p.add_argument("--profile", action="store_true",
                    help="only warm-up and timed steps (no e2e, setup or sweep side measurements), for ncu")
@@ -358,9 +359,12 @@ def north_star(args, rho_d, plain_ms, plain_vc, plain_err, fx):
                 "status": st["status"], "C_err": err, "scheme": PRECISION_NAME[precision]}
 
     mixed, mixed_tc = arm(H.PREC_MIXED), arm(H.PREC_MIXED_TC)
+    best = min((mixed, mixed_tc), key=lambda a: a["ms"])
     return {"plain_ms": round(plain_ms, 3), "plain_vcycles": plain_vc, "plain_C_err": plain_err,
             "target_ratio": 0.5, "mixed": mixed, "mixed_tc": mixed_tc,
-            "learned": "not in the step (saves no V-cycles on fresh designs)", "plain": PRECISION_NAME[0]}
+            "learned_mixed_ms": None, "ratio": best["ratio_over_plain"], "ratio_arm": best["scheme"],
+            "learned": "not in the step (saves no V-cycles on fresh designs): ratio is the faster mixed arm "
+                       "over the plain one", "plain": PRECISION_NAME[0]}
 
 
 FIXTURE = os.path.join(ROOT, "tests", "golden", "oracle_C.json")
@@ -553,10 +557,59 @@ def mma_arm(args):
     return out
 
 
+def batch_arm(args):
+    """--workload batch: designs per second for 24 designs of uneven resolution
+    (8 x 64^3, 8 x 96^3, 8 x 128^3; seeded trig-basis densities at volumes U(0.1,
+    0.5), zero start, six load cases, relthres 1e-3, FP32 V-cycles): one pass = the
+    stencils, the six solves and C of every design.  Three arms through the public
+    API, each timed as the best of --steps passes after --warmup (host clock with
+    the device synchronised, densities resident on the device): the lockstep batch
+    (value), per-design streams and one design at a time; C must agree to the last
+    bit across the arms."""
+    import numpy as np
+    import torch
+
+    import homo3d_b200 as H
+    from homo3d_b200.batch import make_designs, parse_sizes, run_pass
+    sizes = parse_sizes("64x8,96x8,128x8")
+    designs = make_designs(sizes)
+    homs = [H.Homogenization(n, precision=H.PREC_FP32) for n in sizes]
+    rhos = [torch.tensor(r, device="cuda") for _, _, _, r in designs]
+    tol = 1e-3
+    lock = H.Lockstep(homs)
+    res = {}
+    for arm, batched, ls in (("lockstep", True, lock), ("streams", True, None), ("sequential", False, None)):
+        best, C = None, None
+        for rep in range(max(args.warmup, 1) + args.steps):
+            dt, _, C, stats = run_pass(torch, homs, rhos, tol, batched, ls)
+            if rep >= max(args.warmup, 1):
+                best = dt if best is None else min(best, dt)
+        res[arm] = (best, C, [s["vcycles"] for s in stats])
+    lock.close()
+    for hd in homs:
+        hd.close()
+    same = all(np.array_equal(res["lockstep"][1], res[a][1]) for a in ("streams", "sequential"))
+    if not same:
+        raise RuntimeError("batched C differs from the one-at-a-time C")
+    dps = {a: round(len(sizes) / res[a][0], 2) for a in res}
+    return {"metric": "designs per second, 24 designs (8x64^3, 8x96^3, 8x128^3), 6 load cases, relthres 1e-3",
+            "value": dps["lockstep"], "unit": "designs/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(res["lockstep"][0] * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded trig-basis densities, reflect6, volume U(0.1, 0.5), rho^3",
+            "config": {"workload": "batched designs (config 4)", "designs": len(sizes), "relthres": tol,
+                       "precision": "FP32 V-cycles"},
+            "designs_per_s": dps, "C_identical_across_arms": same, "vcycles": res["lockstep"][2],
+            "cpu_baseline": None}
+
+
 def main():
     args = parse()
     if args.workload == "mma":
         print(json.dumps(mma_arm(args)), flush=True)
+        return
+    if args.workload == "batch":
+        print(json.dumps(batch_arm(args)), flush=True)
         return
     if args.impl == "reference":
         out = reference_arm(args)

@@ -127,3 +127,26 @@ def test_short_density_is_refused(torch_cuda):
         hd.update(torch.ones(48 ** 3, dtype=torch.float64, device="cuda"))
     hd.update(_rho(torch, 48, 0, 0.3))
     hd.close()
+
+
+@pytest.mark.parametrize("kw", [dict(coarse_mode=H.COARSE_PROJECT), dict(stencil=H.STENCIL_FP32),
+                                dict(pin_mode=H.PIN_GALERKIN)])
+def test_lockstep_other_modes(torch_cuda, kw):
+    """the projected coarsest solve, FP32 coarse stencils and the Galerkin pin in
+    lockstep, against the same designs one at a time"""
+    torch = torch_cuda
+    designs = [(16, 0, 0.3), (24, 1, 0.4), (32, 2, 0.2), (28, 5, 0.3)]
+    ref = []
+    for n, seed, vol in designs:
+        hd = H.Homogenization(n, precision=H.PREC_FP32, **kw)
+        hd.update(_rho(torch, n, seed, vol))
+        ref.append((hd.elasticMatrix(1e-4), hd.last_stats))
+        hd.close()
+    homs = [H.Homogenization(n, precision=H.PREC_FP32, **kw) for n, _, _ in designs]
+    H.batch_update(homs, [_rho(torch, n, seed, vol) for n, seed, vol in designs])
+    with H.Lockstep(homs) as lk:
+        C = lk.elasticMatrix(1e-4)
+    for i, hd in enumerate(homs):
+        _same_stats(hd.last_stats, ref[i][1])
+        assert np.array_equal(C[i], ref[i][0]), i
+        hd.close()
