@@ -269,6 +269,15 @@ def gpu_arm(args):
     g1.record(stream)
     torch.cuda.synchronize()
     sweep_ms = g0.elapsed_time(g1) / nsweep
+    # the level-1 sweep (27-point FP16 stencils) the same way
+    hd.mg.grids[1].gs_relaxation(1.0, 2)
+    g0.record(stream)
+    hd.mg.grids[1].gs_relaxation(1.0, nsweep)
+    g1.record(stream)
+    torch.cuda.synchronize()
+    sweep1_ms = g0.elapsed_time(g1) / nsweep
+    nv1 = int(np.prod(hd.dims[1]))
+    bpv1 = 243 * 2 + 3 * 72  # FP16 stencil entries + u read and write + f, per vertex
     n3 = args.reso ** 3
     alg_bytes_sweep = 220.0 * n3          # 3L(2 s_u + s_f) + s_rho per vertex, L = 6, FP32
     flops_sweep = 2.0 * (576 + 234 * 6) * n3
@@ -293,6 +302,10 @@ def gpu_arm(args):
                     "d2h_bytes_per_step": 36 * 8},
             "refinements": refs[-1],
             "launch_shapes": hd.tuning(),
+            "level1_sweep": {"kernel": "k_coarse_gs (8 colour launches = one sweep of level 1)",
+                             "vertices": nv1, "bytes_per_vertex": bpv1, "ms": round(sweep1_ms, 4),
+                             "achieved": round(bpv1 * nv1 / (sweep1_ms * 1e-3) / 1e9, 1), "unit": "GB/s",
+                             "frac": round(bpv1 * nv1 / (sweep1_ms * 1e-3) / 1e9 / peaks.get("hbm_gbs"), 4)},
             "gpu_launches": sum(launches_per_step(hd.nlevels, c, args.reso, args.precision != 1, r, coarsest_nv,
                                                   args.precision == 3) for c, r in zip(cycles, refs)),
             "roofline": {"kernel": "k_fine_gs (8 colour launches = one sweep)", "bound": "hbm",
