@@ -537,7 +537,7 @@ int coarsest_batch_create(const Level *const *lv, const double *const *aug, cons
     void *d = nullptr;
     int rc = cudaMalloc(&d, sizeof(CoarsestBatchTab)) == cudaSuccess ? 0 : -2;
     if (rc == 0 && cudaMemcpy(d, t, sizeof(CoarsestBatchTab), cudaMemcpyHostToDevice) != cudaSuccess) rc = -2;
-    if (rc == 0 && nmax * sizeof(double) > 48 * 1024 &&
+    if (rc == 0 && nmax * sizeof(double) + sizeof(CoarsestEnt) > 48 * 1024 &&
         cudaFuncSetAttribute(k_coarse_apply_batch, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)(nmax * sizeof(double))) != cudaSuccess)
         rc = -2;
