@@ -676,6 +676,10 @@ class Lockstep:
     def elasticMatrix(self, tol=1e-2):
         """batch_elasticMatrix over the batch's designs; returns the [n, 6, 6] C and
         sets each design's last_stats"""
+        if getattr(self, "_b", None) is None:
+            raise ValueError("the lockstep batch is closed")
+        if any(getattr(h, "_h", None) is None for h in self.homs):
+            raise ValueError("a handle of the lockstep batch has been closed")
         n = len(self.homs)
         C = np.zeros((n, 36))
         st = (SolveStats * n)()

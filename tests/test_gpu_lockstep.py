@@ -89,6 +89,15 @@ def test_lockstep_refuses_what_it_cannot_batch(torch_cuda):
         assert ei.value.code == H.H3D_ERR_ARG
     for hs in cases[1:4]:
         hs[1].close()
+    # a closed handle or batch is refused before the library is called
+    c = H.Homogenization(16, precision=H.PREC_FP32)
+    lk = H.Lockstep([a, c])
+    c.close()
+    with pytest.raises(ValueError):
+        lk.elasticMatrix(1e-3)
+    lk.close()
+    with pytest.raises(ValueError):
+        lk.elasticMatrix(1e-3)
     a.close()
 
 
