@@ -108,6 +108,7 @@ _SIGS = {
     "h3d_batch_elastic_matrix": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_double, _dp,
                                  ctypes.POINTER(SolveStats), _ip],
     "h3d_lockstep_create": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.POINTER(_vp)],
+    "h3d_lockstep_create_groups": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)],
     "h3d_lockstep_elastic_matrix": [_vp, ctypes.c_double, _dp, ctypes.POINTER(SolveStats), _ip],
     "h3d_lockstep_destroy": [_vp],
     "h3d_penalize": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float],
@@ -664,10 +665,15 @@ class Lockstep:
     H3D_PREC_FP32 designs on one GPU with the same material, stencil precision and
     coarse mode (resolutions below 512); close the batch before its handles."""
 
-    def __init__(self, homs):
+    def __init__(self, homs, groups=None):
+        """groups: parallel branches of the batch graph (None: the library's default)"""
         self.homs = list(homs)
         b = _vp()
-        code = lib().h3d_lockstep_create(_handle_array(self.homs), len(self.homs), ctypes.byref(b))
+        if groups is None:
+            code = lib().h3d_lockstep_create(_handle_array(self.homs), len(self.homs), ctypes.byref(b))
+        else:
+            code = lib().h3d_lockstep_create_groups(_handle_array(self.homs), len(self.homs), int(groups),
+                                                    ctypes.byref(b))
         if code != H3D_OK:
             msg = lib().h3d_last_error(self.homs[0]._h).decode() if self.homs else ""
             raise H3DError(code, msg or "h3d_lockstep_create failed")

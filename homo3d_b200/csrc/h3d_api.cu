@@ -1296,16 +1296,28 @@ int h3d_batch_elastic_matrix(h3d_handle *const *hs, int n, double tol, double *C
 // the down leg's sweep and residual, or the coarsest solve where l is a design's
 // last level; the up leg prolongs and sweeps; then the deflation and the norms.
 // Each design sees its own launches' operations in its own order.
-struct h3d_lockstep {
-    std::vector<h3d_handle *> hs;
-    int n = 0, device = 0, lmax = 0, project = 0;
-    bool f32 = false;
-    KeMat ke;
+// one branch of the batch V-cycle graph: the tables of some of the batch's designs
+struct LockGroup {
+    std::vector<int> members;  // indices into the batch
+    int lmax = 0;
     BatchTab fine, norm;
     BatchTab coarse[MAXLV], xfer[MAXLV], coarsest[MAXLV];
+    cudaStream_t stream = nullptr;  // capture stream of the branch (the batch stream for group 0)
+    cudaEvent_t join = nullptr;
+};
+
+struct h3d_lockstep {
+    std::vector<h3d_handle *> hs;
+    int n = 0, device = 0, project = 0;
+    bool f32 = false;
+    KeMat ke;
+    // the designs are split into groups whose V-cycle launches are parallel branches
+    // of the one batch graph, so one group's launches fill the last partial wave of
+    // another's
+    std::vector<LockGroup> groups;
     cudaStream_t stream = nullptr;
     cudaGraphExec_t graph = nullptr;
-    cudaEvent_t ev0 = nullptr;
+    cudaEvent_t ev0 = nullptr, fork = nullptr;
     int *d_active = nullptr, *h_active = nullptr;
     double *d_norms = nullptr, *h_norms = nullptr;
     std::string err;
@@ -1329,54 +1341,69 @@ int lfail(h3d_lockstep *b, int code, const std::string &msg) {
 void lockstep_free(h3d_lockstep *b) {
     if (b->device >= 0) cudaSetDevice(b->device);
     if (b->graph) cudaGraphExecDestroy(b->graph);
-    batch_tab_free(b->fine);
-    batch_tab_free(b->norm);
-    for (int l = 0; l < MAXLV; l++) {
-        batch_tab_free(b->coarse[l]);
-        batch_tab_free(b->xfer[l]);
-        batch_tab_free(b->coarsest[l]);
+    for (LockGroup &g : b->groups) {
+        batch_tab_free(g.fine);
+        batch_tab_free(g.norm);
+        for (int l = 0; l < MAXLV; l++) {
+            batch_tab_free(g.coarse[l]);
+            batch_tab_free(g.xfer[l]);
+            batch_tab_free(g.coarsest[l]);
+        }
+        if (g.join) cudaEventDestroy(g.join);
+        if (g.stream && g.stream != b->stream) cudaStreamDestroy(g.stream);
     }
     if (b->d_active) cudaFree(b->d_active);
     if (b->h_active) cudaFreeHost(b->h_active);
     if (b->d_norms) cudaFree(b->d_norms);
     if (b->h_norms) cudaFreeHost(b->h_norms);
     if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->fork) cudaEventDestroy(b->fork);
     if (b->stream) cudaStreamDestroy(b->stream);
 }
 
-// the batch V-cycle on b->stream (captured once)
+// one group's share of the batch V-cycle on stream s
+void lockstep_enqueue_group(const h3d_lockstep *b, const LockGroup &g, cudaStream_t s) {
+    launch_fine_sweep_batch(g.fine, b->ke, b->d_active, true, s);
+    for (int l = 1; l < g.lmax; l++) {
+        if (g.xfer[l].n) launch_restrict_batch(g.xfer[l], b->d_active, s);
+        if (g.coarse[l].n) launch_coarse_sweep_batch(g.coarse[l], b->f32, b->d_active, true, s);
+        if (g.coarsest[l].n) launch_coarse_apply_batch(g.coarsest[l], b->d_active, b->project, s);
+    }
+    for (int l = g.lmax - 2; l >= 0; l--) {
+        if (!g.xfer[l + 1].n) continue;
+        launch_prolong_batch(g.xfer[l + 1], b->d_active, l == 0, s);
+        if (l == 0) launch_fine_sweep_batch(g.fine, b->ke, b->d_active, false, s);
+        else launch_coarse_sweep_batch(g.coarse[l], b->f32, b->d_active, false, s);
+    }
+    launch_pin_deflate_batch(g.fine, b->ke, b->d_active, s);
+    launch_norm_finish_batch(g.norm, b->d_active, b->d_norms, s);
+}
+
+// the batch V-cycle on b->stream (captured once): the active flags in, the groups
+// as parallel branches, the norms out
 void lockstep_enqueue(h3d_lockstep *b) {
     cudaStream_t s = b->stream;
     cudaMemcpyAsync(b->d_active, b->h_active, sizeof(int) * b->n, cudaMemcpyHostToDevice, s);
-    launch_fine_sweep_batch(b->fine, b->ke, b->d_active, true, s);
-    for (int l = 1; l < b->lmax; l++) {
-        if (b->xfer[l].n) launch_restrict_batch(b->xfer[l], b->d_active, s);
-        if (b->coarse[l].n) launch_coarse_sweep_batch(b->coarse[l], b->f32, b->d_active, true, s);
-        if (b->coarsest[l].n) launch_coarse_apply_batch(b->coarsest[l], b->d_active, b->project, s);
+    cudaEventRecord(b->fork, s);
+    for (size_t k = 1; k < b->groups.size(); k++) cudaStreamWaitEvent(b->groups[k].stream, b->fork, 0);
+    for (const LockGroup &g : b->groups) lockstep_enqueue_group(b, g, g.stream);
+    for (size_t k = 1; k < b->groups.size(); k++) {
+        cudaEventRecord(b->groups[k].join, b->groups[k].stream);
+        cudaStreamWaitEvent(s, b->groups[k].join, 0);
     }
-    for (int l = b->lmax - 2; l >= 0; l--) {
-        if (!b->xfer[l + 1].n) continue;
-        launch_prolong_batch(b->xfer[l + 1], b->d_active, l == 0, s);
-        if (l == 0) launch_fine_sweep_batch(b->fine, b->ke, b->d_active, false, s);
-        else launch_coarse_sweep_batch(b->coarse[l], b->f32, b->d_active, false, s);
-    }
-    launch_pin_deflate_batch(b->fine, b->ke, b->d_active, s);
-    launch_norm_finish_batch(b->norm, b->d_active, b->d_norms, s);
     cudaMemcpyAsync(b->h_norms, b->d_norms, sizeof(double) * NCASE * b->n, cudaMemcpyDeviceToHost, s);
 }
 
-int lockstep_build(h3d_lockstep *b) {
-    const int n = b->n;
-    std::vector<const Level *> a, c;
+int lockstep_build_group(h3d_lockstep *b, LockGroup &grp) {
+    std::vector<const Level *> a;
     std::vector<const float *> rho;
     std::vector<double *> part, state;
-    std::vector<const double *> aug;
     std::vector<int> des, nblk;
     auto tab_rc = [&](int rc, const char *what) -> int {
         if (rc == 0) return H3D_OK;
         return lfail(b, rc == -2 ? H3D_ERR_NOMEM : H3D_ERR_ARG, std::string("lockstep table: ") + what);
     };
-    for (int i = 0; i < n; i++) {
+    for (int i : grp.members) {
         h3d_handle *h = b->hs[i];
         a.push_back(&h->lv[0]);
         rho.push_back(h->rho);
@@ -1384,16 +1411,18 @@ int lockstep_build(h3d_lockstep *b) {
         state.push_back(h->pin_state);
         des.push_back(i);
         nblk.push_back(fine_residual_blocks(h->lv[0]));
+        grp.lmax = std::max(grp.lmax, h->nl);
     }
-    if (int e = tab_rc(fine_batch_create(a.data(), rho.data(), part.data(), state.data(), des.data(), n, &b->fine),
+    const int m = (int)grp.members.size();
+    if (int e = tab_rc(fine_batch_create(a.data(), rho.data(), part.data(), state.data(), des.data(), m, &grp.fine),
                        "level 0"))
         return e;
-    if (int e = tab_rc(norm_batch_create(part.data(), nblk.data(), des.data(), n, &b->norm), "norms")) return e;
-    for (int l = 1; l < b->lmax; l++) {
+    if (int e = tab_rc(norm_batch_create(part.data(), nblk.data(), des.data(), m, &grp.norm), "norms")) return e;
+    for (int l = 1; l < grp.lmax; l++) {
         std::vector<const Level *> F, Cl, S, Z;
         std::vector<int> dx, ds, dz;
         std::vector<const double *> az;
-        for (int i = 0; i < n; i++) {
+        for (int i : grp.members) {
             h3d_handle *h = b->hs[i];
             if (l >= h->nl) continue;
             F.push_back(&h->lv[l - 1]);
@@ -1409,17 +1438,30 @@ int lockstep_build(h3d_lockstep *b) {
             }
         }
         if (!F.empty())
-            if (int e = tab_rc(transfer_batch_create(F.data(), Cl.data(), dx.data(), (int)F.size(), &b->xfer[l]),
+            if (int e = tab_rc(transfer_batch_create(F.data(), Cl.data(), dx.data(), (int)F.size(), &grp.xfer[l]),
                                "transfers"))
                 return e;
         if (!S.empty())
-            if (int e = tab_rc(coarse_batch_create(S.data(), ds.data(), (int)S.size(), &b->coarse[l]), "coarse level"))
+            if (int e = tab_rc(coarse_batch_create(S.data(), ds.data(), (int)S.size(), &grp.coarse[l]), "coarse level"))
                 return e;
         if (!Z.empty())
-            if (int e = tab_rc(coarsest_batch_create(Z.data(), az.data(), dz.data(), (int)Z.size(), &b->coarsest[l]),
+            if (int e = tab_rc(coarsest_batch_create(Z.data(), az.data(), dz.data(), (int)Z.size(), &grp.coarsest[l]),
                                "coarsest level"))
                 return e;
     }
+    return H3D_OK;
+}
+
+// designs largest first, dealt round-robin to the groups (similar work per branch)
+int lockstep_build(h3d_lockstep *b, int ngroups) {
+    const int n = b->n;
+    std::vector<int> order(n);
+    for (int i = 0; i < n; i++) order[i] = i;
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return b->hs[x]->lv[0].P.nv > b->hs[y]->lv[0].P.nv; });
+    b->groups.resize(ngroups);
+    for (int k = 0; k < n; k++) b->groups[k % ngroups].members.push_back(order[k]);
+    for (LockGroup &g : b->groups) std::sort(g.members.begin(), g.members.end());
     LCK(cudaMalloc(&b->d_active, sizeof(int) * n));
     LCK(cudaMallocHost(&b->h_active, sizeof(int) * n));
     LCK(cudaMalloc(&b->d_norms, sizeof(double) * NCASE * n));
@@ -1429,12 +1471,23 @@ int lockstep_build(h3d_lockstep *b) {
     for (int i = 0; i < n; i++) b->h_active[i] = 1;
     LCK(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
     LCK(cudaEventCreate(&b->ev0));
-    cudaGraph_t g = nullptr;
+    LCK(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    for (size_t k = 0; k < b->groups.size(); k++) {
+        LockGroup &g = b->groups[k];
+        if (int e = lockstep_build_group(b, g)) return e;
+        if (k == 0) {
+            g.stream = b->stream;
+        } else {
+            LCK(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+            LCK(cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming));
+        }
+    }
+    cudaGraph_t gr = nullptr;
     LCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     lockstep_enqueue(b);
-    LCK(cudaStreamEndCapture(b->stream, &g));
-    const cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
-    cudaGraphDestroy(g);
+    LCK(cudaStreamEndCapture(b->stream, &gr));
+    const cudaError_t e = cudaGraphInstantiate(&b->graph, gr, 0);
+    cudaGraphDestroy(gr);
     if (e != cudaSuccess) {
         b->graph = nullptr;
         return lfail(b, H3D_ERR_CUDA, std::string("lockstep graph: ") + cudaGetErrorString(e));
@@ -1514,9 +1567,14 @@ struct LockRun {
 extern "C" {
 
 int h3d_lockstep_create(h3d_handle *const *hs, int n, h3d_lockstep **out) {
+    return h3d_lockstep_create_groups(hs, n, std::min(n, H3D_LOCKSTEP_DEFAULT_GROUPS), out);
+}
+
+int h3d_lockstep_create_groups(h3d_handle *const *hs, int n, int groups, h3d_lockstep **out) {
     if (!out) return H3D_ERR_ARG;
     *out = nullptr;
     if (!hs || n < 1 || n > H3D_LOCKSTEP_MAX) return H3D_ERR_ARG;
+    if (groups < 1 || groups > n) return fail(hs[0], H3D_ERR_ARG, "lockstep: groups must be 1..n");
     for (int i = 0; i < n; i++)
         if (!hs[i]) return H3D_ERR_ARG;
     if (int e = distinct_handles(hs, n)) return e;
@@ -1541,12 +1599,11 @@ int h3d_lockstep_create(h3d_handle *const *hs, int n, h3d_lockstep **out) {
     b->ke = h0->ke;
     b->f32 = h0->cfg.stencil_precision == H3D_STENCIL_FP32;
     b->project = h0->cfg.coarse_mode == H3D_COARSE_PROJECT;
-    for (int i = 0; i < n; i++) b->lmax = std::max(b->lmax, hs[i]->nl);
     if (cudaSetDevice(b->device) != cudaSuccess) {
         delete b;
         return fail(h0, H3D_ERR_CUDA, "cudaSetDevice failed");
     }
-    if (int e = lockstep_build(b)) {
+    if (int e = lockstep_build(b, groups)) {
         fail(h0, e, b->err);
         lockstep_free(b);
         delete b;

@@ -237,7 +237,13 @@ H3D_API int h3d_batch_elastic_matrix(h3d_handle *const *hs, int n, double tol, d
  * handle to the last bit (solve_ms: from the batch's start to the design's end). */
 #define H3D_LOCKSTEP_MAX 64
 typedef struct h3d_lockstep h3d_lockstep;
+/* h3d_lockstep_create_groups with min(n, H3D_LOCKSTEP_DEFAULT_GROUPS) groups */
+#define H3D_LOCKSTEP_DEFAULT_GROUPS 4
 H3D_API int h3d_lockstep_create(h3d_handle *const *hs, int n, h3d_lockstep **out);
+/* groups (1..n): the designs, largest first, are dealt round-robin to groups whose
+ * launches are parallel branches of the batch V-cycle graph, so one group's
+ * launches fill the last partial wave of another's; results do not depend on it */
+H3D_API int h3d_lockstep_create_groups(h3d_handle *const *hs, int n, int groups, h3d_lockstep **out);
 H3D_API int h3d_lockstep_elastic_matrix(h3d_lockstep *b, double tol, double *C, h3d_solve_stats *stats,
                                         int *status);
 H3D_API int h3d_lockstep_destroy(h3d_lockstep *b);

@@ -159,3 +159,29 @@ def test_lockstep_other_modes(torch_cuda, kw):
         _same_stats(hd.last_stats, ref[i][1])
         assert np.array_equal(C[i], ref[i][0]), i
         hd.close()
+
+
+def test_lockstep_groups_give_the_same_result(torch_cuda):
+    """the designs split into 1 to 4 parallel branches of the batch graph: the same
+    C and statistics as one design at a time"""
+    torch = torch_cuda
+    ref = []
+    for n, seed, vol in DESIGNS:
+        hd = H.Homogenization(n, precision=H.PREC_FP32)
+        hd.update(_rho(torch, n, seed, vol))
+        ref.append((hd.elasticMatrix(1e-3), hd.last_stats))
+        hd.close()
+    homs = [H.Homogenization(n, precision=H.PREC_FP32) for n, _, _ in DESIGNS]
+    H.batch_update(homs, [_rho(torch, n, seed, vol) for n, seed, vol in DESIGNS])
+    for groups in (1, 2, 3, 4, len(DESIGNS)):
+        for hd in homs:
+            hd.reset_solutions()
+        with H.Lockstep(homs, groups=groups) as lk:
+            C = lk.elasticMatrix(1e-3)
+        for i, hd in enumerate(homs):
+            _same_stats(hd.last_stats, ref[i][1])
+            assert np.array_equal(C[i], ref[i][0]), (groups, i)
+    with pytest.raises(H.H3DError):
+        H.Lockstep(homs, groups=len(DESIGNS) + 1)
+    for hd in homs:
+        hd.close()
