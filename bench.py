@@ -60,30 +60,67 @@ def parse():
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons sampled every 200 ms in the background."""
+    """SM clocks, power and clock-event (throttle) reasons sampled in the background
+    while the timed region runs: through NVML every 20 ms (read-only queries), or,
+    without NVML, through nvidia-smi every 200 ms."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    BITS = [0x8, 0x40, 0x20, 0x4]  # NVML clock-event reason masks, in NAMES order
 
     def __init__(self, index):
         self.index = index
-        self.rows = []
+        self.rows = []  # (sm MHz, max sm MHz, set of reason names)
         self._stop = threading.Event()
         self._t = None
+        self._nvml = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            h = None
+            try:
+                import torch
+                pr = torch.cuda.get_device_properties(index)
+                bus = "%08x:%02x:%02x.0" % (pr.pci_domain_id, pr.pci_bus_id, pr.pci_device_id)
+                h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+            except Exception:
+                h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self._nvml = (pynvml, h)
+        except Exception:
+            self._nvml = None
+
+    def _sample_nvml(self):
+        nv, h = self._nvml
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        get = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or nv.nvmlDeviceGetCurrentClocksThrottleReasons
+        bits = get(h)
+        return float(sm), float(mx), {n for n, b in zip(self.NAMES, self.BITS) if bits & b}
+
+    def _sample_smi(self):
+        out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
+                              "--format=csv,noheader,nounits"], capture_output=True, text=True,
+                             timeout=5).stdout.strip()
+        if not out:
+            return None
+        r = [c.strip() for c in out.split(",")]
+        sm = float(r[1]) if r[1].replace(".", "").isdigit() else None
+        mx = float(r[2]) if r[2].replace(".", "").isdigit() else None
+        reasons = {self.NAMES[i] for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i] and "Not" not in r[5 + i]}
+        return sm, mx, reasons
 
     def start(self):
         def run():
             while not self._stop.is_set():
                 try:
-                    out = subprocess.run(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + self.FIELDS,
-                                          "--format=csv,noheader,nounits"], capture_output=True, text=True,
-                                         timeout=5).stdout.strip()
-                    if out:
-                        self.rows.append([c.strip() for c in out.split(",")])
+                    row = self._sample_nvml() if self._nvml else self._sample_smi()
+                    if row:
+                        self.rows.append(row)
                 except Exception:
                     pass
-                self._stop.wait(0.2)
+                self._stop.wait(0.02 if self._nvml else 0.2)
         self._t = threading.Thread(target=run, daemon=True)
         self._t.start()
 
@@ -91,13 +128,11 @@ class ClockSampler:
         self._stop.set()
         if self._t:
             self._t.join(timeout=10)
-        sm = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
-        mx = [float(r[2]) for r in self.rows if r[2].replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for r in self.rows for i in range(4) if len(r) > 5 + i and "Active" in r[5 + i]
-                          and "Not" not in r[5 + i]})
+        sm = [r[0] for r in self.rows if r[0] is not None]
+        mx = [r[1] for r in self.rows if r[1] is not None]
+        reasons = sorted(set().union(*[r[2] for r in self.rows])) if self.rows else []
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
-                "reasons": reasons, "samples": len(self.rows)}
+                "reasons": reasons, "samples": len(self.rows), "source": "nvml" if self._nvml else "nvidia-smi"}
 
 
 def dist_init(n):
