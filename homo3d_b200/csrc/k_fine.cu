@@ -483,7 +483,7 @@ __global__ void __launch_bounds__(FBS, RES_MINB) k_fine_residual(FineArgs a, con
 // an ordinary neighbour: its value is held fixed by the correction sweeps, so a
 // nonzero value only translates the solution.  EXACT accumulates the products in
 // FP64 too (the FP32-product form floors near 1e-6 of ||f||, independent of N).
-template <int KC, bool EXACT>
+template <int KC, bool EXACT, int C64 = CPT64>
 __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const KeMat &ke, const KeMat64 &ke64,
                                                        const double *__restrict__ u64, long long p, int cb,
                                                        int kr = KC) {
@@ -491,18 +491,18 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
     const long long me = (long long)K * a.P + p;
     if (K == 7 && p == 0) {
 #pragma unroll
-        for (int q = 0; q < 3 * CPT64; ++q) a.r[fidx(3 * cb + q, me)] = 0.f;
+        for (int q = 0; q < 3 * C64; ++q) a.r[fidx(3 * cb + q, me)] = 0.f;
         return;
     }
     const VertexGeo<KC> g(a, p, K);
     const double *uvp = u64 + fidx(3 * cb, me);
-    double uv[3 * CPT64];
+    double uv[3 * C64];
 #pragma unroll
-    for (int q = 0; q < 3 * CPT64; ++q) uv[q] = __ldg(uvp + q * FVB);
+    for (int q = 0; q < 3 * C64; ++q) uv[q] = __ldg(uvp + q * FVB);
     using Acc = typename std::conditional<EXACT, double, float>::type;
-    Acc acc[3 * CPT64];
+    Acc acc[3 * C64];
 #pragma unroll
-    for (int q = 0; q < 3 * CPT64; ++q) acc[q] = 0;
+    for (int q = 0; q < 3 * C64; ++q) acc[q] = 0;
 #pragma unroll
     for (int d = 0; d < 27; ++d) {
         if (d == 13) continue;
@@ -526,7 +526,7 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
         }
         const double *up = u64 + fidx(3 * cb, nid);  // planes 3cb.. of the neighbour, FVB apart
 #pragma unroll
-        for (int c = 0; c < CPT64; ++c) {
+        for (int c = 0; c < C64; ++c) {
             const Acc d0 = (Acc)(__ldg(up + (3 * c) * FVB) - uv[3 * c]);
             const Acc d1 = (Acc)(__ldg(up + (3 * c + 1) * FVB) - uv[3 * c + 1]);
             const Acc d2 = (Acc)(__ldg(up + (3 * c + 2) * FVB) - uv[3 * c + 2]);
@@ -536,22 +536,23 @@ __device__ __forceinline__ void fine_residual64_vertex(const FineArgs &a, const 
         }
     }
 #pragma unroll
-    for (int q = 0; q < 3 * CPT64; ++q) {
+    for (int q = 0; q < 3 * C64; ++q) {
         const long long o = fidx(3 * cb + q, me);
         a.r[o] = (float)((Acc)a.f[o] - acc[q]);
     }
 }
 
-template <bool EXACT>
-__global__ void __launch_bounds__(FBS, MINB64) k_fine_residual64(FineArgs a, const __grid_constant__ KeMat ke,
+// C64 load cases per thread (NCASE / C64 threads per vertex), MB CTAs per SM
+template <bool EXACT, int C64 = CPT64, int MB = MINB64>
+__global__ void __launch_bounds__(FBS, MB) k_fine_residual64(FineArgs a, const __grid_constant__ KeMat ke,
                                                          const __grid_constant__ KeMat64 ke64,
                                                          const double *__restrict__ u64) {
     long long p;
     int cb, K;
     unsigned bx;
-    colour_task<CPT64>(p, cb, K, bx, blockIdx.x);  // all colours in one launch, colour-minor
+    colour_task<C64>(p, cb, K, bx, blockIdx.x);  // all colours in one launch, colour-minor
     if (p >= a.P) return;
-    fine_residual64_vertex<-1, EXACT>(a, ke, ke64, u64, p, cb, K);
+    fine_residual64_vertex<-1, EXACT, C64>(a, ke, ke64, u64, p, cb, K);
 }
 
 // f(case c) = sum_w (1e-9 + rho_w) * (Ke chi0_c)[rows of the vertex's local node in element w]
