@@ -46,7 +46,7 @@ def parse():
     p.add_argument("--seed", type=int, default=0)
     p.add_argument("--pin-mode", type=int, default=0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--no-north-star", action="store_true", help="skip the mixed-precision arm of the same step")
+    p.add_argument("--no-precision-arms", action="store_true", help="skip the mixed-precision arms of the same step")
     p.add_argument("--workload", default="solve", choices=["solve", "mma", "batch"],
                    help="solve: the homogenization step (default); mma: one MMA design update; "
                         "batch: designs/s of 24 designs of 64^3-128^3 solved together")
@@ -354,14 +354,14 @@ def gpu_arm(args):
             "clocks": clk,
         }
     hd.close()
-    if rank == 0 and world == 1 and args.precision == 0 and not args.no_north_star:
-        result["north_star"] = north_star(args, rho_d, ms_per_solve, vc, c_err, fx)
+    if rank == 0 and world == 1 and args.precision == 0 and not args.no_precision_arms:
+        result["precision_arms"] = precision_arms(args, rho_d, ms_per_solve, vc, c_err, fx)
     if dist is not None:
         dist.destroy_process_group()
     return result
 
 
-def north_star(args, rho_d, plain_ms, plain_vc, plain_err, fx):
+def precision_arms(args, rho_d, plain_ms, plain_vc, plain_err, fx):
     """The precision arms of the same step on the same design, device-timed like the
     headline value: the plain arm (the headline: refined FP32 V-cycles, SIMT
     operator, FP64-accumulated refinement residual) against the mixed arms
