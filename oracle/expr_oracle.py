@@ -1,6 +1,6 @@
 """FP64 numpy restatement of the reference expression layer's radial convolution.
 
-TEST INFRASTRUCTURE ONLY (imported by tests/): the checker of h3d_conv_radial and of
+TEST INFRASTRUCTURE ONLY (imported by tests/): the oracle for h3d_conv_radial and for
 the shear-isotropy MMA loop.  Follows homo3d AutoDiff/TensorExpression.h:1002-1044
 (the Spline4 weight w = 1 - 6 q + 8 q^1.5 - 3 q^2, q = |o|^2 / r^2 < 1, window
 half-width (int)(r + 0.5)) and AutoDiff/TensorExpression.cuh:288-369 (conv_kernel:

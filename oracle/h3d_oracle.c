@@ -1,7 +1,7 @@
 /*
  * h3d_oracle.c -- FP64 CPU restatement of the homo3d periodic-homogenization hot path.
  *
- * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA library
+ * TEST INFRASTRUCTURE ONLY.  This file is the oracle for the CUDA library
  * (homo3d_b200/csrc) and the timed CPU baseline of bench.py.  Nothing in the
  * product links it or calls it.
  *

@@ -1,6 +1,6 @@
 """FP64 numpy restatement of the reference's trig-basis initial density.
 
-TEST INFRASTRUCTURE ONLY (imported by tests/): the checker of the library's
+TEST INFRASTRUCTURE ONLY (imported by tests/): the oracle for the library's
 h3d_init_density_trig.  Follows homo3d homogenization/Framework.cuh:106-222
 (randTribase_sincos_kernel: the basis sum, positions p = (x, y, z) / (dim - 1),
 optionally centred and rotated by a quaternion) and Framework.cuh:238-310 (randTri:

@@ -2,7 +2,7 @@
  * mma_oracle.c -- FP64 CPU restatement of the reference's MMA update
  * (Svanberg's method of moving asymptotes, the 2007 mmasub/subsolv scheme).
  *
- * TEST INFRASTRUCTURE ONLY.  The checker of the CUDA MMA update in
+ * TEST INFRASTRUCTURE ONLY.  The oracle for the CUDA MMA update in
  * homo3d_b200/csrc/k_mma.cu; nothing in the product links it.
  *
  * Follows lavenklau/homo3d optimization/mmaOpt.cu:

@@ -1,6 +1,6 @@
 """NumPy restatement of the learned warm-start network (homo3d_b200/csrc/k_warmnet.cu).
 
-TEST INFRASTRUCTURE ONLY: the checker of the CUDA forward pass and gradients.
+TEST INFRASTRUCTURE ONLY: the oracle for the CUDA forward pass and gradients.
 There is no reference counterpart; this file is pinned by central finite
 differences of its own loss (tests/test_warmnet_oracle.py).
 
