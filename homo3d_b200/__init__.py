@@ -111,6 +111,8 @@ _SIGS = {
     "h3d_lockstep_create_groups": [ctypes.POINTER(_vp), ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp)],
     "h3d_lockstep_elastic_matrix": [_vp, ctypes.c_double, _dp, ctypes.POINTER(SolveStats), _ip],
     "h3d_lockstep_destroy": [_vp],
+    "h3d_lockstep_set_shapes": [_vp, ctypes.c_int, ctypes.c_int],
+    "h3d_lockstep_autotune": [_vp],
     "h3d_penalize": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float],
     "h3d_penalize_backward": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float],
     "h3d_oc_update": [_vp, _vp, _vp, ctypes.c_int64, ctypes.c_float, ctypes.c_float, ctypes.c_float,
@@ -700,6 +702,18 @@ class Lockstep:
             if status[i] not in (H3D_OK, H3D_NOT_CONVERGED):
                 raise H3DError(int(status[i]), "design %d: %s" % (i, lib().h3d_last_error(h._h).decode()))
         return C.reshape(n, 6, 6)
+
+    def autotune(self):
+        """time both launch shapes of every group and level on scratch fields, keep the faster"""
+        code = lib().h3d_lockstep_autotune(self._b)
+        if code != H3D_OK:
+            raise H3DError(code, lib().h3d_lockstep_last_error(self._b).decode())
+
+    def set_shapes(self, fine_shape, coarse_shape):
+        """force the sweeps' launch shapes (0 or 1; 0 and 0 by default)"""
+        code = lib().h3d_lockstep_set_shapes(self._b, int(fine_shape), int(coarse_shape))
+        if code != H3D_OK:
+            raise H3DError(code, lib().h3d_lockstep_last_error(self._b).decode())
 
     def close(self):
         if getattr(self, "_b", None):

@@ -1300,6 +1300,9 @@ int h3d_batch_elastic_matrix(h3d_handle *const *hs, int n, double tol, double *C
 struct LockGroup {
     std::vector<int> members;  // indices into the batch
     int lmax = 0;
+    // launch shapes of the sweeps: level 0, and each coarse level (timed at creation)
+    int fine_shape = 0;
+    int coarse_shape[MAXLV] = {};
     BatchTab fine, norm;
     BatchTab coarse[MAXLV], xfer[MAXLV], coarsest[MAXLV];
     cudaStream_t stream = nullptr;  // capture stream of the branch (the batch stream for group 0)
@@ -1363,17 +1366,17 @@ void lockstep_free(h3d_lockstep *b) {
 
 // one group's share of the batch V-cycle on stream s
 void lockstep_enqueue_group(const h3d_lockstep *b, const LockGroup &g, cudaStream_t s) {
-    launch_fine_sweep_batch(g.fine, b->ke, b->d_active, true, s);
+    launch_fine_sweep_batch(g.fine, b->ke, b->d_active, true, g.fine_shape, s);
     for (int l = 1; l < g.lmax; l++) {
         if (g.xfer[l].n) launch_restrict_batch(g.xfer[l], b->d_active, s);
-        if (g.coarse[l].n) launch_coarse_sweep_batch(g.coarse[l], b->f32, b->d_active, true, s);
+        if (g.coarse[l].n) launch_coarse_sweep_batch(g.coarse[l], b->f32, b->d_active, true, g.coarse_shape[l], s);
         if (g.coarsest[l].n) launch_coarse_apply_batch(g.coarsest[l], b->d_active, b->project, s);
     }
     for (int l = g.lmax - 2; l >= 0; l--) {
         if (!g.xfer[l + 1].n) continue;
         launch_prolong_batch(g.xfer[l + 1], b->d_active, l == 0, s);
-        if (l == 0) launch_fine_sweep_batch(g.fine, b->ke, b->d_active, false, s);
-        else launch_coarse_sweep_batch(g.coarse[l], b->f32, b->d_active, false, s);
+        if (l == 0) launch_fine_sweep_batch(g.fine, b->ke, b->d_active, false, g.fine_shape, s);
+        else launch_coarse_sweep_batch(g.coarse[l], b->f32, b->d_active, false, g.coarse_shape[l], s);
     }
     launch_pin_deflate_batch(g.fine, b->ke, b->d_active, s);
     launch_norm_finish_batch(g.norm, b->d_active, b->d_norms, s);
@@ -1414,7 +1417,8 @@ int lockstep_build_group(h3d_lockstep *b, LockGroup &grp) {
         grp.lmax = std::max(grp.lmax, h->nl);
     }
     const int m = (int)grp.members.size();
-    if (int e = tab_rc(fine_batch_create(a.data(), rho.data(), part.data(), state.data(), des.data(), m, &grp.fine),
+    if (int e = tab_rc(fine_batch_create(a.data(), rho.data(), part.data(), state.data(), des.data(), m, false,
+                                         &grp.fine),
                        "level 0"))
         return e;
     if (int e = tab_rc(norm_batch_create(part.data(), nblk.data(), des.data(), m, &grp.norm), "norms")) return e;
@@ -1442,7 +1446,8 @@ int lockstep_build_group(h3d_lockstep *b, LockGroup &grp) {
                                "transfers"))
                 return e;
         if (!S.empty())
-            if (int e = tab_rc(coarse_batch_create(S.data(), ds.data(), (int)S.size(), &grp.coarse[l]), "coarse level"))
+            if (int e = tab_rc(coarse_batch_create(S.data(), ds.data(), (int)S.size(), false, &grp.coarse[l]),
+                               "coarse level"))
                 return e;
         if (!Z.empty())
             if (int e = tab_rc(coarsest_batch_create(Z.data(), az.data(), dz.data(), (int)Z.size(), &grp.coarsest[l]),
@@ -1450,6 +1455,100 @@ int lockstep_build_group(h3d_lockstep *b, LockGroup &grp) {
                 return e;
     }
     return H3D_OK;
+}
+
+// the batch V-cycle graph with the groups' current launch shapes
+int lockstep_capture(h3d_lockstep *b) {
+    if (b->graph) {
+        cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+    }
+    cudaGraph_t gr = nullptr;
+    LCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    lockstep_enqueue(b);
+    LCK(cudaStreamEndCapture(b->stream, &gr));
+    const cudaError_t e = cudaGraphInstantiate(&b->graph, gr, 0);
+    cudaGraphDestroy(gr);
+    if (e != cudaSuccess) {
+        b->graph = nullptr;
+        return lfail(b, H3D_ERR_CUDA, std::string("lockstep graph: ") + cudaGetErrorString(e));
+    }
+    return H3D_OK;
+}
+
+// the launch shape of each group's sweeps, level by level: both shapes timed on the
+// group's designs with the sweeps iterating on each design's residual field (which
+// every V-cycle rewrites before reading it), the faster one kept; the results do
+// not depend on the choice
+int lockstep_tune(h3d_lockstep *b) {
+    cudaStream_t s = b->stream;
+    cudaEvent_t t0 = nullptr, t1 = nullptr;
+    LCK(cudaEventCreate(&t0));
+    LCK(cudaEventCreate(&t1));
+    LCK(cudaMemcpyAsync(b->d_active, b->h_active, sizeof(int) * b->n, cudaMemcpyHostToDevice, s));
+    int rc = H3D_OK;
+    auto pick = [&](auto &&sweep) -> int {  // the faster of shapes 0 and 1, -1 on failure
+        float best = 0;
+        int which = 0;
+        for (int shape = 0; shape < 2; shape++) {
+            sweep(shape);
+            if (cudaEventRecord(t0, s) != cudaSuccess) return -1;
+            for (int r = 0; r < 3; r++) sweep(shape);
+            if (cudaEventRecord(t1, s) != cudaSuccess || cudaEventSynchronize(t1) != cudaSuccess) return -1;
+            if (cudaGetLastError() != cudaSuccess) return -1;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, t0, t1);
+            if (shape == 0 || ms < best) { best = ms; which = shape; }
+        }
+        return which;
+    };
+    for (LockGroup &g : b->groups) {
+        std::vector<const Level *> a;
+        std::vector<const float *> rho;
+        std::vector<double *> part, state;
+        std::vector<int> des;
+        for (int i : g.members) {
+            h3d_handle *h = b->hs[i];
+            a.push_back(&h->lv[0]);
+            rho.push_back(h->rho);
+            part.push_back(h->partial);
+            state.push_back(h->pin_state);
+            des.push_back(i);
+        }
+        BatchTab tmp;
+        if (fine_batch_create(a.data(), rho.data(), part.data(), state.data(), des.data(), (int)a.size(), true,
+                              &tmp) != 0) {
+            rc = lfail(b, H3D_ERR_NOMEM, "lockstep tuning table");
+            break;
+        }
+        const int fs = pick([&](int shape) { launch_fine_sweep_batch(tmp, b->ke, b->d_active, false, shape, s); });
+        batch_tab_free(tmp);
+        if (fs < 0) { rc = lfail(b, H3D_ERR_CUDA, "lockstep tuning launch failed"); break; }
+        g.fine_shape = fs;
+        for (int l = 1; l < g.lmax && rc == H3D_OK; l++) {
+            if (!g.coarse[l].n) continue;
+            std::vector<const Level *> S;
+            std::vector<int> ds;
+            for (int i : g.members)
+                if (l < b->hs[i]->nl - 1) {
+                    S.push_back(&b->hs[i]->lv[l]);
+                    ds.push_back(i);
+                }
+            BatchTab ct;
+            if (coarse_batch_create(S.data(), ds.data(), (int)S.size(), true, &ct) != 0) {
+                rc = lfail(b, H3D_ERR_NOMEM, "lockstep tuning table");
+                break;
+            }
+            const int cs = pick([&](int shape) { launch_coarse_sweep_batch(ct, b->f32, b->d_active, false, shape, s); });
+            batch_tab_free(ct);
+            if (cs < 0) rc = lfail(b, H3D_ERR_CUDA, "lockstep tuning launch failed");
+            else g.coarse_shape[l] = cs;
+        }
+        if (rc != H3D_OK) break;
+    }
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    return rc;
 }
 
 // designs largest first, dealt round-robin to the groups (similar work per branch)
@@ -1482,17 +1581,7 @@ int lockstep_build(h3d_lockstep *b, int ngroups) {
             LCK(cudaEventCreateWithFlags(&g.join, cudaEventDisableTiming));
         }
     }
-    cudaGraph_t gr = nullptr;
-    LCK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-    lockstep_enqueue(b);
-    LCK(cudaStreamEndCapture(b->stream, &gr));
-    const cudaError_t e = cudaGraphInstantiate(&b->graph, gr, 0);
-    cudaGraphDestroy(gr);
-    if (e != cudaSuccess) {
-        b->graph = nullptr;
-        return lfail(b, H3D_ERR_CUDA, std::string("lockstep graph: ") + cudaGetErrorString(e));
-    }
-    return H3D_OK;
+    return lockstep_capture(b);
 }
 
 // one design of a lockstep solve: SolveRun's FP32 branch with the stale residual
@@ -1611,6 +1700,27 @@ int h3d_lockstep_create_groups(h3d_handle *const *hs, int n, int groups, h3d_loc
     }
     *out = b;
     return H3D_OK;
+}
+
+int h3d_lockstep_autotune(h3d_lockstep *b) {
+    if (!b) return H3D_ERR_ARG;
+    LCK(cudaSetDevice(b->device));
+    LCK(cudaStreamSynchronize(b->stream));
+    if (int e = lockstep_tune(b)) return e;
+    return lockstep_capture(b);
+}
+
+int h3d_lockstep_set_shapes(h3d_lockstep *b, int fine_shape, int coarse_shape) {
+    if (!b) return H3D_ERR_ARG;
+    if (fine_shape < 0 || fine_shape > 1 || coarse_shape < 0 || coarse_shape > 1)
+        return lfail(b, H3D_ERR_ARG, "lockstep launch shapes are 0 or 1");
+    LCK(cudaSetDevice(b->device));
+    LCK(cudaStreamSynchronize(b->stream));
+    for (LockGroup &g : b->groups) {
+        g.fine_shape = fine_shape;
+        for (int l = 0; l < MAXLV; l++) g.coarse_shape[l] = coarse_shape;
+    }
+    return lockstep_capture(b);
 }
 
 int h3d_lockstep_destroy(h3d_lockstep *b) {

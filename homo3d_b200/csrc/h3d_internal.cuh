@@ -368,16 +368,20 @@ void launch_warmnet_to_chi(const Planes &P, const float *y, int R, double *chi, 
 // copy a table to the device (not inside a stream capture) and return 0, -1 for a
 // slot count outside 1..BATCH_MAX, -2 if the device table cannot be allocated.
 // design[i]: slot i's index in the `active` flags the launches read.
-// level 0 of each design: the sweep (shape 0), the seven-colour residual and the
-// deflation (state: the design's deflation state)
+// level 0 of each design: the sweep (launch shape 0: six cases per thread, 1: three),
+// the seven-colour residual and the deflation (state: the design's deflation
+// state); scratch: the sweeps iterate on each design's r instead of u (timing)
 int fine_batch_create(const Level *const *lv0, const float *const *rho, double *const *partial,
-                      double *const *state, const int *design, int n, BatchTab *out);
-void launch_fine_sweep_batch(const BatchTab &t, const KeMat &ke, const int *active, bool residual, cudaStream_t s);
+                      double *const *state, const int *design, int n, bool scratch, BatchTab *out);
+void launch_fine_sweep_batch(const BatchTab &t, const KeMat &ke, const int *active, bool residual, int shape,
+                             cudaStream_t s);
 void launch_pin_deflate_batch(const BatchTab &t, const KeMat &ke, const int *active, cudaStream_t s);
 // one coarse level of each design (all with the same stencil precision): the
-// sweep (shape 0), with residual the down leg's sweep and residual
-int coarse_batch_create(const Level *const *lv, const int *design, int n, BatchTab *out);
-void launch_coarse_sweep_batch(const BatchTab &t, bool f32, const int *active, bool residual, cudaStream_t s);
+// sweep (launch shape 0: two cases per thread, 1: six), with residual the down
+// leg's sweep and residual; scratch as for level 0
+int coarse_batch_create(const Level *const *lv, const int *design, int n, bool scratch, BatchTab *out);
+void launch_coarse_sweep_batch(const BatchTab &t, bool f32, const int *active, bool residual, int shape,
+                               cudaStream_t s);
 // ratio-2 transfers between levels F[i] (even) and C[i]: restriction of F.r into
 // C.f with C.u cleared, prolongation of C.u into F.u (is_root: F is level 0)
 int transfer_batch_create(const Level *const *F, const Level *const *C, const int *design, int n, BatchTab *out);

@@ -1023,20 +1023,24 @@ struct CoarseEnt {
     int design;
 };
 struct CoarseBatchTab {
-    BatchSlices gs;   // CTAs of one colour of the sweep
+    BatchSlices gs;   // CTAs of one colour of the sweep, two cases per thread
+    BatchSlices gs6;  // the same with six cases per thread
     BatchSlices res;  // CTAs of the seven-colour residual
     CoarseEnt e[BATCH_MAX];
 };
 
-template <int K, bool F32, bool RES>
-__global__ void __launch_bounds__(128, BATCH_MINB) k_coarse_gs_batch(const CoarseBatchTab *__restrict__ t,
-                                                                   const int *__restrict__ active) {
+// C cases per thread at MB CTAs per SM: launch shape 0 (C = 2, 6 CTAs/SM) or 1
+// (C = 6, 4 CTAs/SM)
+template <int K, bool F32, bool RES, int C, int MB>
+__global__ void __launch_bounds__(128, MB) k_coarse_gs_batch(const CoarseBatchTab *__restrict__ t,
+                                                           const int *__restrict__ active) {
     __shared__ __align__(16) unsigned buf[sizeof(CoarseArgs) / 4];
-    const int i = batch_slice(t->gs, blockIdx.x);
+    const BatchSlices &sl = C == BATCH_CPT ? t->gs : t->gs6;
+    const int i = batch_slice(sl, blockIdx.x);
     const CoarseEnt &en = t->e[i];
     if (!__ldg(&active[en.design])) return;
     const CoarseArgs &a = stage_args(en.a, buf);
-    coarse_gs_block<K, F32, BATCH_CPT, RES>(a, blockIdx.x - __ldg(&t->gs.start[i]));
+    coarse_gs_block<K, F32, C, RES>(a, blockIdx.x - __ldg(&sl.start[i]));
 }
 
 template <bool F32>
@@ -1063,49 +1067,58 @@ static int upload_tab(const Tab &t, int n, BatchTab *out) {
     return 0;
 }
 
-int coarse_batch_create(const Level *const *lv, const int *design, int n, BatchTab *out) {
+int coarse_batch_create(const Level *const *lv, const int *design, int n, bool scratch, BatchTab *out) {
     if (n < 1 || n > BATCH_MAX) return -1;
     CoarseBatchTab *t = new CoarseBatchTab();
-    t->gs.n = t->res.n = n;
-    t->gs.start[0] = t->res.start[0] = 0;
+    t->gs.n = t->gs6.n = t->res.n = n;
+    t->gs.start[0] = t->gs6.start[0] = t->res.start[0] = 0;
     for (int i = 0; i < n; i++) {
         t->e[i].a = make_cargs(*lv[i]);
+        if (scratch) t->e[i].a.u = t->e[i].a.r;
         t->e[i].design = design[i];
-        const unsigned nb = (unsigned)((t->e[i].a.P + 127) / 128) * (NCASE / BATCH_CPT);
+        const unsigned vb = (unsigned)((t->e[i].a.P + 127) / 128), nb = vb * (NCASE / BATCH_CPT);
         t->gs.start[i + 1] = t->gs.start[i] + nb;
+        t->gs6.start[i + 1] = t->gs6.start[i] + vb;
         t->res.start[i + 1] = t->res.start[i] + nb * 7;
     }
     const int rc = upload_tab(*t, n, out);
     if (rc == 0) {
         out->grid[0] = t->gs.start[n];
         out->grid[1] = t->res.start[n];
+        out->grid[2] = t->gs6.start[n];
     }
     delete t;
     return rc;
 }
 
-template <bool F32>
+template <bool F32, int C, int MB>
 static void coarse_sweep_batch(const BatchTab &t, const int *active, bool residual, cudaStream_t s) {
     const CoarseBatchTab *d = static_cast<const CoarseBatchTab *>(t.dev);
-    const unsigned g = t.grid[0];
-    k_coarse_gs_batch<0, F32, false><<<g, 128, 0, s>>>(d, active);
-    k_coarse_gs_batch<1, F32, false><<<g, 128, 0, s>>>(d, active);
-    k_coarse_gs_batch<2, F32, false><<<g, 128, 0, s>>>(d, active);
-    k_coarse_gs_batch<3, F32, false><<<g, 128, 0, s>>>(d, active);
-    k_coarse_gs_batch<4, F32, false><<<g, 128, 0, s>>>(d, active);
-    k_coarse_gs_batch<5, F32, false><<<g, 128, 0, s>>>(d, active);
-    k_coarse_gs_batch<6, F32, false><<<g, 128, 0, s>>>(d, active);
+    const unsigned g = C == BATCH_CPT ? t.grid[0] : t.grid[2];
+    k_coarse_gs_batch<0, F32, false, C, MB><<<g, 128, 0, s>>>(d, active);
+    k_coarse_gs_batch<1, F32, false, C, MB><<<g, 128, 0, s>>>(d, active);
+    k_coarse_gs_batch<2, F32, false, C, MB><<<g, 128, 0, s>>>(d, active);
+    k_coarse_gs_batch<3, F32, false, C, MB><<<g, 128, 0, s>>>(d, active);
+    k_coarse_gs_batch<4, F32, false, C, MB><<<g, 128, 0, s>>>(d, active);
+    k_coarse_gs_batch<5, F32, false, C, MB><<<g, 128, 0, s>>>(d, active);
+    k_coarse_gs_batch<6, F32, false, C, MB><<<g, 128, 0, s>>>(d, active);
     if (residual) {
-        k_coarse_gs_batch<7, F32, true><<<g, 128, 0, s>>>(d, active);
+        k_coarse_gs_batch<7, F32, true, C, MB><<<g, 128, 0, s>>>(d, active);
         k_coarse_residual_batch<F32><<<t.grid[1], 128, 0, s>>>(d, active);
     } else {
-        k_coarse_gs_batch<7, F32, false><<<g, 128, 0, s>>>(d, active);
+        k_coarse_gs_batch<7, F32, false, C, MB><<<g, 128, 0, s>>>(d, active);
     }
 }
 
-void launch_coarse_sweep_batch(const BatchTab &t, bool f32, const int *active, bool residual, cudaStream_t s) {
-    if (f32) coarse_sweep_batch<true>(t, active, residual, s);
-    else coarse_sweep_batch<false>(t, active, residual, s);
+void launch_coarse_sweep_batch(const BatchTab &t, bool f32, const int *active, bool residual, int shape,
+                               cudaStream_t s) {
+    if (f32) {
+        if (shape == 1) coarse_sweep_batch<true, 6, 4>(t, active, residual, s);
+        else coarse_sweep_batch<true, BATCH_CPT, BATCH_MINB>(t, active, residual, s);
+    } else {
+        if (shape == 1) coarse_sweep_batch<false, 6, 4>(t, active, residual, s);
+        else coarse_sweep_batch<false, BATCH_CPT, BATCH_MINB>(t, active, residual, s);
+    }
 }
 
 // ratio-2 transfers: one slice of ceil(C.nv / 256) CTAs per design for both

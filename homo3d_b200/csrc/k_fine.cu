@@ -892,22 +892,28 @@ struct FineEnt {
     int design;       // its index in the active flags
 };
 struct FineBatchTab {
-    BatchSlices gs;   // CTAs of one colour of the sweep
+    BatchSlices gs;   // CTAs of one colour of the sweep, six cases per thread
+    BatchSlices gs3;  // the same with three cases per thread
     BatchSlices res;  // CTAs of the seven-colour residual
     FineEnt e[BATCH_MAX];
 };
 
-template <int K, bool RES>
-__global__ void __launch_bounds__(FBS, 4) k_fine_gs_batch(const FineBatchTab *__restrict__ t,
-                                                        const int *__restrict__ active,
-                                                        const __grid_constant__ KeMat ke) {
+// C cases per thread at MB CTAs per SM: launch shape 0 (C = 6, 4 CTAs/SM) or 1
+// (C = 3, 5 CTAs/SM, one case pair and one scalar case per thread); the colour that
+// writes the residual runs with six cases per thread in both
+template <int K, bool RES, int C, int MB>
+__global__ void __launch_bounds__(FBS, MB) k_fine_gs_batch(const FineBatchTab *__restrict__ t,
+                                                         const int *__restrict__ active,
+                                                         const __grid_constant__ KeMat ke) {
+    static_assert(!RES || C == 6, "the residual-writing colour runs six cases per thread");
     __shared__ __align__(16) unsigned buf[(sizeof(FineArgs) + 3) / 4];
-    const int i = batch_slice(t->gs, blockIdx.x);
+    const BatchSlices &sl = C == 6 ? t->gs : t->gs3;
+    const int i = batch_slice(sl, blockIdx.x);
     const FineEnt &en = t->e[i];
     if (!__ldg(&active[en.design])) return;
     const FineArgs &a = stage_args(en.a, buf);
-    const unsigned b0 = __ldg(&t->gs.start[i]), b1 = __ldg(&t->gs.start[i + 1]);
-    fine_gs_block<K, 6, RES>(a, ke, en.partial, blockIdx.x - b0, b1 - b0);
+    const unsigned b0 = __ldg(&sl.start[i]), b1 = __ldg(&sl.start[i + 1]);
+    fine_gs_block<K, C, RES>(a, ke, en.partial, blockIdx.x - b0, b1 - b0);
 }
 
 __global__ void __launch_bounds__(FBS, RES_MINB) k_fine_residual_batch(const FineBatchTab *__restrict__ t,
@@ -934,17 +940,19 @@ __global__ void __launch_bounds__(PIN_THREADS) k_pin_deflate_batch(const FineBat
 }
 
 int fine_batch_create(const Level *const *lv0, const float *const *rho, double *const *partial,
-                      double *const *state, const int *design, int n, BatchTab *out) {
+                      double *const *state, const int *design, int n, bool scratch, BatchTab *out) {
     if (n < 1 || n > BATCH_MAX) return -1;
     FineBatchTab *t = new FineBatchTab();
-    t->gs.n = t->res.n = n;
-    t->gs.start[0] = t->res.start[0] = 0;
+    t->gs.n = t->gs3.n = t->res.n = n;
+    t->gs.start[0] = t->gs3.start[0] = t->res.start[0] = 0;
     for (int i = 0; i < n; i++) {
         t->e[i].a = make_args(*lv0[i], rho[i]);
+        if (scratch) t->e[i].a.u = t->e[i].a.r;
         t->e[i].partial = partial[i];
         t->e[i].state = state[i];
         t->e[i].design = design[i];
         t->gs.start[i + 1] = t->gs.start[i] + task_blocks(t->e[i].a, 6);
+        t->gs3.start[i + 1] = t->gs3.start[i] + task_blocks(t->e[i].a, 3);
         t->res.start[i + 1] = t->res.start[i] + task_blocks(t->e[i].a, CPT) * 7;
     }
     void *d = nullptr;
@@ -955,6 +963,7 @@ int fine_batch_create(const Level *const *lv0, const float *const *rho, double *
         out->n = n;
         out->grid[0] = t->gs.start[n];
         out->grid[1] = t->res.start[n];
+        out->grid[2] = t->gs3.start[n];
     } else if (d) {
         cudaFree(d);
     }
@@ -962,22 +971,29 @@ int fine_batch_create(const Level *const *lv0, const float *const *rho, double *
     return rc;
 }
 
-void launch_fine_sweep_batch(const BatchTab &t, const KeMat &ke, const int *active, bool residual, cudaStream_t s) {
+template <int C, int MB>
+static void fine_sweep_batch(const BatchTab &t, const KeMat &ke, const int *active, bool residual, cudaStream_t s) {
     const FineBatchTab *d = static_cast<const FineBatchTab *>(t.dev);
-    const unsigned g = t.grid[0];
-    k_fine_gs_batch<0, false><<<g, FBS, 0, s>>>(d, active, ke);
-    k_fine_gs_batch<1, false><<<g, FBS, 0, s>>>(d, active, ke);
-    k_fine_gs_batch<2, false><<<g, FBS, 0, s>>>(d, active, ke);
-    k_fine_gs_batch<3, false><<<g, FBS, 0, s>>>(d, active, ke);
-    k_fine_gs_batch<4, false><<<g, FBS, 0, s>>>(d, active, ke);
-    k_fine_gs_batch<5, false><<<g, FBS, 0, s>>>(d, active, ke);
-    k_fine_gs_batch<6, false><<<g, FBS, 0, s>>>(d, active, ke);
+    const unsigned g = C == 6 ? t.grid[0] : t.grid[2];
+    k_fine_gs_batch<0, false, C, MB><<<g, FBS, 0, s>>>(d, active, ke);
+    k_fine_gs_batch<1, false, C, MB><<<g, FBS, 0, s>>>(d, active, ke);
+    k_fine_gs_batch<2, false, C, MB><<<g, FBS, 0, s>>>(d, active, ke);
+    k_fine_gs_batch<3, false, C, MB><<<g, FBS, 0, s>>>(d, active, ke);
+    k_fine_gs_batch<4, false, C, MB><<<g, FBS, 0, s>>>(d, active, ke);
+    k_fine_gs_batch<5, false, C, MB><<<g, FBS, 0, s>>>(d, active, ke);
+    k_fine_gs_batch<6, false, C, MB><<<g, FBS, 0, s>>>(d, active, ke);
     if (residual) {
-        k_fine_gs_batch<7, true><<<g, FBS, 0, s>>>(d, active, ke);
+        k_fine_gs_batch<7, true, 6, 4><<<t.grid[0], FBS, 0, s>>>(d, active, ke);
         k_fine_residual_batch<<<t.grid[1], FBS, 0, s>>>(d, active, ke);
     } else {
-        k_fine_gs_batch<7, false><<<g, FBS, 0, s>>>(d, active, ke);
+        k_fine_gs_batch<7, false, C, MB><<<g, FBS, 0, s>>>(d, active, ke);
     }
+}
+
+void launch_fine_sweep_batch(const BatchTab &t, const KeMat &ke, const int *active, bool residual, int shape,
+                             cudaStream_t s) {
+    if (shape == 1) fine_sweep_batch<3, 5>(t, ke, active, residual, s);
+    else fine_sweep_batch<6, 4>(t, ke, active, residual, s);
 }
 
 void launch_pin_deflate_batch(const BatchTab &t, const KeMat &ke, const int *active, cudaStream_t s) {

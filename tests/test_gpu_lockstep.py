@@ -185,3 +185,39 @@ def test_lockstep_groups_give_the_same_result(torch_cuda):
         H.Lockstep(homs, groups=len(DESIGNS) + 1)
     for hd in homs:
         hd.close()
+
+
+def test_lockstep_launch_shapes_give_the_same_result(torch_cuda):
+    """every combination of the sweeps' two launch shapes (level 0: six or three
+    cases per thread; coarse levels: two or six) against one design at a time"""
+    torch = torch_cuda
+    ref = []
+    for n, seed, vol in DESIGNS:
+        hd = H.Homogenization(n, precision=H.PREC_FP32)
+        hd.update(_rho(torch, n, seed, vol))
+        ref.append((hd.elasticMatrix(1e-3), hd.last_stats))
+        hd.close()
+    homs = [H.Homogenization(n, precision=H.PREC_FP32) for n, _, _ in DESIGNS]
+    H.batch_update(homs, [_rho(torch, n, seed, vol) for n, seed, vol in DESIGNS])
+    with H.Lockstep(homs) as lk:
+        for shapes in ((0, 0), (1, 0), (0, 1), (1, 1)):
+            for hd in homs:
+                hd.reset_solutions()
+            lk.set_shapes(*shapes)
+            C = lk.elasticMatrix(1e-3)
+            for i, hd in enumerate(homs):
+                _same_stats(hd.last_stats, ref[i][1])
+                assert np.array_equal(C[i], ref[i][0]), (shapes, i)
+        for hd in homs:
+            hd.reset_solutions()
+        lk.autotune()  # whatever it picks, the same results
+        C = lk.elasticMatrix(1e-3)
+        for i, hd in enumerate(homs):
+            _same_stats(hd.last_stats, ref[i][1])
+            assert np.array_equal(C[i], ref[i][0]), ("tuned", i)
+        for bad in ((2, 0), (0, -1)):
+            with pytest.raises(H.H3DError) as ei:
+                lk.set_shapes(*bad)
+            assert ei.value.code == H.H3D_ERR_ARG
+    for hd in homs:
+        hd.close()
