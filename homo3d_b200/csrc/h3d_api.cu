@@ -1476,33 +1476,26 @@ int lockstep_capture(h3d_lockstep *b) {
     return H3D_OK;
 }
 
-// the launch shape of each group's sweeps, level by level: both shapes timed on the
-// group's designs with the sweeps iterating on each design's residual field (which
-// every V-cycle rewrites before reading it), the faster one kept; the results do
-// not depend on the choice
+// the launch shape of the sweeps, level by level: both shapes timed with the
+// sweeps of every group running together on the groups' streams, as in the batch
+// graph, each iterating on its designs' residual fields (which every V-cycle
+// rewrites before reading them); shape 1 is kept for all groups where it is at least
+// 2 % faster.  The results do not depend on the choice
 int lockstep_tune(h3d_lockstep *b) {
     cudaStream_t s = b->stream;
+    const int ng = (int)b->groups.size();
     cudaEvent_t t0 = nullptr, t1 = nullptr;
     LCK(cudaEventCreate(&t0));
     LCK(cudaEventCreate(&t1));
     LCK(cudaMemcpyAsync(b->d_active, b->h_active, sizeof(int) * b->n, cudaMemcpyHostToDevice, s));
+    int lmax = 0;
+    for (const LockGroup &g : b->groups) lmax = std::max(lmax, g.lmax);
+    // scratch tables: level 0 and every coarse level of every group
+    std::vector<BatchTab> fine(ng);
+    std::vector<std::vector<BatchTab>> coarse(ng, std::vector<BatchTab>(MAXLV));
     int rc = H3D_OK;
-    auto pick = [&](auto &&sweep) -> int {  // the faster of shapes 0 and 1, -1 on failure
-        float best = 0;
-        int which = 0;
-        for (int shape = 0; shape < 2; shape++) {
-            sweep(shape);
-            if (cudaEventRecord(t0, s) != cudaSuccess) return -1;
-            for (int r = 0; r < 3; r++) sweep(shape);
-            if (cudaEventRecord(t1, s) != cudaSuccess || cudaEventSynchronize(t1) != cudaSuccess) return -1;
-            if (cudaGetLastError() != cudaSuccess) return -1;
-            float ms = 0;
-            cudaEventElapsedTime(&ms, t0, t1);
-            if (shape == 0 || ms < best) { best = ms; which = shape; }
-        }
-        return which;
-    };
-    for (LockGroup &g : b->groups) {
+    for (int k = 0; k < ng && rc == H3D_OK; k++) {
+        const LockGroup &g = b->groups[k];
         std::vector<const Level *> a;
         std::vector<const float *> rho;
         std::vector<double *> part, state;
@@ -1515,16 +1508,9 @@ int lockstep_tune(h3d_lockstep *b) {
             state.push_back(h->pin_state);
             des.push_back(i);
         }
-        BatchTab tmp;
         if (fine_batch_create(a.data(), rho.data(), part.data(), state.data(), des.data(), (int)a.size(), true,
-                              &tmp) != 0) {
+                              &fine[k]) != 0)
             rc = lfail(b, H3D_ERR_NOMEM, "lockstep tuning table");
-            break;
-        }
-        const int fs = pick([&](int shape) { launch_fine_sweep_batch(tmp, b->ke, b->d_active, false, shape, s); });
-        batch_tab_free(tmp);
-        if (fs < 0) { rc = lfail(b, H3D_ERR_CUDA, "lockstep tuning launch failed"); break; }
-        g.fine_shape = fs;
         for (int l = 1; l < g.lmax && rc == H3D_OK; l++) {
             if (!g.coarse[l].n) continue;
             std::vector<const Level *> S;
@@ -1534,17 +1520,53 @@ int lockstep_tune(h3d_lockstep *b) {
                     S.push_back(&b->hs[i]->lv[l]);
                     ds.push_back(i);
                 }
-            BatchTab ct;
-            if (coarse_batch_create(S.data(), ds.data(), (int)S.size(), true, &ct) != 0) {
+            if (coarse_batch_create(S.data(), ds.data(), (int)S.size(), true, &coarse[k][l]) != 0)
                 rc = lfail(b, H3D_ERR_NOMEM, "lockstep tuning table");
+        }
+    }
+    // level l (0: the fine level) of every group together, in the given shape
+    auto run = [&](int l, int shape) {
+        cudaEventRecord(b->fork, s);
+        for (int k = 1; k < ng; k++) cudaStreamWaitEvent(b->groups[k].stream, b->fork, 0);
+        for (int k = 0; k < ng; k++) {
+            cudaStream_t gs = b->groups[k].stream;
+            if (l == 0) launch_fine_sweep_batch(fine[k], b->ke, b->d_active, false, shape, gs);
+            else if (coarse[k][l].n) launch_coarse_sweep_batch(coarse[k][l], b->f32, b->d_active, false, shape, gs);
+        }
+        for (int k = 1; k < ng; k++) {
+            cudaEventRecord(b->groups[k].join, b->groups[k].stream);
+            cudaStreamWaitEvent(s, b->groups[k].join, 0);
+        }
+    };
+    for (int l = 0; l < lmax - 1 && rc == H3D_OK; l++) {
+        bool any = l == 0;
+        for (int k = 0; k < ng; k++) any = any || coarse[k][l].n > 0;
+        if (!any) continue;
+        float best = 0;
+        int pick = 0;
+        for (int shape = 0; shape < 2 && rc == H3D_OK; shape++) {
+            run(l, shape);
+            if (cudaEventRecord(t0, s) != cudaSuccess) { rc = lfail(b, H3D_ERR_CUDA, "lockstep tuning"); break; }
+            for (int r = 0; r < 10; r++) run(l, shape);
+            if (cudaEventRecord(t1, s) != cudaSuccess || cudaEventSynchronize(t1) != cudaSuccess ||
+                cudaGetLastError() != cudaSuccess) {
+                rc = lfail(b, H3D_ERR_CUDA, "lockstep tuning launch failed");
                 break;
             }
-            const int cs = pick([&](int shape) { launch_coarse_sweep_batch(ct, b->f32, b->d_active, false, shape, s); });
-            batch_tab_free(ct);
-            if (cs < 0) rc = lfail(b, H3D_ERR_CUDA, "lockstep tuning launch failed");
-            else g.coarse_shape[l] = cs;
+            float ms = 0;
+            cudaEventElapsedTime(&ms, t0, t1);
+            // shape 1 only when clearly faster: the small levels time within the noise
+            if (shape == 0) best = ms;
+            else if (ms < 0.98f * best) pick = 1;
         }
-        if (rc != H3D_OK) break;
+        for (LockGroup &g : b->groups) {
+            if (l == 0) g.fine_shape = pick;
+            else g.coarse_shape[l] = pick;
+        }
+    }
+    for (int k = 0; k < ng; k++) {
+        batch_tab_free(fine[k]);
+        for (BatchTab &t : coarse[k]) batch_tab_free(t);
     }
     cudaEventDestroy(t0);
     cudaEventDestroy(t1);

@@ -250,10 +250,10 @@ H3D_API int h3d_lockstep_elastic_matrix(h3d_lockstep *b, double tol, double *C, 
  * or three load cases per thread; coarse levels: two or six), shape 0 by default;
  * results do not depend on the shapes.  h3d_lockstep_set_shapes forces every group
  * and level to fine_shape / coarse_shape (0 or 1); h3d_lockstep_autotune times both
- * shapes per group and level on scratch fields (each design's residual field) and
- * keeps the faster.  Both recapture the batch graph.  Measured: the timing of one
- * group alone misjudges the groups running together, and the fixed default is 1-3 %
- * faster than the tuned choice for 24-64 designs of 32^3-128^3. */
+ * shapes level by level with the sweeps of all groups running together on scratch
+ * fields (each design's residual field) and keeps shape 1 where it is at least 2 %
+ * faster.  Both recapture the batch graph.  Measured for 24-64 designs of
+ * 16^3-128^3: the tuned choice within 0.6 % of the fixed default. */
 H3D_API int h3d_lockstep_set_shapes(h3d_lockstep *b, int fine_shape, int coarse_shape);
 H3D_API int h3d_lockstep_autotune(h3d_lockstep *b);
 H3D_API int h3d_lockstep_destroy(h3d_lockstep *b);
