@@ -22,9 +22,15 @@ from .density import synthetic_density
 
 
 def solve(torch, n, rho, precision, tol, stencil=STENCIL_FP16):
+    """C of one solve from a zero start, timed in steady state: a first solve on the
+    handle (the launch-shape autotuner, the graph captures) is run and discarded"""
     hd = Homogenization(n, precision=precision, stencil=stencil)
     try:
         hd.update(rho)
+        try:
+            hd.elasticMatrix(max(tol, 1e-2))
+        except H3DError:
+            pass
         hd.reset_solutions()
         hd.sync()
         t0 = time.perf_counter()
