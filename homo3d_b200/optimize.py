@@ -18,7 +18,7 @@ import time
 
 import numpy as np
 
-from . import (COARSE_EXACT, PIN_IDENTITY, PREC_REFINE, STENCIL_FP16, Homogenization, OCOptimizer, symmetrize)
+from . import (COARSE_PROJECT, PIN_IDENTITY, PREC_REFINE, STENCIL_FP16, Homogenization, OCOptimizer, symmetrize)
 from .density import synthetic_density
 
 
@@ -86,14 +86,18 @@ class ConvergeChecker:
 
 def optimize_bulk(reso, vol=0.3, iters=50, seed=0, relthres=1e-2, filter_radius=2.0, step=0.05, damp=0.5,
                   sym="reflect6", finthres=5e-4, stop_on_converge=False, rho0=None, E=10.0, nu=0.3,
-                  coarse_mode=COARSE_EXACT, pin_mode=PIN_IDENTITY, precision=PREC_REFINE, device=0,
+                  coarse_mode=COARSE_PROJECT, pin_mode=PIN_IDENTITY, precision=PREC_REFINE, device=0,
                   on_solve=None, stencil=STENCIL_FP16, objective="bulk", device_step=True):
     """The OC loop of testAutoDiff.cu:282-331 (objective "bulk"), of
     testAutoDiff.cu:334-381 ("shear") or of Framework.cu:208-272 ("npr");
     device_step runs the update after each solve (sensitivity, SIMP backward,
     symmetry, filter, OC, symmetry) as one captured graph (h3d_design_step),
     otherwise as separate entry-point calls; on_solve(hom, rho_phys) is called after every
-    solve (e.g. to record training pairs)."""
+    solve (e.g. to record training pairs).  The coarsest solve projects out the
+    mean of its right-hand side (COARSE_PROJECT, as the reference's null-space
+    projection at the coarsest grid does): after a few OC steps the densities reach
+    their 1e-3 floor (element stiffness contrast ~1e9), where the exact inverse of
+    the pinned coarsest matrix made some designs' V-cycles diverge."""
     obj_fn, grad_fn = OBJECTIVES[objective]
     import torch
 
@@ -178,7 +182,7 @@ def optimize_shear_isotropy(reso, vol=0.3, iters=20, seed=0, relthres=1e-2, filt
     import torch
 
     from . import MMAOptimizer
-    hom = Homogenization(reso, E, nu, COARSE_EXACT, PIN_IDENTITY, precision, device)
+    hom = Homogenization(reso, E, nu, COARSE_PROJECT, PIN_IDENTITY, precision, device)
     n = hom.dims[0]
     ne = n[0] * n[1] * n[2]
     dev = torch.device("cuda", device)
